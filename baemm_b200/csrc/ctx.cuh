@@ -1,0 +1,123 @@
+// The context behind baemm_ctx: the device-resident mesh, the loaded operator
+// parameters, work buffers and the solvers.  Mirrors the state of the
+// reference class Helmholtz_OpenCL (MemberVariables.hpp:36-98) with the
+// OpenCL objects replaced by device buffers on one CUDA stream.
+#pragma once
+#include <complex>
+#include <string>
+#include <vector>
+
+#include "krylov.cuh"
+#include "ops.cuh"
+
+namespace baemm
+{
+
+using zc = std::complex<double>;
+
+class Ctx
+{
+public:
+    Ctx(const double *coords, int64_t nv, const int32_t *tris, int64_t nt, const double *meas, int64_t nm, int device,
+        int cpu_threads);
+    ~Ctx();
+
+    // ---- state ----------------------------------------------------------------
+    int device = 0;
+    int cpu_threads = 1;
+    cudaStream_t own_stream = nullptr;
+    cudaStream_t stream = nullptr;
+    MeshDev mesh;
+    std::vector<double> meas_h;                     // nm x 3 (as given)
+    std::vector<int32_t> mass_outer_h, mass_inner_h;
+
+    int wave_count = 0, wave_chunk_size = 16, wave_chunk_count = 0;
+    std::vector<double> kappa_h;
+    std::vector<zc> coeff_h;                        // unscaled, wcc x 4
+    double factor_h = 1.0;
+    OpFlags flags;
+    std::vector<ChunkParamsF> prm_f_h;
+    std::vector<ChunkParamsD> prm_d_h;
+    DevBuf<ChunkParamsF> prm_f;
+    DevBuf<ChunkParamsD> prm_d;
+    bool operators_loaded = false;
+
+    bool use_diagonal = true;
+    int block_size = 64;
+    int gmres_max_iter = 30, gmres_max_restarts = 3;
+    int apply_mode = BAEMM_APPLY_FP32;
+    int ir_max_steps = 0;
+    double ir_inner_tol = 1e-4;
+    baemm_solve_stats stats{};
+    bool profiling = false;
+    cudaEvent_t prof_ev[4] = {nullptr, nullptr, nullptr, nullptr};
+    bool prof_valid = false;
+    std::string last_error;
+
+    // work buffers
+    DevBuf<float2> Btri_f, Ctri_f, ff_partial_f;
+    DevBuf<double2> Btri_d, Ctri_d, ff_partial_d;
+    DevBuf<float> dirs_f;
+    DevBuf<double> dirs_d;
+    DevBuf<double2> io_a, io_b, io_c;   // host-API staging
+    DevBuf<double> io_r1, io_r2, tri_r;
+    // solver scratch (one buffer per role; the compositions nest)
+    DevBuf<double2> sv_wave, sv_phi, sv_bc, sv_bcw, sv_hw, sv_dv, sv_prod, sv_res, sv_d, sv_tmp;
+    DevBuf<double> sv_xn, sv_yw, sv_ytri, sv_ys;
+    CgSolver cg;
+    GmresSolver<double2> gmres_c;
+    GmresSolver<double> gmres_r;
+
+    // ---- parameters -------------------------------------------------------------
+    // LoadParameters.hpp:20-81
+    void load_parameters(const double *kappa, const zc *coeff, int wc, int wcs, double factor);
+    void require_loaded() const;
+
+    // ---- operators on device blocks (async on `stream`) --------------------------
+    template <class Text>
+    void apply_boundary(Text alpha, const Text *B, int64_t ldB, Text beta, Text *C, int64_t ldC);
+    // Far field: C (nm x wc) = alpha FF B + beta C   (ApplyFarFieldOperators.hpp:356-412)
+    void apply_farfield(zc alpha, const double2 *B, int64_t ldB, zc beta, double2 *C, int64_t ldC);
+    // Incident wave: C = alpha wave + beta C (CreateIncidentWave.hpp:54-127), dirs on host (wcs x 3)
+    void incident(zc alpha, const double *dirs, zc beta, double2 *C, int64_t ldC, int type);
+    // Herglotz wave of g (device, nm x ld): C = alpha HW + beta C (CreateHerglotzWave.hpp:50-95)
+    void herglotz(zc alpha, const double2 *g, int64_t ldg, zc beta, double2 *C, int64_t ldC);
+    // The O(N wc) and O(m N wc) steps around the dense apply (incident and
+    // Herglotz waves, far field, mass values, normal-field helpers) run in FP64
+    // when the apply is FP64 or when FP64 iterative refinement is on.
+    bool aux_fp64() const { return apply_mode == BAEMM_APPLY_FP64 || ir_max_steps > 0; }
+    bool mass_values_fp64() const { return aux_fp64(); }
+    // CG mass inverse on real columns (device); returns convergence
+    bool mass_inverse_real(const double *X, int64_t ldX, double *Y, int64_t ldY, int ncols, double tol);
+    bool mass_inverse_complex(const double2 *X, int64_t ldX, double2 *Y, int64_t ldY, int ncols, double tol);
+
+    // ---- solvers (device blocks, nv x wc) -------------------------------------------
+    // GMRES on the loaded boundary operators with P = M^-1 (BoundaryPotential_parameters /
+    // DirichletToNeumann core, FarField.hpp:706-768, 828-874), optional FP64 refinement.
+    void bie_solve(const double *kappa, const zc *coeff4, const double2 *rhs, double2 *sol, int wcc, int wcs,
+                   double cg_tol, double gmres_tol);
+    void boundary_potential(const double *kappa, zc *coeff, const double2 *wave, double2 *phi, const double *eta,
+                            int wcc, int wcs, double cg_tol, double gmres_tol);
+    void dirichlet_to_neumann(const double *kappa, const double2 *wave, double2 *du_dn, int wcc, int wcs,
+                              double cg_tol, double gmres_tol);
+    void farfield_parameters(const double *kappa, int wcc, const double *inc, int wcs, double2 *Y, int type,
+                             const double *eta, double cg_tol, double gmres_tol);
+    void derivative_helper(const double *kappa, int wcc, const double *inc, int wcs, double2 *du_dn, int type,
+                           double cg_tol, double gmres_tol);
+    void dot_with_normals(const double *X, double *Y, double cg_tol);
+    void multiply_with_normals(const double2 *X, double *Y, double factor, double cg_tol);
+    void derivative(const double *kappa, int wcc, const double *inc, int wcs, const double *X, double2 *Y,
+                    const double2 *du_dn, double cg_tol, double gmres_tol);
+    void adjoint_derivative(const double *kappa, int wcc, const double *inc, int wcs, const double2 *g, double *Y,
+                            const double2 *du_dn, double cg_tol, double gmres_tol);
+
+    void sync();
+    std::string device_info() const;
+
+private:
+    void build_topology(const int32_t *tris);
+    template <class R>
+    void dense_apply(const cplx<R> *Btri, cplx<R> *Ctri);
+};
+
+} // namespace baemm

@@ -1,0 +1,724 @@
+// Device CG (mass inverse) and batched GMRES.  See krylov.cuh for the
+// algorithm definitions.  Column reductions are two-level and deterministic:
+// each block reduces its row range in shared memory and writes one partial
+// per column; a single-block finalize kernel sums the partials in block
+// order.
+#include "krylov.cuh"
+
+#include <algorithm>
+#include <cmath>
+
+namespace baemm
+{
+namespace
+{
+
+constexpr int RT = 256;          // threads per reduction block
+constexpr int kTargetBlocks = 296;
+
+struct Layout
+{
+    int cp = 1, rp = 1, nchunk = 1, nblk = 1;
+    int64_t rows_per_block = 1;
+};
+
+Layout make_layout(int64_t n, int c)
+{
+    Layout L;
+    L.cp = std::min(c, RT);
+    L.rp = RT / L.cp;
+    L.nchunk = ceil_div(c, L.cp);
+    int64_t rpb = std::max<int64_t>(L.rp, (n + kTargetBlocks - 1) / kTargetBlocks);
+    rpb = ((rpb + L.rp - 1) / L.rp) * L.rp;
+    L.rows_per_block = rpb;
+    L.nblk = std::max(1, ceil_div(n, rpb));
+    return L;
+}
+
+// ---- scalar helpers for S = double / double2 ---------------------------------
+__device__ __forceinline__ double re(double a) { return a; }
+__device__ __forceinline__ double re(double2 a) { return a.x; }
+__device__ __forceinline__ double im(double) { return 0.0; }
+__device__ __forceinline__ double im(double2 a) { return a.y; }
+template <class S> __device__ __forceinline__ S mkS(double x, double y);
+template <> __device__ __forceinline__ double mkS<double>(double x, double) { return x; }
+template <> __device__ __forceinline__ double2 mkS<double2>(double x, double y) { return make_double2(x, y); }
+__device__ __forceinline__ double Sabs2(double a) { return a * a; }
+__device__ __forceinline__ double Sabs2(double2 a) { return a.x * a.x + a.y * a.y; }
+__device__ __forceinline__ double Smul(double a, double b) { return a * b; }
+__device__ __forceinline__ double2 Smul(double2 a, double2 b) { return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x); }
+__device__ __forceinline__ double Sconj(double a) { return a; }
+__device__ __forceinline__ double2 Sconj(double2 a) { return make_double2(a.x, -a.y); }
+__device__ __forceinline__ double Sadd(double a, double b) { return a + b; }
+__device__ __forceinline__ double2 Sadd(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ double Ssub(double a, double b) { return a - b; }
+__device__ __forceinline__ double2 Ssub(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
+__device__ __forceinline__ double Sscale(double a, double s) { return a * s; }
+__device__ __forceinline__ double2 Sscale(double2 a, double s) { return make_double2(a.x * s, a.y * s); }
+__device__ __forceinline__ double Sdiv(double a, double b) { return a / b; }
+__device__ __forceinline__ double2 Sdiv(double2 a, double2 b)
+{
+    const double d = b.x * b.x + b.y * b.y;
+    return make_double2((a.x * b.x + a.y * b.y) / d, (a.y * b.x - a.x * b.y) / d);
+}
+template <class S> constexpr int kWords = sizeof(S) / sizeof(double);
+
+// Block reduction of one value per (row-lane, column) into partial[out_index].
+__device__ __forceinline__ void block_reduce_store(double v, double *sm, int tr, int tc, int cp, int rp, bool active,
+                                                   double *dst)
+{
+    sm[threadIdx.x] = active ? v : 0.0;
+    __syncthreads();
+    if (tr == 0 && active)
+    {
+        double s = 0.0;
+        for (int q = 0; q < rp; ++q) s += sm[q * cp + tc];
+        *dst = s;
+    }
+    __syncthreads();
+}
+
+// ============================== CG =============================================
+// col_ layout: [0,c) rz  [c,2c) bn  [2c,3c) alpha  [3c,4c) beta ; flags_: [0] done [1] iters [2..) conv
+
+template <class RV>
+__global__ void cg_init_kernel(int64_t n, int c, int cp, int rp, int64_t rpb, const double *__restrict__ b,
+                               int64_t ldb, const RV *__restrict__ L, double *__restrict__ x, double *__restrict__ r,
+                               double *__restrict__ z, double *__restrict__ p, double *__restrict__ partial)
+{
+    __shared__ double sm[RT];
+    const int tr = threadIdx.x / cp, tc = threadIdx.x % cp;
+    const int k = blockIdx.y * cp + tc;
+    const bool active = tr < rp && k < c;
+    double rz = 0.0, bb = 0.0;
+    if (active)
+    {
+        const int64_t r0 = blockIdx.x * rpb, r1 = min(n, r0 + rpb);
+        for (int64_t row = r0 + tr; row < r1; row += rp)
+        {
+            const double bv = b[row * ldb + k];
+            const double zv = (double)L[row] * bv;
+            const int64_t e = row * c + k;
+            x[e] = 0.0; r[e] = bv; z[e] = zv; p[e] = zv;
+            rz += bv * zv;
+            bb += bv * bv;
+        }
+    }
+    double *out = partial + (int64_t)blockIdx.x * 2 * c;
+    block_reduce_store(rz, sm, tr, tc, cp, rp, active, out + k);
+    block_reduce_store(bb, sm, tr, tc, cp, rp, active, out + c + k);
+}
+
+__global__ void cg_finalize_init_kernel(int c, int nblk, const double *__restrict__ partial, double *__restrict__ col,
+                                        int *__restrict__ flags, double tol)
+{
+    int all = 1;
+    for (int k = threadIdx.x; k < c; k += blockDim.x)
+    {
+        double rz = 0.0, bb = 0.0;
+        for (int q = 0; q < nblk; ++q) { rz += partial[(int64_t)q * 2 * c + k]; bb += partial[(int64_t)q * 2 * c + c + k]; }
+        const double bn = sqrt(bb);
+        col[k] = rz;
+        col[c + k] = bn;
+        col[2 * c + k] = 0.0;
+        col[3 * c + k] = 0.0;
+        const int cv = (bn <= tol * bn) ? 1 : 0;
+        flags[2 + k] = cv;
+        all &= cv;
+    }
+    all = __syncthreads_and(all);
+    if (threadIdx.x == 0) { flags[0] = all; flags[1] = 0; }
+}
+
+template <class RV>
+__global__ void cg_matvec_kernel(int64_t n, int c, int cp, int rp, int64_t rpb, const int32_t *__restrict__ mo,
+                                 const int32_t *__restrict__ mi, const RV *__restrict__ mv, const double *__restrict__ p,
+                                 double *__restrict__ q, double *__restrict__ partial, const int *__restrict__ flags)
+{
+    if (flags[0]) return;
+    __shared__ double sm[RT];
+    const int tr = threadIdx.x / cp, tc = threadIdx.x % cp;
+    const int k = blockIdx.y * cp + tc;
+    const bool active = tr < rp && k < c;
+    double pq = 0.0;
+    if (active)
+    {
+        const int64_t r0 = blockIdx.x * rpb, r1 = min(n, r0 + rpb);
+        for (int64_t row = r0 + tr; row < r1; row += rp)
+        {
+            double s = 0.0;
+            for (int32_t e = mo[row]; e < mo[row + 1]; ++e) s += (double)mv[e] * p[(int64_t)mi[e] * c + k];
+            q[row * c + k] = s;
+            pq += p[row * c + k] * s;
+        }
+    }
+    block_reduce_store(pq, sm, tr, tc, cp, rp, active, partial + (int64_t)blockIdx.x * c + k);
+}
+
+__global__ void cg_finalize_alpha_kernel(int c, int nblk, const double *__restrict__ partial, double *__restrict__ col,
+                                         const int *__restrict__ flags)
+{
+    if (flags[0]) return;
+    for (int k = threadIdx.x; k < c; k += blockDim.x)
+    {
+        double pq = 0.0;
+        for (int q = 0; q < nblk; ++q) pq += partial[(int64_t)q * c + k];
+        col[2 * c + k] = (flags[2 + k] || pq == 0.0) ? 0.0 : col[k] / pq;
+    }
+}
+
+template <class RV>
+__global__ void cg_update_kernel(int64_t n, int c, int cp, int rp, int64_t rpb, const RV *__restrict__ L,
+                                 const double *__restrict__ col, double *__restrict__ x, double *__restrict__ r,
+                                 double *__restrict__ z, const double *__restrict__ p, const double *__restrict__ q,
+                                 double *__restrict__ partial, const int *__restrict__ flags)
+{
+    if (flags[0]) return;
+    __shared__ double sm[RT];
+    const int tr = threadIdx.x / cp, tc = threadIdx.x % cp;
+    const int k = blockIdx.y * cp + tc;
+    const bool active = tr < rp && k < c;
+    double rz = 0.0, rr = 0.0;
+    if (active)
+    {
+        const double a = col[2 * c + k];
+        const int64_t r0 = blockIdx.x * rpb, r1 = min(n, r0 + rpb);
+        for (int64_t row = r0 + tr; row < r1; row += rp)
+        {
+            const int64_t e = row * c + k;
+            x[e] += a * p[e];
+            const double rv = r[e] - a * q[e];
+            r[e] = rv;
+            const double zv = (double)L[row] * rv;
+            z[e] = zv;
+            rz += rv * zv;
+            rr += rv * rv;
+        }
+    }
+    double *out = partial + (int64_t)blockIdx.x * 2 * c;
+    block_reduce_store(rz, sm, tr, tc, cp, rp, active, out + k);
+    block_reduce_store(rr, sm, tr, tc, cp, rp, active, out + c + k);
+}
+
+__global__ void cg_finalize_beta_kernel(int c, int nblk, const double *__restrict__ partial, double *__restrict__ col,
+                                        int *__restrict__ flags, double tol)
+{
+    if (flags[0]) return;
+    int all = 1;
+    for (int k = threadIdx.x; k < c; k += blockDim.x)
+    {
+        double rzn = 0.0, rr = 0.0;
+        for (int q = 0; q < nblk; ++q) { rzn += partial[(int64_t)q * 2 * c + k]; rr += partial[(int64_t)q * 2 * c + c + k]; }
+        const int was = flags[2 + k];
+        col[3 * c + k] = (was || col[k] == 0.0) ? 0.0 : rzn / col[k];
+        col[k] = rzn;
+        const int cv = was || (sqrt(rr) <= tol * col[c + k]);
+        flags[2 + k] = cv;
+        all &= cv;
+    }
+    all = __syncthreads_and(all);
+    if (threadIdx.x == 0) { flags[0] = all; flags[1] += 1; }
+}
+
+__global__ void cg_pupdate_kernel(int64_t total, int c, const double *__restrict__ col, const double *__restrict__ z,
+                                  double *__restrict__ p, const int *__restrict__ flags)
+{
+    if (flags[0]) return;
+    const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= total) return;
+    const int k = (int)(e % c);
+    p[e] = z[e] + col[3 * c + k] * p[e];
+}
+
+__global__ void cg_output_kernel(int64_t n, int c, const double *__restrict__ x, double *__restrict__ y, int64_t ldy)
+{
+    const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= n * c) return;
+    const int64_t row = e / c;
+    const int k = (int)(e - row * c);
+    y[row * ldy + k] = x[e];
+}
+
+// ============================== GMRES ==========================================
+
+// partial[blk][i*c + k] (S words) = sum_rows conj(V_i[r,k]) w[r,k], i < nvec.
+// The vectors are taken in groups of kGroup so the accumulators stay in
+// registers; w is re-read per group (it is L2-resident).
+constexpr int kGroup = 8;
+template <class S>
+__global__ void gs_dot_kernel(int64_t n, int c, int cp, int rp, int64_t rpb, const S *__restrict__ V, int nvec,
+                              const S *__restrict__ w, double *__restrict__ partial)
+{
+    __shared__ double sm[RT];
+    const int tr = threadIdx.x / cp, tc = threadIdx.x % cp;
+    const int k = blockIdx.y * cp + tc;
+    const bool active = tr < rp && k < c;
+    const int64_t stride = n * c;
+    constexpr int W = kWords<S>;
+    double *out = partial + (int64_t)blockIdx.x * nvec * c * W;
+    const int64_t r0 = blockIdx.x * rpb, r1 = min(n, r0 + rpb);
+    for (int g0 = 0; g0 < nvec; g0 += kGroup)
+    {
+        double ax[kGroup], ay[kGroup];
+        #pragma unroll
+        for (int i = 0; i < kGroup; ++i) { ax[i] = 0.0; ay[i] = 0.0; }
+        if (active)
+        {
+            for (int64_t row = r0 + tr; row < r1; row += rp)
+            {
+                const S wv = w[row * c + k];
+                #pragma unroll
+                for (int i = 0; i < kGroup; ++i)
+                {
+                    if (g0 + i < nvec)
+                    {
+                        const S v = V[(g0 + i) * stride + row * c + k];
+                        ax[i] += re(v) * re(wv) + im(v) * im(wv);
+                        ay[i] += re(v) * im(wv) - im(v) * re(wv);
+                    }
+                }
+            }
+        }
+        #pragma unroll
+        for (int i = 0; i < kGroup; ++i)
+        {
+            if (g0 + i < nvec)
+            {
+                double *dst = out + ((int64_t)(g0 + i) * c + k) * W;
+                block_reduce_store(ax[i], sm, tr, tc, cp, rp, active, dst);
+                if (W == 2) block_reduce_store(ay[i], sm, tr, tc, cp, rp, active, dst + 1);
+            }
+        }
+    }
+}
+
+// h[i*c+k] = sum_blk partial; H[(i*m + j)*c + k] (+)= h
+template <class S>
+__global__ void gs_finalize_kernel(int c, int nblk, int nvec, const double *__restrict__ partial, S *__restrict__ h,
+                                   S *__restrict__ H, int m, int j, int accumulate)
+{
+    const int item = blockIdx.x * blockDim.x + threadIdx.x;
+    if (item >= nvec * c) return;
+    constexpr int W = kWords<S>;
+    double sx = 0.0, sy = 0.0;
+    for (int q = 0; q < nblk; ++q)
+    {
+        const double *src = partial + ((int64_t)q * nvec * c + item) * W;
+        sx += src[0];
+        if (W == 2) sy += src[1];
+    }
+    const S v = mkS<S>(sx, sy);
+    h[item] = v;
+    const int i = item / c, k = item - i * c;
+    S &dst = H[((int64_t)i * m + j) * c + k];
+    dst = accumulate ? Sadd(dst, v) : v;
+}
+
+template <class S>
+__global__ void gs_update_kernel(int64_t n, int c, const S *__restrict__ V, int nvec, const S *__restrict__ h,
+                                 S *__restrict__ w)
+{
+    const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= n * c) return;
+    const int k = (int)(e % c);
+    const int64_t stride = n * c;
+    S acc = w[e];
+    for (int i = 0; i < nvec; ++i) acc = Ssub(acc, Smul(h[i * c + k], V[i * stride + e]));
+    w[e] = acc;
+}
+
+template <class S>
+__global__ void norm_partial_kernel(int64_t n, int c, int cp, int rp, int64_t rpb, const S *__restrict__ w,
+                                    double *__restrict__ partial)
+{
+    __shared__ double sm[RT];
+    const int tr = threadIdx.x / cp, tc = threadIdx.x % cp;
+    const int k = blockIdx.y * cp + tc;
+    const bool active = tr < rp && k < c;
+    double s = 0.0;
+    if (active)
+    {
+        const int64_t r0 = blockIdx.x * rpb, r1 = min(n, r0 + rpb);
+        for (int64_t row = r0 + tr; row < r1; row += rp) s += Sabs2(w[row * c + k]);
+    }
+    block_reduce_store(s, sm, tr, tc, cp, rp, active, partial + (int64_t)blockIdx.x * c + k);
+}
+
+// hn[k] = ||w_k||; mode 0: H[(j+1)m + j] = hn ; mode 1: start of a cycle (res, g, bnorm)
+template <class S>
+__global__ void norm_finalize_kernel(int c, int nblk, const double *__restrict__ partial, double *__restrict__ hn,
+                                     S *__restrict__ H, int m, int j, int mode, double *__restrict__ res,
+                                     S *__restrict__ g, double *__restrict__ bnorm, int *__restrict__ flags, double tol)
+{
+    int all = 1;
+    for (int k = threadIdx.x; k < c; k += blockDim.x)
+    {
+        double s = 0.0;
+        for (int q = 0; q < nblk; ++q) s += partial[(int64_t)q * c + k];
+        const double nv = sqrt(s);
+        hn[k] = nv;
+        if (mode == 0)
+            H[((int64_t)(j + 1) * m + j) * c + k] = mkS<S>(nv, 0.0);
+        else
+        {
+            if (mode == 2) bnorm[k] = nv;   // first cycle: ||P b||
+            res[k] = nv;
+            for (int i = 0; i <= m; ++i) g[(int64_t)i * c + k] = mkS<S>(i == 0 ? nv : 0.0, 0.0);
+            all &= (nv <= tol * bnorm[k]) ? 1 : 0;
+        }
+    }
+    if (mode != 0)
+    {
+        all = __syncthreads_and(all);
+        if (threadIdx.x == 0) flags[0] = all;
+    }
+}
+
+template <class S>
+__global__ void normalize_kernel(int64_t n, int c, const S *__restrict__ w, const double *__restrict__ hn,
+                                 S *__restrict__ v)
+{
+    const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= n * c) return;
+    const double d = hn[e % c];
+    v[e] = d > 0.0 ? Sscale(w[e], 1.0 / d) : mkS<S>(0.0, 0.0);
+}
+
+template <class S>
+__global__ void givens_kernel(int c, int m, int j, S *__restrict__ H, double *__restrict__ cs, S *__restrict__ sn,
+                              S *__restrict__ g, double *__restrict__ res, const double *__restrict__ bnorm,
+                              int *__restrict__ flags, double tol)
+{
+    int all = 1;
+    for (int k = threadIdx.x; k < c; k += blockDim.x)
+    {
+        for (int i = 0; i < j; ++i)
+        {
+            S &h0 = H[((int64_t)i * m + j) * c + k];
+            S &h1 = H[((int64_t)(i + 1) * m + j) * c + k];
+            const double cc = cs[i * c + k];
+            const S s = sn[i * c + k];
+            const S t0 = Sadd(Sscale(h0, cc), Smul(s, h1));
+            const S t1 = Sadd(Sscale(Smul(Sconj(s), h0), -1.0), Sscale(h1, cc));
+            h0 = t0;
+            h1 = t1;
+        }
+        S &a = H[((int64_t)j * m + j) * c + k];
+        S &b = H[((int64_t)(j + 1) * m + j) * c + k];
+        const double aa = sqrt(Sabs2(a)), bb = sqrt(Sabs2(b));
+        double cc;
+        S s;
+        if (aa == 0.0)
+        {
+            cc = 0.0;
+            s = mkS<S>(1.0, 0.0);
+            a = b;
+        }
+        else
+        {
+            const double t = sqrt(aa * aa + bb * bb);
+            cc = aa / t;
+            const S ua = Sscale(a, 1.0 / aa);
+            s = Sscale(Smul(ua, Sconj(b)), 1.0 / t);
+            a = Sscale(ua, t);
+        }
+        b = mkS<S>(0.0, 0.0);
+        cs[j * c + k] = cc;
+        sn[j * c + k] = s;
+        const S gj = g[(int64_t)j * c + k];
+        g[(int64_t)j * c + k] = Sscale(gj, cc);
+        const S gn = Sscale(Smul(Sconj(s), gj), -1.0);
+        g[(int64_t)(j + 1) * c + k] = gn;
+        const double rn = sqrt(Sabs2(gn));
+        res[k] = rn;
+        all &= (rn <= tol * bnorm[k]) ? 1 : 0;
+    }
+    all = __syncthreads_and(all);
+    if (threadIdx.x == 0) flags[0] = all;
+}
+
+template <class S>
+__global__ void backsolve_kernel(int c, int m, int jend, const S *__restrict__ H, const S *__restrict__ g,
+                                 S *__restrict__ y)
+{
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= c) return;
+    for (int i = jend - 1; i >= 0; --i)
+    {
+        S s = g[(int64_t)i * c + k];
+        for (int l = i + 1; l < jend; ++l) s = Ssub(s, Smul(H[((int64_t)i * m + l) * c + k], y[(int64_t)l * c + k]));
+        const S d = H[((int64_t)i * m + i) * c + k];
+        y[(int64_t)i * c + k] = (Sabs2(d) == 0.0) ? mkS<S>(0.0, 0.0) : Sdiv(s, d);
+    }
+}
+
+template <class S>
+__global__ void update_x_kernel(int64_t n, int c, int jend, const S *__restrict__ V, const S *__restrict__ y,
+                                S *__restrict__ x)
+{
+    const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= n * c) return;
+    const int k = (int)(e % c);
+    const int64_t stride = n * c;
+    S acc = x[e];
+    for (int i = 0; i < jend; ++i) acc = Sadd(acc, Smul(y[(int64_t)i * c + k], V[i * stride + e]));
+    x[e] = acc;
+}
+
+template <class S>
+__global__ void residual_kernel(int64_t total, const S *__restrict__ b, const S *__restrict__ Ax, S *__restrict__ r)
+{
+    const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= total) return;
+    r[e] = Ssub(b[e], Ax[e]);
+}
+
+template <class S>
+__global__ void gather_kernel(int64_t n, int c, const S *__restrict__ src, int64_t lds, S *__restrict__ dst)
+{
+    const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= n * c) return;
+    const int64_t row = e / c;
+    dst[e] = src[row * lds + (e - row * c)];
+}
+
+template <class S>
+__global__ void output_kernel(int64_t n, int c, S alpha, const S *__restrict__ x, S beta, S *__restrict__ out,
+                              int64_t ldo)
+{
+    const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= n * c) return;
+    const int64_t row = e / c;
+    S *o = &out[row * ldo + (e - row * c)];
+    const S ax = Smul(alpha, x[e]);
+    *o = (Sabs2(beta) == 0.0) ? ax : Sadd(ax, Smul(beta, *o));
+}
+
+inline int eg(int64_t n) { return ceil_div(n, 256); }
+
+} // namespace
+
+// =================================== CG host ======================================
+CgSolver::~CgSolver()
+{
+    if (host_flags_) cudaFreeHost(host_flags_);
+}
+
+bool CgSolver::solve_mass(const MeshDev &m, bool fp64_values, const double *b, int64_t ldb, double *y, int64_t ldy,
+                          int c, double tol, int max_iter, cudaStream_t st, int *iterations)
+{
+    const int64_t n = m.nv;
+    BAEMM_REQUIRE(c >= 1 && c <= kMaxKrylovColumns, BAEMM_ERR_SIZE, "CG column count out of range");
+    const int64_t N = n * c;
+    x_.reserve(N); r_.reserve(N); z_.reserve(N); p_.reserve(N); q_.reserve(N);
+    col_.reserve(4 * (size_t)c);
+    flags_.reserve(2 + (size_t)c);
+    const Layout L = make_layout(n, c);
+    partial_.reserve((size_t)L.nblk * 2 * c);
+    if (!host_flags_) BAEMM_CUDA(cudaMallocHost(&host_flags_, 2 * sizeof(int)));
+    dim3 grid(L.nblk, L.nchunk);
+    const int fin = std::min(1024, ((c + 31) / 32) * 32);
+    auto run = [&](auto Lv, auto Mv) {
+        cg_init_kernel<<<grid, RT, 0, st>>>(n, c, L.cp, L.rp, L.rows_per_block, b, ldb, Lv, x_.p, r_.p, z_.p, p_.p,
+                                            partial_.p);
+        cg_finalize_init_kernel<<<1, fin, 0, st>>>(c, L.nblk, partial_.p, col_.p, flags_.p, tol);
+        for (int it = 0; it < max_iter; ++it)
+        {
+            cg_matvec_kernel<<<grid, RT, 0, st>>>(n, c, L.cp, L.rp, L.rows_per_block, m.mass_outer, m.mass_inner, Mv,
+                                                  p_.p, q_.p, partial_.p, flags_.p);
+            cg_finalize_alpha_kernel<<<1, fin, 0, st>>>(c, L.nblk, partial_.p, col_.p, flags_.p);
+            cg_update_kernel<<<grid, RT, 0, st>>>(n, c, L.cp, L.rp, L.rows_per_block, Lv, col_.p, x_.p, r_.p, z_.p,
+                                                  p_.p, q_.p, partial_.p, flags_.p);
+            cg_finalize_beta_kernel<<<1, fin, 0, st>>>(c, L.nblk, partial_.p, col_.p, flags_.p, tol);
+            cg_pupdate_kernel<<<eg(N), 256, 0, st>>>(N, c, col_.p, z_.p, p_.p, flags_.p);
+        }
+    };
+    if (fp64_values) run(m.lumped_d.p, m.mass_d.p);
+    else run(m.lumped_f.p, m.mass_f.p);
+    BAEMM_LAUNCH_CHECK();
+    cg_output_kernel<<<eg(N), 256, 0, st>>>(n, c, x_.p, y, ldy);
+    BAEMM_LAUNCH_CHECK();
+    BAEMM_CUDA(cudaMemcpyAsync(host_flags_, flags_.p, 2 * sizeof(int), cudaMemcpyDeviceToHost, st));
+    BAEMM_CUDA(cudaStreamSynchronize(st));
+    if (iterations) *iterations = host_flags_[1];
+    return host_flags_[0] != 0;
+}
+
+// =================================== GMRES host ===================================
+template <class S>
+GmresSolver<S>::~GmresSolver()
+{
+    if (host_flags_) cudaFreeHost(host_flags_);
+    if (host_res_) cudaFreeHost(host_res_);
+}
+
+template <class S>
+size_t GmresSolver<S>::device_bytes() const
+{
+    return (V_.n + H_.n + sn_.n + g_.n + h_.n + y_.n + w_.n + tmp_.n + x_.n + b_.n) * sizeof(S) +
+           (cs_.n + res_.n + bnorm_.n + hn_.n + partial_.n) * sizeof(double);
+}
+
+template <class S>
+typename GmresSolver<S>::Stats GmresSolver<S>::solve(int64_t n, int c, int restart, int cycles, const Op &A,
+                                                     const Op &P, S alpha, const S *b, int64_t ldb, S beta, S *x_out,
+                                                     int64_t ldx, double tol, cudaStream_t st)
+{
+    BAEMM_REQUIRE(c >= 1 && c <= kMaxKrylovColumns, BAEMM_ERR_SIZE, "GMRES column count out of range");
+    BAEMM_REQUIRE(restart >= 1 && restart <= kMaxRestart, BAEMM_ERR_SIZE, "GMRES restart length out of range");
+    BAEMM_REQUIRE(cycles >= 1, BAEMM_ERR_ARG, "GMRES needs at least one cycle");
+    const int m = restart;
+    const int64_t N = n * c;
+    V_.reserve((size_t)(m + 1) * N);
+    H_.reserve((size_t)(m + 1) * m * c);
+    sn_.reserve((size_t)m * c); cs_.reserve((size_t)m * c);
+    g_.reserve((size_t)(m + 1) * c);
+    h_.reserve((size_t)(m + 1) * c);
+    y_.reserve((size_t)m * c);
+    w_.reserve(N); tmp_.reserve(N); x_.reserve(N); b_.reserve(N);
+    res_.reserve(c); bnorm_.reserve(c); hn_.reserve(c);
+    flags_.reserve(4);
+    const Layout L = make_layout(n, c);
+    constexpr int W = kWords<S>;
+    partial_.reserve((size_t)L.nblk * (m + 1) * c * W);
+    if (!host_flags_) BAEMM_CUDA(cudaMallocHost(&host_flags_, 4 * sizeof(int)));
+    if (host_cap_ < c)
+    {
+        if (host_res_) cudaFreeHost(host_res_);
+        BAEMM_CUDA(cudaMallocHost(&host_res_, 2 * (size_t)c * sizeof(double)));
+        host_cap_ = c;
+    }
+    dim3 grid(L.nblk, L.nchunk);
+    const int fin = std::min(1024, ((c + 31) / 32) * 32);
+
+    auto read_flag = [&]() {
+        BAEMM_CUDA(cudaMemcpyAsync(host_flags_, flags_.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+        BAEMM_CUDA(cudaStreamSynchronize(st));
+        return host_flags_[0] != 0;
+    };
+    // hn = ||w|| columnwise, with `mode` as in norm_finalize_kernel
+    auto norms = [&](const S *w, int j, int mode) {
+        norm_partial_kernel<S><<<grid, RT, 0, st>>>(n, c, L.cp, L.rp, L.rows_per_block, w, partial_.p);
+        norm_finalize_kernel<S><<<1, fin, 0, st>>>(c, L.nblk, partial_.p, hn_.p, H_.p, m, j, mode, res_.p, g_.p,
+                                                   bnorm_.p, flags_.p, tol);
+        BAEMM_LAUNCH_CHECK();
+    };
+
+    Stats stats;
+    gather_kernel<S><<<eg(N), 256, 0, st>>>(n, c, b, ldb, b_.p);
+    BAEMM_CUDA(cudaMemsetAsync(x_.p, 0, N * sizeof(S), st));
+    BAEMM_LAUNCH_CHECK();
+    bool conv = false;
+    for (int cyc = 0; cyc < cycles; ++cyc)
+    {
+        if (cyc == 0)
+        {
+            P(b_.p, w_.p);
+            norms(w_.p, 0, 2);
+        }
+        else
+        {
+            A(x_.p, tmp_.p);
+            residual_kernel<S><<<eg(N), 256, 0, st>>>(N, b_.p, tmp_.p, tmp_.p);
+            P(tmp_.p, w_.p);
+            norms(w_.p, 0, 1);
+        }
+        if (read_flag()) { conv = true; break; }
+        normalize_kernel<S><<<eg(N), 256, 0, st>>>(n, c, w_.p, hn_.p, V_.p);
+        BAEMM_CUDA(cudaMemsetAsync(H_.p, 0, (size_t)(m + 1) * m * c * sizeof(S), st));
+        int jend = 0;
+        for (int j = 0; j < m; ++j)
+        {
+            S *Vj = V_.p + (int64_t)j * N;
+            A(Vj, tmp_.p);
+            P(tmp_.p, w_.p);
+            const int nvec = j + 1;
+            const int fg = ceil_div((int64_t)nvec * c, 256);
+            for (int pass = 0; pass < 2; ++pass)
+            {
+                gs_dot_kernel<S><<<grid, RT, 0, st>>>(n, c, L.cp, L.rp, L.rows_per_block, V_.p, nvec, w_.p,
+                                                      partial_.p);
+                gs_finalize_kernel<S><<<fg, 256, 0, st>>>(c, L.nblk, nvec, partial_.p, h_.p, H_.p, m, j, pass);
+                gs_update_kernel<S><<<eg(N), 256, 0, st>>>(n, c, V_.p, nvec, h_.p, w_.p);
+            }
+            norms(w_.p, j, 0);
+            normalize_kernel<S><<<eg(N), 256, 0, st>>>(n, c, w_.p, hn_.p, V_.p + (int64_t)(j + 1) * N);
+            givens_kernel<S><<<1, fin, 0, st>>>(c, m, j, H_.p, cs_.p, sn_.p, g_.p, res_.p, bnorm_.p, flags_.p, tol);
+            BAEMM_LAUNCH_CHECK();
+            stats.iterations++;
+            jend = j + 1;
+            if (read_flag()) { conv = true; break; }
+        }
+        backsolve_kernel<S><<<ceil_div(c, 128), 128, 0, st>>>(c, m, jend, H_.p, g_.p, y_.p);
+        update_x_kernel<S><<<eg(N), 256, 0, st>>>(n, c, jend, V_.p, y_.p, x_.p);
+        BAEMM_LAUNCH_CHECK();
+        if (conv) break;
+    }
+    output_kernel<S><<<eg(N), 256, 0, st>>>(n, c, alpha, x_.p, beta, x_out, ldx);
+    BAEMM_LAUNCH_CHECK();
+    BAEMM_CUDA(cudaMemcpyAsync(host_res_, res_.p, c * sizeof(double), cudaMemcpyDeviceToHost, st));
+    BAEMM_CUDA(cudaMemcpyAsync(host_res_ + c, bnorm_.p, c * sizeof(double), cudaMemcpyDeviceToHost, st));
+    BAEMM_CUDA(cudaStreamSynchronize(st));
+    stats.converged = conv;
+    stats.max_rel_res = 0.0;
+    for (int k = 0; k < c; ++k)
+        if (host_res_[c + k] > 0) stats.max_rel_res = std::max(stats.max_rel_res, host_res_[k] / host_res_[c + k]);
+    return stats;
+}
+
+namespace
+{
+__global__ void dot_partial_kernel(const double *__restrict__ a, const double *__restrict__ b, int64_t n,
+                                   double *__restrict__ partial)
+{
+    __shared__ double sm[RT];
+    double s = 0.0;
+    for (int64_t e = (int64_t)blockIdx.x * RT + threadIdx.x; e < n; e += (int64_t)gridDim.x * RT) s += a[e] * b[e];
+    sm[threadIdx.x] = s;
+    __syncthreads();
+    for (int w = RT / 2; w > 0; w >>= 1)
+    {
+        if (threadIdx.x < w) sm[threadIdx.x] += sm[threadIdx.x + w];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) partial[blockIdx.x] = sm[0];
+}
+} // namespace
+
+double device_dot(const double *a, const double *b, int64_t n, cudaStream_t st)
+{
+    constexpr int nb = 256;
+    static thread_local DevBuf<double> partial;
+    std::vector<double> h(nb);
+    dot_partial_kernel<<<nb, RT, 0, st>>>(a, b, n, partial.reserve(nb));
+    BAEMM_LAUNCH_CHECK();
+    BAEMM_CUDA(cudaMemcpyAsync(h.data(), partial.p, nb * sizeof(double), cudaMemcpyDeviceToHost, st));
+    BAEMM_CUDA(cudaStreamSynchronize(st));
+    double s = 0.0;
+    for (double v : h) s += v;
+    return s;
+}
+
+void device_colnorms(const double2 *w, int64_t n, int c, double *out_host, cudaStream_t st)
+{
+    const Layout L = make_layout(n, c);
+    static thread_local DevBuf<double> partial;
+    partial.reserve((size_t)L.nblk * c);
+    norm_partial_kernel<double2><<<dim3(L.nblk, L.nchunk), RT, 0, st>>>(n, c, L.cp, L.rp, L.rows_per_block, w,
+                                                                        partial.p);
+    BAEMM_LAUNCH_CHECK();
+    std::vector<double> h((size_t)L.nblk * c);
+    BAEMM_CUDA(cudaMemcpyAsync(h.data(), partial.p, h.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
+    BAEMM_CUDA(cudaStreamSynchronize(st));
+    for (int k = 0; k < c; ++k)
+    {
+        double s = 0.0;
+        for (int q = 0; q < L.nblk; ++q) s += h[(size_t)q * c + k];
+        out_host[k] = std::sqrt(s);
+    }
+}
+
+template class GmresSolver<double>;
+template class GmresSolver<double2>;
+
+} // namespace baemm

@@ -1,0 +1,101 @@
+// Host-side launchers of the device kernels (all asynchronous on `st`).
+// Layouts (row-major, complex interleaved):
+//   mid4 / nrm4      nt x 4 reals (xyz, w = 0)      float and double copies
+//   area, a3, diag   nt reals (a3 = area/3, the AvOp value)
+//   Btri / Ctri      nt x wc complex (internal precision R)
+//   vertex blocks    nv x ld complex (external precision)
+//   AvOp             per triangle its 3 vertex ids sorted ascending (tri_sorted)
+//   AvOp^T           CSR over vertices: avt_outer (nv+1), avt_inner (3 nt) = triangle ids ascending
+//   Mass             CSR over vertices: mass_outer, mass_inner (sorted), values float and double
+#pragma once
+#include "common.cuh"
+
+namespace baemm
+{
+
+struct MeshDev
+{
+    int64_t nv = 0, nt = 0, nm = 0;
+    DevBuf<double> coords;       // nv x 3
+    DevBuf<int32_t> tris;        // nt x 3 (as given)
+    DevBuf<int32_t> tri_sorted;  // nt x 3 (AvOp columns, sorted)
+    DevBuf<int32_t> avt_outer, avt_inner;
+    DevBuf<int32_t> mass_outer, mass_inner;
+    DevBuf<float> mid_f, nrm_f, area_f, a3_f, diag_f, mass_f, lumped_f, meas_f;
+    DevBuf<double> mid_d, nrm_d, area_d, a3_d, diag_d, mass_d, lumped_d, meas_d;
+};
+
+// ---- mesh.cu -------------------------------------------------------------------
+// Initialize.hpp:57-302 (geometry and single-layer diagonal) in precision R.
+void launch_geometry(const MeshDev &m, bool fp64, cudaStream_t st);
+// MassOp values (Initialize.hpp:214-247, 329-334) and areas_lumped_inv
+// (Initialize.hpp:339-353), after launch_geometry.
+void launch_mass_values(const MeshDev &m, bool fp64, cudaStream_t st);
+
+// ---- sparse.cu -----------------------------------------------------------------
+// AvOp (PL -> PC): Btri[t,k] = a3_t * sum_q Bin[v_q, k]; Text = float2/double2, R = internal.
+template <class Text, class R>
+void launch_avop(const MeshDev &m, const Text *Bin, int64_t ldB, int wc, cplx<R> *Btri, cudaStream_t st);
+
+struct EpilogueArgs
+{
+    bool layers = false;      // add alpha * AvOp^T (Ctri [+ SL diagonal])
+    bool sl_diag = false;     // SL diagonal (ApplySingleLayerDiagonal.hpp:397-454)
+    bool mass = false;        // add alpha * c0 * M Bin (ApplyBoundaryOperators.hpp:363-387)
+    int wc = 0, wcs = 1;
+};
+// C_out[v,k] = [layers] alpha * sum_{t ∋ v} a3_t (Ctri[t,k] + diag-term) + [mass] alpha c0 (M Bin)[v,k]
+//              + beta * C_out[v,k]   (beta == 0 overwrites)
+template <class Text, class R>
+void launch_epilogue(const MeshDev &m, const EpilogueArgs &a, const cplx<R> *Ctri, const cplx<R> *Btri,
+                     const void *chunk_params, const Text *Bin, int64_t ldB, Text alpha, Text beta,
+                     Text *Cout, int64_t ldC, cudaStream_t st);
+
+// Real-column helpers of FarField.hpp:886-1022.
+// Yw[v] = sum_t a3_t * (n_t . (AvOp X)_t / a_t)       (DotWithNormals_PL, FarField.hpp:980-1012)
+void launch_dot_with_normals_weak(const MeshDev &m, bool fp64, const double *X, double *Ytri, double *Yw,
+                                  cudaStream_t st);
+// Yw[v,d] = factor * sum_t a3_t * Re((AvOp X)_t) / a_t * n_t[d]   (FarField.hpp:914-942)
+void launch_mult_with_normals_weak(const MeshDev &m, bool fp64, const double2 *X, double factor, double *Ytri,
+                                   double *Yw, cudaStream_t st);
+// bdr[v,k] = -s[v] * du[v,k]   (FarField.hpp:288-300)
+void launch_scale_rows_neg(int64_t nv, int wc, const double *s, const double2 *du, double2 *out, cudaStream_t st);
+// prod[v] = sum_k du[v,k] * dv[v,k]   (HadamardProduct.hpp:18-25, no conjugation)
+void launch_row_dot(int64_t nv, int wc, const double2 *du, const double2 *dv, double2 *out, cudaStream_t st);
+
+// Mass SpMM on real columns: Y = alpha M X + beta Y (values in fp64 or fp32-widened).
+void launch_mass_dot_real(const MeshDev &m, bool fp64_values, double alpha, const double *X, int64_t ldX,
+                          double beta, double *Y, int64_t ldY, int ncols, cudaStream_t st);
+// Lumped inverse on real columns: Y = L X.
+void launch_lumped_real(const MeshDev &m, bool fp64_values, const double *X, int64_t ldX, double *Y, int64_t ldY,
+                        int ncols, cudaStream_t st);
+// Strided copies / conversions of external blocks.
+template <class Tsrc, class Tdst>
+void launch_copy_block(int64_t rows, int cols, const Tsrc *src, int64_t lds, Tdst *dst, int64_t ldd, cudaStream_t st);
+// y = a * x + b * y over rows x cols (double or double2 element types)
+template <class T>
+void launch_axpby(int64_t rows, int cols, T a, const T *x, int64_t ldx, T b, T *y, int64_t ldy, cudaStream_t st);
+
+// ---- dense.cu ------------------------------------------------------------------
+// Dense boundary kernel (BoundaryOperatorKernel.cl:5-239): Ctri = K(kappa) Btri
+// chunk by chunk, the self pair excluded.  R = float (plain FP32) or double.
+template <class R>
+void launch_boundary_dense(const MeshDev &m, const OpFlags &f, const void *chunk_params, int wc, int wcs,
+                           const cplx<R> *Btri, cplx<R> *Ctri, cudaStream_t st);
+// Far-field kernel (FarFieldOperatorKernel.cl:5-178) with source splitting and
+// a deterministic second-pass reduction; Cout = alpha F + beta Cout.
+template <class R>
+void launch_farfield(const MeshDev &m, const OpFlags &f, const void *chunk_params, int wc, int wcs,
+                     const cplx<R> *Btri, cplx<R> *partial, size_t partial_cap, double2 alpha, double2 beta,
+                     double2 *Cout, int64_t ldC, cudaStream_t st);
+size_t farfield_partial_elems(const MeshDev &m, int wc, int wcs);
+// Herglotz kernel (HerglotzWaveKernel.cl:5-176) applied to conj(g).
+template <class R>
+void launch_herglotz(const MeshDev &m, const OpFlags &f, const void *chunk_params, int wc, int wcs,
+                     const double2 *g, int64_t ldg, cplx<R> *Ctri, cudaStream_t st);
+// Incident waves at the midpoints (IncidentWaveKernel_Plane.hpp:189-233, _Radial.hpp:5-57).
+template <class R>
+void launch_incident(const MeshDev &m, const void *chunk_params, int wc, int wcs, const R *dirs, int type,
+                     cplx<R> *Ctri, cudaStream_t st);
+
+} // namespace baemm

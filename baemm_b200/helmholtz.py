@@ -1,0 +1,475 @@
+"""Python mirror of the reference class BAEMM::Helmholtz_OpenCL over the C ABI.
+
+Method names, argument order and meaning follow Helmholtz_OpenCL.hpp and the
+member fragments it includes (ApplyBoundaryOperators.hpp, FarField.hpp, ...),
+so code written against the reference reads the same.  Arrays are numpy
+(host, copied through the device on every call, as the reference does) or
+torch CUDA tensors (device-resident, no host round trip) for the operator
+applies.  Complex blocks are row-major ``rows x ld`` with ``ld >= wave_count``.
+
+Errors: every C call returns a status; a non-zero status raises BaemmError
+with the library's message (the reference prints and continues).
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _capi
+from ._capi import APPLY_FP32, APPLY_FP64, APPLY_TC, WAVE_PLANE, WAVE_RADIAL, BaemmError, SolveStats
+
+__all__ = ["Helmholtz_CUDA", "WaveType", "BaemmError", "APPLY_FP32", "APPLY_TC", "APPLY_FP64"]
+
+
+class WaveType:
+    """BAEMM_Common.hpp:7-11."""
+    Plane = WAVE_PLANE
+    Radial = WAVE_RADIAL
+
+
+def _dp(a):
+    return a.ctypes.data_as(_capi.dp)
+
+
+def _fp(a):
+    return a.ctypes.data_as(_capi.fp)
+
+
+def _cz(x) -> np.ndarray:
+    return np.array([complex(x).real, complex(x).imag], dtype=np.float64)
+
+
+def _cc(x) -> np.ndarray:
+    return np.array([complex(x).real, complex(x).imag], dtype=np.float32)
+
+
+def _is_torch_cuda(x) -> bool:
+    return type(x).__module__.startswith("torch") and getattr(x, "is_cuda", False)
+
+
+def _coeff(coeff) -> np.ndarray:
+    return np.ascontiguousarray(np.asarray(coeff, dtype=np.complex128).reshape(-1, 4))
+
+
+def _f64(a) -> np.ndarray:
+    return np.ascontiguousarray(np.asarray(a, dtype=np.float64))
+
+
+def _check_out(a, dtype, name):
+    if not (isinstance(a, np.ndarray) and a.dtype == dtype and a.ndim == 2 and a.flags.c_contiguous):
+        raise TypeError(f"{name} must be a C-contiguous 2-D numpy array of dtype {np.dtype(dtype).name}")
+
+
+class Helmholtz_CUDA:
+    """Drop-in for Helmholtz_OpenCL(coords, nv, tris, nt, meas, nm, device, threads)
+    (Helmholtz_OpenCL.hpp:175-249)."""
+
+    def __init__(self, vertex_coords, triangles, meas_directions, device: int = 0, cpu_threads: int = 1):
+        L = _capi.lib()
+        self._coords = _f64(vertex_coords).reshape(-1, 3)
+        self._tris = np.ascontiguousarray(np.asarray(triangles, dtype=np.int64).reshape(-1, 3))
+        self._meas = _f64(meas_directions).reshape(-1, 3)
+        h = C.c_void_p()
+        st = L.baemm_create(_dp(self._coords), self._coords.shape[0],
+                            self._tris.ctypes.data_as(_capi.i64p), self._tris.shape[0],
+                            _dp(self._meas), self._meas.shape[0], int(device), int(cpu_threads), C.byref(h))
+        if st != 0:
+            raise BaemmError(st, L.baemm_last_error(None).decode())
+        self._h = h
+        self._lib = L
+
+    # --- lifecycle ---------------------------------------------------------------
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.baemm_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def _ck(self, st):
+        if st != 0:
+            raise BaemmError(st, self._lib.baemm_last_error(self._h).decode())
+
+    # --- getters / setters (GetSetters.hpp) ----------------------------------------
+    def ClassName(self) -> str:
+        return self._lib.baemm_class_name().decode()
+
+    def DeviceInfo(self) -> str:
+        buf = C.create_string_buffer(4096)
+        self._ck(self._lib.baemm_device_info(self._h, buf, 4096))
+        return buf.value.decode()
+
+    def VertexCount(self) -> int:
+        return int(self._lib.baemm_vertex_count(self._h))
+
+    def SimplexCount(self) -> int:
+        return int(self._lib.baemm_simplex_count(self._h))
+
+    def GetMeasCount(self) -> int:
+        return int(self._lib.baemm_meas_count(self._h))
+
+    def GetWaveCount(self) -> int:
+        return int(self._lib.baemm_get_wave_count(self._h))
+
+    def GetWaveChunkSize(self) -> int:
+        return int(self._lib.baemm_get_wave_chunk_size(self._h))
+
+    def SetWaveChunkSize(self, wcs: int):
+        self._ck(self._lib.baemm_set_wave_chunk_size(self._h, int(wcs)))
+
+    def GetBlockSize(self) -> int:
+        return int(self._lib.baemm_get_block_size(self._h))
+
+    def SetBlockSize(self, bs: int):
+        self._ck(self._lib.baemm_set_block_size(self._h, int(bs)))
+
+    def UseDiagonal(self, use_it: bool):
+        self._ck(self._lib.baemm_use_diagonal(self._h, int(bool(use_it))))
+
+    @property
+    def gmres_max_iter(self) -> int:
+        a, b = C.c_int(), C.c_int()
+        self._ck(self._lib.baemm_get_gmres_params(self._h, C.byref(a), C.byref(b)))
+        return a.value
+
+    @gmres_max_iter.setter
+    def gmres_max_iter(self, v: int):
+        self._ck(self._lib.baemm_set_gmres_params(self._h, int(v), self.gmres_max_restarts))
+
+    @property
+    def gmres_max_restarts(self) -> int:
+        a, b = C.c_int(), C.c_int()
+        self._ck(self._lib.baemm_get_gmres_params(self._h, C.byref(a), C.byref(b)))
+        return b.value
+
+    @gmres_max_restarts.setter
+    def gmres_max_restarts(self, v: int):
+        self._ck(self._lib.baemm_set_gmres_params(self._h, self.gmres_max_iter, int(v)))
+
+    def SetApplyMode(self, mode: int):
+        self._ck(self._lib.baemm_set_apply_mode(self._h, int(mode)))
+
+    def GetApplyMode(self) -> int:
+        return int(self._lib.baemm_get_apply_mode(self._h))
+
+    def SetRefinement(self, max_steps: int, inner_tol: float = 1e-4):
+        self._ck(self._lib.baemm_set_refinement(self._h, int(max_steps), float(inner_tol)))
+
+    def LastSolveStats(self) -> dict:
+        s = SolveStats()
+        self._ck(self._lib.baemm_last_solve_stats(self._h, C.byref(s)))
+        return {f: getattr(s, f) for f, _ in SolveStats._fields_}
+
+    def _tri_field(self, fn, width):
+        out = np.zeros((self.SimplexCount(), width) if width > 1 else self.SimplexCount(), dtype=np.float32)
+        self._ck(fn(self._h, _fp(out)))
+        return out
+
+    def Areas(self) -> np.ndarray:
+        return self._tri_field(self._lib.baemm_get_areas, 1)
+
+    TriangleAreas = Areas
+
+    def TriangleNormals(self) -> np.ndarray:
+        return self._tri_field(self._lib.baemm_get_triangle_normals, 4)
+
+    def TriangleMidpoints(self) -> np.ndarray:
+        return self._tri_field(self._lib.baemm_get_triangle_midpoints, 4)
+
+    def SingleLayerDiagonal(self) -> np.ndarray:
+        return self._tri_field(self._lib.baemm_get_single_layer_diagonal, 1)
+
+    def MassMatrix(self):
+        """CSR (outer, inner, values) of the P1 mass matrix (GetSetters.hpp:113-116)."""
+        nnz = C.c_int64()
+        self._ck(self._lib.baemm_get_mass_matrix(self._h, None, None, None, C.byref(nnz)))
+        outer = np.zeros(self.VertexCount() + 1, np.int64)
+        inner = np.zeros(nnz.value, np.int32)
+        vals = np.zeros(nnz.value, np.float32)
+        self._ck(self._lib.baemm_get_mass_matrix(self._h, outer.ctypes.data_as(_capi.i64p),
+                                                 inner.ctypes.data_as(_capi.i32p), _fp(vals), C.byref(nnz)))
+        return outer, inner, vals
+
+    def SetProfiling(self, on: bool):
+        self._ck(self._lib.baemm_set_profiling(self._h, int(bool(on))))
+
+    def LastApplyTimes(self):
+        """Device ms of the last boundary apply: (AvOp, dense kernel, epilogue)."""
+        ms = np.zeros(3, np.float32)
+        self._ck(self._lib.baemm_last_apply_times(self._h, _fp(ms)))
+        return tuple(float(x) for x in ms)
+
+    @staticmethod
+    def KernelLaunchCount() -> int:
+        return int(_capi.lib().baemm_kernel_launch_count())
+
+    def stream(self) -> int:
+        return int(self._lib.baemm_stream(self._h) or 0)
+
+    def SetStream(self, stream_handle: int | None):
+        self._ck(self._lib.baemm_set_stream(self._h, C.c_void_p(stream_handle or 0)))
+
+    def Synchronize(self):
+        self._ck(self._lib.baemm_synchronize(self._h))
+
+    # --- parameters / operators ----------------------------------------------------
+    def LoadParameters(self, kappa, coeff, wave_count, wave_chunk_size, factor=1.0):
+        k, c = _f64(kappa), _coeff(coeff)
+        self._ck(self._lib.baemm_load_parameters(self._h, _dp(k), _dp(c.view(np.float64)), int(wave_count),
+                                                 int(wave_chunk_size), float(factor)))
+
+    def LoadBoundaryOperators_PL(self, kappa, coeff, wave_count, wave_chunk_size):
+        k, c = _f64(kappa), _coeff(coeff)
+        self._ck(self._lib.baemm_load_boundary_operators(self._h, _dp(k), _dp(c.view(np.float64)),
+                                                         int(wave_count), int(wave_chunk_size)))
+
+    def UnloadBoundaryOperators_PL(self):
+        self._ck(self._lib.baemm_unload_boundary_operators(self._h))
+
+    def ApplyBoundaryOperators_PL(self, alpha, B_in, beta, C_out, kappa=None, coeff=None, wave_count=None,
+                                  wave_chunk_size=None):
+        """C_out = alpha * A * B_in + beta * C_out (ApplyBoundaryOperators.hpp:238-391).
+
+        With kappa/coeff/wave_count/wave_chunk_size given, loads, applies and
+        unloads (the first overload); otherwise uses the loaded operators.
+        numpy complex128 / complex64 host blocks or torch CUDA complex tensors.
+        """
+        full = kappa is not None
+        if full:
+            self.LoadBoundaryOperators_PL(kappa, coeff, wave_count, wave_chunk_size)
+        try:
+            if _is_torch_cuda(B_in):
+                import torch
+                if B_in.dtype == torch.complex128:
+                    self._ck(self._lib.baemm_apply_boundary_operators_dev_z(
+                        self._h, _dp(_cz(alpha)), C.c_void_p(B_in.data_ptr()), B_in.stride(0),
+                        _dp(_cz(beta)), C.c_void_p(C_out.data_ptr()), C_out.stride(0)))
+                elif B_in.dtype == torch.complex64:
+                    self._ck(self._lib.baemm_apply_boundary_operators_dev_c(
+                        self._h, _fp(_cc(alpha)), C.c_void_p(B_in.data_ptr()), B_in.stride(0),
+                        _fp(_cc(beta)), C.c_void_p(C_out.data_ptr()), C_out.stride(0)))
+                else:
+                    raise TypeError("B_in must be complex64 or complex128")
+            elif isinstance(B_in, np.ndarray) and B_in.dtype == np.complex64:
+                _check_out(C_out, np.complex64, "C_out")
+                B = np.ascontiguousarray(B_in)
+                self._ck(self._lib.baemm_apply_boundary_operators_c(
+                    self._h, _fp(_cc(alpha)), _fp(B.view(np.float32)), B.shape[1], _fp(_cc(beta)),
+                    _fp(C_out.view(np.float32)), C_out.shape[1]))
+            else:
+                _check_out(C_out, np.complex128, "C_out")
+                B = np.ascontiguousarray(B_in, dtype=np.complex128)
+                self._ck(self._lib.baemm_apply_boundary_operators_z(
+                    self._h, _dp(_cz(alpha)), _dp(B.view(np.float64)), B.shape[1], _dp(_cz(beta)),
+                    _dp(C_out.view(np.float64)), C_out.shape[1]))
+        finally:
+            if full:
+                self.UnloadBoundaryOperators_PL()
+        return C_out
+
+    def ApplyFarFieldOperators_PL(self, alpha, B_in, beta, C_out, kappa=None, coeff=None, wave_count=None,
+                                  wave_chunk_size=None):
+        """C_out (meas x wc) = alpha (c1 FF_SL + c2 FF_DL) B_in + beta C_out
+        (ApplyFarFieldOperators.hpp:334-412)."""
+        if _is_torch_cuda(B_in):
+            if kappa is not None:
+                self.LoadParameters(kappa, coeff, wave_count, wave_chunk_size)
+            self._ck(self._lib.baemm_apply_far_field_operators_dev_z(
+                self._h, _dp(_cz(alpha)), C.c_void_p(B_in.data_ptr()), B_in.stride(0), _dp(_cz(beta)),
+                C.c_void_p(C_out.data_ptr()), C_out.stride(0)))
+            return C_out
+        _check_out(C_out, np.complex128, "C_out")
+        B = np.ascontiguousarray(B_in, dtype=np.complex128)
+        if kappa is not None:
+            k, c = _f64(kappa), _coeff(coeff)
+            self._ck(self._lib.baemm_apply_far_field_operators_z(
+                self._h, _dp(_cz(alpha)), _dp(B.view(np.float64)), B.shape[1], _dp(_cz(beta)),
+                _dp(C_out.view(np.float64)), C_out.shape[1], _dp(k), _dp(c.view(np.float64)), int(wave_count),
+                int(wave_chunk_size)))
+        else:
+            self._ck(self._lib.baemm_apply_far_field_operators_loaded_z(
+                self._h, _dp(_cz(alpha)), _dp(B.view(np.float64)), B.shape[1], _dp(_cz(beta)),
+                _dp(C_out.view(np.float64)), C_out.shape[1]))
+        return C_out
+
+    def CreateIncidentWave_PL(self, alpha, incident_directions, beta, C_out, kappa, coeff, wave_count,
+                              wave_chunk_size, wave_type=WaveType.Plane):
+        """C_out = alpha * wave + beta * C_out (CreateIncidentWave.hpp:21-50)."""
+        _check_out(C_out, np.complex128, "C_out")
+        d = _f64(incident_directions).reshape(-1, 3)
+        k, c = _f64(kappa), _coeff(coeff)
+        self._ck(self._lib.baemm_create_incident_wave_z(
+            self._h, _dp(_cz(alpha)), _dp(d), d.shape[0], _dp(_cz(beta)), _dp(C_out.view(np.float64)),
+            C_out.shape[1], _dp(k), _dp(c.view(np.float64)), int(wave_count), int(wave_chunk_size),
+            int(wave_type)))
+        return C_out
+
+    def CreateHerglotzWave_PL(self, alpha, g, beta, C_out, kappa, coeff, wave_count, wave_chunk_size):
+        """C_out = alpha * HerglotzWave(g) + beta * C_out (CreateHerglotzWave.hpp:25-44)."""
+        _check_out(C_out, np.complex128, "C_out")
+        G = np.ascontiguousarray(g, dtype=np.complex128)
+        k, c = _f64(kappa), _coeff(coeff)
+        self._ck(self._lib.baemm_create_herglotz_wave_z(
+            self._h, _dp(_cz(alpha)), _dp(G.view(np.float64)), G.shape[1], _dp(_cz(beta)),
+            _dp(C_out.view(np.float64)), C_out.shape[1], _dp(k), _dp(c.view(np.float64)), int(wave_count),
+            int(wave_chunk_size)))
+        return C_out
+
+    def ApplyMassInverse(self, X, Y, cg_tol, nrhs=None):
+        """Y = M^-1 X by CG (ApplyMassInverse.hpp:6-156); real or complex columns."""
+        if np.iscomplexobj(X):
+            Xc = np.ascontiguousarray(X, dtype=np.complex128)
+            _check_out(Y, np.complex128, "Y")
+            n = Xc.shape[1] if nrhs is None else nrhs
+            self._ck(self._lib.baemm_apply_mass_inverse_z(self._h, _dp(Xc.view(np.float64)), Xc.shape[1],
+                                                          _dp(Y.view(np.float64)), Y.shape[1], int(n),
+                                                          float(cg_tol)))
+        else:
+            Xr = _f64(X)
+            if Xr.ndim == 1:
+                Xr = Xr[:, None]
+            Yv = Y if Y.ndim == 2 else Y.reshape(-1, 1)
+            n = Xr.shape[1] if nrhs is None else nrhs
+            self._ck(self._lib.baemm_apply_mass_inverse_d(self._h, _dp(Xr), Xr.shape[1], _dp(Yv), Yv.shape[1],
+                                                          int(n), float(cg_tol)))
+        return Y
+
+    def ApplyLumpedMassInverse(self, X, Y, nrhs=None):
+        if np.iscomplexobj(X):
+            Xc = np.ascontiguousarray(X, dtype=np.complex128)
+            n = Xc.shape[1] if nrhs is None else nrhs
+            self._ck(self._lib.baemm_apply_lumped_mass_inverse_z(self._h, _dp(Xc.view(np.float64)), Xc.shape[1],
+                                                                 _dp(Y.view(np.float64)), Y.shape[1], int(n)))
+        else:
+            Xr = _f64(X)
+            n = Xr.shape[1] if nrhs is None else nrhs
+            self._ck(self._lib.baemm_apply_lumped_mass_inverse_d(self._h, _dp(Xr), Xr.shape[1], _dp(Y), Y.shape[1],
+                                                                 int(n)))
+        return Y
+
+    def MassDot(self, alpha, X, beta, Y):
+        """Y = alpha M X + beta Y on real columns (MassMatrix().Dot)."""
+        Xr = _f64(X)
+        self._ck(self._lib.baemm_mass_dot_d(self._h, float(alpha), _dp(Xr), Xr.shape[1], float(beta), _dp(Y),
+                                            Y.shape[1], Xr.shape[1]))
+        return Y
+
+    # --- solvers (FarField.hpp) -----------------------------------------------------
+    def FarField(self, kappa, inc_directions, Y_out, wave_type=WaveType.Plane, cg_tol=1e-5, gmres_tol=1e-4):
+        return self.FarField_parameters(kappa, inc_directions, Y_out, wave_type, None, cg_tol, gmres_tol)
+
+    def FarField_parameters(self, kappa, inc_directions, Y_out, wave_type=WaveType.Plane, eta=None, cg_tol=1e-5,
+                            gmres_tol=1e-4):
+        k = _f64(kappa)
+        d = _f64(inc_directions).reshape(-1, 3)
+        _check_out(Y_out, np.complex128, "Y_out")
+        e = _f64(eta) if eta is not None else None
+        self._ck(self._lib.baemm_far_field_parameters(self._h, _dp(k), k.size, _dp(d), d.shape[0],
+                                                      _dp(Y_out.view(np.float64)), int(wave_type),
+                                                      _dp(e) if e is not None else None, float(cg_tol),
+                                                      float(gmres_tol)))
+        return Y_out
+
+    def BoundaryPotential(self, kappa, coeff_out, wave, phi, wave_chunk_size, cg_tol, gmres_tol):
+        k = _f64(kappa)
+        W = np.ascontiguousarray(wave, dtype=np.complex128)
+        self._ck(self._lib.baemm_boundary_potential(self._h, _dp(k), _dp(coeff_out.view(np.float64)),
+                                                    _dp(W.view(np.float64)), _dp(phi.view(np.float64)), k.size,
+                                                    int(wave_chunk_size), float(cg_tol), float(gmres_tol)))
+        return phi
+
+    def DirichletToNeumann(self, kappa, wave, neumann_trace, wave_chunk_size, cg_tol, gmres_tol):
+        k = _f64(kappa)
+        W = np.ascontiguousarray(wave, dtype=np.complex128)
+        self._ck(self._lib.baemm_dirichlet_to_neumann(self._h, _dp(k), _dp(W.view(np.float64)),
+                                                      _dp(neumann_trace.view(np.float64)), k.size,
+                                                      int(wave_chunk_size), float(cg_tol), float(gmres_tol)))
+        return neumann_trace
+
+    def Derivative_FF_Helper(self, kappa, inc_directions, du_dn, wave_type=WaveType.Plane, cg_tol=1e-5,
+                             gmres_tol=1e-4):
+        k = _f64(kappa)
+        d = _f64(inc_directions).reshape(-1, 3)
+        self._ck(self._lib.baemm_derivative_ff_helper(self._h, _dp(k), k.size, _dp(d), d.shape[0],
+                                                      _dp(du_dn.view(np.float64)), int(wave_type), float(cg_tol),
+                                                      float(gmres_tol)))
+        return du_dn
+
+    def _du_dn_ptr(self, du_dn):
+        if du_dn is None:
+            return _capi.dp()   # NULL: the library callocs and fills it
+        return du_dn.view(np.float64).ctypes.data_as(_capi.dp)
+
+    def _take_du_dn(self, ptr, du_dn, wc):
+        if du_dn is not None:
+            return du_dn
+        n = self.VertexCount() * wc
+        arr = np.ctypeslib.as_array(ptr, shape=(2 * n,)).copy().view(np.complex128).reshape(-1, wc)
+        self._lib.baemm_free(C.cast(ptr, C.c_void_p))
+        return arr
+
+    def Derivative_FF(self, kappa, inc_directions, X_in, Y_out, du_dn=None, wave_type=WaveType.Plane, cg_tol=1e-5,
+                      gmres_tol=1e-4):
+        """Returns (Y_out, du_dn); du_dn=None lets the library compute it (FarField.hpp:273-283)."""
+        k = _f64(kappa)
+        d = _f64(inc_directions).reshape(-1, 3)
+        X = _f64(X_in).reshape(-1, 3)
+        ptr = self._du_dn_ptr(du_dn)
+        self._ck(self._lib.baemm_derivative_ff(self._h, _dp(k), k.size, _dp(d), d.shape[0], _dp(X),
+                                               _dp(Y_out.view(np.float64)), C.byref(ptr), int(wave_type),
+                                               float(cg_tol), float(gmres_tol)))
+        return Y_out, self._take_du_dn(ptr, du_dn, k.size * d.shape[0])
+
+    def AdjointDerivative_FF(self, kappa, inc_directions, g, Y_out, du_dn=None, wave_type=WaveType.Plane,
+                             cg_tol=1e-5, gmres_tol=1e-4):
+        k = _f64(kappa)
+        d = _f64(inc_directions).reshape(-1, 3)
+        G = np.ascontiguousarray(g, dtype=np.complex128)
+        ptr = self._du_dn_ptr(du_dn)
+        self._ck(self._lib.baemm_adjoint_derivative_ff(self._h, _dp(k), k.size, _dp(d), d.shape[0],
+                                                       _dp(G.view(np.float64)), _dp(Y_out), C.byref(ptr),
+                                                       int(wave_type), float(cg_tol), float(gmres_tol)))
+        return Y_out, self._take_du_dn(ptr, du_dn, k.size * d.shape[0])
+
+    def GaussNewtonSolve(self, kappa, inc_directions, M, P, alpha, B_in, beta, X_out, du_dn,
+                         wave_type=WaveType.Plane, cg_tol=1e-5, gmres_tol_inner=5e-3, gmres_tol_outer=1e-2,
+                         solver: int = 0) -> bool:
+        """X = alpha (M + DF* DF)^-1 B + beta X (FarField.hpp:457-604).
+
+        M, P: callables (x, y) on numpy (n, 3) float64 arrays, writing y in place.
+        solver 0 = GMRES (the reference), 1 = CG.
+        """
+        k = _f64(kappa)
+        d = _f64(inc_directions).reshape(-1, 3)
+        n = self.VertexCount()
+        B = _f64(B_in)
+
+        def wrap(f):
+            def cb(x, y, _user):
+                xa = np.ctypeslib.as_array(x, shape=(n, 3))
+                ya = np.ctypeslib.as_array(y, shape=(n, 3))
+                f(xa, ya)
+            return _capi.REAL_OP(cb)
+
+        Mc, Pc = wrap(M), wrap(P)
+        ptr = self._du_dn_ptr(du_dn)
+        ok = C.c_int(0)
+        self._ck(self._lib.baemm_gauss_newton_solve(self._h, _dp(k), k.size, _dp(d), d.shape[0], Mc, None, Pc, None,
+                                                    float(alpha), _dp(B), B.shape[1], float(beta), _dp(X_out),
+                                                    X_out.shape[1], C.byref(ptr), int(wave_type), float(cg_tol),
+                                                    float(gmres_tol_inner), float(gmres_tol_outer), int(solver),
+                                                    C.byref(ok)))
+        if du_dn is None:
+            self._take_du_dn(ptr, None, k.size * d.shape[0])
+        return bool(ok.value)

@@ -1,0 +1,364 @@
+#!/usr/bin/env python
+"""Benchmark: GInteractions/s of BAEMM's boundary-operator apply on B200.
+
+Workload (one "step" = one operator apply): the large-block apply -- torus
+with major radius 1.0 and minor radius 0.4 on a 160 x 480 parametric grid,
+2 triangles per quad (76800 vertices, 153600 triangles); 64 right-hand sides
+= 4 wavenumbers {2, 4, 8, 16} x 16 complex64 vertex vectors, re/im iid N(0,1)
+(seed 0); single- plus double-layer operator of the mixed indirect BIE
+(coefficients per chunk: mass 0, SL -i kappa, DL 1, adjoint DL 0) with the
+singular SL diagonal.  Interactions per apply I = N_t * N_s * wave_count.
+
+  value  device time of the apply (AvOp, dense kernel, AvOp^T epilogue) with
+         inputs resident in HBM, L2 flushed (256 MiB write) before every step
+  e2e    the same apply through the host-pointer C ABI call
+         (baemm_apply_boundary_operators_c) from pinned host memory,
+         host->device and device->host copies inside the timed region
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--mode fp32|fp64]
+  python bench.py --impl reference ...   # the reference's own kernel on the host cores
+
+Multi-GPU (torchrun, one process per GPU): independent replicas of the same
+workload per rank (the operator apply does not exchange data); value = all
+ranks' interactions / the max over ranks of the timed device time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "GInteractions/s per operator apply"
+UNIT = "GInteractions/s"
+WORKLOAD = "torus R1.0 r0.4 160x480 grid (76800 V, 153600 T), 64 RHS = kappa {2,4,8,16} x 16, SL+DL apply"
+KAPPA = np.array([2.0, 4.0, 8.0, 16.0])
+WCS = 16
+WC = 64
+
+
+def coefficients(kappa):
+    return np.array([[0.0, -1j * k, 1.0, 0.0] for k in kappa], np.complex128)
+
+
+def build_workload(seed=0, small=False):
+    """The torus workload; small=True is the 80 x 240 grid (38400 triangles)
+    used only for ncu captures of the same kernels."""
+    from baemm_b200 import meshes
+    coords, tris = meshes.torus(1.0, 0.4, 80, 240) if small else meshes.torus(1.0, 0.4, 160, 480)
+    rng = np.random.default_rng(seed)
+    B = (rng.standard_normal((coords.shape[0], WC)) + 1j * rng.standard_normal((coords.shape[0], WC)))
+    return coords, tris, B.astype(np.complex64)
+
+
+def load_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return {"hbm_gbs": d.get("hbm_gbs", 6650.0), "bf16_tflops": d.get("bf16_tflops", 1590.0),
+                "bf16_tflops_sustained": d.get("bf16_tflops_sustained", 1400.0), "source": "of measured"}
+    return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0, "source": "of fallback"}
+
+
+def load_traffic():
+    """Per-launch DRAM bytes of the dense kernel from the committed ncu summary, if any."""
+    p = os.path.join(ROOT, "profiles", "boundary_dense_torus.json")
+    if os.path.exists(p):
+        try:
+            return json.load(open(p)).get("dram_bytes_per_launch")
+        except Exception:
+            return None
+    return None
+
+
+# ---------------------------------------------------------------------------
+# clocks sampled during the timed region
+# ---------------------------------------------------------------------------
+REASON_BITS = {
+    0x1: "gpu_idle", 0x2: "applications_clocks_setting", 0x4: "sw_power_cap", 0x8: "hw_slowdown",
+    0x10: "sync_boost", 0x20: "sw_thermal_slowdown", 0x40: "hw_thermal_slowdown", 0x80: "hw_power_brake_slowdown",
+    0x100: "display_clock_setting",
+}
+
+
+class ClockSampler:
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index),
+                 "--query-gpu=clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], [], 0
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 4:
+                continue
+            try:
+                s, m = float(parts[0]), float(parts[1])
+                r = int(parts[3], 16) if parts[3].startswith("0x") else int(parts[3])
+            except ValueError:
+                continue
+            sm.append(s)
+            mx.append(m)
+            if s > 0.5 * m:    # under load
+                reasons |= r
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"], "samples": 0}
+        names = [n for b, n in REASON_BITS.items() if reasons & b and n != "gpu_idle"]
+        loaded = [s for s, m in zip(sm, mx) if s > 0.5 * m] or sm
+        return {"sm_mhz": float(np.median(loaded)), "sm_max_mhz": float(max(mx)), "reasons": names,
+                "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+# the reference's own kernel on the host (CPU baseline and --impl reference)
+# ---------------------------------------------------------------------------
+def reference_rows_rate(coords, tris, B_vertex, target_seconds=15.0, threads=0):
+    """GInteractions/s of the reference BoundaryOperatorKernel.cl (compiled as
+    C++, oracle/_ref) on a contiguous block of target rows against all sources.
+    Cost is separable per target row, so rows/s scales exactly to the full apply."""
+    from oracle import oracle as O
+    if not O.ref_available():
+        return None
+    orc = O.Oracle(coords, tris, np.eye(3), precision=32, threads=threads)
+    mid, nrm, area, _ = orc.geometry()
+    n = tris.shape[0]
+    # B_tri = AvOp B (PL -> PC), as the reference does before the kernel
+    a3 = (area / 3.0).astype(np.float64)
+    Btri = (a3[:, None] * B_vertex[tris].sum(axis=1)).astype(np.complex64)
+    cs = O.scaled_coefficients(coefficients(KAPPA))
+    nthreads = threads or O.reflib().refcl_max_threads()
+    rows = max(nthreads, 8)
+    t0 = time.perf_counter()
+    O.ref_boundary(mid, nrm, Btri, KAPPA, cs, WCS, 0, rows, threads)
+    dt = time.perf_counter() - t0
+    rows2 = int(min(n - rows, max(rows, rows * target_seconds / max(dt, 1e-3))))
+    t0 = time.perf_counter()
+    O.ref_boundary(mid, nrm, Btri, KAPPA, cs, WCS, rows, rows + rows2, threads)
+    dt = time.perf_counter() - t0
+    inter = rows2 * n * WC
+    return {"value": inter / dt / 1e9, "unit": UNIT, "cores": int(nthreads), "kind": "reference",
+            "seconds": dt, "rows": rows2,
+            "sample": f"reference BoundaryOperatorKernel.cl (oracle/_ref, compiled as C++) on {rows2} contiguous "
+                      f"target rows x all {n} sources x 64 RHS, OpenMP over rows; scaled per interaction "
+                      f"(cost is separable per target row); AvOp/AvOp^T (O(N wc)) not in the sample"}
+
+
+def run_reference_arm(args, rank, world):
+    if rank != 0:
+        return 0
+    coords, tris, B = build_workload()
+    cpu = reference_rows_rate(coords, tris, B, target_seconds=float(os.environ.get("BAEMM_REF_SECONDS", "12")))
+    if cpu is None:
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libbaemm_refcl.so not built"}))
+        return 0
+    vals = [cpu["value"]]
+    for _ in range(max(0, args.steps - 1)):
+        c2 = reference_rows_rate(coords, tris, B, target_seconds=float(os.environ.get("BAEMM_REF_SECONDS", "12")))
+        vals.append(c2["value"])
+    v = float(np.mean(vals))
+    n = tris.shape[0]
+    line = {
+        "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": n * n * WC / (v * 1e9) * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "fp32", "data": "synthetic",
+        "config": {"workload": WORKLOAD if not args.small else "SMALL torus 80x240 (profiling only)", "interactions_per_step": n * n * WC, "parallelism": "host cores",
+                   "l2": "n/a (CPU)"},
+        "cpu_baseline": {"value": v, "unit": UNIT, "cores": cpu["cores"], "kind": "reference",
+                         "sample": cpu["sample"]},
+        "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+    return 0
+
+
+# ---------------------------------------------------------------------------
+# the CUDA arm
+# ---------------------------------------------------------------------------
+def run_gpu_arm(args, rank, world, local_rank):
+    import torch
+    from baemm_b200 import APPLY_FP32, APPLY_FP64, Helmholtz_CUDA
+
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+    coords, tris, B = build_workload(seed=0, small=args.small)
+    nv, nt = coords.shape[0], tris.shape[0]
+    inter = nt * nt * WC
+    H = Helmholtz_CUDA(coords, tris, np.eye(3), device=local_rank)
+    mode = {"fp32": APPLY_FP32, "fp64": APPLY_FP64}[args.mode]
+    H.SetApplyMode(mode)
+    kap, coeff = KAPPA, coefficients(KAPPA)
+    stream = torch.cuda.Stream()
+    H.SetStream(stream.cuda_stream)
+    H.SetProfiling(True)
+    Bd = torch.from_numpy(B).cuda()
+    Cd = torch.zeros_like(Bd)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    H.LoadBoundaryOperators_PL(kap, coeff, WC, WCS)
+
+    def step():
+        H.ApplyBoundaryOperators_PL(1.0, Bd, 0.0, Cd)
+
+    with torch.cuda.stream(stream):
+        for _ in range(args.warmup):
+            flush.fill_(1.0)
+            step()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    launches0 = H.KernelLaunchCount()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    dense_ms = []
+    with ClockSampler(torch.cuda.current_device()) as clk:
+        with torch.cuda.stream(stream):
+            for k in range(args.steps):
+                flush.fill_(float(k))
+                ev[k][0].record(stream)
+                step()
+                ev[k][1].record(stream)
+                dense_ms.append(H.LastApplyTimes()[1])
+        torch.cuda.synchronize()
+    launches = H.KernelLaunchCount() - launches0 - 0  # library kernels only (flush is torch's)
+    step_ms = [a.elapsed_time(b) for a, b in ev]
+    total_ms = float(np.sum(step_ms))
+    if dist:
+        t = torch.tensor([total_ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+    value = world * inter * args.steps / (total_ms * 1e-3) / 1e9
+
+    # ---- e2e through the host-pointer C ABI (pinned host buffers) -----------------
+    Bh = torch.from_numpy(B).pin_memory().numpy()
+    Ch = torch.zeros(B.shape, dtype=torch.complex64).pin_memory().numpy()
+    H.SetStream(None)
+    for _ in range(max(1, args.warmup // 2)):
+        H.ApplyBoundaryOperators_PL(1.0, Bh, 0.0, Ch)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    e2e_ms = []
+    for k in range(args.steps):
+        flush.fill_(float(k))
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        H.ApplyBoundaryOperators_PL(1.0, Bh, 0.0, Ch)   # H2D, apply, D2H, synchronised
+        e2e_ms.append((time.perf_counter() - t0) * 1e3)
+    e2e_total = float(np.sum(e2e_ms))
+    if dist:
+        t = torch.tensor([e2e_total], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_total = float(t.item())
+    e2e_value = world * inter * args.steps / (e2e_total * 1e-3) / 1e9
+    H.UnloadBoundaryOperators_PL()
+
+    if rank != 0:
+        H.close()
+        return 0
+    peaks = load_peaks()
+    dense_avg = float(np.mean(dense_ms))
+    flops = 8.0 * inter
+    achieved = flops / (dense_avg * 1e-3) / 1e12
+    traffic = load_traffic()
+    cpu = None
+    if world == 1 and not args.no_cpu_baseline:
+        cpu = reference_rows_rate(coords, tris, B, target_seconds=float(os.environ.get("BAEMM_REF_SECONDS", "12")))
+    # model bound of the plain FP32 form: contraction FMAs + ~20 FP32 ops per generated entry
+    n_k = len(KAPPA)
+    fp32_ops = 2.0 * (4.0 * inter) + 20.0 * nt * nt * n_k
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": args.mode, "data": "synthetic",
+        "config": {"workload": WORKLOAD if not args.small else "SMALL torus 80x240 (profiling only)", "interactions_per_step": inter, "wave_count": WC,
+                   "wave_chunk_size": WCS, "kappa": KAPPA.tolist(), "apply_mode": args.mode,
+                   "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+                   "l2": "flushed (256 MiB write) before every timed step",
+                   "phase_ms_last": list(H.LastApplyTimes()) if False else None},
+        "roofline": {"bound": "tensor", "kernel": "boundary_dense_kernel", "achieved": achieved,
+                     "peak": peaks["bf16_tflops"], "unit": "TFLOP/s", "frac": achieved / peaks["bf16_tflops"],
+                     "peak_source": peaks["source"] + " (dense bf16 burst)",
+                     "algorithmic": "8 * N_t * N_s * wave_count FLOPs per launch (complex MACs)",
+                     "dense_kernel_ms": dense_avg, "traffic": traffic,
+                     "fp32_model_tflops": fp32_ops / (dense_avg * 1e-3) / 1e12},
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(B.nbytes),
+                "d2h_bytes_per_step": int(B.nbytes), "ms_per_step": e2e_total / args.steps},
+        "gpu_launches": int(launches),
+        "clocks": clk.summary(),
+    }
+    if cpu is not None:
+        line["cpu_baseline"] = {"value": cpu["value"], "unit": UNIT, "cores": cpu["cores"], "kind": cpu["kind"],
+                                "sample": cpu["sample"]}
+    print(json.dumps(line), flush=True)
+    H.close()
+    return 0
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="cuda", choices=["cuda", "reference"])
+    ap.add_argument("--mode", default="fp32", choices=["fp32", "fp64"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--small", action="store_true", help="38400-triangle torus (profiling captures only)")
+    args = ap.parse_args(argv)
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        return run_reference_arm(args, rank, world)
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    try:
+        return run_gpu_arm(args, rank, world, local_rank)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    sys.exit(main())

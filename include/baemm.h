@@ -1,0 +1,268 @@
+/* baemm.h -- C ABI of libbaemm_cuda.so, the B200 (sm_100a) implementation of
+ * BAEMM's boundary-element Helmholtz operator path.
+ *
+ * Every entry point replaces one public member of the reference class
+ * BAEMM::Helmholtz_OpenCL (HenrikSchumacher/BAEMM); the reference interface is
+ * cited beside each declaration (path:line within that project).  The C++
+ * drop-in class in Helmholtz_CUDA.hpp wraps these calls with the reference's
+ * templated signatures.
+ *
+ * Conventions
+ *   - Plain pointers and sizes only.  Complex arrays are interleaved (re, im)
+ *     pairs, row-major "rows x ld" exactly as the reference lays them out.
+ *     `_z` = complex<double> external data, `_c` = complex<float>, `_d` = double.
+ *   - Host-pointer entry points copy inputs to the device and results back
+ *     (the reference's semantics).  `_dev_` entry points take device pointers
+ *     and run on the context's stream without host synchronisation.
+ *   - Every call returns a baemm_status; 0 is success.  The text of the last
+ *     error of a context is available from baemm_last_error().
+ *   - A context is externally synchronised: one thread at a time (the
+ *     reference class is not thread-safe either).
+ *   - There is no CPU fallback: without a usable CUDA device baemm_create
+ *     fails with BAEMM_ERR_CUDA.
+ */
+#ifndef BAEMM_H
+#define BAEMM_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct baemm_ctx baemm_ctx;
+
+typedef enum baemm_status
+{
+    BAEMM_OK                = 0,
+    BAEMM_ERR_ARG           = 1,  /* invalid argument (null pointer, bad size, ld < wave_count, ...) */
+    BAEMM_ERR_CUDA          = 2,  /* a CUDA call failed; see baemm_last_error */
+    BAEMM_ERR_ALLOC         = 3,  /* device or host allocation failed */
+    BAEMM_ERR_NOT_LOADED    = 4,  /* operator applied before baemm_load_boundary_operators */
+    BAEMM_ERR_NOT_CONVERGED = 5,  /* a solver stopped at its iteration limit */
+    BAEMM_ERR_SIZE          = 6,  /* size outside the supported range */
+    BAEMM_ERR_TIMEOUT       = 7   /* a bounded device-side wait gave up */
+} baemm_status;
+
+/* Wave types (BAEMM_Common.hpp:7-11). */
+#define BAEMM_WAVE_PLANE  201
+#define BAEMM_WAVE_RADIAL 202
+
+/* Arithmetic of the dense boundary-operator apply (no reference counterpart;
+ * the reference has FP32 only, Definitions.hpp:3-6). */
+#define BAEMM_APPLY_FP32 0   /* plain: FP32 generation and FP32 SIMT contraction */
+#define BAEMM_APPLY_TC   1   /* compensated: split hi+lo operands on the tensor cores, FP32 accumulate */
+#define BAEMM_APPLY_FP64 2   /* FP64 generation and contraction */
+
+/* Solver statistics of the last GMRES / CG run (the reference discards them,
+ * FarField.hpp:764, 870). */
+typedef struct baemm_solve_stats
+{
+    int32_t gmres_iterations;
+    int32_t gmres_converged;
+    double  gmres_relative_residual;
+    int32_t cg_iterations;         /* max over the mass-inverse calls of that solve */
+    int32_t cg_converged;
+    int32_t refinement_steps;      /* FP64 iterative-refinement steps (0 = none) */
+    double  seconds;
+} baemm_solve_stats;
+
+/* User operator on n x 3 real host arrays (the M and P callables of
+ * GaussNewtonSolve, FarField.hpp:457-479). */
+typedef void (*baemm_real_op)(const double *x, double *y, void *user);
+
+/* ---- lifecycle ---------------------------------------------------------- */
+
+/* Helmholtz_OpenCL(coords, nv, tris, nt, meas, nm, device_num, threads)
+ * (Helmholtz_OpenCL.hpp:175-249) and the variant without device_num
+ * (Helmholtz_OpenCL.hpp:109-159; pass device = 0).  coords: nv x 3,
+ * triangles: nt x 3 (0-based), meas_directions: nm x 3.  cpu_threads is
+ * accepted for signature parity and bounds the host threads of set-up. */
+int baemm_create(const double *coords, int64_t vertex_count,
+                 const int64_t *triangles, int64_t simplex_count,
+                 const double *meas_directions, int64_t meas_count,
+                 int device, int cpu_threads, baemm_ctx **out);
+int baemm_create_i32(const double *coords, int64_t vertex_count,
+                     const int32_t *triangles, int64_t simplex_count,
+                     const double *meas_directions, int64_t meas_count,
+                     int device, int cpu_threads, baemm_ctx **out);
+/* ~Helmholtz_OpenCL (Helmholtz_OpenCL.hpp:251-282). */
+void baemm_destroy(baemm_ctx *ctx);
+const char *baemm_last_error(const baemm_ctx *ctx);
+/* DeviceInfo (Helmholtz_OpenCL.hpp:343-391); writes a NUL-terminated text. */
+int baemm_device_info(baemm_ctx *ctx, char *buf, size_t len);
+/* ClassName (Helmholtz_OpenCL.hpp:395-398): "Helmholtz_CUDA". */
+const char *baemm_class_name(void);
+/* The CUDA stream the context runs on (cudaStream_t). */
+void *baemm_stream(baemm_ctx *ctx);
+/* Use an external stream (e.g. a framework's current stream); NULL = own stream. */
+int baemm_set_stream(baemm_ctx *ctx, void *stream);
+int baemm_synchronize(baemm_ctx *ctx);
+
+/* ---- getters / setters (GetSetters.hpp, MemberVariables.hpp:93-98) ------- */
+int64_t baemm_vertex_count(const baemm_ctx *ctx);          /* GetSetters.hpp:103-106 */
+int64_t baemm_simplex_count(const baemm_ctx *ctx);         /* GetSetters.hpp:108-111 */
+int64_t baemm_meas_count(const baemm_ctx *ctx);            /* GetSetters.hpp:164-167 */
+int baemm_get_wave_count(const baemm_ctx *ctx);            /* GetSetters.hpp:130-133 */
+int baemm_get_wave_chunk_size(const baemm_ctx *ctx);       /* GetSetters.hpp:142-145 */
+int baemm_set_wave_chunk_size(baemm_ctx *ctx, int wcs);    /* GetSetters.hpp:147-152 */
+int baemm_get_block_size(const baemm_ctx *ctx);            /* GetSetters.hpp:159-162 */
+int baemm_set_block_size(baemm_ctx *ctx, int block_size);  /* GetSetters.hpp:180-188 (recorded; tiles are chosen by the library) */
+int baemm_use_diagonal(baemm_ctx *ctx, int use_it);        /* GetSetters.hpp:210-213 */
+int baemm_set_gmres_params(baemm_ctx *ctx, int max_iter, int max_restarts); /* MemberVariables.hpp:97-98 */
+int baemm_get_gmres_params(const baemm_ctx *ctx, int *max_iter, int *max_restarts);
+int baemm_set_apply_mode(baemm_ctx *ctx, int mode);        /* BAEMM_APPLY_*; no reference counterpart */
+int baemm_get_apply_mode(const baemm_ctx *ctx);
+/* FP64 iterative refinement around the inner GMRES (0 = off, the reference's
+ * behaviour).  When on, the solve's outer residual uses the FP64 apply and
+ * the inner GMRES uses the context's apply mode. No reference counterpart. */
+int baemm_set_refinement(baemm_ctx *ctx, int max_steps, double inner_tol);
+/* Areas / TriangleAreas (GetSetters.hpp:123-126, 195-198): nt floats. */
+int baemm_get_areas(baemm_ctx *ctx, float *out);
+/* TriangleNormals / TriangleMidpoints (GetSetters.hpp:200-208): nt x 4 floats (w = 0). */
+int baemm_get_triangle_normals(baemm_ctx *ctx, float *out4);
+int baemm_get_triangle_midpoints(baemm_ctx *ctx, float *out4);
+/* SingleLayerDiagonal (GetSetters.hpp:190-193): nt floats. */
+int baemm_get_single_layer_diagonal(baemm_ctx *ctx, float *out);
+/* MassMatrix (GetSetters.hpp:113-116) as CSR: outer (nv+1), inner (nnz),
+ * values (nnz).  Call with outer == NULL to query *nnz only. */
+int baemm_get_mass_matrix(baemm_ctx *ctx, int64_t *outer, int32_t *inner, float *values, int64_t *nnz);
+/* Statistics of the last solve on this context. */
+int baemm_last_solve_stats(const baemm_ctx *ctx, baemm_solve_stats *out);
+
+/* ---- parameters and operators -------------------------------------------- */
+
+/* LoadParameters (LoadParameters.hpp:20-81): kappa (wave_chunk_count reals),
+ * coeff (wave_chunk_count x 4 complex: mass, SL, DL, adjoint DL).  SL/DL/DL'
+ * are scaled by factor/(4 pi).  wave_count must be a multiple of wcs. */
+int baemm_load_parameters(baemm_ctx *ctx, const double *kappa, const double *coeff,
+                          int wave_count, int wave_chunk_size, double factor);
+/* LoadBoundaryOperators_PL / UnloadBoundaryOperators_PL
+ * (ApplyBoundaryOperators.hpp:261-284). */
+int baemm_load_boundary_operators(baemm_ctx *ctx, const double *kappa, const double *coeff,
+                                  int wave_count, int wave_chunk_size);
+int baemm_unload_boundary_operators(baemm_ctx *ctx);
+
+/* ApplyBoundaryOperators_PL (ApplyBoundaryOperators.hpp:289-391), operators
+ * already loaded: C_out = alpha * A * B_in + beta * C_out on vertex_count x
+ * wave_count blocks, A = c0 M + c1 SL + c2 DL + c3 DL' per wave chunk. */
+int baemm_apply_boundary_operators_z(baemm_ctx *ctx, const double alpha[2], const double *B_in, int64_t ldB,
+                                     const double beta[2], double *C_out, int64_t ldC);
+int baemm_apply_boundary_operators_c(baemm_ctx *ctx, const float alpha[2], const float *B_in, int64_t ldB,
+                                     const float beta[2], float *C_out, int64_t ldC);
+int baemm_apply_boundary_operators_dev_z(baemm_ctx *ctx, const double alpha[2], const double *B_in, int64_t ldB,
+                                         const double beta[2], double *C_out, int64_t ldC);
+int baemm_apply_boundary_operators_dev_c(baemm_ctx *ctx, const float alpha[2], const float *B_in, int64_t ldB,
+                                         const float beta[2], float *C_out, int64_t ldC);
+/* The overload that loads, applies and unloads in one call
+ * (ApplyBoundaryOperators.hpp:238-256). */
+int baemm_apply_boundary_operators_full_z(baemm_ctx *ctx, const double alpha[2], const double *B_in, int64_t ldB,
+                                          const double beta[2], double *C_out, int64_t ldC,
+                                          const double *kappa, const double *coeff, int wave_count,
+                                          int wave_chunk_size);
+
+/* ApplyFarFieldOperators_PL (ApplyFarFieldOperators.hpp:334-412):
+ * C_out (meas_count x wave_count) = alpha * (c1 FF_SL + c2 FF_DL) B_in + beta * C_out.
+ * The `_loaded` variant uses the parameters already loaded
+ * (ApplyFarFieldOperators.hpp:356-359). */
+int baemm_apply_far_field_operators_z(baemm_ctx *ctx, const double alpha[2], const double *B_in, int64_t ldB,
+                                      const double beta[2], double *C_out, int64_t ldC,
+                                      const double *kappa, const double *coeff, int wave_count,
+                                      int wave_chunk_size);
+int baemm_apply_far_field_operators_loaded_z(baemm_ctx *ctx, const double alpha[2], const double *B_in,
+                                             int64_t ldB, const double beta[2], double *C_out, int64_t ldC);
+int baemm_apply_far_field_operators_dev_z(baemm_ctx *ctx, const double alpha[2], const double *B_in, int64_t ldB,
+                                          const double beta[2], double *C_out, int64_t ldC);
+
+/* CreateIncidentWave_PL (CreateIncidentWave.hpp:21-50): weak-form incident
+ * waves, C_out (vertex_count x wave_count) = alpha * wave + beta * C_out.
+ * incident_directions: inc_count x 3 (plane directions or point sources). */
+int baemm_create_incident_wave_z(baemm_ctx *ctx, const double alpha[2], const double *incident_directions,
+                                 int inc_count, const double beta[2], double *C_out, int64_t ldC,
+                                 const double *kappa, const double *coeff, int wave_count, int wave_chunk_size,
+                                 int wave_type);
+
+/* CreateHerglotzWave_PL (CreateHerglotzWave.hpp:25-44): weak-form Herglotz
+ * waves of the kernel g (meas_count x wave_count). */
+int baemm_create_herglotz_wave_z(baemm_ctx *ctx, const double alpha[2], const double *g, int64_t ldg,
+                                 const double beta[2], double *C_out, int64_t ldC,
+                                 const double *kappa, const double *coeff, int wave_count, int wave_chunk_size);
+
+/* ApplyMassInverse (ApplyMassInverse.hpp:6-156): Y = M^-1 X by CG
+ * (<= 20 iterations, lumped-mass preconditioner).  _z: nrhs complex columns,
+ * _d: nrhs real columns. */
+int baemm_apply_mass_inverse_z(baemm_ctx *ctx, const double *X, int64_t ldX, double *Y, int64_t ldY,
+                               int nrhs, double cg_tol);
+int baemm_apply_mass_inverse_d(baemm_ctx *ctx, const double *X, int64_t ldX, double *Y, int64_t ldY,
+                               int nrhs, double cg_tol);
+/* ApplyLumpedMassInverse (ApplyMassInverse.hpp:161-197). */
+int baemm_apply_lumped_mass_inverse_z(baemm_ctx *ctx, const double *X, int64_t ldX, double *Y, int64_t ldY,
+                                      int nrhs);
+int baemm_apply_lumped_mass_inverse_d(baemm_ctx *ctx, const double *X, int64_t ldX, double *Y, int64_t ldY,
+                                      int nrhs);
+/* MassMatrix().Dot as used by callers (Example_GaussNewton/main.cpp:391-395):
+ * Y = alpha M X + beta Y on nrhs real columns. */
+int baemm_mass_dot_d(baemm_ctx *ctx, double alpha, const double *X, int64_t ldX, double beta, double *Y,
+                     int64_t ldY, int nrhs);
+
+/* ---- solvers (FarField.hpp) ---------------------------------------------- */
+
+/* FarField<WC> (FarField.hpp:28-70); Y_out: meas_count x (wcc*wcs). */
+int baemm_far_field(baemm_ctx *ctx, const double *kappa, int wave_chunk_count, const double *inc_directions,
+                    int wave_chunk_size, double *Y_out, int wave_type, double cg_tol, double gmres_tol);
+/* FarField_parameters (FarField.hpp:90-144) with coupling parameters eta. */
+int baemm_far_field_parameters(baemm_ctx *ctx, const double *kappa, int wave_chunk_count,
+                               const double *inc_directions, int wave_chunk_size, double *Y_out, int wave_type,
+                               const double *eta, double cg_tol, double gmres_tol);
+/* BoundaryPotential (FarField.hpp:626-658): solves (1/2 M - i kappa SL + DL) phi = wave;
+ * writes the used coefficients to coeff (wcc x 4 complex). */
+int baemm_boundary_potential(baemm_ctx *ctx, const double *kappa, double *coeff, const double *wave, double *phi,
+                             int wave_chunk_count, int wave_chunk_size, double cg_tol, double gmres_tol);
+/* DirichletToNeumann (FarField.hpp:790-879): solves (1/2 M - i kappa SL + DL') psi = wave. */
+int baemm_dirichlet_to_neumann(baemm_ctx *ctx, const double *kappa, const double *wave, double *neumann_trace,
+                               int wave_chunk_count, int wave_chunk_size, double cg_tol, double gmres_tol);
+/* Derivative_FF_Helper (FarField.hpp:148-207); du_dn: vertex_count x wc. */
+int baemm_derivative_ff_helper(baemm_ctx *ctx, const double *kappa, int wave_chunk_count,
+                               const double *inc_directions, int wave_chunk_size, double *du_dn, int wave_type,
+                               double cg_tol, double gmres_tol);
+/* Derivative_FF (FarField.hpp:227-321).  X_in: vertex_count x 3 reals,
+ * Y_out: meas_count x wc.  *du_dn == NULL: the library allocates it with
+ * calloc (release with baemm_free or free) and fills it, as the reference
+ * does (FarField.hpp:273-283). */
+int baemm_derivative_ff(baemm_ctx *ctx, const double *kappa, int wave_chunk_count, const double *inc_directions,
+                        int wave_chunk_size, const double *X_in, double *Y_out, double **du_dn, int wave_type,
+                        double cg_tol, double gmres_tol);
+/* AdjointDerivative_FF (FarField.hpp:342-428).  g: meas_count x wc complex,
+ * Y_out: vertex_count x 3 reals. */
+int baemm_adjoint_derivative_ff(baemm_ctx *ctx, const double *kappa, int wave_chunk_count,
+                                const double *inc_directions, int wave_chunk_size, const double *g, double *Y_out,
+                                double **du_dn, int wave_type, double cg_tol, double gmres_tol);
+/* GaussNewtonSolve (FarField.hpp:457-604): X = alpha (M + DF* DF)^-1 B + beta X
+ * by GMRES (solver = 0, the reference) or CG (solver = 1) on 3 * vertex_count
+ * reals.  M and P act on vertex_count x 3 host arrays.  *succeeded receives
+ * the reference's bool. */
+int baemm_gauss_newton_solve(baemm_ctx *ctx, const double *kappa, int wave_chunk_count,
+                             const double *inc_directions, int wave_chunk_size, baemm_real_op M, void *M_user,
+                             baemm_real_op P, void *P_user, double alpha, const double *B_in, int64_t ldB,
+                             double beta, double *X_out, int64_t ldX, double **du_dn, int wave_type, double cg_tol,
+                             double gmres_tol_inner, double gmres_tol_outer, int solver, int *succeeded);
+
+/* ---- tracing (the reference's Tools profiler, ptic/ptoc) -------------------- */
+
+/* Per-phase CUDA-event timing of boundary applies on this context (0 = off). */
+int baemm_set_profiling(baemm_ctx *ctx, int on);
+/* Device milliseconds of the last boundary apply: ms3[0] AvOp, ms3[1] dense
+ * kernel, ms3[2] epilogue (AvOp^T + SL diagonal + mass).  Synchronises on
+ * the apply.  Needs profiling on. */
+int baemm_last_apply_times(baemm_ctx *ctx, float *ms3);
+/* Number of kernels this library has launched in the process so far. */
+int64_t baemm_kernel_launch_count(void);
+
+/* Release memory the library allocated for the caller (du_dn). */
+void baemm_free(void *p);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* BAEMM_H */

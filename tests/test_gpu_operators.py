@@ -1,0 +1,265 @@
+"""GPU parity of the operator applies against the oracle (through the C ABI).
+
+Tolerances: FP32 path within 1e-5 relative (Frobenius) of the FP32 oracle and
+within 3e-5 of the FP64 oracle (the FP32 path's own rounding); FP64 path
+within 1e-11 of the FP64 oracle.
+"""
+import numpy as np
+import pytest
+
+from baemm_b200 import APPLY_FP32, APPLY_FP64, BaemmError, Helmholtz_CUDA, WaveType, meshes
+from oracle import oracle as O
+from tests.helpers import crandn, relerr
+
+pytestmark = pytest.mark.gpu
+
+FP32_TOL = 1e-5
+FP32_VS64_TOL = 3e-5
+FP64_TOL = 1e-11
+
+COEFFS = {
+    "mass": [1.5 - 0.5j, 0, 0, 0],
+    "sl": [0, 1, 0, 0],
+    "dl": [0, 0, 1, 0],
+    "adl": [0, 0, 0, 1],
+    "bie": [0.5, -1j, 1, 0],
+    "dtn": [0.5, -1j, 0, 1],
+    "all": [0.25 + 1j, 1 + 0.5j, 1 - 2j, 0.3j],
+}
+WAVES = {  # name: (wave_count, wave_chunk_size, kappa list)
+    "w16": (16, 16, [2.0]),
+    "w32": (32, 16, [4.0, 8.0]),
+    "w8x4": (8, 4, [1.0, 3.0]),
+    "w64": (64, 16, [2.0, 4.0, 8.0, 16.0]),
+    "w64x32": (64, 32, [3.0, 6.0]),
+}
+
+
+@pytest.fixture(scope="module")
+def env():
+    coords, tris = meshes.icosphere(3)
+    meas = meshes.fibonacci_sphere(48)
+    H = Helmholtz_CUDA(coords, tris, meas)
+    o32 = O.Oracle(coords, tris, meas, precision=32)
+    o64 = O.Oracle(coords, tris, meas, precision=64)
+    yield coords, tris, meas, H, o32, o64
+    H.close()
+
+
+def _coeff(name, kap):
+    return np.array([COEFFS[name] if name != "bie" else [0.5, -1j * k, 1, 0] for k in kap], np.complex128)
+
+
+def test_geometry_matches_oracle(env):
+    coords, tris, meas, H, o32, o64 = env
+    mid, nrm, area, diag = o32.geometry()
+    assert relerr(H.Areas(), area) < 1e-6
+    assert relerr(H.TriangleMidpoints(), mid) < 1e-6
+    assert relerr(H.TriangleNormals(), nrm) < 1e-6
+    assert relerr(H.SingleLayerDiagonal(), diag) < 1e-5
+    assert H.VertexCount() == coords.shape[0] and H.SimplexCount() == tris.shape[0]
+    assert H.GetMeasCount() == meas.shape[0]
+    assert H.ClassName() == "Helmholtz_CUDA"
+    assert "DEVICE_NAME" in H.DeviceInfo()
+
+
+def test_mass_matrix_matches_oracle(env):
+    coords, tris, meas, H, o32, o64 = env
+    go, gi, gv = H.MassMatrix()
+    oo, oi, ov = o32.mass_matrix()
+    assert np.array_equal(go, oo) and np.array_equal(gi, oi)
+    assert relerr(gv, ov) < 1e-6
+
+
+@pytest.mark.parametrize("cname", list(COEFFS))
+@pytest.mark.parametrize("wname", ["w16", "w32", "w8x4"])
+def test_apply_boundary_fp32(env, cname, wname):
+    coords, tris, meas, H, o32, o64 = env
+    wc, wcs, kap = WAVES[wname]
+    coeff = _coeff(cname, kap)
+    rng = np.random.default_rng(hash((cname, wname)) % 2**32)
+    nv = coords.shape[0]
+    B = crandn(rng, nv, wc + 3)          # ld > wave_count
+    C0 = crandn(rng, nv, wc + 1)
+    alpha, beta = 0.7 - 0.2j, 0.3 + 0.1j
+    Cg = C0.copy()
+    H.SetApplyMode(APPLY_FP32)
+    H.ApplyBoundaryOperators_PL(alpha, B, beta, Cg, kap, coeff, wc, wcs)
+    C32 = C0.copy()
+    o32.ApplyBoundaryOperators_PL(alpha, B, beta, C32, kap, coeff, wc, wcs)
+    C64 = C0.copy()
+    o64.ApplyBoundaryOperators_PL(alpha, B, beta, C64, kap, coeff, wc, wcs)
+    assert relerr(Cg[:, :wc], C32[:, :wc]) < FP32_TOL
+    assert relerr(Cg[:, :wc], C64[:, :wc]) < FP32_VS64_TOL
+    assert np.array_equal(Cg[:, wc:], C0[:, wc:])   # columns beyond wave_count untouched
+
+
+@pytest.mark.parametrize("cname", ["sl", "dl", "adl", "all"])
+@pytest.mark.parametrize("wname", ["w16", "w64", "w64x32"])
+def test_apply_boundary_fp64(env, cname, wname):
+    coords, tris, meas, H, o32, o64 = env
+    wc, wcs, kap = WAVES[wname]
+    coeff = _coeff(cname, kap)
+    rng = np.random.default_rng(17)
+    B = crandn(rng, coords.shape[0], wc)
+    Cg = np.zeros_like(B)
+    H.SetApplyMode(APPLY_FP64)
+    try:
+        H.ApplyBoundaryOperators_PL(1.0, B, 0.0, Cg, kap, coeff, wc, wcs)
+    finally:
+        H.SetApplyMode(APPLY_FP32)
+    C64 = np.zeros_like(B)
+    o64.ApplyBoundaryOperators_PL(1.0, B, 0.0, C64, kap, coeff, wc, wcs)
+    assert relerr(Cg, C64) < FP64_TOL
+
+
+def test_apply_complex64_and_device_paths(env):
+    import torch
+    coords, tris, meas, H, o32, o64 = env
+    wc, wcs, kap = WAVES["w32"]
+    coeff = _coeff("all", kap)
+    rng = np.random.default_rng(5)
+    B = crandn(rng, coords.shape[0], wc)
+    ref = np.zeros_like(B)
+    o32.ApplyBoundaryOperators_PL(1.0, B, 0.0, ref, kap, coeff, wc, wcs)
+    # complex64 host blocks (the reference's Complex)
+    C64h = np.zeros(B.shape, np.complex64)
+    H.ApplyBoundaryOperators_PL(1.0, B.astype(np.complex64), 0.0, C64h, kap, coeff, wc, wcs)
+    assert relerr(C64h, ref) < FP32_TOL
+    # device-resident torch tensors, loaded operators (Load / Apply / Unload)
+    H.LoadBoundaryOperators_PL(kap, coeff, wc, wcs)
+    Bd = torch.from_numpy(B).cuda()
+    Cd = torch.zeros_like(Bd)
+    H.SetStream(torch.cuda.current_stream().cuda_stream)
+    H.ApplyBoundaryOperators_PL(1.0, Bd, 0.0, Cd)
+    torch.cuda.synchronize()
+    H.SetStream(None)
+    H.UnloadBoundaryOperators_PL()
+    assert relerr(Cd.cpu().numpy(), ref) < FP32_TOL
+
+
+def test_apply_is_deterministic(env):
+    coords, tris, meas, H, o32, o64 = env
+    wc, wcs, kap = WAVES["w32"]
+    coeff = _coeff("bie", kap)
+    B = crandn(np.random.default_rng(1), coords.shape[0], wc)
+    C1, C2 = np.zeros_like(B), np.zeros_like(B)
+    H.ApplyBoundaryOperators_PL(1.0, B, 0.0, C1, kap, coeff, wc, wcs)
+    H.ApplyBoundaryOperators_PL(1.0, B, 0.0, C2, kap, coeff, wc, wcs)
+    assert np.array_equal(C1, C2)
+
+
+def test_use_diagonal_off(env):
+    coords, tris, meas, H, o32, o64 = env
+    wc, wcs, kap = WAVES["w16"]
+    coeff = _coeff("sl", kap)
+    B = crandn(np.random.default_rng(2), coords.shape[0], wc)
+    Cg, Co = np.zeros_like(B), np.zeros_like(B)
+    H.UseDiagonal(False)
+    o32.UseDiagonal(False)
+    try:
+        H.ApplyBoundaryOperators_PL(1.0, B, 0.0, Cg, kap, coeff, wc, wcs)
+        o32.ApplyBoundaryOperators_PL(1.0, B, 0.0, Co, kap, coeff, wc, wcs)
+    finally:
+        H.UseDiagonal(True)
+        o32.UseDiagonal(True)
+    assert relerr(Cg, Co) < FP32_TOL
+
+
+@pytest.mark.parametrize("mode", [APPLY_FP32, APPLY_FP64])
+@pytest.mark.parametrize("cname", ["sl", "dl", "bie"])
+def test_far_field(env, mode, cname):
+    coords, tris, meas, H, o32, o64 = env
+    wc, wcs, kap = WAVES["w32"]
+    coeff = _coeff(cname, kap)
+    rng = np.random.default_rng(9)
+    B = crandn(rng, coords.shape[0], wc)
+    F0 = crandn(rng, meas.shape[0], wc)
+    Fg = F0.copy()
+    H.SetApplyMode(mode)
+    try:
+        H.ApplyFarFieldOperators_PL(0.5 + 0.5j, B, -0.25, Fg, kap, coeff, wc, wcs)
+    finally:
+        H.SetApplyMode(APPLY_FP32)
+    Fo = F0.copy()
+    (o32 if mode == APPLY_FP32 else o64).ApplyFarFieldOperators_PL(0.5 + 0.5j, B, -0.25, Fo, kap, coeff, wc, wcs)
+    assert relerr(Fg, Fo) < (FP32_TOL if mode == APPLY_FP32 else FP64_TOL)
+
+
+@pytest.mark.parametrize("mode", [APPLY_FP32, APPLY_FP64])
+def test_herglotz_wave(env, mode):
+    coords, tris, meas, H, o32, o64 = env
+    wc, wcs, kap = WAVES["w32"]
+    coeff = np.array([[0, -1j * k, 1, 0] for k in kap])
+    rng = np.random.default_rng(10)
+    g = crandn(rng, meas.shape[0], wc)
+    Cg, Co = np.zeros((coords.shape[0], wc), complex), np.zeros((coords.shape[0], wc), complex)
+    H.SetApplyMode(mode)
+    try:
+        H.CreateHerglotzWave_PL(1.0, g, 0.0, Cg, kap, coeff, wc, wcs)
+    finally:
+        H.SetApplyMode(APPLY_FP32)
+    (o32 if mode == APPLY_FP32 else o64).CreateHerglotzWave_PL(1.0, g, 0.0, Co, kap, coeff, wc, wcs)
+    assert relerr(Cg, Co) < (FP32_TOL if mode == APPLY_FP32 else FP64_TOL)
+
+
+@pytest.mark.parametrize("wtype", [WaveType.Plane, WaveType.Radial])
+@pytest.mark.parametrize("mode", [APPLY_FP32, APPLY_FP64])
+def test_incident_wave(env, wtype, mode):
+    coords, tris, meas, H, o32, o64 = env
+    wc, wcs, kap = WAVES["w32"]
+    coeff = np.array([[0, -1j * k, 1, 0] for k in kap])
+    dirs = meshes.fibonacci_sphere(wcs) * (2.5 if wtype == WaveType.Radial else 1.0)
+    C0 = crandn(np.random.default_rng(3), coords.shape[0], wc)
+    Cg, Co = C0.copy(), C0.copy()
+    H.SetApplyMode(mode)
+    try:
+        H.CreateIncidentWave_PL(1.0 - 1j, dirs, 0.5, Cg, kap, coeff, wc, wcs, wtype)
+    finally:
+        H.SetApplyMode(APPLY_FP32)
+    (o32 if mode == APPLY_FP32 else o64).CreateIncidentWave_PL(1.0 - 1j, dirs, 0.5, Co, kap, coeff, wc, wcs, wtype)
+    assert relerr(Cg, Co) < (FP32_TOL if mode == APPLY_FP32 else FP64_TOL)
+
+
+@pytest.mark.parametrize("mode", [APPLY_FP32, APPLY_FP64])
+def test_mass_inverse_and_lumped(env, mode):
+    """CG mass inverse (20 iterations max).  The FP32 path uses the float mass
+    values of the reference (Sparse_T<float>), which differ from the oracle's in
+    the last bits, so the two M^-1 agree to ~1e-7; the FP64 path to 1e-11."""
+    coords, tris, meas, H, o32, o64 = env
+    orc, tol = (o32, 1e-6) if mode == APPLY_FP32 else (o64, 1e-11)
+    rng = np.random.default_rng(4)
+    nv = coords.shape[0]
+    X = crandn(rng, nv, 8)
+    Xr = rng.standard_normal((nv, 3))
+    Yg, Yo = np.zeros_like(X), np.zeros_like(X)
+    Yr, Yro = np.zeros_like(Xr), np.zeros_like(Xr)
+    Lg, Lo = np.zeros_like(X), np.zeros_like(X)
+    H.SetApplyMode(mode)
+    try:
+        H.ApplyMassInverse(X, Yg, 1e-10)
+        H.ApplyMassInverse(Xr, Yr, 1e-10)
+        H.ApplyLumpedMassInverse(X, Lg)
+    finally:
+        H.SetApplyMode(APPLY_FP32)
+    orc.ApplyMassInverse(X, Yo, 1e-10)
+    orc.ApplyMassInverse(Xr, Yro, 1e-10)
+    orc.ApplyLumpedMassInverse(X, Lo)
+    assert relerr(Yg, Yo) < tol
+    assert relerr(Yr, Yro) < tol
+    assert relerr(Lg, Lo) < (1e-6 if mode == APPLY_FP32 else 1e-14)
+
+
+def test_error_statuses(env):
+    coords, tris, meas, H, o32, o64 = env
+    B = np.zeros((coords.shape[0], 16), complex)
+    with pytest.raises(BaemmError, match="NOT_LOADED"):
+        H.ApplyBoundaryOperators_PL(1.0, B, 0.0, B.copy())
+    with pytest.raises(BaemmError, match="ERR_SIZE"):
+        H.ApplyBoundaryOperators_PL(1.0, B, 0.0, B.copy(), [1.0], [[0, 1, 0, 0]], 16, 12)
+    with pytest.raises(BaemmError, match="ERR_ARG"):
+        H.ApplyBoundaryOperators_PL(1.0, B[:, :8], 0.0, B.copy(), [1.0], [[0, 1, 0, 0]], 16, 16)
+    # the context stays usable after the errors
+    C = np.zeros_like(B)
+    H.ApplyBoundaryOperators_PL(1.0, B + 1, 0.0, C, [1.0], [[0, 1, 0, 0]], 16, 16)
+    assert np.isfinite(C).all() and np.abs(C).max() > 0

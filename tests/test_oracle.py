@@ -1,0 +1,143 @@
+"""CPU tests of the oracle: pinned against the reference's own kernels (the
+golden fixtures from oracle/_ref, and the live shim build when present) and
+against closed-form properties of the geometry, mass matrix and solvers."""
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from tests.helpers import crandn, relerr
+
+
+def _oracle_for(golden, precision):
+    return O.Oracle(golden["coords"], golden["tris"], golden["meas"], precision=precision)
+
+
+def test_oracle_geometry_matches_fixture(golden):
+    o = _oracle_for(golden, 32)
+    mid, nrm, area, diag = o.geometry()
+    assert np.array_equal(mid.astype(np.float32), golden["mid4"])
+    assert np.array_equal(nrm.astype(np.float32), golden["nrm4"])
+    assert np.array_equal(area.astype(np.float32), golden["area"])
+
+
+@pytest.mark.parametrize("name", ["sl", "dl", "adl", "bie_dl", "mix_2k", "wcs4"])
+def test_oracle_boundary_kernel_pinned_to_reference(golden, name):
+    B, Cref = golden[f"bnd_{name}_B"], golden[f"bnd_{name}_C"]
+    coeff, kappa, wcs = golden[f"bnd_{name}_coeff"], golden[f"bnd_{name}_kappa"], int(golden[f"bnd_{name}_wcs"])
+    wc = B.shape[1]
+    c32 = _oracle_for(golden, 32).boundary_kernel_tri(B, kappa, coeff, wc, wcs)
+    c64 = _oracle_for(golden, 64).boundary_kernel_tri(B, kappa, coeff, wc, wcs)
+    # FP32 restatement vs the reference's FP32 kernel: rounding only
+    assert relerr(c32, Cref) < 2e-6
+    # the reference's FP32 kernel vs the FP64 twin: the FP32 path's own error
+    assert relerr(Cref, c64) < 2e-5
+
+
+@pytest.mark.parametrize("name", ["ff_sl", "ff_mix"])
+def test_oracle_farfield_kernel_pinned_to_reference(golden, name):
+    B, Cref = golden[f"{name}_B"], golden[f"{name}_C"]
+    coeff, kappa, wcs = golden[f"{name}_coeff"], golden[f"{name}_kappa"], int(golden[f"{name}_wcs"])
+    wc = B.shape[1]
+    f32 = _oracle_for(golden, 32).farfield_kernel_tri(B, kappa, coeff, wc, wcs)
+    f64 = _oracle_for(golden, 64).farfield_kernel_tri(B, kappa, coeff, wc, wcs)
+    assert relerr(f32, Cref) < 2e-6
+    assert relerr(Cref, f64) < 2e-5
+
+
+def test_oracle_herglotz_kernel_pinned_to_reference(golden):
+    G, Cref = golden["hw_G"], golden["hw_C"]
+    coeff, kappa, wcs = golden["hw_coeff"], golden["hw_kappa"], int(golden["hw_wcs"])
+    h32 = _oracle_for(golden, 32).herglotz_kernel_tri(G, kappa, coeff, G.shape[1], wcs)
+    h64 = _oracle_for(golden, 64).herglotz_kernel_tri(G, kappa, coeff, G.shape[1], wcs)
+    assert relerr(h32, Cref) < 2e-6
+    assert relerr(Cref, h64) < 2e-5
+
+
+@pytest.mark.skipif(not O.ref_available(), reason="oracle/_ref not built here")
+def test_oracle_vs_live_reference_kernel(sphere3):
+    coords, tris = sphere3
+    rng = np.random.default_rng(7)
+    o = O.Oracle(coords, tris, np.eye(3), precision=32)
+    mid, nrm, _, _ = o.geometry()
+    B = crandn(rng, tris.shape[0], 32, dtype=np.complex64)
+    kappa = np.array([6.0, 11.0])
+    coeff = np.array([[0, 0.3 - 1j, 2.0 + 0.5j, -1.0j]] * 2)
+    Cref = O.ref_boundary(mid, nrm, B, kappa, O.scaled_coefficients(coeff), 16)
+    assert relerr(o.boundary_kernel_tri(B, kappa, coeff, 32, 16), Cref) < 3e-6
+
+
+def _self_integral_quadrature(p0, p1, p2, nq=4000):
+    """Integral of 1/|y - c| over the triangle (c = centroid) by splitting at c
+    into three sub-triangles and integrating R(theta) in polar coordinates."""
+    c = (p0 + p1 + p2) / 3.0
+    total = 0.0
+    for a, b in ((p0, p1), (p1, p2), (p2, p0)):
+        u, v = a - c, b - c
+        e1 = u / np.linalg.norm(u)
+        nrm = np.cross(u, v)
+        e2 = np.cross(nrm, e1); e2 /= np.linalg.norm(e2)
+        ang = np.arctan2(v @ e2, v @ e1)
+        t = (np.arange(nq) + 0.5) / nq * ang
+        dirs = np.outer(np.cos(t), e1) + np.outer(np.sin(t), e2)
+        # ray-segment intersection distance R(t) from c to edge a-b
+        d = b - a
+        R = []
+        for w in dirs:
+            M = np.stack([w, -d], axis=1)
+            sol, *_ = np.linalg.lstsq(M, a - c, rcond=None)
+            R.append(sol[0])
+        total += np.sum(R) * ang / nq
+    return total
+
+
+def test_single_layer_diagonal_matches_quadrature():
+    rng = np.random.default_rng(3)
+    coords = np.array([[0.0, 0.0, 0.0], [1.0, 0.1, 0.0], [0.3, 0.8, 0.2]]) + rng.standard_normal(3) * 0.01
+    tris = np.array([[0, 1, 2]])
+    o = O.Oracle(coords, tris, np.eye(3), precision=64)
+    _, _, area, diag = o.geometry()
+    q = _self_integral_quadrature(coords[0], coords[1], coords[2])
+    assert abs(diag[0] * area[0] - q) / q < 1e-5
+
+
+def test_mass_matrix_properties(sphere2):
+    coords, tris = sphere2
+    o = O.Oracle(coords, tris, np.eye(3), precision=64)
+    outer, inner, val = o.mass_matrix()
+    _, _, area, _ = o.geometry()
+    n = coords.shape[0]
+    M = np.zeros((n, n))
+    for v in range(n):
+        M[v, inner[outer[v]:outer[v + 1]]] = val[outer[v]:outer[v + 1]]
+    assert np.allclose(M, M.T)
+    assert abs(M.sum() - area.sum()) < 1e-12 * area.sum()
+    # 1^T M 1 = total area; lumped inverse is 1/(sum a/9) (Initialize.hpp:339-353)
+    L = o.lumped_inverse_diag()
+    assert np.allclose(1.0 / L, M.sum(axis=1) / 3.0)  # row sum = sum a/3, lumped = sum a/9
+    assert np.all(np.linalg.eigvalsh(M) > 0)
+
+
+def test_gmres_restatement_solves_dense_system():
+    rng = np.random.default_rng(11)
+    n, k = 60, 3
+    A = np.eye(n) * 4 + crandn(rng, n, n) / np.sqrt(n)
+    b = crandn(rng, n, k)
+    x, ok, its = O.gmres_dense(A, b, restart=30, cycles=4, tol=1e-12)
+    assert ok
+    assert relerr(x, np.linalg.solve(A, b)) < 1e-10
+
+
+def test_mass_inverse_restatement(sphere2):
+    coords, tris = sphere2
+    o = O.Oracle(coords, tris, np.eye(3), precision=64)
+    outer, inner, val = o.mass_matrix()
+    n = coords.shape[0]
+    M = np.zeros((n, n))
+    for v in range(n):
+        M[v, inner[outer[v]:outer[v + 1]]] = val[outer[v]:outer[v + 1]]
+    rng = np.random.default_rng(5)
+    X = crandn(rng, n, 4)
+    Y = np.zeros_like(X)
+    # 20 CG iterations (ApplyMassInverse.hpp:48) reach ~1e-9 on this mesh
+    assert o.ApplyMassInverse(X, Y, 1e-8)
+    assert relerr(M @ Y, X) < 1e-8
