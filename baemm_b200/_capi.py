@@ -81,6 +81,7 @@ SIGNATURES = {
     "baemm_apply_boundary_operators_c": (I, [vp, fp, fp, I64, fp, fp, I64]),
     "baemm_apply_boundary_operators_dev_z": (I, [vp, dp, vp, I64, dp, vp, I64]),
     "baemm_apply_boundary_operators_dev_c": (I, [vp, fp, vp, I64, fp, vp, I64]),
+    "baemm_apply_boundary_operators_noalloc_dev_c": (I, [vp, fp, vp, I64, fp, vp, I64]),
     "baemm_apply_boundary_operators_full_z": (I, [vp, dp, dp, I64, dp, dp, I64, dp, dp, I, I]),
     "baemm_apply_far_field_operators_z": (I, [vp, dp, dp, I64, dp, dp, I64, dp, dp, I, I]),
     "baemm_apply_far_field_operators_loaded_z": (I, [vp, dp, dp, I64, dp, dp, I64]),

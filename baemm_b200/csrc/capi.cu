@@ -7,12 +7,6 @@
 
 #include "ctx.cuh"
 
-struct baemm_ctx
-{
-    baemm::Ctx *impl = nullptr;
-    std::string create_error;
-};
-
 using baemm::Ctx;
 using baemm::DevBuf;
 using baemm::Error;

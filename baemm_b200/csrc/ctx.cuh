@@ -121,3 +121,9 @@ private:
 };
 
 } // namespace baemm
+
+// The opaque handle of the C ABI (include/baemm.h).
+struct baemm_ctx
+{
+    baemm::Ctx *impl = nullptr;
+};

@@ -155,6 +155,19 @@ int baemm_apply_boundary_operators_dev_z(baemm_ctx *ctx, const double alpha[2], 
                                          const double beta[2], double *C_out, int64_t ldC);
 int baemm_apply_boundary_operators_dev_c(baemm_ctx *ctx, const float alpha[2], const float *B_in, int64_t ldB,
                                          const float beta[2], float *C_out, int64_t ldC);
+/* Allocation-free variant of baemm_apply_boundary_operators_dev_c.  No
+ * counterpart in the reference.  For callers that must not allocate device
+ * memory while they run (inside CUDA stream capture, latency-critical loops,
+ * hosts that own all device memory): the triangle-level intermediate blocks
+ * live in one fixed 32 MiB __device__ array of the library instead of
+ * cudaMalloc'ed buffers, so the call allocates and frees nothing.
+ * Limit: 2 * simplex_count * wave_count * 8 bytes <= 32 MiB, else
+ * BAEMM_ERR_SIZE.  Plain FP32 apply mode only; operators loaded beforehand.
+ * The array's device address is looked up on the first call on a device
+ * (make it before any stream capture).  All calls share the array: calls
+ * that overlap on the GPU race and must be serialised by the caller. */
+int baemm_apply_boundary_operators_noalloc_dev_c(baemm_ctx *ctx, const float alpha[2], const float *B_in,
+                                                 int64_t ldB, const float beta[2], float *C_out, int64_t ldC);
 /* The overload that loads, applies and unloads in one call
  * (ApplyBoundaryOperators.hpp:238-256). */
 int baemm_apply_boundary_operators_full_z(baemm_ctx *ctx, const double alpha[2], const double *B_in, int64_t ldB,
