@@ -21,6 +21,9 @@ WAVE_RADIAL = 202
 APPLY_FP32 = 0
 APPLY_TC = 1
 APPLY_FP64 = 2
+TUNE_DENSE_VARIANT = 1
+TUNE_TC_SEGMENT = 2
+TUNE_TC_CTAS = 3
 
 dp = C.POINTER(C.c_double)
 fp = C.POINTER(C.c_float)
@@ -67,6 +70,8 @@ SIGNATURES = {
     "baemm_get_gmres_params": (I, [vp, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
     "baemm_set_apply_mode": (I, [vp, I]),
     "baemm_get_apply_mode": (I, [vp]),
+    "baemm_set_tuning": (I, [vp, I, I]),
+    "baemm_get_tuning": (I, [vp, I]),
     "baemm_set_refinement": (I, [vp, I, D]),
     "baemm_get_areas": (I, [vp, fp]),
     "baemm_get_triangle_normals": (I, [vp, fp]),

@@ -257,10 +257,7 @@ void *baemm_stream(baemm_ctx *ctx) { return (ctx && ctx->impl) ? (void *)ctx->im
 
 int baemm_set_stream(baemm_ctx *ctx, void *stream)
 {
-    return guarded(ctx, [&](Ctx &c) {
-        c.sync();
-        c.stream = stream ? (cudaStream_t)stream : c.own_stream;
-    });
+    return guarded(ctx, [&](Ctx &c) { c.switch_stream((cudaStream_t)stream); });
 }
 
 int baemm_synchronize(baemm_ctx *ctx)
@@ -313,10 +310,39 @@ int baemm_get_gmres_params(const baemm_ctx *ctx, int *max_iter, int *max_restart
 int baemm_set_apply_mode(baemm_ctx *ctx, int mode)
 {
     return guarded(ctx, [&](Ctx &c) {
-        BAEMM_REQUIRE(mode == BAEMM_APPLY_FP32 || mode == BAEMM_APPLY_FP64, BAEMM_ERR_ARG,
-                      "unsupported apply mode");
+        BAEMM_REQUIRE(mode == BAEMM_APPLY_FP32 || mode == BAEMM_APPLY_TC || mode == BAEMM_APPLY_FP64,
+                      BAEMM_ERR_ARG, "unsupported apply mode");
         c.apply_mode = mode;
     });
+}
+int baemm_set_tuning(baemm_ctx *ctx, int key, int value)
+{
+    return guarded(ctx, [&](Ctx &c) {
+        switch (key)
+        {
+            case BAEMM_TUNE_DENSE_VARIANT:
+                BAEMM_REQUIRE(value >= 0 && value < baemm::kDenseVariants, BAEMM_ERR_ARG, "unknown kernel variant");
+                c.dense_variant = value;
+                break;
+            case BAEMM_TUNE_TC_SEGMENT:
+                BAEMM_REQUIRE(value >= 1, BAEMM_ERR_ARG, "segment length must be >= 1");
+                c.tc_seg_tiles = value;
+                break;
+            case BAEMM_TUNE_TC_CTAS:
+                BAEMM_REQUIRE(value >= 0 && value <= 65535, BAEMM_ERR_ARG, "grid size must be in [0, 65535]");
+                c.tc_ctas = value;
+                break;
+            default: throw Error(BAEMM_ERR_ARG, "unknown tuning key");
+        }
+    });
+}
+int baemm_get_tuning(const baemm_ctx *ctx, int key)
+{
+    if (!ctx || !ctx->impl) return -1;
+    if (key == BAEMM_TUNE_DENSE_VARIANT) return ctx->impl->dense_variant;
+    if (key == BAEMM_TUNE_TC_SEGMENT) return ctx->impl->tc_seg_tiles;
+    if (key == BAEMM_TUNE_TC_CTAS) return ctx->impl->tc_ctas;
+    return -1;
 }
 int baemm_get_apply_mode(const baemm_ctx *ctx) { return (ctx && ctx->impl) ? ctx->impl->apply_mode : -1; }
 int baemm_set_refinement(baemm_ctx *ctx, int max_steps, double inner_tol)

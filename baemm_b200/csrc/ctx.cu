@@ -61,13 +61,17 @@ Ctx::Ctx(const double *coords, int64_t nv, const int32_t *tris, int64_t nt, cons
                                cudaMemcpyHostToDevice, stream));
     BAEMM_CUDA(cudaMemcpyAsync(mesh.meas_d.reserve(md.size()), md.data(), md.size() * sizeof(double),
                                cudaMemcpyHostToDevice, stream));
+    BAEMM_CUDA(cudaMemsetAsync(tc_err.reserve(1), 0, sizeof(int), stream));
+    BAEMM_CUDA(cudaMallocHost(&tc_err_host, sizeof(int)));
     sync();
 }
 
 Ctx::~Ctx()
 {
+    if (tc_err_host) cudaFreeHost(tc_err_host);
     for (auto &e : prof_ev)
         if (e) cudaEventDestroy(e);
+    if (handoff_ev) cudaEventDestroy(handoff_ev);
     if (own_stream)
     {
         cudaStreamSynchronize(own_stream);
@@ -75,7 +79,37 @@ Ctx::~Ctx()
     }
 }
 
-void Ctx::sync() { BAEMM_CUDA(cudaStreamSynchronize(stream)); }
+void Ctx::switch_stream(cudaStream_t s)
+{
+    if (!s) s = own_stream;
+    if (s == stream) return;
+    if (!handoff_ev) BAEMM_CUDA(cudaEventCreateWithFlags(&handoff_ev, cudaEventDisableTiming));
+    BAEMM_CUDA(cudaEventRecord(handoff_ev, stream));
+    BAEMM_CUDA(cudaStreamWaitEvent(s, handoff_ev, 0));
+    stream = s;
+}
+
+void Ctx::sync()
+{
+    BAEMM_CUDA(cudaStreamSynchronize(stream));
+    if (tc_pending) check_tc_error();
+}
+
+// The tensor-core kernel reports a bounded wait that gave up through tc_err.
+void Ctx::check_tc_error()
+{
+    tc_pending = false;
+    BAEMM_CUDA(cudaMemcpyAsync(tc_err_host, tc_err.p, sizeof(int), cudaMemcpyDeviceToHost, stream));
+    BAEMM_CUDA(cudaStreamSynchronize(stream));
+    if (*tc_err_host != 0)
+    {
+        const int code = *tc_err_host;
+        BAEMM_CUDA(cudaMemsetAsync(tc_err.p, 0, sizeof(int), stream));
+        BAEMM_CUDA(cudaStreamSynchronize(stream));
+        throw Error(BAEMM_ERR_TIMEOUT, "tensor-core apply: a bounded device wait gave up (code " +
+                                           std::to_string(code) + ")");
+    }
+}
 
 // Integer topology (host): AvOp columns sorted per triangle (Initialize.hpp:307-313),
 // AvOp^T as a vertex -> triangle CSR in ascending triangle order (Initialize.hpp:315),
@@ -192,8 +226,16 @@ void Ctx::dense_apply(const cplx<R> *Btri, cplx<R> *Ctri)
 {
     if constexpr (std::is_same<R, double>::value)
         launch_boundary_dense<double>(mesh, flags, prm_d.p, wave_count, wave_chunk_size, Btri, Ctri, stream);
+    else if (apply_mode == BAEMM_APPLY_TC && tc_supported(wave_count, wave_chunk_size))
+    {
+        const size_t ws_elems = tc_workspace_elems(tc_ctas);
+        launch_boundary_tc(mesh, flags, prm_f.p, wave_count, wave_chunk_size, Btri, Ctri, tc_ws.reserve(ws_elems),
+                           ws_elems, tc_err.p, stream, tc_seg_tiles, tc_ctas);
+        tc_pending = true;
+    }
     else
-        launch_boundary_dense<float>(mesh, flags, prm_f.p, wave_count, wave_chunk_size, Btri, Ctri, stream);
+        launch_boundary_dense<float>(mesh, flags, prm_f.p, wave_count, wave_chunk_size, Btri, Ctri, stream,
+                                     dense_variant);
 }
 
 // ApplyBoundaryOperators.hpp:289-391 on device blocks.

@@ -46,11 +46,19 @@ public:
     int block_size = 64;
     int gmres_max_iter = 30, gmres_max_restarts = 3;
     int apply_mode = BAEMM_APPLY_FP32;
+    int dense_variant = 0;            // plain FP32 dense kernel variant (launch_boundary_dense)
+    int tc_seg_tiles = 4;             // tensor-core form: tiles per TMEM partial sum
+    int tc_ctas = 0;                  // tensor-core form: persistent grid size (0 = one CTA per SM)
+    DevBuf<float2> tc_ws;             // tensor-core form: partial sums of target blocks split between CTAs
     int ir_max_steps = 0;
     double ir_inner_tol = 1e-4;
     baemm_solve_stats stats{};
+    DevBuf<int> tc_err;               // error word of the tensor-core kernel's bounded waits
+    int *tc_err_host = nullptr;
+    bool tc_pending = false;          // a tensor-core launch since the last error check
     bool profiling = false;
     cudaEvent_t prof_ev[4] = {nullptr, nullptr, nullptr, nullptr};
+    cudaEvent_t handoff_ev = nullptr;   // orders a newly set stream after the previous one
     bool prof_valid = false;
     std::string last_error;
 
@@ -112,6 +120,10 @@ public:
                             const double2 *du_dn, double cg_tol, double gmres_tol);
 
     void sync();
+    void check_tc_error();
+    // Continue on stream `s` (null: the own stream), ordered after the work
+    // already queued on the current one, without a host synchronisation.
+    void switch_stream(cudaStream_t s);
     std::string device_info() const;
 
 private:

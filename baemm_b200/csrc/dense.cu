@@ -18,6 +18,7 @@
 
 namespace baemm
 {
+
 namespace
 {
 
@@ -32,7 +33,7 @@ __device__ __forceinline__ void acc_sincos(double x, double *s, double *c) { sin
 __device__ __forceinline__ float drsqrt(float x) { return rsqrtf(x); }
 __device__ __forceinline__ double drsqrt(double x) { return rsqrt(x); }
 
-constexpr int kTargets = 128;   // targets per CTA (one per thread)
+constexpr int kTargets = 128;   // threads per CTA (one target per thread per pass)
 constexpr int kTile = 64;       // sources per shared-memory tile
 
 template <class R, int COLS>
@@ -155,6 +156,155 @@ boundary_dense_kernel(const R *__restrict__ mid4, const R *__restrict__ nrm4, co
         #pragma unroll
         for (int k = 0; k < COLS; ++k) out[k] = acc[k];
     }
+}
+
+// Plain FP32 form with packed FP32x2 arithmetic (sm_100 FFMA2).  Each thread
+// owns TT targets (i, i + 128, ...) and the 16 columns of one wave chunk.  A
+// complex MAC  c += a b  is two packed FMAs:
+//     c += (a.re, a.re) * (b.re, b.im)
+//     c += (a.im, a.im) * (-b.im, b.re)
+// so the tile stages every RHS row twice, as b and as the swapped, negated
+// (-b.im, b.re).  Half the issue slots of the scalar form for the same FMA-pipe
+// work; TT > 1 shares every staged RHS row between TT targets.
+constexpr int kPackedCols = 16;
+
+struct PackedTile
+{
+    float4 y[kTile];
+    float4 mu[kTile];
+    float2 B[kTile][kPackedCols];
+    float2 Bw[kTile][kPackedCols];
+};
+
+template <int TT, bool SL, bool DL, bool ADL>
+__global__ void __launch_bounds__(kTargets, TT == 1 ? 4 : 3)
+boundary_packed_kernel(const float *__restrict__ mid4, const float *__restrict__ nrm4, const float2 *__restrict__ B,
+                       float2 *__restrict__ C, const ChunkParamsF *__restrict__ prm, int n, int wc, int wcs)
+{
+    __shared__ PackedTile tile;
+    const int col0 = blockIdx.y * kPackedCols;
+    const int ch = col0 / wcs;
+    const float kap = prm[ch].kappa;
+    const float2 c1 = prm[ch].c[1], c2 = prm[ch].c[2], c3 = prm[ch].c[3];
+    int ti[TT];
+    float3 x[TT], nu[TT];
+    #pragma unroll
+    for (int t = 0; t < TT; ++t)
+    {
+        ti[t] = blockIdx.x * (kTargets * TT) + t * kTargets + threadIdx.x;
+        x[t] = make_float3(0.f, 0.f, 0.f);
+        nu[t] = make_float3(0.f, 0.f, 0.f);
+        if (ti[t] < n)
+        {
+            const float4 m = reinterpret_cast<const float4 *>(mid4)[ti[t]];
+            x[t] = make_float3(m.x, m.y, m.z);
+            if (ADL)
+            {
+                const float4 q = reinterpret_cast<const float4 *>(nrm4)[ti[t]];
+                nu[t] = make_float3(q.x, q.y, q.z);
+            }
+        }
+    }
+    float2 acc[TT][kPackedCols];
+    #pragma unroll
+    for (int t = 0; t < TT; ++t)
+        #pragma unroll
+        for (int k = 0; k < kPackedCols; ++k) acc[t][k] = make_float2(0.f, 0.f);
+
+    for (int j0 = 0; j0 < n; j0 += kTile)
+    {
+        __syncthreads();
+        {
+            const int tid = threadIdx.x;
+            if (tid < kTile)
+            {
+                const int j = j0 + tid;
+                tile.y[tid] = (j < n) ? reinterpret_cast<const float4 *>(mid4)[j] : make_float4(0.f, 0.f, 0.f, 0.f);
+            }
+            else if (DL && tid < 2 * kTile)
+            {
+                const int sidx = tid - kTile, j = j0 + sidx;
+                tile.mu[sidx] = (j < n) ? reinterpret_cast<const float4 *>(nrm4)[j] : make_float4(0.f, 0.f, 0.f, 0.f);
+            }
+            for (int idx = tid; idx < kTile * kPackedCols; idx += kTargets)
+            {
+                const int sidx = idx / kPackedCols, k = idx % kPackedCols, j = j0 + sidx;
+                const float2 b = (j < n) ? B[(int64_t)j * wc + col0 + k] : make_float2(0.f, 0.f);
+                tile.B[sidx][k] = b;
+                tile.Bw[sidx][k] = make_float2(-b.y, b.x);
+            }
+        }
+        __syncthreads();
+        const int smax = min(kTile, n - j0);
+        for (int s = 0; s < smax; ++s)
+        {
+            const float4 yv = tile.y[s];
+            float4 mv = make_float4(0.f, 0.f, 0.f, 0.f);
+            if (DL) mv = tile.mu[s];
+            float2 Ar[TT], Ai[TT];
+            #pragma unroll
+            for (int t = 0; t < TT; ++t)
+            {
+                const float zx = yv.x - x[t].x, zy = yv.y - x[t].y, zz = yv.z - x[t].z;
+                const float r2 = zx * zx + zy * zy + zz * zz;
+                const float rinv = (j0 + s == ti[t]) ? 0.f : rsqrtf(r2);
+                const float r = r2 * rinv;
+                const float kr = kap * r;
+                float sn, cs;
+                __sincosf(kr, &sn, &cs);
+                float ax = 0.f, ay = 0.f;
+                if (SL)
+                {
+                    const float er = cs * rinv, ei = sn * rinv;
+                    ax = c1.x * er - c1.y * ei;
+                    ay = c1.x * ei + c1.y * er;
+                }
+                if (DL || ADL)
+                {
+                    const float r3 = rinv * rinv * rinv;
+                    const float g0 = -(kr * sn + cs) * r3;
+                    const float g1 = (kr * cs - sn) * r3;
+                    float fx = 0.f, fy = 0.f;
+                    if (DL)
+                    {
+                        const float dm = zx * mv.x + zy * mv.y + zz * mv.z;
+                        fx += c2.x * dm;
+                        fy += c2.y * dm;
+                    }
+                    if (ADL)
+                    {
+                        const float dn = zx * nu[t].x + zy * nu[t].y + zz * nu[t].z;
+                        fx -= c3.x * dn;
+                        fy -= c3.y * dn;
+                    }
+                    ax += fx * g0 - fy * g1;
+                    ay += fx * g1 + fy * g0;
+                }
+                Ar[t] = make_float2(ax, ax);
+                Ai[t] = make_float2(ay, ay);
+            }
+            #pragma unroll
+            for (int k = 0; k < kPackedCols; ++k)
+            {
+                const float2 b = tile.B[s][k], bw = tile.Bw[s][k];
+                #pragma unroll
+                for (int t = 0; t < TT; ++t)
+                {
+                    acc[t][k] = __ffma2_rn(Ar[t], b, acc[t][k]);
+                    acc[t][k] = __ffma2_rn(Ai[t], bw, acc[t][k]);
+                }
+            }
+        }
+    }
+    #pragma unroll
+    for (int t = 0; t < TT; ++t)
+        if (ti[t] < n)
+        {
+            float4 *out = reinterpret_cast<float4 *>(&C[(int64_t)ti[t] * wc + col0]);
+            #pragma unroll
+            for (int k = 0; k < kPackedCols; k += 2)
+                out[k / 2] = make_float4(acc[t][k].x, acc[t][k].y, acc[t][k + 1].x, acc[t][k + 1].y);
+        }
 }
 
 template <class R, int COLS, bool SL, bool DL>
@@ -404,11 +554,31 @@ template <> const double *geo_meas<double>(const MeshDev &m) { return m.meas_d; 
 
 inline int cols_for(int wcs) { return wcs < 16 ? wcs : 16; }
 
+template <int TT>
+void packed_dispatch(int code, int n, int wc, int wcs, const float *mid, const float *nrm, const float2 *B, float2 *C,
+                     const ChunkParamsF *p, cudaStream_t st)
+{
+    dim3 grid(ceil_div(n, kTargets * TT), wc / kPackedCols);
+#define BAEMM_PK(SL, DL, ADL) boundary_packed_kernel<TT, SL, DL, ADL><<<grid, kTargets, 0, st>>>(mid, nrm, B, C, p, n, wc, wcs)
+    switch (code)
+    {
+        case 1: BAEMM_PK(true, false, false); break;
+        case 2: BAEMM_PK(false, true, false); break;
+        case 3: BAEMM_PK(true, true, false); break;
+        case 4: BAEMM_PK(false, false, true); break;
+        case 5: BAEMM_PK(true, false, true); break;
+        case 6: BAEMM_PK(false, true, true); break;
+        case 7: BAEMM_PK(true, true, true); break;
+        default: break;
+    }
+#undef BAEMM_PK
+}
+
 } // namespace
 
 template <class R>
 void launch_boundary_dense(const MeshDev &m, const OpFlags &f, const void *chunk_params, int wc, int wcs,
-                           const cplx<R> *Btri, cplx<R> *Ctri, cudaStream_t st)
+                           const cplx<R> *Btri, cplx<R> *Ctri, cudaStream_t st, int variant)
 {
     if (!f.any_layer() || m.nt == 0) return;
     const int n = (int)m.nt;
@@ -416,6 +586,17 @@ void launch_boundary_dense(const MeshDev &m, const OpFlags &f, const void *chunk
     dim3 grid(ceil_div(n, kTargets), wc / cols);
     const auto *p = static_cast<const typename Prm<R>::type *>(chunk_params);
     const R *mid = geo_mid<R>(m), *nrm = geo_nrm<R>(m);
+    if constexpr (std::is_same<R, float>::value)
+    {
+        if (cols == kPackedCols && variant > 0)
+        {
+            const int code = (f.sl() ? 1 : 0) | (f.dl() ? 2 : 0) | (f.adl() ? 4 : 0);
+            if (variant == 2) packed_dispatch<2>(code, n, wc, wcs, mid, nrm, Btri, Ctri, p, st);
+            else packed_dispatch<1>(code, n, wc, wcs, mid, nrm, Btri, Ctri, p, st);
+            BAEMM_LAUNCH_CHECK();
+            return;
+        }
+    }
     switch (cols)
     {
         case 1: boundary_cols<R, 1>(f, grid, st, mid, nrm, Btri, Ctri, p, n, wc, wcs); break;
@@ -508,9 +689,9 @@ void launch_incident(const MeshDev &m, const void *chunk_params, int wc, int wcs
 }
 
 template void launch_boundary_dense<float>(const MeshDev &, const OpFlags &, const void *, int, int, const float2 *,
-                                           float2 *, cudaStream_t);
+                                           float2 *, cudaStream_t, int);
 template void launch_boundary_dense<double>(const MeshDev &, const OpFlags &, const void *, int, int, const double2 *,
-                                            double2 *, cudaStream_t);
+                                            double2 *, cudaStream_t, int);
 template void launch_farfield<float>(const MeshDev &, const OpFlags &, const void *, int, int, const float2 *, float2 *,
                                      size_t, double2, double2, double2 *, int64_t, cudaStream_t);
 template void launch_farfield<double>(const MeshDev &, const OpFlags &, const void *, int, int, const double2 *,

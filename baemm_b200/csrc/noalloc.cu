@@ -108,7 +108,8 @@ extern "C" int baemm_apply_boundary_operators_noalloc_dev_c(baemm_ctx *ctx, cons
             if (layers)
             {
                 launch_avop<float2, float>(c.mesh, B, ldB, wc, Bt, c.stream);
-                launch_boundary_dense<float>(c.mesh, c.flags, c.prm_f.p, wc, c.wave_chunk_size, Bt, Ct, c.stream);
+                launch_boundary_dense<float>(c.mesh, c.flags, c.prm_f.p, wc, c.wave_chunk_size, Bt, Ct, c.stream,
+                                             c.dense_variant);
             }
             launch_epilogue<float2, float>(c.mesh, ea, Ct, Bt, c.prm_f.p, B, ldB, al, be, C, ldC, c.stream);
         }

@@ -79,9 +79,24 @@ void launch_axpby(int64_t rows, int cols, T a, const T *x, int64_t ldx, T b, T *
 // ---- dense.cu ------------------------------------------------------------------
 // Dense boundary kernel (BoundaryOperatorKernel.cl:5-239): Ctri = K(kappa) Btri
 // chunk by chunk, the self pair excluded.  R = float (plain FP32) or double.
+// variant (FP32, 16-column groups): 0 scalar FMA kernel, 1 / 2 packed FP32x2
+// kernel with 1 / 2 targets per thread.
+constexpr int kDenseVariants = 3;
 template <class R>
 void launch_boundary_dense(const MeshDev &m, const OpFlags &f, const void *chunk_params, int wc, int wcs,
-                           const cplx<R> *Btri, cplx<R> *Ctri, cudaStream_t st);
+                           const cplx<R> *Btri, cplx<R> *Ctri, cudaStream_t st, int variant = 2);
+// Compensated tensor-core dense kernel (tc.cu): TF32 hi/lo split, three
+// tcgen05 MMAs per K step, FP32 accumulation in TMEM.  wave_chunk_size 16.
+// `err` (device int) receives a non-zero code when a bounded wait gave up.
+bool tc_supported(int wc, int wcs);
+// seg_tiles: 16-source tiles accumulated in TMEM before the partial sum is
+// added to FP32 registers (bounds the tensor-core accumulation chain).
+void launch_boundary_tc(const MeshDev &m, const OpFlags &f, const void *chunk_params, int wc, int wcs,
+                        const float2 *Btri, float2 *Ctri, float2 *ws, size_t ws_elems, int *err, cudaStream_t st,
+                        int seg_tiles = 4, int ctas = 0);
+// float2 elements of the tensor-core workspace for a persistent grid of `ctas`
+// CTAs (0: one per SM of the current device).
+size_t tc_workspace_elems(int ctas = 0);
 // Far-field kernel (FarFieldOperatorKernel.cl:5-178) with source splitting and
 // a deterministic second-pass reduction; Cout = alpha F + beta Cout.
 template <class R>

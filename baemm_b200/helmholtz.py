@@ -12,12 +12,15 @@ with the library's message (the reference prints and continues).
 """
 from __future__ import annotations
 
+import contextlib
 import ctypes as C
 
 import numpy as np
 
 from . import _capi
 from ._capi import APPLY_FP32, APPLY_FP64, APPLY_TC, WAVE_PLANE, WAVE_RADIAL, BaemmError, SolveStats
+
+_CUDA_STREAM_LEGACY = 0x1   # cudaStreamLegacy
 
 __all__ = ["Helmholtz_CUDA", "WaveType", "BaemmError", "APPLY_FP32", "APPLY_TC", "APPLY_FP64"]
 
@@ -78,6 +81,7 @@ class Helmholtz_CUDA:
             raise BaemmError(st, L.baemm_last_error(None).decode())
         self._h = h
         self._lib = L
+        self._user_stream = None   # set by SetStream; otherwise torch tensors join torch's current stream
 
     # --- lifecycle ---------------------------------------------------------------
     def close(self):
@@ -163,6 +167,18 @@ class Helmholtz_CUDA:
     def GetApplyMode(self) -> int:
         return int(self._lib.baemm_get_apply_mode(self._h))
 
+    def SetTuning(self, key: int, value: int):
+        self._ck(self._lib.baemm_set_tuning(self._h, int(key), int(value)))
+
+    def GetTuning(self, key: int) -> int:
+        return int(self._lib.baemm_get_tuning(self._h, int(key)))
+
+    def SetKernelVariant(self, variant: int):
+        self.SetTuning(_capi.TUNE_DENSE_VARIANT, variant)
+
+    def GetKernelVariant(self) -> int:
+        return self.GetTuning(_capi.TUNE_DENSE_VARIANT)
+
     def SetRefinement(self, max_steps: int, inner_tol: float = 1e-4):
         self._ck(self._lib.baemm_set_refinement(self._h, int(max_steps), float(inner_tol)))
 
@@ -218,7 +234,33 @@ class Helmholtz_CUDA:
         return int(self._lib.baemm_stream(self._h) or 0)
 
     def SetStream(self, stream_handle: int | None):
+        """Enqueue on `stream_handle` (a cudaStream_t as int; the stream must
+        outlive its use).  None or 0 returns to the default: the context's own
+        stream for host arrays, and for torch CUDA tensors torch's current
+        stream of the tensor's device, joined for the duration of each call."""
         self._ck(self._lib.baemm_set_stream(self._h, C.c_void_p(stream_handle or 0)))
+        self._user_stream = stream_handle or None
+
+    @contextlib.contextmanager
+    def _on_torch_stream(self, t):
+        # Device-pointer calls are asynchronous: they run on the stream that
+        # produced their inputs and will consume their outputs, which for torch
+        # tensors is torch's current stream.  The context is handed over to it
+        # for the call and back afterwards (event ordering, no host sync), so it
+        # never keeps a torch stream that may be destroyed later.
+        if self._user_stream is not None:
+            yield
+            return
+        import torch
+        # torch's default stream is the legacy default stream (handle 0), which
+        # the C ABI spells cudaStreamLegacy (0x1); a null handle there means the
+        # context's own non-blocking stream.
+        s = int(torch.cuda.current_stream(t.device).cuda_stream) or _CUDA_STREAM_LEGACY
+        self._ck(self._lib.baemm_set_stream(self._h, C.c_void_p(s)))
+        try:
+            yield
+        finally:
+            self._ck(self._lib.baemm_set_stream(self._h, C.c_void_p(0)))
 
     def Synchronize(self):
         self._ck(self._lib.baemm_synchronize(self._h))
@@ -252,15 +294,14 @@ class Helmholtz_CUDA:
             if _is_torch_cuda(B_in):
                 import torch
                 if B_in.dtype == torch.complex128:
-                    self._ck(self._lib.baemm_apply_boundary_operators_dev_z(
-                        self._h, _dp(_cz(alpha)), C.c_void_p(B_in.data_ptr()), B_in.stride(0),
-                        _dp(_cz(beta)), C.c_void_p(C_out.data_ptr()), C_out.stride(0)))
+                    fn, cs, ptr = self._lib.baemm_apply_boundary_operators_dev_z, _cz, _dp
                 elif B_in.dtype == torch.complex64:
-                    self._ck(self._lib.baemm_apply_boundary_operators_dev_c(
-                        self._h, _fp(_cc(alpha)), C.c_void_p(B_in.data_ptr()), B_in.stride(0),
-                        _fp(_cc(beta)), C.c_void_p(C_out.data_ptr()), C_out.stride(0)))
+                    fn, cs, ptr = self._lib.baemm_apply_boundary_operators_dev_c, _cc, _fp
                 else:
                     raise TypeError("B_in must be complex64 or complex128")
+                with self._on_torch_stream(B_in):
+                    self._ck(fn(self._h, ptr(cs(alpha)), C.c_void_p(B_in.data_ptr()), B_in.stride(0),
+                                ptr(cs(beta)), C.c_void_p(C_out.data_ptr()), C_out.stride(0)))
             elif isinstance(B_in, np.ndarray) and B_in.dtype == np.complex64:
                 _check_out(C_out, np.complex64, "C_out")
                 B = np.ascontiguousarray(B_in)
@@ -285,9 +326,10 @@ class Helmholtz_CUDA:
         if _is_torch_cuda(B_in):
             if kappa is not None:
                 self.LoadParameters(kappa, coeff, wave_count, wave_chunk_size)
-            self._ck(self._lib.baemm_apply_far_field_operators_dev_z(
-                self._h, _dp(_cz(alpha)), C.c_void_p(B_in.data_ptr()), B_in.stride(0), _dp(_cz(beta)),
-                C.c_void_p(C_out.data_ptr()), C_out.stride(0)))
+            with self._on_torch_stream(B_in):
+                self._ck(self._lib.baemm_apply_far_field_operators_dev_z(
+                    self._h, _dp(_cz(alpha)), C.c_void_p(B_in.data_ptr()), B_in.stride(0), _dp(_cz(beta)),
+                    C.c_void_p(C_out.data_ptr()), C_out.stride(0)))
             return C_out
         _check_out(C_out, np.complex128, "C_out")
         B = np.ascontiguousarray(B_in, dtype=np.complex128)

@@ -211,7 +211,7 @@ def run_reference_arm(args, rank, world):
 # ---------------------------------------------------------------------------
 def run_gpu_arm(args, rank, world, local_rank):
     import torch
-    from baemm_b200 import APPLY_FP32, APPLY_FP64, Helmholtz_CUDA
+    from baemm_b200 import APPLY_FP32, APPLY_FP64, APPLY_TC, Helmholtz_CUDA
 
     torch.cuda.set_device(local_rank)
     dist = None
@@ -221,7 +221,7 @@ def run_gpu_arm(args, rank, world, local_rank):
     nv, nt = coords.shape[0], tris.shape[0]
     inter = nt * nt * WC
     H = Helmholtz_CUDA(coords, tris, np.eye(3), device=local_rank)
-    mode = {"fp32": APPLY_FP32, "fp64": APPLY_FP64}[args.mode]
+    mode = {"fp32": APPLY_FP32, "fp64": APPLY_FP64, "tc": APPLY_TC}[args.mode]
     H.SetApplyMode(mode)
     kap, coeff = KAPPA, coefficients(KAPPA)
     stream = torch.cuda.Stream()
@@ -336,7 +336,8 @@ def main(argv=None):
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="cuda", choices=["cuda", "reference"])
-    ap.add_argument("--mode", default="fp32", choices=["fp32", "fp64"])
+    ap.add_argument("--mode", default="tc", choices=["fp32", "tc", "fp64"],
+                    help="apply arithmetic: plain FP32, compensated tensor-core (default), FP64")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--small", action="store_true", help="38400-triangle torus (profiling captures only)")
     args = ap.parse_args(argv)

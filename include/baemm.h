@@ -96,7 +96,12 @@ int baemm_device_info(baemm_ctx *ctx, char *buf, size_t len);
 const char *baemm_class_name(void);
 /* The CUDA stream the context runs on (cudaStream_t). */
 void *baemm_stream(baemm_ctx *ctx);
-/* Use an external stream (e.g. a framework's current stream); NULL = own stream. */
+/* Use an external stream (e.g. a framework's current stream); NULL = own
+ * (non-blocking) stream; cudaStreamLegacy ((void *)0x1) = the legacy default
+ * stream.  Work enqueued afterwards is ordered after the work already queued
+ * on the previous stream (an event, no host synchronisation).  The stream must
+ * outlive its use by the context.  No reference counterpart (the reference
+ * owns its OpenCL queue). */
 int baemm_set_stream(baemm_ctx *ctx, void *stream);
 int baemm_synchronize(baemm_ctx *ctx);
 
@@ -114,6 +119,19 @@ int baemm_set_gmres_params(baemm_ctx *ctx, int max_iter, int max_restarts); /* M
 int baemm_get_gmres_params(const baemm_ctx *ctx, int *max_iter, int *max_restarts);
 int baemm_set_apply_mode(baemm_ctx *ctx, int mode);        /* BAEMM_APPLY_*; no reference counterpart */
 int baemm_get_apply_mode(const baemm_ctx *ctx);
+/* Kernel tuning knobs (no reference counterpart; results are the same sums):
+ *   BAEMM_TUNE_DENSE_VARIANT  plain FP32 dense kernel: 0 scalar FMA (default),
+ *                             1 / 2 packed FP32x2 with 1 / 2 targets per thread
+ *   BAEMM_TUNE_TC_SEGMENT     tensor-core form: 16-source tiles accumulated in
+ *                             TMEM before each partial sum is added in FP32
+ *                             registers (default 4; bounds the accumulation chain)
+ *   BAEMM_TUNE_TC_CTAS        tensor-core form: persistent grid size (default 0 =
+ *                             one CTA per SM) */
+#define BAEMM_TUNE_DENSE_VARIANT 1
+#define BAEMM_TUNE_TC_SEGMENT    2
+#define BAEMM_TUNE_TC_CTAS       3
+int baemm_set_tuning(baemm_ctx *ctx, int key, int value);
+int baemm_get_tuning(const baemm_ctx *ctx, int key);
 /* FP64 iterative refinement around the inner GMRES (0 = off, the reference's
  * behaviour).  When on, the solve's outer residual uses the FP64 apply and
  * the inner GMRES uses the context's apply mode. No reference counterpart. */

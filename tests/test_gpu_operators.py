@@ -7,7 +7,7 @@ within 1e-11 of the FP64 oracle.
 import numpy as np
 import pytest
 
-from baemm_b200 import APPLY_FP32, APPLY_FP64, BaemmError, Helmholtz_CUDA, WaveType, meshes
+from baemm_b200 import APPLY_FP32, APPLY_FP64, APPLY_TC, BaemmError, Helmholtz_CUDA, WaveType, _capi, meshes
 from oracle import oracle as O
 from tests.helpers import crandn, relerr
 
@@ -113,6 +113,86 @@ def test_apply_boundary_fp64(env, cname, wname):
     assert relerr(Cg, C64) < FP64_TOL
 
 
+@pytest.mark.parametrize("cname", ["sl", "dl", "adl", "bie", "all"])
+@pytest.mark.parametrize("wname", ["w16", "w32", "w64"])
+def test_apply_boundary_tensor_core(env, cname, wname):
+    """Compensated tensor-core form (TF32 hi/lo, FP32 accumulation): within
+    1e-5 of the FP64 oracle (the same bar as the FP32 path)."""
+    coords, tris, meas, H, o32, o64 = env
+    wc, wcs, kap = WAVES[wname]
+    coeff = _coeff(cname, kap)
+    rng = np.random.default_rng(41)
+    B = crandn(rng, coords.shape[0], wc + 2)
+    C0 = crandn(rng, coords.shape[0], wc)
+    Cg = C0.copy()
+    H.SetApplyMode(APPLY_TC)
+    try:
+        H.ApplyBoundaryOperators_PL(0.5 - 1j, B, 0.25, Cg, kap, coeff, wc, wcs)
+    finally:
+        H.SetApplyMode(APPLY_FP32)
+    C64, C32 = C0.copy(), C0.copy()
+    o64.ApplyBoundaryOperators_PL(0.5 - 1j, B, 0.25, C64, kap, coeff, wc, wcs)
+    o32.ApplyBoundaryOperators_PL(0.5 - 1j, B, 0.25, C32, kap, coeff, wc, wcs)
+    assert relerr(Cg, C64) < FP32_VS64_TOL
+    assert relerr(Cg, C32) < FP32_VS64_TOL
+
+
+@pytest.mark.parametrize("ctas", [1, 3, 7, 61, 148, 60000])
+@pytest.mark.parametrize("wshape", [(64, [2.0, 4.0, 8.0, 16.0]), (48, [1.0, 5.0, 9.0]),
+                                    (128, [1.0, 2.0, 3.0, 4.0, 5.0, 6.0, 7.0, 8.0])])
+def test_tensor_core_persistent_grid(env, ctas, wshape):
+    """The persistent tensor-core grid splits target blocks between CTAs at any
+    grid size (1 CTA, odd sizes, one 16-source tile per CTA); the split blocks
+    are summed by the fix-up pass.  Same bar as the FP32 path against the FP64
+    oracle, and repeated calls are bitwise identical at a fixed grid size."""
+    coords, tris, meas, H, o32, o64 = env
+    wc, kap = wshape
+    coeff = _coeff("all", kap)
+    rng = np.random.default_rng(1234 + wc)
+    B = crandn(rng, coords.shape[0], wc)
+    C64 = np.zeros_like(B)
+    o64.ApplyBoundaryOperators_PL(1.0, B, 0.0, C64, kap, coeff, wc, 16)
+    H.SetApplyMode(APPLY_TC)
+    H.SetTuning(_capi.TUNE_TC_CTAS, ctas)
+    try:
+        assert H.GetTuning(_capi.TUNE_TC_CTAS) == ctas
+        C1, C2 = np.zeros_like(B), np.zeros_like(B)
+        H.ApplyBoundaryOperators_PL(1.0, B, 0.0, C1, kap, coeff, wc, 16)
+        H.ApplyBoundaryOperators_PL(1.0, B, 0.0, C2, kap, coeff, wc, 16)
+    finally:
+        H.SetTuning(_capi.TUNE_TC_CTAS, 0)
+        H.SetApplyMode(APPLY_FP32)
+    assert relerr(C1, C64) < FP32_VS64_TOL
+    assert np.array_equal(C1, C2)
+
+
+def test_device_path_follows_torch_stream(env):
+    """Without SetStream, torch CUDA tensors are processed on torch's current
+    stream, so reading the result back through torch needs no extra sync."""
+    import torch
+    coords, tris, meas, H, o32, o64 = env
+    wc, wcs, kap = WAVES["w64"]
+    coeff = _coeff("bie", kap)
+    B = crandn(np.random.default_rng(77), coords.shape[0], wc)
+    ref = np.zeros_like(B)
+    o32.ApplyBoundaryOperators_PL(1.0, B, 0.0, ref, kap, coeff, wc, wcs)
+    H.LoadBoundaryOperators_PL(kap, coeff, wc, wcs)
+    try:
+        for mode in (APPLY_FP32, APPLY_TC):
+            H.SetApplyMode(mode)
+            for stream in (torch.cuda.current_stream(), torch.cuda.Stream()):
+                with torch.cuda.stream(stream):
+                    Bd = torch.from_numpy(B).to("cuda", non_blocking=True)
+                    Cd = torch.full_like(Bd, float("nan"))
+                    H.ApplyBoundaryOperators_PL(1.0, Bd, 0.0, Cd)
+                    out = Cd.cpu().numpy()   # synchronises torch's stream only
+                assert relerr(out, ref) < FP32_VS64_TOL
+    finally:
+        H.SetApplyMode(APPLY_FP32)
+        H.UnloadBoundaryOperators_PL()
+        H.SetStream(None)
+
+
 def test_apply_complex64_and_device_paths(env):
     import torch
     coords, tris, meas, H, o32, o64 = env
@@ -136,6 +216,24 @@ def test_apply_complex64_and_device_paths(env):
     H.SetStream(None)
     H.UnloadBoundaryOperators_PL()
     assert relerr(Cd.cpu().numpy(), ref) < FP32_TOL
+
+
+@pytest.mark.parametrize("variant", [0, 1, 2])
+@pytest.mark.parametrize("cname", ["bie", "all"])
+def test_dense_kernel_variants(env, variant, cname):
+    """Every plain FP32 dense-kernel variant (scalar, packed x1, packed x2) matches the oracle."""
+    coords, tris, meas, H, o32, o64 = env
+    wc, wcs, kap = WAVES["w64x32"]
+    coeff = _coeff(cname, kap)
+    B = crandn(np.random.default_rng(31), coords.shape[0], wc)
+    Cg, Co = np.zeros_like(B), np.zeros_like(B)
+    H.SetKernelVariant(variant)
+    try:
+        H.ApplyBoundaryOperators_PL(1.0, B, 0.0, Cg, kap, coeff, wc, wcs)
+    finally:
+        H.SetKernelVariant(0)
+    o32.ApplyBoundaryOperators_PL(1.0, B, 0.0, Co, kap, coeff, wc, wcs)
+    assert relerr(Cg, Co) < FP32_TOL
 
 
 def test_apply_is_deterministic(env):
