@@ -228,9 +228,14 @@ void Ctx::dense_apply(const cplx<R> *Btri, cplx<R> *Ctri)
         launch_boundary_dense<double>(mesh, flags, prm_d.p, wave_count, wave_chunk_size, Btri, Ctri, stream);
     else if (apply_mode == BAEMM_APPLY_TC && tc_supported(wave_count, wave_chunk_size))
     {
+        if (!tc_geo_ready)
+        {
+            launch_tc_tile_geometry(mesh, mesh.tgeo_f.reserve(tc_tile_geometry_floats(mesh.nt)), stream);
+            tc_geo_ready = true;
+        }
         const size_t ws_elems = tc_workspace_elems(tc_ctas);
-        launch_boundary_tc(mesh, flags, prm_f.p, wave_count, wave_chunk_size, Btri, Ctri, tc_ws.reserve(ws_elems),
-                           ws_elems, tc_err.p, stream, tc_seg_tiles, tc_ctas);
+        launch_boundary_tc(mesh, flags, prm_f.p, wave_count, wave_chunk_size, mesh.tgeo_f.p, Btri, Ctri,
+                           tc_ws.reserve(ws_elems), ws_elems, tc_err.p, stream, tc_seg_tiles, tc_ctas);
         tc_pending = true;
     }
     else

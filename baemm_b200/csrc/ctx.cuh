@@ -50,6 +50,7 @@ public:
     int tc_seg_tiles = 4;             // tensor-core form: tiles per TMEM partial sum
     int tc_ctas = 0;                  // tensor-core form: persistent grid size (0 = one CTA per SM)
     DevBuf<float2> tc_ws;             // tensor-core form: partial sums of target blocks split between CTAs
+    bool tc_geo_ready = false;        // mesh.tgeo_f built
     int ir_max_steps = 0;
     double ir_inner_tol = 1e-4;
     baemm_solve_stats stats{};

@@ -22,6 +22,7 @@ struct MeshDev
     DevBuf<int32_t> avt_outer, avt_inner;
     DevBuf<int32_t> mass_outer, mass_inner;
     DevBuf<float> mid_f, nrm_f, area_f, a3_f, diag_f, mass_f, lumped_f, meas_f;
+    DevBuf<float> tgeo_f;        // tensor-core form: source geometry per 16-source tile (lazily built)
     DevBuf<double> mid_d, nrm_d, area_d, a3_d, diag_d, mass_d, lumped_d, meas_d;
 };
 
@@ -92,8 +93,11 @@ bool tc_supported(int wc, int wcs);
 // seg_tiles: 16-source tiles accumulated in TMEM before the partial sum is
 // added to FP32 registers (bounds the tensor-core accumulation chain).
 void launch_boundary_tc(const MeshDev &m, const OpFlags &f, const void *chunk_params, int wc, int wcs,
-                        const float2 *Btri, float2 *Ctri, float2 *ws, size_t ws_elems, int *err, cudaStream_t st,
-                        int seg_tiles = 4, int ctas = 0);
+                        const float *tgeo, const float2 *Btri, float2 *Ctri, float2 *ws, size_t ws_elems, int *err,
+                        cudaStream_t st, int seg_tiles = 4, int ctas = 0);
+// Source geometry of the tensor-core form, per 16-source tile (built once per mesh).
+size_t tc_tile_geometry_floats(int64_t nt);
+void launch_tc_tile_geometry(const MeshDev &m, float *tgeo, cudaStream_t st);
 // float2 elements of the tensor-core workspace for a persistent grid of `ctas`
 // CTAs (0: one per SM of the current device).
 size_t tc_workspace_elems(int ctas = 0);

@@ -3,11 +3,17 @@
 // The apply C_i = sum_j A_ij(kappa) B_j of BoundaryOperatorKernel.cl:5-239 as
 // a real GEMM per wave chunk (16 right-hand sides):
 //     [C_re | C_im]  (128 x 32)  =  A  (128 x 2S)  x  Bimg^T  (2S x 32)
-// with A[i][2s] = Re A_is, A[i][2s+1] = Im A_is and, for each source s,
-//     Bimg[q][2s] = Re b_sq,  Bimg[q][2s+1] = -Im b_sq,
-//     Bimg[16+q][2s] = Im b_sq, Bimg[16+q][2s+1] = Re b_sq   (q < 16).
+// with the K index ordered by source pairs (s0, s1) = (2p, 2p + 1):
+//     A[i][4p .. 4p+3]      = (Re A_is0, Re A_is1, Im A_is0, Im A_is1),
+//     Bimg[q][4p .. 4p+3]   = (Re b_s0q, Re b_s1q, -Im b_s0q, -Im b_s1q),
+//     Bimg[16+q][4p .. 4p+3] = (Im b_s0q, Im b_s1q, Re b_s0q, Re b_s1q)   (q < 16),
+// so that the generators evaluate two sources per packed FP32x2 instruction
+// and each packed result is already in the register order of the TMEM store.
 // Operands are split into TF32 hi + lo parts and the product is compensated:
 //     A B ~= Ahi Bhi + Alo Bhi + Ahi Blo       (FP32 accumulation in TMEM),
+// issued as two MMAs per K step: Ahi [Bhi | Blo] (N = 64, into a main and a
+// correction half of the chunk's accumulator) and Alo Bhi (N = 32, into the
+// correction half); a tcgen05.mma costs about the same for N = 32 and 64.
 // which keeps ~21 bits per product (TF32 hi+lo), well inside 1e-5 relative.
 //
 // Work unit = (group of up to 4 chunks, block of 128 targets, 16-source tile).
@@ -20,16 +26,16 @@
 // Warp roles (384 threads):
 //   warps 0-7   generators: thread (lane quarter q = warp % 4, half g = warp / 4)
 //               owns target row 32 q + lane and sources 8 g .. 8 g + 7 of each
-//               16-source K tile; it evaluates the kernel entries in registers
-//               (geometry shared by all chunks), splits them into hi / lo and
-//               writes them straight into TMEM (tcgen05.st), so the A operand
-//               never touches shared memory;
+//               16-source K tile; it evaluates the kernel entries in registers,
+//               two sources per FP32x2 instruction (geometry shared by all
+//               chunks), splits them into hi / lo and writes them straight into
+//               TMEM (tcgen05.st), so the A operand never touches shared memory;
 //   warps 8-9   expanders: expand the tile's 16 B_tri rows into hi / lo K-major
 //               SWIZZLE_128B images in shared memory;
 //   warp 10     bulk-copy producer: cp.async.bulk of the raw tile (B_tri rows,
 //               midpoints, normals) into shared memory;
-//   warp 11     MMA issuer: 12 tcgen05.mma (kind::tf32, A from TMEM, B from
-//               shared memory, M 128, N 32, K 8) per chunk and tile.
+//   warp 11     MMA issuer: 8 tcgen05.mma (kind::tf32, A from TMEM, B from
+//               shared memory, M 128, K 8) per chunk and tile.
 // Pipelines use mbarriers (A stages in TMEM, B stages in shared memory).
 // Every wait is bounded: on time-out the CTA raises a shared abort flag, writes
 // an error code for the host, waits (bounded) for its issued MMAs and frees
@@ -37,6 +43,7 @@
 #include "ops.cuh"
 
 #include <algorithm>
+#include <cstddef>
 #include <mutex>
 
 namespace baemm
@@ -56,18 +63,27 @@ constexpr int TC_ASTAGES = 4;      // A stages in TMEM (one chunk of one tile ea
 constexpr int TC_BSTAGES = 3;      // expanded B image stages in shared memory
 constexpr int TC_RSTAGES = 6;      // raw tile stages filled by bulk copies
 constexpr uint32_t TC_TMEM_COLS = 512;
-constexpr uint32_t TC_ACC_COLS = TC_CHMAX * TC_N;    // one accumulator buffer (128 columns)
-constexpr uint32_t TC_ACOL = 2 * TC_ACC_COLS;        // A stages after two accumulator buffers
+constexpr uint32_t TC_DCOLS = 2 * TC_N;             // per chunk: main (Ahi Bhi) | correction (Ahi Blo + Alo Bhi)
+constexpr uint32_t TC_ACC_COLS = TC_CHMAX * TC_DCOLS;   // the TMEM accumulator (256 columns)
+constexpr uint32_t TC_ACOL = TC_ACC_COLS;             // A stages after the accumulator
 constexpr int TC_IMG = TC_N * 128;                   // one K-major SW128 image: 32 rows x 128 B
 constexpr uint64_t kWaitNs = 200ull * 1000 * 1000;   // 200 ms per wait (a pipeline stage takes microseconds)
 
-// Raw tile: the 16 source rows of B_tri (this CTA's columns) plus their
-// midpoints and normals, filled by cp.async.bulk.
+// Source geometry of one 16-source tile, structure of arrays (built once per
+// mesh by tc_tile_geometry_kernel; padding sources past the end are zero).
+struct TcTileGeo
+{
+    float x[TC_SRC], y[TC_SRC], z[TC_SRC];      // midpoints
+    float mx[TC_SRC], my[TC_SRC], mz[TC_SRC];   // unit normals
+};
+static_assert(sizeof(TcTileGeo) % 16 == 0, "bulk copies move multiples of 16 bytes");
+
+// Raw tile: the 16 source rows of B_tri (this CTA's columns) plus the tile's
+// geometry, filled by cp.async.bulk.
 struct TcRaw
 {
     float2 b[TC_SRC][TC_CHMAX * 16];   // 8 KB
-    float4 y[TC_SRC];
-    float4 mu[TC_SRC];
+    TcTileGeo geo;
 };
 
 struct __align__(1024) TcSmem
@@ -77,11 +93,21 @@ struct __align__(1024) TcSmem
     uint64_t a_full[TC_ASTAGES], a_empty[TC_ASTAGES];
     uint64_t b_full[TC_BSTAGES], b_empty[TC_BSTAGES];
     uint64_t r_full[TC_RSTAGES], r_empty[TC_RSTAGES];
-    uint64_t seg_full[2], seg_empty[2];
+    uint64_t seg_full, seg_empty;   // TMEM accumulator: segment summed / drained
     uint32_t tmem_base;
     int abort_flag;
-    float4 prm[TC_MAXCHUNKS][2];   // (kappa, c1.x, c1.y, c2.x), (c2.y, c3.x, c3.y, 0)
+    // per chunk, broadcast pairs (v, v): kappa, -kappa, c1.x, c1.y, -c2.x, -c2.y, c3.x, c3.y
+    alignas(16) float2 prm[TC_MAXCHUNKS][8];
+    // FP32 sums of the TMEM partial sums, one padded row per target (the
+    // 16-byte pad spreads the rows of a quarter-warp over all banks)
+    alignas(16) float2 acc[TC_M][TC_CHMAX * 16 + 2];   // accessed as float4
 };
+
+static_assert(sizeof(TcSmem) + 1024 <= 227 * 1024, "shared memory per CTA");
+static_assert(offsetof(TcSmem, acc) % 16 == 0 && (sizeof(float2) * (TC_CHMAX * 16 + 2)) % 16 == 0,
+              "accumulator rows are read and written as float4");
+static_assert(offsetof(TcSmem, raw) % 16 == 0 && offsetof(TcRaw, geo) % 16 == 0 && sizeof(TcRaw) % 16 == 0,
+              "bulk-copy destinations are 16-byte aligned");
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
@@ -138,6 +164,60 @@ __device__ __forceinline__ bool wait_bar(uint64_t *bar, uint32_t parity, volatil
     return false;
 }
 
+// Non-blocking test of the phase (no suspension).
+__device__ __forceinline__ bool mbar_test_wait(uint64_t *bar, uint32_t parity)
+{
+    uint32_t ok;
+    asm volatile("{\n\t.reg .pred p;\n\t"
+                 "mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+                 "selp.u32 %0, 1, 0, p;\n\t}"
+                 : "=r"(ok)
+                 : "r"(smem_u32(bar)), "r"(parity)
+                 : "memory");
+    return ok != 0;
+}
+
+// Bounded wait for the roles that run ahead of the generators (producer,
+// expanders): they poll with a growing __nanosleep between tests, so that
+// their waiting takes few issue slots from the generator warps that share
+// their SM sub-partition.  The MMA issuer is on the critical path and uses
+// wait_bar.  Same contract as wait_bar.
+__device__ __forceinline__ bool wait_bar_sleepy(uint64_t *bar, uint32_t parity, volatile int *abort_flag, int *err,
+                                                int code, bool honour_abort = true)
+{
+    if (mbar_test_wait(bar, parity)) return true;
+    const uint64_t t0 = global_ns();
+    uint32_t ns = 32;
+    for (uint32_t it = 1;; ++it)
+    {
+        __nanosleep(ns);
+        if (mbar_test_wait(bar, parity)) return true;
+        ns = ns < 256u ? 2u * ns : 256u;
+        if ((it & 15u) == 0)
+        {
+            if (honour_abort && (*abort_flag || *(volatile int *)err)) return false;
+            if (global_ns() - t0 > kWaitNs) break;
+        }
+    }
+    *abort_flag = 1;
+    atomicExch(err, code);
+    return false;
+}
+
+// One lane of a converged warp (the lowest), for the single-thread
+// instructions (bulk copies, tcgen05.mma, tcgen05.commit).  Warp-wide loops
+// with an elected issuer keep the loop state warp-uniform, so the compiler can
+// hold the MMA operands in uniform registers.
+__device__ __forceinline__ bool elect_one()
+{
+    uint32_t p = 0;
+    asm volatile("{\n\t.reg .pred P;\n\t"
+                 "elect.sync _|P, 0xffffffff;\n\t"
+                 "selp.u32 %0, 1, 0, P;\n\t}"
+                 : "=r"(p));
+    return p != 0;
+}
+
 __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
 
@@ -151,11 +231,21 @@ __device__ __forceinline__ uint32_t to_tf32(float x) { return (__float_as_uint(x
 
 // hi = tf32(x) (round to nearest), lo = x - hi exactly in FP32.  The tensor
 // core reads the top 19 bits of lo; |lo| <= 2^-11 |x|, so the bits it drops
-// are below 2^-21 |x|.
+// are below 2^-21 |x|.  Used for the right-hand sides (expanded once per tile).
 __device__ __forceinline__ void split_tf32(float x, uint32_t &hi, uint32_t &lo)
 {
     hi = to_tf32(x);
     lo = __float_as_uint(x - __uint_as_float(hi));
+}
+
+// Cheaper split for the generated kernel entries (two instructions): hi is x
+// itself, of which the tensor core reads the top 19 bits (x truncated to
+// TF32); lo = x - trunc(x) is exact, |lo| < 2^-10 |x|, and the bits of lo the
+// tensor core drops are below 2^-20 |x|.
+__device__ __forceinline__ void split_tf32_trunc(float x, uint32_t &hi, uint32_t &lo)
+{
+    hi = __float_as_uint(x);
+    lo = __float_as_uint(x - __uint_as_float(hi & 0xffffe000u));
 }
 
 __device__ __forceinline__ void tmem_st16(uint32_t taddr, const uint32_t (&v)[16])
@@ -188,16 +278,19 @@ __device__ __forceinline__ uint64_t sw128_desc(const void *p)
     return d;
 }
 
-// Instruction descriptor: D F32, A/B TF32, both K-major, N = 32, M = 128.
-constexpr uint32_t kIdescTf32 = (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(TC_N >> 3) << 17) |
-                                ((uint32_t)(TC_M >> 4) << 24);
+// Instruction descriptor: D F32, A/B TF32, both K-major, M = 128, N = n.
+__host__ __device__ constexpr uint32_t idesc_tf32(int n)
+{
+    return (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(TC_M >> 4) << 24);
+}
 
-__device__ __forceinline__ void mma_tf32(uint32_t d_tmem, uint32_t a_tmem, uint64_t b_desc, uint32_t accumulate)
+__device__ __forceinline__ void mma_tf32(uint32_t d_tmem, uint32_t a_tmem, uint64_t b_desc, uint32_t accumulate,
+                                         uint32_t idesc)
 {
     asm volatile("{\n\t.reg .pred p;\n\t"
                  "setp.ne.b32 p, %4, 0;\n\t"
                  "tcgen05.mma.cta_group::1.kind::tf32 [%0], [%1], %2, %3, p;\n\t}" ::"r"(d_tmem),
-                 "r"(a_tmem), "l"(b_desc), "r"(kIdescTf32), "r"(accumulate)
+                 "r"(a_tmem), "l"(b_desc), "r"(idesc), "r"(accumulate)
                  : "memory");
 }
 
@@ -261,9 +354,9 @@ struct PieceIter
 
 template <int CH, bool SL, bool DL, bool ADL>
 __global__ void __launch_bounds__(TC_THREADS, 1)
-boundary_tc_kernel(const float *__restrict__ mid4, const float *__restrict__ nrm4, const float2 *__restrict__ Btri,
-                   float2 *__restrict__ Ctri, float2 *__restrict__ ws, const ChunkParamsF *__restrict__ prm,
-                   const TcPlan plan, int *err)
+boundary_tc_kernel(const float *__restrict__ mid4, const float *__restrict__ nrm4, const TcTileGeo *__restrict__ tgeo,
+                   const float2 *__restrict__ Btri, float2 *__restrict__ Ctri, float2 *__restrict__ ws,
+                   const ChunkParamsF *__restrict__ prm, const TcPlan plan, int *err)
 {
     extern __shared__ __align__(1024) uint8_t smem_raw[];
     // Align inside the shared window by pointer arithmetic on the shared array,
@@ -291,15 +384,17 @@ boundary_tc_kernel(const float *__restrict__ mid4, const float *__restrict__ nrm
             mbar_init(&sm.r_full[k], 1);
             mbar_init(&sm.r_empty[k], TC_GEN_THREADS + TC_EXP_THREADS);
         }
-        for (int k = 0; k < 2; ++k) { mbar_init(&sm.seg_full[k], 1); mbar_init(&sm.seg_empty[k], TC_GEN_THREADS); }
+        mbar_init(&sm.seg_full, 1);
+        mbar_init(&sm.seg_empty, TC_GEN_THREADS);
         sm.abort_flag = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     for (int c = tid; c < wc / 16; c += blockDim.x)
     {
         const ChunkParamsF p = prm[c];
-        sm.prm[c][0] = make_float4(p.kappa, p.c[1].x, p.c[1].y, p.c[2].x);
-        sm.prm[c][1] = make_float4(p.c[2].y, p.c[3].x, p.c[3].y, 0.f);
+        const float v[8] = {p.kappa, -p.kappa, p.c[1].x, p.c[1].y, -p.c[2].x, -p.c[2].y, p.c[3].x, p.c[3].y};
+        #pragma unroll
+        for (int k = 0; k < 8; ++k) sm.prm[c][k] = make_float2(v[k], v[k]);
     }
     if (warp == 0)
     {
@@ -316,67 +411,81 @@ boundary_tc_kernel(const float *__restrict__ mid4, const float *__restrict__ nrm
     if (tid < TC_GEN_THREADS)
     {
         // ------------------------------ generators ------------------------------
+        constexpr int CC = CH >= 2 ? 2 : 1;   // chunks evaluated together (independent work for latency hiding)
         const int q = warp & 3, g = warp >> 2;
+        const int row = q * 32 + lane;
         const uint32_t lane_addr = tbase + ((uint32_t)(q * 32) << 16);
-        float2 racc[CH][8];
+        float2 *acc_row = &sm.acc[row][g * 8];
         bool ok = true;
-        int pending = -1;   // A stage written but not yet published
+        int pending[CC];    // A stages written but not yet published
+        int npending = 0;
         int T = 0, SG = 0;  // tiles and TMEM segments handled so far by this CTA
         auto publish = [&]() {
-            if (pending >= 0)
+            if (npending > 0)
             {
                 asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
                 tc_fence_before();
-                mbar_arrive(&sm.a_full[pending]);
-                pending = -1;
+                #pragma unroll
+                for (int k = 0; k < CC; ++k)
+                    if (k < npending) mbar_arrive(&sm.a_full[pending[k]]);
+                npending = 0;
             }
         };
-        // add the finished TMEM partial sum of segment `sg` to the registers
-        auto drain = [&](int sg) {
-            const int buf = sg & 1;
-            const bool got = wait_bar(&sm.seg_full[buf], (uint32_t)(sg >> 1) & 1u, abort_flag, err, 2);
+        // add (or, first in a piece, store) the finished TMEM partial sum of
+        // segment `sg` (main + correction) into this thread's accumulator row
+        auto drain = [&](int sg, bool first) {
+            const bool got = wait_bar(&sm.seg_full, (uint32_t)sg & 1u, abort_flag, err, 2);
             if (!__all_sync(0xffffffffu, got)) return false;
             tc_fence_after();
             #pragma unroll
             for (int c = 0; c < CH; ++c)
             {
-                uint32_t re[8], im[8];
-                const uint32_t col = (uint32_t)buf * TC_ACC_COLS + (uint32_t)(c * TC_N + g * 8);
+                uint32_t re[8], im[8], cre[8], cim[8];
+                const uint32_t col = (uint32_t)(c * TC_DCOLS + g * 8);
                 tmem_ld8(lane_addr + col, re);
                 tmem_ld8(lane_addr + col + 16u, im);
+                tmem_ld8(lane_addr + col + (uint32_t)TC_N, cre);
+                tmem_ld8(lane_addr + col + (uint32_t)TC_N + 16u, cim);
                 asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+                float4 *a4 = reinterpret_cast<float4 *>(acc_row + c * 16);
                 #pragma unroll
-                for (int k = 0; k < 8; ++k)
+                for (int k = 0; k < 4; ++k)
                 {
-                    racc[c][k].x += __uint_as_float(re[k]);
-                    racc[c][k].y += __uint_as_float(im[k]);
+                    float4 v = first ? make_float4(0.f, 0.f, 0.f, 0.f) : a4[k];
+                    v.x += __uint_as_float(re[2 * k]) + __uint_as_float(cre[2 * k]);
+                    v.y += __uint_as_float(im[2 * k]) + __uint_as_float(cim[2 * k]);
+                    v.z += __uint_as_float(re[2 * k + 1]) + __uint_as_float(cre[2 * k + 1]);
+                    v.w += __uint_as_float(im[2 * k + 1]) + __uint_as_float(cim[2 * k + 1]);
+                    a4[k] = v;
                 }
             }
             tc_fence_before();
-            mbar_arrive(&sm.seg_empty[buf]);
+            mbar_arrive(&sm.seg_empty);
             return true;
         };
         PieceIter it(plan, k_cta);
         int cg, blk, tb, te;
         bool first_piece = true;
+        const float2 m1 = make_float2(-1.f, -1.f);
         while (ok && it.next(plan, cg, blk, tb, te))
         {
-            const int i = blk * TC_M + q * 32 + lane;
-            float x0 = 0.f, x1 = 0.f, x2 = 0.f, n0 = 0.f, n1 = 0.f, n2 = 0.f;
+            const int i = blk * TC_M + row;
+            // -x_i and nu_i as broadcast pairs
+            float2 nx0 = make_float2(0.f, 0.f), nx1 = nx0, nx2 = nx0, tn0 = nx0, tn1 = nx0, tn2 = nx0;
             if (i < n)
             {
                 const float4 m = reinterpret_cast<const float4 *>(mid4)[i];
-                x0 = m.x; x1 = m.y; x2 = m.z;
+                nx0 = make_float2(-m.x, -m.x); nx1 = make_float2(-m.y, -m.y); nx2 = make_float2(-m.z, -m.z);
                 if (ADL)
                 {
                     const float4 v = reinterpret_cast<const float4 *>(nrm4)[i];
-                    n0 = v.x; n1 = v.y; n2 = v.z;
+                    tn0 = make_float2(v.x, v.x); tn1 = make_float2(v.y, v.y); tn2 = make_float2(v.z, v.z);
                 }
             }
-            #pragma unroll
-            for (int c = 0; c < CH; ++c)
-                #pragma unroll
-                for (int k = 0; k < 8; ++k) racc[c][k] = make_float2(0.f, 0.f);
+            bool first_drain = true;
+            // A finished segment is drained right after the next segment's first
+            // step is queued, so the tensor core has work waiting when it resumes.
+            int drain_due = -1;
             for (int t = tb; t < te; ++t, ++T)
             {
                 const int rs = T % TC_RSTAGES;
@@ -384,112 +493,177 @@ boundary_tc_kernel(const float *__restrict__ mid4, const float *__restrict__ nrm
                     const bool got = wait_bar(&sm.r_full[rs], (uint32_t)(T / TC_RSTAGES) & 1u, abort_flag, err, 1);
                     if (!__all_sync(0xffffffffu, got)) { ok = false; break; }
                 }
-                // per source: 1/r, r, (z.mu_j)/r^2, (z.nu_i)/r^2; shared by every chunk
-                float rinv[8], r[8], dmu[8], dnu[8];
-                #pragma unroll
-                for (int s8 = 0; s8 < 8; ++s8)
+                // per source pair: 1/r, r, (z.mu_j)/r^3, (z.nu_i)/r^3; shared by every chunk
+                float2 rinv[4], r[4], dmu[4], dnu[4];
                 {
-                    const int sl = g * 8 + s8, j = t * TC_SRC + sl;
-                    // rows past the end were not copied: never read them
-                    const bool inside = j < n;
-                    const float4 y = inside ? sm.raw[rs].y[sl] : make_float4(x0, x1, x2, 0.f);
-                    const float zx = y.x - x0, zy = y.y - x1, zz = y.z - x2;
-                    const bool valid = inside && (j != i);
-                    const float r2 = zx * zx + zy * zy + zz * zz;
-                    rinv[s8] = valid ? rsqrtf(r2) : 0.f;
-                    r[s8] = r2 * rinv[s8];
-                    const float rinv2 = rinv[s8] * rinv[s8];
-                    if (DL)
+                    const TcTileGeo &G = sm.raw[rs].geo;
+                    // tiles that hold the target itself or padding past the end need masks
+                    const bool special = (t == ntiles - 1) || (t * TC_SRC < blk * TC_M + TC_M && t * TC_SRC + TC_SRC > blk * TC_M);
+                    #pragma unroll
+                    for (int p = 0; p < 4; ++p)
                     {
-                        const float4 mu = inside ? sm.raw[rs].mu[sl] : make_float4(0.f, 0.f, 0.f, 0.f);
-                        dmu[s8] = (zx * mu.x + zy * mu.y + zz * mu.z) * rinv2;
+                        const int sl = g * 8 + 2 * p;
+                        const float2 zx = __fadd2_rn(*reinterpret_cast<const float2 *>(&G.x[sl]), nx0);
+                        const float2 zy = __fadd2_rn(*reinterpret_cast<const float2 *>(&G.y[sl]), nx1);
+                        const float2 zz = __fadd2_rn(*reinterpret_cast<const float2 *>(&G.z[sl]), nx2);
+                        const float2 r2 = __ffma2_rn(zz, zz, __ffma2_rn(zy, zy, __fmul2_rn(zx, zx)));
+                        float ri0 = rsqrtf(r2.x), ri1 = rsqrtf(r2.y);
+                        if (special)
+                        {
+                            const int j = t * TC_SRC + sl;
+                            if (!(j < n && j != i)) ri0 = 0.f;
+                            if (!(j + 1 < n && j + 1 != i)) ri1 = 0.f;
+                        }
+                        rinv[p] = make_float2(ri0, ri1);
+                        r[p] = __fmul2_rn(r2, rinv[p]);
+                        const float2 ri3 = __fmul2_rn(__fmul2_rn(rinv[p], rinv[p]), rinv[p]);
+                        if (DL)
+                        {
+                            const float2 mx = *reinterpret_cast<const float2 *>(&G.mx[sl]);
+                            const float2 my = *reinterpret_cast<const float2 *>(&G.my[sl]);
+                            const float2 mz = *reinterpret_cast<const float2 *>(&G.mz[sl]);
+                            dmu[p] = __fmul2_rn(__ffma2_rn(zz, mz, __ffma2_rn(zy, my, __fmul2_rn(zx, mx))), ri3);
+                        }
+                        if (ADL) dnu[p] = __fmul2_rn(__ffma2_rn(zz, tn2, __ffma2_rn(zy, tn1, __fmul2_rn(zx, tn0))), ri3);
                     }
-                    if (ADL) dnu[s8] = (zx * n0 + zy * n1 + zz * n2) * rinv2;
                 }
                 mbar_arrive(&sm.r_empty[rs]);
-                for (int c = 0; c < CH; ++c)
+                // not unrolled: the step body is large, and two copies of it
+                // overflow the instruction cache
+                #pragma unroll 1
+                for (int c0 = 0; c0 < CH; c0 += CC)
                 {
-                    const float4 p0 = sm.prm[cg * CH + c][0], p1 = sm.prm[cg * CH + c][1];
-                    const float kap = p0.x;
-                    const float c1x = p0.y, c1y = p0.z, c2x = p0.w, c2y = p1.x, c3x = p1.y, c3y = p1.z;
-                    uint32_t hi[16], lo[16];
+                    // test the A stages this step fills now; the answer arrives during the math
+                    int stage[CC];
+                    bool ready[CC];
                     #pragma unroll
-                    for (int s8 = 0; s8 < 8; ++s8)
+                    for (int k = 0; k < CC; ++k)
                     {
-                        // A = e^{i k r} g / r,  g = c1 + w (i k r - 1),  w = (c2 (z.mu_j) - c3 (z.nu_i)) / r^2
-                        const float kr = kap * r[s8];
-                        float sn, cs;
-                        __sincosf(kr, &sn, &cs);
-                        float gx = SL ? c1x : 0.f, gy = SL ? c1y : 0.f;
-                        if (DL || ADL)
-                        {
-                            float wx = 0.f, wy = 0.f;
-                            if (DL) { wx = c2x * dmu[s8]; wy = c2y * dmu[s8]; }
-                            if (ADL) { wx -= c3x * dnu[s8]; wy -= c3y * dnu[s8]; }
-                            gx = gx - wx - kr * wy;
-                            gy = gy - wy + kr * wx;
-                        }
-                        const float tx = gx * rinv[s8], ty = gy * rinv[s8];
-                        const float ax = cs * tx - sn * ty;
-                        const float ay = sn * tx + cs * ty;
-                        split_tf32(ax, hi[2 * s8], lo[2 * s8]);
-                        split_tf32(ay, hi[2 * s8 + 1], lo[2 * s8 + 1]);
+                        const int u = T * CH + c0 + k;
+                        stage[k] = u % TC_ASTAGES;
+                        ready[k] = u < TC_ASTAGES ||
+                                   mbar_test_wait(&sm.a_empty[stage[k]], (uint32_t)((u / TC_ASTAGES) - 1) & 1u);
                     }
-                    // publish the previous stage now that its stores had this chunk's math to land
+                    uint32_t hi[CC][16], lo[CC][16];
+                    #pragma unroll
+                    for (int k = 0; k < CC; ++k)
+                    {
+                        const float2 *P = sm.prm[cg * CH + c0 + k];
+                        const float2 kap = P[0], nkap = P[1], c1x = P[2], c1y = P[3];
+                        const float2 nc2x = P[4], nc2y = P[5], c3x = P[6], c3y = P[7];
+                        #pragma unroll
+                        for (int p = 0; p < 4; ++p)
+                        {
+                            // A = e^{i k r} h,  h = c1 / r + w (i k r - 1) = c1 / r + u + i k r (-u),  u = -w
+                            //   hx = c1x / r + ux + k r uy,   hy = c1y / r + uy - k r ux
+                            const float2 kr = __fmul2_rn(kap, r[p]);
+                            float sn0, cs0, sn1, cs1;
+                            __sincosf(kr.x, &sn0, &cs0);
+                            __sincosf(kr.y, &sn1, &cs1);
+                            const float2 cs = make_float2(cs0, cs1), sn = make_float2(sn0, sn1);
+                            float2 hx = make_float2(0.f, 0.f), hy = make_float2(0.f, 0.f);
+                            if (SL)
+                            {
+                                hx = __fmul2_rn(c1x, rinv[p]);
+                                hy = __fmul2_rn(c1y, rinv[p]);
+                            }
+                            if (DL || ADL)
+                            {
+                                float2 ux = make_float2(0.f, 0.f), uy = make_float2(0.f, 0.f);
+                                if (DL) { ux = __fmul2_rn(nc2x, dmu[p]); uy = __fmul2_rn(nc2y, dmu[p]); }
+                                if (ADL) { ux = __ffma2_rn(c3x, dnu[p], ux); uy = __ffma2_rn(c3y, dnu[p], uy); }
+                                const float2 nkr = __fmul2_rn(nkap, r[p]);
+                                hx = __ffma2_rn(kr, uy, __fadd2_rn(hx, ux));
+                                hy = __ffma2_rn(nkr, ux, __fadd2_rn(hy, uy));
+                            }
+                            // (ax, ay) = (hx cs - hy sn, hx sn + hy cs)
+                            const float2 msn = __fmul2_rn(m1, sn);
+                            const float2 ax = __ffma2_rn(hy, msn, __fmul2_rn(hx, cs));
+                            const float2 ay = __ffma2_rn(hy, cs, __fmul2_rn(hx, sn));
+                            // hi = the FP32 bits (read as TF32 by the tensor core), lo = x - trunc_tf32(x)
+                            const float2 tx = make_float2(__uint_as_float(__float_as_uint(ax.x) & 0xffffe000u),
+                                                          __uint_as_float(__float_as_uint(ax.y) & 0xffffe000u));
+                            const float2 ty = make_float2(__uint_as_float(__float_as_uint(ay.x) & 0xffffe000u),
+                                                          __uint_as_float(__float_as_uint(ay.y) & 0xffffe000u));
+                            const float2 lx = __ffma2_rn(tx, m1, ax), ly = __ffma2_rn(ty, m1, ay);
+                            hi[k][4 * p + 0] = __float_as_uint(ax.x);
+                            hi[k][4 * p + 1] = __float_as_uint(ax.y);
+                            hi[k][4 * p + 2] = __float_as_uint(ay.x);
+                            hi[k][4 * p + 3] = __float_as_uint(ay.y);
+                            lo[k][4 * p + 0] = __float_as_uint(lx.x);
+                            lo[k][4 * p + 1] = __float_as_uint(lx.y);
+                            lo[k][4 * p + 2] = __float_as_uint(ly.x);
+                            lo[k][4 * p + 3] = __float_as_uint(ly.y);
+                        }
+                    }
+                    // publish the previous step's stages now that their stores had this step's math to land
                     publish();
-                    const int u = T * CH + c;
-                    const int stage = u % TC_ASTAGES;
-                    bool got = true;
-                    if (u >= TC_ASTAGES)
-                        got = wait_bar(&sm.a_empty[stage], (uint32_t)((u / TC_ASTAGES) - 1) & 1u, abort_flag, err, 3);
+                    #pragma unroll
+                    for (int k = 0; k < CC; ++k)
+                        if (!ready[k])
+                        {
+                            const int u = T * CH + c0 + k;
+                            ready[k] = wait_bar(&sm.a_empty[stage[k]], (uint32_t)((u / TC_ASTAGES) - 1) & 1u,
+                                                abort_flag, err, 3);
+                        }
                     // the tcgen05 stores below are warp-collective: the warp agrees on the outcome
-                    if (!__all_sync(0xffffffffu, got)) { ok = false; break; }
+                    bool all = true;
+                    #pragma unroll
+                    for (int k = 0; k < CC; ++k) all = all && ready[k];
+                    if (!__all_sync(0xffffffffu, all)) { ok = false; break; }
                     tc_fence_after();
-                    const uint32_t acol = TC_ACOL + (uint32_t)stage * 64u + (uint32_t)g * 16u;
-                    tmem_st16(lane_addr + acol, hi);
-                    tmem_st16(lane_addr + acol + 32u, lo);
-                    pending = stage;
+                    #pragma unroll
+                    for (int k = 0; k < CC; ++k)
+                    {
+                        const uint32_t acol = TC_ACOL + (uint32_t)stage[k] * 64u + (uint32_t)g * 16u;
+                        tmem_st16(lane_addr + acol, hi[k]);
+                        tmem_st16(lane_addr + acol + 32u, lo[k]);
+                        pending[k] = stage[k];
+                    }
+                    npending = CC;
+                    if (drain_due >= 0)
+                    {
+                        publish();
+                        if (!drain(drain_due, first_drain)) { ok = false; break; }
+                        first_drain = false;
+                        drain_due = -1;
+                    }
                 }
                 if (!ok) break;
                 const int lt = t - tb;
                 if (lt % S == S - 1 || t == te - 1)
                 {
-                    // segment SG finished generating: drain the previous one of this piece
-                    publish();
-                    if (lt >= S && !drain(SG - 1)) { ok = false; break; }
-                    if (t == te - 1 && !drain(SG)) { ok = false; break; }
+                    // segment SG finished generating
+                    if (t == te - 1)
+                    {
+                        publish();
+                        if (!drain(SG, first_drain)) { ok = false; break; }
+                        first_drain = false;
+                    }
+                    else
+                        drain_due = SG;
                     ++SG;
                 }
             }
             if (!ok) break;
             // ------------------------------ piece epilogue ------------------------------
             const int cw = CH * 16;
+            float2 *dst = nullptr;
             if (tb == 0 && te == ntiles)
             {
-                if (i < n)
-                {
-                    #pragma unroll
-                    for (int c = 0; c < CH; ++c)
-                    {
-                        float4 *out = reinterpret_cast<float4 *>(&Ctri[(int64_t)i * wc + cg * cw + c * 16 + g * 8]);
-                        #pragma unroll
-                        for (int k = 0; k < 8; k += 2)
-                            out[k / 2] = make_float4(racc[c][k].x, racc[c][k].y, racc[c][k + 1].x, racc[c][k + 1].y);
-                    }
-                }
+                if (i < n) dst = &Ctri[(int64_t)i * wc + cg * cw];
             }
             else
+                dst = &ws[((int64_t)(k_cta * 2 + (first_piece ? 0 : 1)) * TC_M + row) * (TC_CHMAX * 16)];
+            if (dst)
             {
-                const int slot = first_piece ? 0 : 1;
-                const int row = q * 32 + lane;
                 #pragma unroll
                 for (int c = 0; c < CH; ++c)
                 {
-                    float4 *out = reinterpret_cast<float4 *>(
-                        &ws[((int64_t)(k_cta * 2 + slot) * TC_M + row) * (TC_CHMAX * 16) + c * 16 + g * 8]);
+                    const float4 *a4 = reinterpret_cast<const float4 *>(acc_row + c * 16);
+                    float4 *out = reinterpret_cast<float4 *>(dst + c * 16 + g * 8);
                     #pragma unroll
-                    for (int k = 0; k < 8; k += 2)
-                        out[k / 2] = make_float4(racc[c][k].x, racc[c][k].y, racc[c][k + 1].x, racc[c][k + 1].y);
+                    for (int k = 0; k < 4; ++k) out[k] = a4[k];
                 }
             }
             first_piece = false;
@@ -512,9 +686,9 @@ boundary_tc_kernel(const float *__restrict__ mid4, const float *__restrict__ nrm
             for (int t = tb; t < te; ++t, ++T)
             {
                 const int rs = T % TC_RSTAGES, b = T % TC_BSTAGES;
-                if (!wait_bar(&sm.r_full[rs], (uint32_t)(T / TC_RSTAGES) & 1u, abort_flag, err, 4)) { ok = false; break; }
+                if (!wait_bar_sleepy(&sm.r_full[rs], (uint32_t)(T / TC_RSTAGES) & 1u, abort_flag, err, 4)) { ok = false; break; }
                 if (T >= TC_BSTAGES &&
-                    !wait_bar(&sm.b_empty[b], (uint32_t)((T / TC_BSTAGES) - 1) & 1u, abort_flag, err, 5))
+                    !wait_bar_sleepy(&sm.b_empty[b], (uint32_t)((T / TC_BSTAGES) - 1) & 1u, abort_flag, err, 5))
                 {
                     ok = false;
                     break;
@@ -535,11 +709,11 @@ boundary_tc_kernel(const float *__restrict__ mid4, const float *__restrict__ nrm
                     constexpr uint32_t sgn = 0x80000000u;
                     uint8_t *hi_img = sm.img[b][c][0];
                     uint8_t *lo_img = sm.img[b][c][1];
-                    // row qq: (re, -im) per source; row qq + 16: (im, re)
-                    *reinterpret_cast<uint4 *>(hi_img + img_off16(qq, sp)) = make_uint4(hr0, hi0 ^ sgn, hr1, hi1 ^ sgn);
-                    *reinterpret_cast<uint4 *>(lo_img + img_off16(qq, sp)) = make_uint4(lr0, li0 ^ sgn, lr1, li1 ^ sgn);
-                    *reinterpret_cast<uint4 *>(hi_img + img_off16(qq + 16, sp)) = make_uint4(hi0, hr0, hi1, hr1);
-                    *reinterpret_cast<uint4 *>(lo_img + img_off16(qq + 16, sp)) = make_uint4(li0, lr0, li1, lr1);
+                    // row qq (real part of C): (Re b0, Re b1, -Im b0, -Im b1); row qq + 16: (Im b0, Im b1, Re b0, Re b1)
+                    *reinterpret_cast<uint4 *>(hi_img + img_off16(qq, sp)) = make_uint4(hr0, hr1, hi0 ^ sgn, hi1 ^ sgn);
+                    *reinterpret_cast<uint4 *>(lo_img + img_off16(qq, sp)) = make_uint4(lr0, lr1, li0 ^ sgn, li1 ^ sgn);
+                    *reinterpret_cast<uint4 *>(hi_img + img_off16(qq + 16, sp)) = make_uint4(hi0, hi1, hr0, hr1);
+                    *reinterpret_cast<uint4 *>(lo_img + img_off16(qq + 16, sp)) = make_uint4(li0, li1, lr0, lr1);
                 }
                 asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
                 mbar_arrive(&sm.r_empty[rs]);
@@ -550,29 +724,28 @@ boundary_tc_kernel(const float *__restrict__ mid4, const float *__restrict__ nrm
     else if (warp == (TC_GEN_THREADS + TC_EXP_THREADS) / 32)
     {
         // ------------------------------ bulk-copy producer ------------------------------
-        if (lane == 0)
+        const int cw = CH * 16;
+        const uint32_t row_bytes = (uint32_t)(cw * sizeof(float2));
+        PieceIter it(plan, k_cta);
+        int cg, blk, tb, te, T = 0;
+        bool ok = true;
+        while (ok && it.next(plan, cg, blk, tb, te))
         {
-            const int cw = CH * 16;
-            const uint32_t row_bytes = (uint32_t)(cw * sizeof(float2));
-            PieceIter it(plan, k_cta);
-            int cg, blk, tb, te, T = 0;
-            bool ok = true;
-            while (ok && it.next(plan, cg, blk, tb, te))
+            for (int t = tb; t < te; ++t, ++T)
             {
-                for (int t = tb; t < te; ++t, ++T)
+                const int rs = T % TC_RSTAGES;
+                if (T >= TC_RSTAGES)
                 {
-                    const int rs = T % TC_RSTAGES;
-                    if (T >= TC_RSTAGES &&
-                        !wait_bar(&sm.r_empty[rs], (uint32_t)((T / TC_RSTAGES) - 1) & 1u, abort_flag, err, 6))
-                    {
-                        ok = false;
-                        break;
-                    }
+                    const bool got =
+                        wait_bar_sleepy(&sm.r_empty[rs], (uint32_t)((T / TC_RSTAGES) - 1) & 1u, abort_flag, err, 6);
+                    if (!__all_sync(0xffffffffu, got)) { ok = false; break; }
+                }
+                if (elect_one())
+                {
                     const int j0 = t * TC_SRC;
                     const int rows = min(TC_SRC, n - j0);
-                    mbar_expect_tx(&sm.r_full[rs], (uint32_t)rows * (row_bytes + 32u));
-                    bulk_g2s(sm.raw[rs].y, mid4 + 4 * (int64_t)j0, (uint32_t)rows * 16u, &sm.r_full[rs]);
-                    bulk_g2s(sm.raw[rs].mu, nrm4 + 4 * (int64_t)j0, (uint32_t)rows * 16u, &sm.r_full[rs]);
+                    mbar_expect_tx(&sm.r_full[rs], (uint32_t)rows * row_bytes + (uint32_t)sizeof(TcTileGeo));
+                    bulk_g2s(&sm.raw[rs].geo, tgeo + t, (uint32_t)sizeof(TcTileGeo), &sm.r_full[rs]);
                     // one contiguous block when the tile's rows are whole B_tri rows of
                     // exactly the raw row width; otherwise one copy per row
                     if (CH == TC_CHMAX && cw == wc)
@@ -582,12 +755,14 @@ boundary_tc_kernel(const float *__restrict__ mid4, const float *__restrict__ nrm
                             bulk_g2s(sm.raw[rs].b[sl], Btri + (int64_t)(j0 + sl) * wc + cg * cw, row_bytes,
                                      &sm.r_full[rs]);
                 }
+                __syncwarp();
             }
         }
     }
-    else if (lane == 0)
+    else
     {
         // ------------------------------ MMA issuer ------------------------------
+        // The whole warp runs the loop and waits; one elected lane issues.
         bool ok = true;
         int T = 0, SG = 0;
         PieceIter it(plan, k_cta);
@@ -598,55 +773,58 @@ boundary_tc_kernel(const float *__restrict__ mid4, const float *__restrict__ nrm
             {
                 const int b = T % TC_BSTAGES;
                 const int lt = t - tb;
-                const int buf = SG & 1;
                 const bool first = (lt % S) == 0;
-                if (!wait_bar(&sm.b_full[b], (uint32_t)(T / TC_BSTAGES) & 1u, abort_flag, err, 7)) { ok = false; break; }
-                if (first && SG >= 2 &&
-                    !wait_bar(&sm.seg_empty[buf], (uint32_t)((SG >> 1) - 1) & 1u, abort_flag, err, 8))
                 {
-                    ok = false;
-                    break;
+                    bool got = wait_bar(&sm.b_full[b], (uint32_t)(T / TC_BSTAGES) & 1u, abort_flag, err, 7);
+                    // a new segment overwrites the accumulator: the previous one must be drained
+                    if (got && first && SG >= 1)
+                        got = wait_bar(&sm.seg_empty, (uint32_t)(SG - 1) & 1u, abort_flag, err, 8);
+                    if (!__all_sync(0xffffffffu, got)) { ok = false; break; }
                 }
                 for (int c = 0; c < CH; ++c)
                 {
                     const int u = T * CH + c;
                     const int stage = u % TC_ASTAGES;
-                    if (!wait_bar(&sm.a_full[stage], (uint32_t)(u / TC_ASTAGES) & 1u, abort_flag, err, 9))
-                    {
-                        ok = false;
-                        break;
-                    }
+                    const bool got = wait_bar(&sm.a_full[stage], (uint32_t)(u / TC_ASTAGES) & 1u, abort_flag, err, 9);
+                    if (!__all_sync(0xffffffffu, got)) { ok = false; break; }
                     tc_fence_after();
-                    const uint32_t d = tbase + (uint32_t)buf * TC_ACC_COLS + (uint32_t)(c * TC_N);
+                    const uint32_t d = tbase + (uint32_t)(c * TC_DCOLS);
                     const uint32_t a_hi = tbase + TC_ACOL + (uint32_t)stage * 64u;
                     const uint32_t a_lo = a_hi + 32u;
-                    const uint64_t b_hi = sw128_desc(sm.img[b][c][0]);
-                    const uint64_t b_lo = sw128_desc(sm.img[b][c][1]);
-                    #pragma unroll
-                    for (int ks = 0; ks < 4; ++ks)
+                    // the hi image's 32 rows are followed by the lo image's 32 rows
+                    // (same 1024-byte group stride): one N = 64 operand [Bhi | Blo]
+                    const uint64_t b_hilo = sw128_desc(sm.img[b][c][0]);
+                    if (elect_one())
                     {
-                        const uint64_t koff = (uint64_t)(ks * 32 >> 4);
-                        mma_tf32(d, a_lo + 8u * ks, b_hi + koff, (!first || ks > 0) ? 1u : 0u);
-                        mma_tf32(d, a_hi + 8u * ks, b_lo + koff, 1u);
-                        mma_tf32(d, a_hi + 8u * ks, b_hi + koff, 1u);
+                        #pragma unroll
+                        for (int ks = 0; ks < 4; ++ks)
+                        {
+                            const uint64_t koff = (uint64_t)(ks * 32 >> 4);
+                            // [main | corr] (+)= Ahi [Bhi | Blo];  corr += Alo Bhi
+                            mma_tf32(d, a_hi + 8u * ks, b_hilo + koff, (!first || ks > 0) ? 1u : 0u,
+                                     idesc_tf32(2 * TC_N));
+                            mma_tf32(d + (uint32_t)TC_N, a_lo + 8u * ks, b_hilo + koff, 1u, idesc_tf32(TC_N));
+                        }
+                        mma_commit(&sm.a_empty[stage]);
                     }
-                    mma_commit(&sm.a_empty[stage]);
+                    __syncwarp();
                 }
                 if (!ok) break;
-                mma_commit(&sm.b_empty[b]);
-                if (lt % S == S - 1 || t == te - 1)
+                if (elect_one())
                 {
-                    mma_commit(&sm.seg_full[buf]);
-                    ++SG;
+                    mma_commit(&sm.b_empty[b]);
+                    if (lt % S == S - 1 || t == te - 1) mma_commit(&sm.seg_full);
                 }
+                __syncwarp();
+                if (lt % S == S - 1 || t == te - 1) ++SG;
             }
         }
         if (!ok)
         {
             // wait (bounded) for the MMAs already issued before the TMEM is freed
-            const int buf = SG & 1;
-            mma_commit(&sm.seg_full[buf]);
-            wait_bar(&sm.seg_full[buf], (uint32_t)((SG >> 1) & 1), abort_flag, err, 10, false);
+            if (elect_one()) mma_commit(&sm.seg_full);
+            __syncwarp();
+            wait_bar(&sm.seg_full, (uint32_t)SG & 1u, abort_flag, err, 10, false);
         }
     }
 
@@ -657,6 +835,25 @@ boundary_tc_kernel(const float *__restrict__ mid4, const float *__restrict__ nrm
         tc_fence_after();
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tbase), "r"(TC_TMEM_COLS) : "memory");
     }
+}
+
+// Midpoints and normals of each 16-source tile as structure of arrays (zeros
+// past the last triangle).
+__global__ void tc_tile_geometry_kernel(const float *__restrict__ mid4, const float *__restrict__ nrm4,
+                                        TcTileGeo *__restrict__ out, int n, int ntiles)
+{
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= ntiles * TC_SRC) return;
+    const int t = e / TC_SRC, s = e - t * TC_SRC;
+    float4 m = make_float4(0.f, 0.f, 0.f, 0.f), v = m;
+    if (e < n)
+    {
+        m = reinterpret_cast<const float4 *>(mid4)[e];
+        v = reinterpret_cast<const float4 *>(nrm4)[e];
+    }
+    TcTileGeo &G = out[t];
+    G.x[s] = m.x; G.y[s] = m.y; G.z[s] = m.z;
+    G.mx[s] = v.x; G.my[s] = v.y; G.mz[s] = v.z;
 }
 
 // Adds the workspace slots of every target block that was split between CTAs,
@@ -685,8 +882,8 @@ __global__ void tc_fixup_kernel(const float2 *__restrict__ ws, float2 *__restric
 }
 
 template <int CH, bool SL, bool DL, bool ADL>
-void tc_launch(cudaStream_t st, const float *mid, const float *nrm, const float2 *B, float2 *C, float2 *ws,
-               const ChunkParamsF *p, const TcPlan &plan, int *err)
+void tc_launch(cudaStream_t st, const float *mid, const float *nrm, const TcTileGeo *tg, const float2 *B, float2 *C,
+               float2 *ws, const ChunkParamsF *p, const TcPlan &plan, int *err)
 {
     // More than half of the SM's shared memory, so one CTA per SM: the CTA
     // allocates all 512 TMEM columns and a second resident CTA would only wait.
@@ -698,22 +895,22 @@ void tc_launch(cudaStream_t st, const float *mid, const float *nrm, const float2
                                     (int)bytes);
     });
     BAEMM_CUDA(attr);
-    boundary_tc_kernel<CH, SL, DL, ADL><<<plan.ctas, TC_THREADS, bytes, st>>>(mid, nrm, B, C, ws, p, plan, err);
+    boundary_tc_kernel<CH, SL, DL, ADL><<<plan.ctas, TC_THREADS, bytes, st>>>(mid, nrm, tg, B, C, ws, p, plan, err);
 }
 
 template <int CH>
-void tc_flags(int code, cudaStream_t st, const float *mid, const float *nrm, const float2 *B, float2 *C, float2 *ws,
-              const ChunkParamsF *p, const TcPlan &plan, int *err)
+void tc_flags(int code, cudaStream_t st, const float *mid, const float *nrm, const TcTileGeo *tg, const float2 *B,
+              float2 *C, float2 *ws, const ChunkParamsF *p, const TcPlan &plan, int *err)
 {
     switch (code)
     {
-        case 1: tc_launch<CH, true, false, false>(st, mid, nrm, B, C, ws, p, plan, err); break;
-        case 2: tc_launch<CH, false, true, false>(st, mid, nrm, B, C, ws, p, plan, err); break;
-        case 3: tc_launch<CH, true, true, false>(st, mid, nrm, B, C, ws, p, plan, err); break;
-        case 4: tc_launch<CH, false, false, true>(st, mid, nrm, B, C, ws, p, plan, err); break;
-        case 5: tc_launch<CH, true, false, true>(st, mid, nrm, B, C, ws, p, plan, err); break;
-        case 6: tc_launch<CH, false, true, true>(st, mid, nrm, B, C, ws, p, plan, err); break;
-        case 7: tc_launch<CH, true, true, true>(st, mid, nrm, B, C, ws, p, plan, err); break;
+        case 1: tc_launch<CH, true, false, false>(st, mid, nrm, tg, B, C, ws, p, plan, err); break;
+        case 2: tc_launch<CH, false, true, false>(st, mid, nrm, tg, B, C, ws, p, plan, err); break;
+        case 3: tc_launch<CH, true, true, false>(st, mid, nrm, tg, B, C, ws, p, plan, err); break;
+        case 4: tc_launch<CH, false, false, true>(st, mid, nrm, tg, B, C, ws, p, plan, err); break;
+        case 5: tc_launch<CH, true, false, true>(st, mid, nrm, tg, B, C, ws, p, plan, err); break;
+        case 6: tc_launch<CH, false, true, true>(st, mid, nrm, tg, B, C, ws, p, plan, err); break;
+        case 7: tc_launch<CH, true, true, true>(st, mid, nrm, tg, B, C, ws, p, plan, err); break;
         default: break;
     }
 }
@@ -740,9 +937,20 @@ size_t tc_workspace_elems(int ctas)
     return (size_t)ctas * 2 * TC_M * TC_CHMAX * 16;
 }
 
+size_t tc_tile_geometry_floats(int64_t nt) { return (size_t)ceil_div(nt, TC_SRC) * (sizeof(TcTileGeo) / sizeof(float)); }
+
+void launch_tc_tile_geometry(const MeshDev &m, float *tgeo, cudaStream_t st)
+{
+    if (m.nt == 0) return;
+    const int n = (int)m.nt, ntiles = ceil_div(n, TC_SRC);
+    tc_tile_geometry_kernel<<<ceil_div((int64_t)ntiles * TC_SRC, 256), 256, 0, st>>>(
+        m.mid_f, m.nrm_f, reinterpret_cast<TcTileGeo *>(tgeo), n, ntiles);
+    BAEMM_LAUNCH_CHECK();
+}
+
 void launch_boundary_tc(const MeshDev &m, const OpFlags &f, const void *chunk_params, int wc, int wcs,
-                        const float2 *Btri, float2 *Ctri, float2 *ws, size_t ws_elems, int *err, cudaStream_t st,
-                        int seg_tiles, int ctas)
+                        const float *tgeo, const float2 *Btri, float2 *Ctri, float2 *ws, size_t ws_elems, int *err,
+                        cudaStream_t st, int seg_tiles, int ctas)
 {
     BAEMM_REQUIRE(tc_supported(wc, wcs), BAEMM_ERR_SIZE,
                   "tensor-core apply needs wave_chunk_size 16 and wave_count <= 512");
@@ -762,9 +970,11 @@ void launch_boundary_tc(const MeshDev &m, const OpFlags &f, const void *chunk_pa
     const int code = (f.sl() ? 1 : 0) | (f.dl() ? 2 : 0) | (f.adl() ? 4 : 0);
     const auto *p = static_cast<const ChunkParamsF *>(chunk_params);
     const float *mid = m.mid_f, *nrm = m.nrm_f;
-    if (CH == 4) tc_flags<4>(code, st, mid, nrm, Btri, Ctri, ws, p, plan, err);
-    else if (CH == 2) tc_flags<2>(code, st, mid, nrm, Btri, Ctri, ws, p, plan, err);
-    else tc_flags<1>(code, st, mid, nrm, Btri, Ctri, ws, p, plan, err);
+    const auto *tg = reinterpret_cast<const TcTileGeo *>(tgeo);
+    BAEMM_REQUIRE(tg, BAEMM_ERR_ARG, "tensor-core tile geometry missing");
+    if (CH == 4) tc_flags<4>(code, st, mid, nrm, tg, Btri, Ctri, ws, p, plan, err);
+    else if (CH == 2) tc_flags<2>(code, st, mid, nrm, tg, Btri, Ctri, ws, p, plan, err);
+    else tc_flags<1>(code, st, mid, nrm, tg, Btri, Ctri, ws, p, plan, err);
     BAEMM_LAUNCH_CHECK();
     tc_fixup_kernel<<<plan.ncg * plan.nblk, 256, 0, st>>>(ws, Ctri, plan, CH * 16);
     BAEMM_LAUNCH_CHECK();
