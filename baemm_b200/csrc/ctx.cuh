@@ -47,7 +47,7 @@ public:
     int gmres_max_iter = 30, gmres_max_restarts = 3;
     int apply_mode = BAEMM_APPLY_FP32;
     int dense_variant = 0;            // plain FP32 dense kernel variant (launch_boundary_dense)
-    int tc_seg_tiles = 4;             // tensor-core form: tiles per TMEM partial sum
+    int tc_seg_tiles = 16;            // tensor-core form: tiles per TMEM partial sum
     int tc_ctas = 0;                  // tensor-core form: persistent grid size (0 = one CTA per SM)
     DevBuf<float2> tc_ws;             // tensor-core form: partial sums of target blocks split between CTAs
     bool tc_geo_ready = false;        // mesh.tgeo_f built

@@ -10,12 +10,16 @@ with major radius 1.0 and minor radius 0.4 on a 160 x 480 parametric grid,
 singular SL diagonal.  Interactions per apply I = N_t * N_s * wave_count.
 
   value  device time of the apply (AvOp, dense kernel, AvOp^T epilogue) with
-         inputs resident in HBM, L2 flushed (256 MiB write) before every step
+         inputs resident in HBM, L2 flushed (256 MiB write) before every step;
+         default arithmetic: the compensated tensor-core form (TF32 hi+lo
+         operands, FP32 accumulation); --mode fp32 is the plain SIMT form
+  compare  the plain FP32 apply timed the same way, and both forms' relative
+         error against the FP64 apply of the same inputs (Frobenius norm)
   e2e    the same apply through the host-pointer C ABI call
          (baemm_apply_boundary_operators_c) from pinned host memory,
          host->device and device->host copies inside the timed region
 
-  python bench.py [--gpus N] [--steps K] [--warmup W] [--mode fp32|fp64]
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--mode tc|fp32|fp64]
   python bench.py --impl reference ...   # the reference's own kernel on the host cores
 
 Multi-GPU (torchrun, one process per GPU): independent replicas of the same
@@ -69,12 +73,13 @@ def load_peaks():
     return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0, "source": "of fallback"}
 
 
-def load_traffic():
-    """Per-launch DRAM bytes of the dense kernel from the committed ncu summary, if any."""
-    p = os.path.join(ROOT, "profiles", "boundary_dense_torus.json")
+def load_traffic(mode):
+    """Per-launch DRAM bytes (read + write) of the dense kernel on this workload,
+    from the committed ncu summary (profiles/traffic_torus.json), if any."""
+    p = os.path.join(ROOT, "profiles", "traffic_torus.json")
     if os.path.exists(p):
         try:
-            return json.load(open(p)).get("dram_bytes_per_launch")
+            return json.load(open(p)).get(mode)
         except Exception:
             return None
     return None
@@ -286,6 +291,37 @@ def run_gpu_arm(args, rank, world, local_rank):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2e_total = float(t.item())
     e2e_value = world * inter * args.steps / (e2e_total * 1e-3) / 1e9
+    # ---- plain FP32 form and accuracy against the FP64 apply (rank 0, untimed for value) ----
+    compare = None
+    if rank == 0 and not args.no_compare:
+        H.SetStream(stream.cuda_stream)
+        with torch.cuda.stream(stream):
+            C_mode = Cd.clone()
+            H.SetApplyMode(APPLY_FP64)
+            Bz = Bd.to(torch.complex128)
+            Cz = torch.zeros_like(Bz)
+            H.ApplyBoundaryOperators_PL(1.0, Bz, 0.0, Cz)
+            fp64_ms = H.LastApplyTimes()[1]
+            H.SetApplyMode(APPLY_FP32)
+            Cp = torch.zeros_like(Bd)
+            plain_ms = []
+            for k in range(2):
+                flush.fill_(float(k))
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                H.ApplyBoundaryOperators_PL(1.0, Bd, 0.0, Cp)
+                e1.record(stream)
+                plain_ms.append((e0, e1))
+        torch.cuda.synchronize()
+        H.SetApplyMode(mode)
+        ref = Cz.cpu().numpy()
+        nref = float(np.linalg.norm(ref))
+        err = {args.mode: float(np.linalg.norm(C_mode.cpu().numpy().astype(np.complex128) - ref) / nref),
+               "fp32": float(np.linalg.norm(Cp.cpu().numpy().astype(np.complex128) - ref) / nref)}
+        p_ms = float(np.mean([a.elapsed_time(b) for a, b in plain_ms]))
+        compare = {"plain_fp32_ms_per_step": p_ms, "speedup_vs_plain_fp32": p_ms / (total_ms / args.steps),
+                   "rel_err_vs_fp64": err, "fp64_dense_ms": fp64_ms,
+                   "note": "relative Frobenius error of the apply output against the FP64 apply of the same inputs"}
     H.UnloadBoundaryOperators_PL()
 
     if rank != 0:
@@ -295,13 +331,39 @@ def run_gpu_arm(args, rank, world, local_rank):
     dense_avg = float(np.mean(dense_ms))
     flops = 8.0 * inter
     achieved = flops / (dense_avg * 1e-3) / 1e12
-    traffic = load_traffic()
+    traffic = load_traffic(args.mode)
+    kernel_name = {"tc": "boundary_tc_kernel", "fp32": "boundary_dense_kernel", "fp64": "boundary_dense_kernel<double>"}[args.mode]
     cpu = None
     if world == 1 and not args.no_cpu_baseline:
         cpu = reference_rows_rate(coords, tris, B, target_seconds=float(os.environ.get("BAEMM_REF_SECONDS", "12")))
-    # model bound of the plain FP32 form: contraction FMAs + ~20 FP32 ops per generated entry
+    # Roofline model of the apply (algorithmic work per launch):
+    #   W = 8 I contraction FLOPs, G = N_t N_s n_k kernel evaluations (2 MUFU sincos
+    #   + 20 FP32 FLOPs each) and N_t N_s rsqrt;
+    #   plain form T* = (W + 20 G) / P_fp32,
+    #   tensor-core form T* = max(W / P_tf32, (2 G + N_t N_s) / P_mufu, 20 G / P_fp32).
     n_k = len(KAPPA)
-    fp32_ops = 2.0 * (4.0 * inter) + 20.0 * nt * nt * n_k
+    G = float(nt) * nt * n_k
+    clk_mhz = None
+    cs = clk.summary()
+    if cs.get("sm_mhz"):
+        clk_mhz = cs["sm_mhz"]
+    f_hz = (clk_mhz or 1965.0) * 1e6
+    n_sm = torch.cuda.get_device_properties(torch.cuda.current_device()).multi_processor_count
+    p_fp32 = n_sm * 128 * 2 * f_hz               # FFMA: 128 lanes/SM/clk
+    p_mufu = n_sm * 16 * f_hz                    # MUFU: 16 lanes/SM/clk
+    p_tf32 = peaks["bf16_tflops"] * 1e12 / 2.0   # dense TF32 = half the measured dense BF16 rate
+    terms = {"tensor_tf32_ms": 8.0 * inter / p_tf32 * 1e3, "mufu_ms": (2 * G + float(nt) * nt) / p_mufu * 1e3,
+             "fp32_ms": 20.0 * G / p_fp32 * 1e3}
+    if args.mode == "tc":
+        t_star = max(terms.values())
+        limiter = max(terms, key=terms.get)
+    else:
+        t_star = (8.0 * inter + 20.0 * G) / p_fp32 * 1e3
+        limiter = "fp32_ms"
+    model = {"T_star_ms": t_star, "limiter": limiter, "terms_ms": terms, "frac": t_star / dense_avg,
+             "clock_mhz": clk_mhz or 1965.0,
+             "peaks": "P_fp32 = SMs x 256 FLOP/clk, P_mufu = SMs x 16/clk at the sampled SM clock; "
+                      "P_tf32 = measured dense BF16 / 2"}
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
@@ -311,17 +373,18 @@ def run_gpu_arm(args, rank, world, local_rank):
                    "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
                    "l2": "flushed (256 MiB write) before every timed step",
                    "phase_ms_last": list(H.LastApplyTimes()) if False else None},
-        "roofline": {"bound": "tensor", "kernel": "boundary_dense_kernel", "achieved": achieved,
+        "roofline": {"bound": "tensor", "kernel": kernel_name, "achieved": achieved,
                      "peak": peaks["bf16_tflops"], "unit": "TFLOP/s", "frac": achieved / peaks["bf16_tflops"],
                      "peak_source": peaks["source"] + " (dense bf16 burst)",
-                     "algorithmic": "8 * N_t * N_s * wave_count FLOPs per launch (complex MACs)",
-                     "dense_kernel_ms": dense_avg, "traffic": traffic,
-                     "fp32_model_tflops": fp32_ops / (dense_avg * 1e-3) / 1e12},
+                     "algorithmic": "8 * N_t * N_s * wave_count FLOPs per launch (complex MACs), counted once",
+                     "dense_kernel_ms": dense_avg, "traffic": traffic, "model": model},
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(B.nbytes),
                 "d2h_bytes_per_step": int(B.nbytes), "ms_per_step": e2e_total / args.steps},
         "gpu_launches": int(launches),
         "clocks": clk.summary(),
     }
+    if compare is not None:
+        line["compare"] = compare
     if cpu is not None:
         line["cpu_baseline"] = {"value": cpu["value"], "unit": UNIT, "cores": cpu["cores"], "kind": cpu["kind"],
                                 "sample": cpu["sample"]}
@@ -339,6 +402,7 @@ def main(argv=None):
     ap.add_argument("--mode", default="tc", choices=["fp32", "tc", "fp64"],
                     help="apply arithmetic: plain FP32, compensated tensor-core (default), FP64")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-compare", action="store_true", help="skip the plain-FP32 and FP64 comparison applies")
     ap.add_argument("--small", action="store_true", help="38400-triangle torus (profiling captures only)")
     args = ap.parse_args(argv)
     rank = int(os.environ.get("RANK", "0"))

@@ -123,8 +123,9 @@ int baemm_get_apply_mode(const baemm_ctx *ctx);
  *   BAEMM_TUNE_DENSE_VARIANT  plain FP32 dense kernel: 0 scalar FMA (default),
  *                             1 / 2 packed FP32x2 with 1 / 2 targets per thread
  *   BAEMM_TUNE_TC_SEGMENT     tensor-core form: 16-source tiles accumulated in
- *                             TMEM before each partial sum is added in FP32
- *                             registers (default 4; bounds the accumulation chain)
+ *                             TMEM before each partial sum is added to the FP32
+ *                             sums in shared memory (default 16; bounds the
+ *                             tensor-core accumulation chain)
  *   BAEMM_TUNE_TC_CTAS        tensor-core form: persistent grid size (default 0 =
  *                             one CTA per SM) */
 #define BAEMM_TUNE_DENSE_VARIANT 1
