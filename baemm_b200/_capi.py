@@ -24,6 +24,7 @@ APPLY_FP64 = 2
 TUNE_DENSE_VARIANT = 1
 TUNE_TC_SEGMENT = 2
 TUNE_TC_CTAS = 3
+TUNE_TC_STAGGER = 4
 
 dp = C.POINTER(C.c_double)
 fp = C.POINTER(C.c_float)

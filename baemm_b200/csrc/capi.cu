@@ -328,6 +328,10 @@ int baemm_set_tuning(baemm_ctx *ctx, int key, int value)
                 BAEMM_REQUIRE(value >= 1, BAEMM_ERR_ARG, "segment length must be >= 1");
                 c.tc_seg_tiles = value;
                 break;
+            case BAEMM_TUNE_TC_STAGGER:
+                BAEMM_REQUIRE(value >= -1 && value <= 1 << 20, BAEMM_ERR_ARG, "stagger must be -1 or >= 0");
+                c.tc_stagger = value;
+                break;
             case BAEMM_TUNE_TC_CTAS:
                 BAEMM_REQUIRE(value >= 0 && value <= 65535, BAEMM_ERR_ARG, "grid size must be in [0, 65535]");
                 c.tc_ctas = value;
@@ -342,6 +346,7 @@ int baemm_get_tuning(const baemm_ctx *ctx, int key)
     if (key == BAEMM_TUNE_DENSE_VARIANT) return ctx->impl->dense_variant;
     if (key == BAEMM_TUNE_TC_SEGMENT) return ctx->impl->tc_seg_tiles;
     if (key == BAEMM_TUNE_TC_CTAS) return ctx->impl->tc_ctas;
+    if (key == BAEMM_TUNE_TC_STAGGER) return ctx->impl->tc_stagger;
     return -1;
 }
 int baemm_get_apply_mode(const baemm_ctx *ctx) { return (ctx && ctx->impl) ? ctx->impl->apply_mode : -1; }

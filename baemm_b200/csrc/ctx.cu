@@ -235,7 +235,7 @@ void Ctx::dense_apply(const cplx<R> *Btri, cplx<R> *Ctri)
         }
         const size_t ws_elems = tc_workspace_elems(tc_ctas);
         launch_boundary_tc(mesh, flags, prm_f.p, wave_count, wave_chunk_size, mesh.tgeo_f.p, Btri, Ctri,
-                           tc_ws.reserve(ws_elems), ws_elems, tc_err.p, stream, tc_seg_tiles, tc_ctas);
+                           tc_ws.reserve(ws_elems), ws_elems, tc_err.p, stream, tc_seg_tiles, tc_ctas, tc_stagger);
         tc_pending = true;
     }
     else

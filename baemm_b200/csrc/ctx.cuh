@@ -49,6 +49,7 @@ public:
     int dense_variant = 0;            // plain FP32 dense kernel variant (launch_boundary_dense)
     int tc_seg_tiles = 16;            // tensor-core form: tiles per TMEM partial sum
     int tc_ctas = 0;                  // tensor-core form: persistent grid size (0 = one CTA per SM)
+    int tc_stagger = 0;               // tensor-core form: sweep offset between CTAs (tiles; -1 = spread)
     DevBuf<float2> tc_ws;             // tensor-core form: partial sums of target blocks split between CTAs
     bool tc_geo_ready = false;        // mesh.tgeo_f built
     int ir_max_steps = 0;

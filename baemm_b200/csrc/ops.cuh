@@ -94,7 +94,7 @@ bool tc_supported(int wc, int wcs);
 // added to FP32 registers (bounds the tensor-core accumulation chain).
 void launch_boundary_tc(const MeshDev &m, const OpFlags &f, const void *chunk_params, int wc, int wcs,
                         const float *tgeo, const float2 *Btri, float2 *Ctri, float2 *ws, size_t ws_elems, int *err,
-                        cudaStream_t st, int seg_tiles = 4, int ctas = 0);
+                        cudaStream_t st, int seg_tiles = 16, int ctas = 0, int stagger = 0);
 // Source geometry of the tensor-core form, per 16-source tile (built once per mesh).
 size_t tc_tile_geometry_floats(int64_t nt);
 void launch_tc_tile_geometry(const MeshDev &m, float *tgeo, cudaStream_t st);

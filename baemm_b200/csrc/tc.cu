@@ -17,12 +17,14 @@
 // which keeps ~21 bits per product (TF32 hi+lo), well inside 1e-5 relative.
 //
 // Work unit = (group of up to 4 chunks, block of 128 targets, 16-source tile).
-// The grid is persistent (one CTA per SM, it holds all 512 TMEM columns) and
-// splits the linear range of units evenly ("stream-K"): a CTA walks its range
-// as pieces (runs of tiles of one target block).  A piece covering a whole
-// block writes C_tri; a partial piece (at most the first and the last of a
-// CTA) writes its partial sums to a workspace slot, and tc_fixup_kernel adds
-// the slots of each split block in CTA order (deterministic).
+// The grid is persistent (one CTA per SM, it holds all 512 TMEM columns).
+// Whole target blocks are dealt out in waves (all CTAs sweep the source tiles
+// in step, so the tiles in use stay cached); the blocks left over after the
+// last full wave are split evenly by tiles ("stream-K").  A piece covering a
+// whole block writes C_tri; a partial piece (at most the first and the last
+// tail piece of a CTA) writes its partial sums to a workspace slot, and
+// tc_fixup_kernel adds the slots of each split block in CTA order
+// (deterministic).
 // Warp roles (384 threads):
 //   warps 0-7   generators: thread (lane quarter q = warp % 4, half g = warp / 4)
 //               owns target row 32 q + lane and sources 8 g .. 8 g + 7 of each
@@ -318,36 +320,68 @@ __device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t by
 // elements 4 sp .. 4 sp + 3, of row `row` in a K-major SWIZZLE_128B image.
 __device__ __forceinline__ uint32_t img_off16(int row, int sp) { return (uint32_t)(row * 128 + ((sp ^ (row & 7)) << 4)); }
 
-// The partition of the unit range over the persistent grid.
+// The schedule over the persistent grid of `ctas` CTAs.  Blocks (cg, blk) are
+// numbered b = cg * nblk + blk.  The first full_waves * ctas blocks are whole
+// pieces, CTA k taking blocks k, k + ctas, ...: in each wave every CTA sweeps
+// the source tiles from the first, in step with the others, so the tiles being
+// read at any time stay few and cached.  The remaining blocks ("tail") are
+// split evenly by 16-source tiles ("stream-K"): CTA k takes the tail units
+// [tail_start(k), tail_start(k + 1)), where a unit is one tile of one block.
 struct TcPlan
 {
     int n, wc, nblk, ntiles, ncg, seg_tiles;
-    int64_t units;   // ncg * nblk * ntiles
-    int ctas;        // grid size (<= units)
+    int ctas;          // grid size
+    int full_waves;    // whole blocks per CTA before the tail
+    int tail_blocks;   // ncg * nblk - full_waves * ctas
+    int64_t tail_units;   // tail_blocks * ntiles
+    int stagger;       // whole-block sweeps of CTA k start at tile (k % 8) * stagger; -1: k * ntiles / ctas
 };
 
-__host__ __device__ __forceinline__ int64_t tc_start(const TcPlan &p, int k) { return (int64_t)k * p.units / p.ctas; }
-// The CTA whose range holds unit x.
+__host__ __device__ __forceinline__ int64_t tc_tail_start(const TcPlan &p, int k)
+{
+    return (int64_t)k * p.tail_units / p.ctas;
+}
+// The CTA whose tail range holds tail unit x (a CTA with an empty range holds none).
 __host__ __device__ __forceinline__ int tc_cta_of(const TcPlan &p, int64_t x)
 {
-    return (int)(((x + 1) * p.ctas - 1) / p.units);
+    return (int)(((x + 1) * p.ctas - 1) / p.tail_units);
 }
 
-// Walks a CTA's unit range as pieces (cg, blk, tiles [tb, te)).
+// Walks a CTA's work as pieces (cg, blk, tiles [tb, te)); `slot` is the
+// workspace slot of a partial tail piece (0: the CTA's first tail piece,
+// 1: its last); `rot` rotates the tile order of a whole-block piece (source
+// tile = (t + rot) mod ntiles), 0 for tail pieces.
 struct PieceIter
 {
-    int64_t u, u1;
-    int per_cg;
-    __device__ PieceIter(const TcPlan &p, int k) : u(tc_start(p, k)), u1(tc_start(p, k + 1)), per_cg(p.nblk * p.ntiles) {}
-    __device__ bool next(const TcPlan &p, int &cg, int &blk, int &tb, int &te)
+    int k, w;
+    int64_t u, u0, u1;
+    __device__ PieceIter(const TcPlan &p, int k_)
+        : k(k_), w(0), u(tc_tail_start(p, k_)), u0(tc_tail_start(p, k_)), u1(tc_tail_start(p, k_ + 1)) {}
+    __device__ bool next(const TcPlan &p, int &cg, int &blk, int &tb, int &te, int &slot, int &rot)
     {
-        if (u >= u1) return false;
-        cg = (int)(u / per_cg);
-        const int rem = (int)(u - (int64_t)cg * per_cg);
-        blk = rem / p.ntiles;
-        tb = rem - blk * p.ntiles;
-        te = (int)min((int64_t)p.ntiles, (int64_t)tb + (u1 - u));
-        u += te - tb;
+        int b;
+        rot = 0;
+        if (w < p.full_waves)
+        {
+            b = w * p.ctas + k;
+            ++w;
+            tb = 0;
+            te = p.ntiles;
+            slot = 0;
+            rot = p.stagger < 0 ? (int)((int64_t)k * p.ntiles / p.ctas) : (int)(((int64_t)(k % 8) * p.stagger) % p.ntiles);
+        }
+        else
+        {
+            if (u >= u1) return false;
+            const int j = (int)(u / p.ntiles);
+            b = p.full_waves * p.ctas + j;
+            tb = (int)(u - (int64_t)j * p.ntiles);
+            te = (int)min((int64_t)p.ntiles, (int64_t)tb + (u1 - u));
+            slot = (u == u0) ? 0 : 1;
+            u += te - tb;
+        }
+        cg = b / p.nblk;
+        blk = b - cg * p.nblk;
         return true;
     }
 };
@@ -464,10 +498,9 @@ boundary_tc_kernel(const float *__restrict__ mid4, const float *__restrict__ nrm
             return true;
         };
         PieceIter it(plan, k_cta);
-        int cg, blk, tb, te;
-        bool first_piece = true;
+        int cg, blk, tb, te, slot, rot;
         const float2 m1 = make_float2(-1.f, -1.f);
-        while (ok && it.next(plan, cg, blk, tb, te))
+        while (ok && it.next(plan, cg, blk, tb, te, slot, rot))
         {
             const int i = blk * TC_M + row;
             // -x_i and nu_i as broadcast pairs
@@ -489,6 +522,7 @@ boundary_tc_kernel(const float *__restrict__ mid4, const float *__restrict__ nrm
             for (int t = tb; t < te; ++t, ++T)
             {
                 const int rs = T % TC_RSTAGES;
+                const int ts = t + rot < ntiles ? t + rot : t + rot - ntiles;   // source tile (rot < ntiles)
                 {
                     const bool got = wait_bar(&sm.r_full[rs], (uint32_t)(T / TC_RSTAGES) & 1u, abort_flag, err, 1);
                     if (!__all_sync(0xffffffffu, got)) { ok = false; break; }
@@ -498,7 +532,7 @@ boundary_tc_kernel(const float *__restrict__ mid4, const float *__restrict__ nrm
                 {
                     const TcTileGeo &G = sm.raw[rs].geo;
                     // tiles that hold the target itself or padding past the end need masks
-                    const bool special = (t == ntiles - 1) || (t * TC_SRC < blk * TC_M + TC_M && t * TC_SRC + TC_SRC > blk * TC_M);
+                    const bool special = (ts == ntiles - 1) || (ts * TC_SRC < blk * TC_M + TC_M && ts * TC_SRC + TC_SRC > blk * TC_M);
                     #pragma unroll
                     for (int p = 0; p < 4; ++p)
                     {
@@ -510,7 +544,7 @@ boundary_tc_kernel(const float *__restrict__ mid4, const float *__restrict__ nrm
                         float ri0 = rsqrtf(r2.x), ri1 = rsqrtf(r2.y);
                         if (special)
                         {
-                            const int j = t * TC_SRC + sl;
+                            const int j = ts * TC_SRC + sl;
                             if (!(j < n && j != i)) ri0 = 0.f;
                             if (!(j + 1 < n && j + 1 != i)) ri1 = 0.f;
                         }
@@ -654,7 +688,7 @@ boundary_tc_kernel(const float *__restrict__ mid4, const float *__restrict__ nrm
                 if (i < n) dst = &Ctri[(int64_t)i * wc + cg * cw];
             }
             else
-                dst = &ws[((int64_t)(k_cta * 2 + (first_piece ? 0 : 1)) * TC_M + row) * (TC_CHMAX * 16)];
+                dst = &ws[((int64_t)(k_cta * 2 + slot) * TC_M + row) * (TC_CHMAX * 16)];
             if (dst)
             {
                 #pragma unroll
@@ -666,7 +700,6 @@ boundary_tc_kernel(const float *__restrict__ mid4, const float *__restrict__ nrm
                     for (int k = 0; k < 4; ++k) out[k] = a4[k];
                 }
             }
-            first_piece = false;
         }
         if (!ok) publish();
     }
@@ -679,9 +712,9 @@ boundary_tc_kernel(const float *__restrict__ mid4, const float *__restrict__ nrm
         const int lt = tid - TC_GEN_THREADS;
         constexpr int items = (TC_SRC / 2) * CH * 16;
         PieceIter it(plan, k_cta);
-        int cg, blk, tb, te, T = 0;
+        int cg, blk, tb, te, slot, rot, T = 0;
         bool ok = true;
-        while (ok && it.next(plan, cg, blk, tb, te))
+        while (ok && it.next(plan, cg, blk, tb, te, slot, rot))
         {
             for (int t = tb; t < te; ++t, ++T)
             {
@@ -693,7 +726,8 @@ boundary_tc_kernel(const float *__restrict__ mid4, const float *__restrict__ nrm
                     ok = false;
                     break;
                 }
-                const int nsrc = n - t * TC_SRC;   // valid rows in this tile (may exceed 16)
+                const int ts = t + rot < ntiles ? t + rot : t + rot - ntiles;   // source tile (rot < ntiles)
+                const int nsrc = n - ts * TC_SRC;   // valid rows in this tile (may exceed 16)
                 #pragma unroll 2
                 for (int e = lt; e < items; e += TC_EXP_THREADS)
                 {
@@ -727,9 +761,9 @@ boundary_tc_kernel(const float *__restrict__ mid4, const float *__restrict__ nrm
         const int cw = CH * 16;
         const uint32_t row_bytes = (uint32_t)(cw * sizeof(float2));
         PieceIter it(plan, k_cta);
-        int cg, blk, tb, te, T = 0;
+        int cg, blk, tb, te, slot, rot, T = 0;
         bool ok = true;
-        while (ok && it.next(plan, cg, blk, tb, te))
+        while (ok && it.next(plan, cg, blk, tb, te, slot, rot))
         {
             for (int t = tb; t < te; ++t, ++T)
             {
@@ -742,10 +776,11 @@ boundary_tc_kernel(const float *__restrict__ mid4, const float *__restrict__ nrm
                 }
                 if (elect_one())
                 {
-                    const int j0 = t * TC_SRC;
+                    const int ts = t + rot < ntiles ? t + rot : t + rot - ntiles;   // source tile (rot < ntiles)
+                    const int j0 = ts * TC_SRC;
                     const int rows = min(TC_SRC, n - j0);
                     mbar_expect_tx(&sm.r_full[rs], (uint32_t)rows * row_bytes + (uint32_t)sizeof(TcTileGeo));
-                    bulk_g2s(&sm.raw[rs].geo, tgeo + t, (uint32_t)sizeof(TcTileGeo), &sm.r_full[rs]);
+                    bulk_g2s(&sm.raw[rs].geo, tgeo + ts, (uint32_t)sizeof(TcTileGeo), &sm.r_full[rs]);
                     // one contiguous block when the tile's rows are whole B_tri rows of
                     // exactly the raw row width; otherwise one copy per row
                     if (CH == TC_CHMAX && cw == wc)
@@ -766,8 +801,8 @@ boundary_tc_kernel(const float *__restrict__ mid4, const float *__restrict__ nrm
         bool ok = true;
         int T = 0, SG = 0;
         PieceIter it(plan, k_cta);
-        int cg, blk, tb, te;
-        while (ok && it.next(plan, cg, blk, tb, te))
+        int cg, blk, tb, te, slot, rot;
+        while (ok && it.next(plan, cg, blk, tb, te, slot, rot))
         {
             for (int t = tb; t < te; ++t, ++T)
             {
@@ -860,8 +895,10 @@ __global__ void tc_tile_geometry_kernel(const float *__restrict__ mid4, const fl
 // in CTA order, and writes the block's rows of C_tri.
 __global__ void tc_fixup_kernel(const float2 *__restrict__ ws, float2 *__restrict__ Ctri, const TcPlan plan, int cw)
 {
-    const int cg = blockIdx.x / plan.nblk, blk = blockIdx.x - cg * plan.nblk;
-    const int64_t lo = ((int64_t)cg * plan.nblk + blk) * plan.ntiles, hi = lo + plan.ntiles;
+    const int j = blockIdx.x;   // tail block
+    const int b = plan.full_waves * plan.ctas + j;
+    const int cg = b / plan.nblk, blk = b - cg * plan.nblk;
+    const int64_t lo = (int64_t)j * plan.ntiles, hi = lo + plan.ntiles;
     const int k_first = tc_cta_of(plan, lo), k_last = tc_cta_of(plan, hi - 1);
     if (k_first == k_last) return;   // written directly by its CTA
     for (int e = threadIdx.x; e < TC_M * cw; e += blockDim.x)
@@ -872,7 +909,9 @@ __global__ void tc_fixup_kernel(const float2 *__restrict__ ws, float2 *__restric
         float2 acc = make_float2(0.f, 0.f);
         for (int k = k_first; k <= k_last; ++k)
         {
-            const int slot = (tc_start(plan, k) >= lo) ? 0 : 1;   // the CTA's first piece, or its last
+            const int64_t s0 = tc_tail_start(plan, k);
+            if (tc_tail_start(plan, k + 1) == s0) continue;   // no tail units: wrote nothing
+            const int slot = (s0 >= lo) ? 0 : 1;             // the CTA's first tail piece, or its last
             const float2 v = ws[((int64_t)(k * 2 + slot) * TC_M + row) * (TC_CHMAX * 16) + col];
             acc.x += v.x;
             acc.y += v.y;
@@ -950,7 +989,7 @@ void launch_tc_tile_geometry(const MeshDev &m, float *tgeo, cudaStream_t st)
 
 void launch_boundary_tc(const MeshDev &m, const OpFlags &f, const void *chunk_params, int wc, int wcs,
                         const float *tgeo, const float2 *Btri, float2 *Ctri, float2 *ws, size_t ws_elems, int *err,
-                        cudaStream_t st, int seg_tiles, int ctas)
+                        cudaStream_t st, int seg_tiles, int ctas, int stagger)
 {
     BAEMM_REQUIRE(tc_supported(wc, wcs), BAEMM_ERR_SIZE,
                   "tensor-core apply needs wave_chunk_size 16 and wave_count <= 512");
@@ -963,9 +1002,13 @@ void launch_boundary_tc(const MeshDev &m, const OpFlags &f, const void *chunk_pa
     plan.nblk = ceil_div(plan.n, TC_M);
     plan.ntiles = ceil_div(plan.n, TC_SRC);
     plan.seg_tiles = std::max(1, seg_tiles);
-    plan.units = (int64_t)plan.ncg * plan.nblk * plan.ntiles;
+    const int blocks = plan.ncg * plan.nblk;
     if (ctas <= 0) ctas = device_sm_count();
-    plan.ctas = (int)std::min<int64_t>(ctas, plan.units);
+    plan.ctas = (int)std::min<int64_t>(ctas, (int64_t)blocks * plan.ntiles);
+    plan.full_waves = blocks / plan.ctas;
+    plan.tail_blocks = blocks - plan.full_waves * plan.ctas;
+    plan.tail_units = (int64_t)plan.tail_blocks * plan.ntiles;
+    plan.stagger = stagger;
     BAEMM_REQUIRE(ws && ws_elems >= tc_workspace_elems(plan.ctas), BAEMM_ERR_ARG, "tensor-core workspace too small");
     const int code = (f.sl() ? 1 : 0) | (f.dl() ? 2 : 0) | (f.adl() ? 4 : 0);
     const auto *p = static_cast<const ChunkParamsF *>(chunk_params);
@@ -976,8 +1019,11 @@ void launch_boundary_tc(const MeshDev &m, const OpFlags &f, const void *chunk_pa
     else if (CH == 2) tc_flags<2>(code, st, mid, nrm, tg, Btri, Ctri, ws, p, plan, err);
     else tc_flags<1>(code, st, mid, nrm, tg, Btri, Ctri, ws, p, plan, err);
     BAEMM_LAUNCH_CHECK();
-    tc_fixup_kernel<<<plan.ncg * plan.nblk, 256, 0, st>>>(ws, Ctri, plan, CH * 16);
-    BAEMM_LAUNCH_CHECK();
+    if (plan.tail_blocks > 0)
+    {
+        tc_fixup_kernel<<<plan.tail_blocks, 256, 0, st>>>(ws, Ctri, plan, CH * 16);
+        BAEMM_LAUNCH_CHECK();
+    }
 }
 
 } // namespace baemm

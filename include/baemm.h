@@ -127,10 +127,14 @@ int baemm_get_apply_mode(const baemm_ctx *ctx);
  *                             sums in shared memory (default 16; bounds the
  *                             tensor-core accumulation chain)
  *   BAEMM_TUNE_TC_CTAS        tensor-core form: persistent grid size (default 0 =
- *                             one CTA per SM) */
+ *                             one CTA per SM)
+ *   BAEMM_TUNE_TC_STAGGER     tensor-core form: CTA k starts its sweep of the
+ *                             source tiles at tile (k % 8) * value (default 0:
+ *                             all in step); -1 spreads the starts over all tiles */
 #define BAEMM_TUNE_DENSE_VARIANT 1
 #define BAEMM_TUNE_TC_SEGMENT    2
 #define BAEMM_TUNE_TC_CTAS       3
+#define BAEMM_TUNE_TC_STAGGER    4
 int baemm_set_tuning(baemm_ctx *ctx, int key, int value);
 int baemm_get_tuning(const baemm_ctx *ctx, int key);
 /* FP64 iterative refinement around the inner GMRES (0 = off, the reference's

@@ -166,6 +166,29 @@ def test_tensor_core_persistent_grid(env, ctas, wshape):
     assert np.array_equal(C1, C2)
 
 
+@pytest.mark.parametrize("stagger", [-1, 0, 3, 1000])
+def test_tensor_core_sweep_stagger(env, stagger):
+    """Rotating the source-tile order of whole-block pieces (the sweep
+    stagger) changes only the summation order: same bar against FP64."""
+    coords, tris, meas, H, o32, o64 = env
+    kap = [2.0, 4.0, 8.0, 16.0]
+    coeff = _coeff("all", kap)
+    B = crandn(np.random.default_rng(99), coords.shape[0], 64)
+    C64 = np.zeros_like(B)
+    o64.ApplyBoundaryOperators_PL(1.0, B, 0.0, C64, kap, coeff, 64, 16)
+    H.SetApplyMode(APPLY_TC)
+    H.SetTuning(_capi.TUNE_TC_CTAS, 3)
+    H.SetTuning(_capi.TUNE_TC_STAGGER, stagger)
+    try:
+        C = np.zeros_like(B)
+        H.ApplyBoundaryOperators_PL(1.0, B, 0.0, C, kap, coeff, 64, 16)
+    finally:
+        H.SetTuning(_capi.TUNE_TC_STAGGER, 0)
+        H.SetTuning(_capi.TUNE_TC_CTAS, 0)
+        H.SetApplyMode(APPLY_FP32)
+    assert relerr(C, C64) < FP32_VS64_TOL
+
+
 def test_device_path_follows_torch_stream(env):
     """Without SetStream, torch CUDA tensors are processed on torch's current
     stream, so reading the result back through torch needs no extra sync."""
