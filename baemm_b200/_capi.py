@@ -46,6 +46,19 @@ class SolveStats(C.Structure):
     ]
 
 
+class TuneResult(C.Structure):
+    _fields_ = [
+        ("apply_mode", C.c_int32),
+        ("dense_variant", C.c_int32),
+        ("tc_segment", C.c_int32),
+        ("tc_ctas", C.c_int32),
+        ("tc_stagger", C.c_int32),
+        ("candidates", C.c_int32),
+        ("best_ms", C.c_double),
+        ("before_ms", C.c_double),
+    ]
+
+
 I, I64, D = C.c_int, C.c_int64, C.c_double
 # name -> (restype, argtypes); every symbol declared in include/baemm.h
 SIGNATURES = {
@@ -72,6 +85,7 @@ SIGNATURES = {
     "baemm_set_apply_mode": (I, [vp, I]),
     "baemm_get_apply_mode": (I, [vp]),
     "baemm_set_tuning": (I, [vp, I, I]),
+    "baemm_autotune": (I, [vp, I, I, C.POINTER(TuneResult)]),
     "baemm_get_tuning": (I, [vp, I]),
     "baemm_set_refinement": (I, [vp, I, D]),
     "baemm_get_areas": (I, [vp, fp]),

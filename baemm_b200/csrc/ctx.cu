@@ -213,6 +213,16 @@ void Ctx::load_parameters(const double *kappa, const zc *coeff, int wc, int wcs,
                                stream));
     BAEMM_CUDA(cudaMemcpyAsync(prm_d.reserve(wcc), prm_d_h.data(), wcc * sizeof(ChunkParamsD), cudaMemcpyHostToDevice,
                                stream));
+    // The tensor-core form works on groups of 16 columns: one parameter set per
+    // group (a chunk of wave_chunk_size = 16 m columns repeats its set m times).
+    if (wcs % 16 == 0)
+    {
+        const int groups = wc / 16, rep = wcs / 16;
+        prm16_f_h.resize(groups);
+        for (int gi = 0; gi < groups; ++gi) prm16_f_h[gi] = prm_f_h[gi / rep];
+        BAEMM_CUDA(cudaMemcpyAsync(prm16_f.reserve(groups), prm16_f_h.data(), groups * sizeof(ChunkParamsF),
+                                   cudaMemcpyHostToDevice, stream));
+    }
 }
 
 void Ctx::require_loaded() const
@@ -234,7 +244,7 @@ void Ctx::dense_apply(const cplx<R> *Btri, cplx<R> *Ctri)
             tc_geo_ready = true;
         }
         const size_t ws_elems = tc_workspace_elems(tc_ctas);
-        launch_boundary_tc(mesh, flags, prm_f.p, wave_count, wave_chunk_size, mesh.tgeo_f.p, Btri, Ctri,
+        launch_boundary_tc(mesh, flags, prm16_f.p, wave_count, wave_chunk_size, mesh.tgeo_f.p, Btri, Ctri,
                            tc_ws.reserve(ws_elems), ws_elems, tc_err.p, stream, tc_seg_tiles, tc_ctas, tc_stagger);
         tc_pending = true;
     }
@@ -289,6 +299,7 @@ void Ctx::apply_boundary(Text alpha, const Text *B, int64_t ldB, Text beta, Text
     prof_valid = profiling;
 }
 
+template void Ctx::dense_apply<float>(const float2 *, float2 *);
 template void Ctx::apply_boundary<double2>(double2, const double2 *, int64_t, double2, double2 *, int64_t);
 template void Ctx::apply_boundary<float2>(float2, const float2 *, int64_t, float2, float2 *, int64_t);
 

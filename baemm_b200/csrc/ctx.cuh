@@ -39,6 +39,8 @@ public:
     std::vector<ChunkParamsF> prm_f_h;
     std::vector<ChunkParamsD> prm_d_h;
     DevBuf<ChunkParamsF> prm_f;
+    std::vector<ChunkParamsF> prm16_f_h;   // per 16-column group (tensor-core form)
+    DevBuf<ChunkParamsF> prm16_f;
     DevBuf<ChunkParamsD> prm_d;
     bool operators_loaded = false;
 
@@ -127,6 +129,9 @@ public:
     // already queued on the current one, without a host synchronisation.
     void switch_stream(cudaStream_t s);
     std::string device_info() const;
+    // Times the dense-kernel settings of `mode` on the loaded operators and
+    // keeps the fastest (tune.cu).
+    void autotune(int mode, int repeats, baemm_tune_result *out);
 
 private:
     void build_topology(const int32_t *tris);

@@ -968,7 +968,8 @@ int device_sm_count()
 
 } // namespace
 
-bool tc_supported(int wc, int wcs) { return wcs == 16 && wc % 16 == 0 && wc <= 16 * TC_MAXCHUNKS; }
+// Groups of 16 columns share a wavenumber: wave_chunk_size a multiple of 16.
+bool tc_supported(int wc, int wcs) { return wcs % 16 == 0 && wcs > 0 && wc % wcs == 0 && wc <= 16 * TC_MAXCHUNKS; }
 
 size_t tc_workspace_elems(int ctas)
 {
@@ -992,7 +993,7 @@ void launch_boundary_tc(const MeshDev &m, const OpFlags &f, const void *chunk_pa
                         cudaStream_t st, int seg_tiles, int ctas, int stagger)
 {
     BAEMM_REQUIRE(tc_supported(wc, wcs), BAEMM_ERR_SIZE,
-                  "tensor-core apply needs wave_chunk_size 16 and wave_count <= 512");
+                  "tensor-core apply needs wave_chunk_size a multiple of 16 and wave_count <= 512");
     if (!f.any_layer() || m.nt == 0) return;
     TcPlan plan;
     plan.n = (int)m.nt;

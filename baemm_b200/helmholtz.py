@@ -182,6 +182,13 @@ class Helmholtz_CUDA:
     def SetRefinement(self, max_steps: int, inner_tol: float = 1e-4):
         self._ck(self._lib.baemm_set_refinement(self._h, int(max_steps), float(inner_tol)))
 
+    def Autotune(self, mode=APPLY_TC, repeats: int = 2) -> dict:
+        """Time the dense-kernel settings of `mode` on the loaded operators and
+        keep the fastest (baemm_autotune); returns the chosen settings and times."""
+        r = _capi.TuneResult()
+        self._ck(self._lib.baemm_autotune(self._h, int(mode), int(repeats), C.byref(r)))
+        return {f: getattr(r, f) for f, _ in _capi.TuneResult._fields_}
+
     def LastSolveStats(self) -> dict:
         s = SolveStats()
         self._ck(self._lib.baemm_last_solve_stats(self._h, C.byref(s)))

@@ -52,7 +52,9 @@ typedef enum baemm_status
 /* Arithmetic of the dense boundary-operator apply (no reference counterpart;
  * the reference has FP32 only, Definitions.hpp:3-6). */
 #define BAEMM_APPLY_FP32 0   /* plain: FP32 generation and FP32 SIMT contraction */
-#define BAEMM_APPLY_TC   1   /* compensated: split hi+lo operands on the tensor cores, FP32 accumulate */
+#define BAEMM_APPLY_TC   1   /* compensated: split hi+lo operands on the tensor cores, FP32 accumulate;
+                              * needs wave_chunk_size a multiple of 16 and wave_count <= 512, other
+                              * shapes run the plain FP32 kernel */
 #define BAEMM_APPLY_FP64 2   /* FP64 generation and contraction */
 
 /* Solver statistics of the last GMRES / CG run (the reference discards them,
@@ -137,6 +139,25 @@ int baemm_get_apply_mode(const baemm_ctx *ctx);
 #define BAEMM_TUNE_TC_STAGGER    4
 int baemm_set_tuning(baemm_ctx *ctx, int key, int value);
 int baemm_get_tuning(const baemm_ctx *ctx, int key);
+/* Autotuner (no reference counterpart): times the dense-kernel settings of
+ * `mode` (BAEMM_APPLY_FP32: the three plain variants; BAEMM_APPLY_TC: the
+ * tensor-core segment lengths 4/8/16/32) on the loaded operators, with the
+ * mesh and wave counts of the context, `repeats` timed runs each (>= 1),
+ * keeps the fastest in the context and reports it.  A TC request whose wave
+ * shape the tensor-core form does not support tunes the plain kernel.
+ * Requires baemm_load_boundary_operators; synchronises the context. */
+typedef struct baemm_tune_result
+{
+    int32_t apply_mode;      /* the form tuned (BAEMM_APPLY_*) */
+    int32_t dense_variant;   /* chosen BAEMM_TUNE_DENSE_VARIANT (plain form) */
+    int32_t tc_segment;      /* chosen BAEMM_TUNE_TC_SEGMENT (tensor-core form) */
+    int32_t tc_ctas;         /* BAEMM_TUNE_TC_CTAS in force */
+    int32_t tc_stagger;      /* BAEMM_TUNE_TC_STAGGER in force */
+    int32_t candidates;      /* settings timed */
+    double  best_ms;         /* dense-kernel time of the chosen setting */
+    double  before_ms;       /* dense-kernel time of the setting in force before */
+} baemm_tune_result;
+int baemm_autotune(baemm_ctx *ctx, int mode, int repeats, baemm_tune_result *out);
 /* FP64 iterative refinement around the inner GMRES (0 = off, the reference's
  * behaviour).  When on, the solve's outer residual uses the FP64 apply and
  * the inner GMRES uses the context's apply mode. No reference counterpart. */

@@ -51,4 +51,5 @@ def test_null_context_is_rejected():
     L = _capi.lib()
     assert L.baemm_synchronize(None) == 1
     assert L.baemm_vertex_count(None) == -1
+    assert L.baemm_autotune(None, 1, 1, None) == 1
     L.baemm_destroy(None)   # no-op

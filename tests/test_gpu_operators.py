@@ -166,6 +166,24 @@ def test_tensor_core_persistent_grid(env, ctas, wshape):
     assert np.array_equal(C1, C2)
 
 
+@pytest.mark.parametrize("wc,wcs,kap", [(64, 32, [3.0, 6.0]), (128, 64, [2.0, 5.0]), (32, 32, [4.0])])
+def test_tensor_core_wider_chunks(env, wc, wcs, kap):
+    """wave_chunk_size a multiple of 16 (the Gauss-Newton configuration uses
+    32): the tensor-core form runs each wavenumber over its 16-column groups."""
+    coords, tris, meas, H, o32, o64 = env
+    coeff = _coeff("all", kap)
+    B = crandn(np.random.default_rng(5 + wc), coords.shape[0], wc)
+    C64 = np.zeros_like(B)
+    o64.ApplyBoundaryOperators_PL(1.0, B, 0.0, C64, kap, coeff, wc, wcs)
+    H.SetApplyMode(APPLY_TC)
+    try:
+        C = np.zeros_like(B)
+        H.ApplyBoundaryOperators_PL(1.0, B, 0.0, C, kap, coeff, wc, wcs)
+    finally:
+        H.SetApplyMode(APPLY_FP32)
+    assert relerr(C, C64) < FP32_VS64_TOL
+
+
 @pytest.mark.parametrize("stagger", [-1, 0, 3, 1000])
 def test_tensor_core_sweep_stagger(env, stagger):
     """Rotating the source-tile order of whole-block pieces (the sweep
@@ -186,6 +204,37 @@ def test_tensor_core_sweep_stagger(env, stagger):
         H.SetTuning(_capi.TUNE_TC_STAGGER, 0)
         H.SetTuning(_capi.TUNE_TC_CTAS, 0)
         H.SetApplyMode(APPLY_FP32)
+    assert relerr(C, C64) < FP32_VS64_TOL
+
+
+@pytest.mark.parametrize("mode", [APPLY_TC, APPLY_FP32])
+def test_autotune_keeps_results(env, mode):
+    """The autotuner picks one of its candidates, keeps it in the context, and
+    the apply with the chosen setting meets the same bar against FP64."""
+    coords, tris, meas, H, o32, o64 = env
+    kap = [2.0, 4.0, 8.0, 16.0]
+    coeff = _coeff("bie", kap)
+    B = crandn(np.random.default_rng(3), coords.shape[0], 64)
+    C64 = np.zeros_like(B)
+    o64.ApplyBoundaryOperators_PL(1.0, B, 0.0, C64, kap, coeff, 64, 16)
+    H.LoadBoundaryOperators_PL(kap, coeff, 64, 16)
+    seg0, var0 = H.GetTuning(_capi.TUNE_TC_SEGMENT), H.GetTuning(_capi.TUNE_DENSE_VARIANT)
+    try:
+        r = H.Autotune(mode, repeats=1)
+        assert r["apply_mode"] == mode and r["best_ms"] > 0 and r["best_ms"] <= r["before_ms"] * 1.5
+        if mode == APPLY_TC:
+            assert r["candidates"] == 4 and r["tc_segment"] in (4, 8, 16, 32)
+            assert H.GetTuning(_capi.TUNE_TC_SEGMENT) == r["tc_segment"]
+        else:
+            assert r["candidates"] == 3 and H.GetTuning(_capi.TUNE_DENSE_VARIANT) == r["dense_variant"]
+        H.SetApplyMode(mode)
+        C = np.zeros_like(B)
+        H.ApplyBoundaryOperators_PL(1.0, B, 0.0, C)
+    finally:
+        H.SetApplyMode(APPLY_FP32)
+        H.SetTuning(_capi.TUNE_TC_SEGMENT, seg0)
+        H.SetTuning(_capi.TUNE_DENSE_VARIANT, var0)
+        H.UnloadBoundaryOperators_PL()
     assert relerr(C, C64) < FP32_VS64_TOL
 
 
