@@ -393,6 +393,63 @@ def run_gpu_arm(args, rank, world, local_rank):
     return 0
 
 
+# ---------------------------------------------------------------------------
+# the scattering-solve workload (--workload solve): not the headline line
+# ---------------------------------------------------------------------------
+SOLVE_WORKLOAD = ("unit icosphere level 6 (40962 V, 81920 T), kappa {4, 8} x 16 plane waves (Fibonacci "
+                  "directions), far field at 256 Fibonacci directions, mixed indirect BIE, GMRES(30) + CG M^-1")
+
+
+def run_solve_workload(args):
+    """FarField (FarField.hpp:28-144) on the scattering-solve configuration:
+    plain FP32 apply, compensated tensor-core apply, the tensor-core apply
+    inside FP64 iterative refinement, and the FP64 path; errors of the far
+    field against the FP64 solve at residual 1e-10 (the FP64 device path is
+    held to 1e-11 of the FP64 oracle by the tests at smaller sizes)."""
+    import torch
+    from baemm_b200 import APPLY_FP32, APPLY_FP64, APPLY_TC, Helmholtz_CUDA, WaveType, meshes
+    coords, tris = meshes.icosphere(args.solve_level)
+    meas = meshes.fibonacci_sphere(256)
+    inc = meshes.fibonacci_sphere(16)
+    kap = np.array([4.0, 8.0])
+    H = Helmholtz_CUDA(coords, tris, meas)
+
+    def solve(mode, gmres_tol, ir_steps=0, inner=1e-5):
+        H.SetApplyMode(mode)
+        H.SetRefinement(ir_steps, inner)
+        F = np.zeros((meas.shape[0], 32), complex)
+        H.FarField(kap, inc, F, WaveType.Plane, 1e-10, gmres_tol)   # warm (buffers, set-up)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        H.FarField(kap, inc, F, WaveType.Plane, 1e-10, gmres_tol)
+        dt = time.perf_counter() - t0
+        st = H.LastSolveStats()
+        H.SetRefinement(0)
+        H.SetApplyMode(APPLY_FP32)
+        return F, dt, st
+
+    F64, t64, s64 = solve(APPLY_FP64, 1e-10)
+    runs = {"fp64_tol1e-10": (F64, t64, s64)}
+    runs["fp32_tol1e-6"] = solve(APPLY_FP32, 1e-6)
+    runs["tc_tol1e-6"] = solve(APPLY_TC, 1e-6)
+    runs["tc_fp64ir_tol1e-10"] = solve(APPLY_TC, 1e-10, ir_steps=8, inner=1e-5)
+    n64 = float(np.linalg.norm(F64))
+    res = {}
+    for name, (F, dt, st) in runs.items():
+        res[name] = {"seconds": dt, "solves_per_s": 1.0 / dt, "gmres_iterations": st["gmres_iterations"],
+                     "refinement_steps": st["refinement_steps"],
+                     "gmres_relative_residual": st["gmres_relative_residual"],
+                     "far_field_rel_err_vs_fp64": float(np.linalg.norm(F - F64) / n64)}
+    line = {"metric": "scattering solves/s (FarField)", "value": res["tc_fp64ir_tol1e-10"]["solves_per_s"],
+            "unit": "solves/s", "n_gpus": 1, "higher_is_better": True, "data": "synthetic",
+            "config": {"workload": SOLVE_WORKLOAD if args.solve_level == 6 else f"icosphere level {args.solve_level}",
+                       "triangles": int(tris.shape[0]), "wave_count": 32, "meas_count": 256},
+            "runs": res}
+    print(json.dumps(line), flush=True)
+    H.close()
+    return 0
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -403,6 +460,9 @@ def main(argv=None):
                     help="apply arithmetic: plain FP32, compensated tensor-core (default), FP64")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-compare", action="store_true", help="skip the plain-FP32 and FP64 comparison applies")
+    ap.add_argument("--workload", default="apply", choices=["apply", "solve"],
+                    help="apply: the headline operator-apply line; solve: the scattering-solve configuration")
+    ap.add_argument("--solve-level", type=int, default=6, help="icosphere level of --workload solve")
     ap.add_argument("--small", action="store_true", help="38400-triangle torus (profiling captures only)")
     args = ap.parse_args(argv)
     rank = int(os.environ.get("RANK", "0"))
@@ -410,6 +470,8 @@ def main(argv=None):
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         return run_reference_arm(args, rank, world)
+    if args.workload == "solve":
+        return run_solve_workload(args) if rank == 0 else 0
     if world > 1:
         import datetime
 

@@ -4,7 +4,7 @@ import numpy as np
 import pytest
 from scipy.special import eval_legendre, spherical_jn, spherical_yn
 
-from baemm_b200 import APPLY_FP32, APPLY_FP64, Helmholtz_CUDA, WaveType, meshes
+from baemm_b200 import APPLY_FP32, APPLY_FP64, APPLY_TC, Helmholtz_CUDA, WaveType, meshes
 from oracle import oracle as O
 from tests.helpers import crandn, relerr
 
@@ -60,18 +60,22 @@ def test_far_field_fp64_matches_oracle(env):
     assert relerr(Fg, Fo) < 1e-9
 
 
-def test_far_field_refined_fp32_reaches_fp64(env):
-    """FP32 apply inside FP64 iterative refinement reaches the FP64 solution."""
+@pytest.mark.parametrize("mode", [APPLY_FP32, APPLY_TC])
+def test_far_field_refined_fp32_reaches_fp64(env, mode):
+    """FP32 (plain or compensated tensor-core) apply inside FP64 iterative
+    refinement reaches the FP64 solution."""
     coords, tris, meas, inc, H, o32, o64 = env
     kap = np.array([3.0])
     Fg = np.zeros((meas.shape[0], 16), complex)
     Fo = np.zeros_like(Fg)
     H.SetRefinement(6, 1e-5)
+    H.SetApplyMode(mode)
     try:
         H.FarField(kap, inc, Fg, WaveType.Plane, 1e-12, 1e-11)
         st = H.LastSolveStats()
     finally:
         H.SetRefinement(0)
+        H.SetApplyMode(APPLY_FP32)
     o64.FarField(kap, inc, Fo, WaveType.Plane, 1e-12, 1e-12)
     assert st["refinement_steps"] >= 1 and st["gmres_converged"] == 1
     assert relerr(Fg, Fo) < 1e-8
