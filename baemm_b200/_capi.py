@@ -85,6 +85,9 @@ SIGNATURES = {
     "baemm_set_apply_mode": (I, [vp, I]),
     "baemm_get_apply_mode": (I, [vp]),
     "baemm_set_tuning": (I, [vp, I, I]),
+    "baemm_set_mesh": (I, [vp, dp, I64, i64p, I64]),
+    "baemm_set_graphs": (I, [vp, I]),
+    "baemm_graph_stats": (I, [vp, i64p, i64p]),
     "baemm_autotune": (I, [vp, I, I, C.POINTER(TuneResult)]),
     "baemm_get_tuning": (I, [vp, I]),
     "baemm_set_refinement": (I, [vp, I, D]),

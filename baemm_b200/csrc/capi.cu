@@ -228,6 +228,22 @@ int baemm_create(const double *coords, int64_t nv, const int64_t *tris, int64_t 
     return create_impl(coords, nv, t.data(), nt, meas, nm, device, cpu_threads, out);
 }
 
+int baemm_set_mesh(baemm_ctx *ctx, const double *coords, int64_t nv, const int64_t *tris, int64_t nt)
+{
+    return guarded(ctx, [&](Ctx &c) {
+        BAEMM_REQUIRE(coords && tris && nv > 0 && nt > 0, BAEMM_ERR_ARG, "invalid mesh arguments");
+        BAEMM_REQUIRE(nt <= (int64_t)1 << 30 && nv <= (int64_t)1 << 30, BAEMM_ERR_SIZE, "mesh too large");
+        std::vector<int32_t> t(3 * nt);
+        for (int64_t e = 0; e < 3 * nt; ++e)
+        {
+            BAEMM_REQUIRE(tris[e] >= 0 && tris[e] < nv, BAEMM_ERR_ARG,
+                          "triangle index out of range at entry " + std::to_string(e));
+            t[e] = (int32_t)tris[e];
+        }
+        c.set_mesh(coords, nv, t.data(), nt);
+    });
+}
+
 void baemm_destroy(baemm_ctx *ctx)
 {
     if (!ctx) return;
@@ -289,7 +305,10 @@ int baemm_set_block_size(baemm_ctx *ctx, int bs)
 }
 int baemm_use_diagonal(baemm_ctx *ctx, int use_it)
 {
-    return guarded(ctx, [&](Ctx &c) { c.use_diagonal = use_it != 0; });
+    return guarded(ctx, [&](Ctx &c) {
+        c.use_diagonal = use_it != 0;
+        ++c.graph_state;
+    });
 }
 int baemm_set_gmres_params(baemm_ctx *ctx, int max_iter, int max_restarts)
 {
@@ -313,11 +332,27 @@ int baemm_set_apply_mode(baemm_ctx *ctx, int mode)
         BAEMM_REQUIRE(mode == BAEMM_APPLY_FP32 || mode == BAEMM_APPLY_TC || mode == BAEMM_APPLY_FP64,
                       BAEMM_ERR_ARG, "unsupported apply mode");
         c.apply_mode = mode;
+        ++c.graph_state;
     });
+}
+int baemm_set_graphs(baemm_ctx *ctx, int on)
+{
+    return guarded(ctx, [&](Ctx &c) {
+        c.use_graphs = on != 0;
+        if (!c.use_graphs) c.clear_graphs();
+    });
+}
+int baemm_graph_stats(const baemm_ctx *ctx, int64_t *captures, int64_t *replays)
+{
+    if (!ctx || !ctx->impl) return BAEMM_ERR_ARG;
+    if (captures) *captures = ctx->impl->graph_captures;
+    if (replays) *replays = ctx->impl->graph_replays;
+    return BAEMM_OK;
 }
 int baemm_set_tuning(baemm_ctx *ctx, int key, int value)
 {
     return guarded(ctx, [&](Ctx &c) {
+        ++c.graph_state;
         switch (key)
         {
             case BAEMM_TUNE_DENSE_VARIANT:

@@ -30,6 +30,9 @@ struct Error : std::runtime_error
 
 // Process-wide count of kernel launches (reported by baemm_kernel_launch_count).
 extern std::atomic<long long> g_kernel_launches;
+// Bumped by every device-buffer (re)allocation of the library: a captured CUDA
+// graph holds raw pointers and is valid only while this stays unchanged.
+extern std::atomic<long long> g_devbuf_epoch;
 #define BAEMM_LAUNCH_CHECK()                                                                \
     do {                                                                                    \
         BAEMM_CUDA(cudaGetLastError());                                                     \
@@ -74,6 +77,7 @@ struct DevBuf
                 }
             }
             n = count;
+            g_devbuf_epoch.fetch_add(1, std::memory_order_relaxed);
         }
         return p;
     }

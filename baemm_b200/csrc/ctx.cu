@@ -3,12 +3,14 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstring>
 #include <sstream>
 
 namespace baemm
 {
 
 std::atomic<long long> g_kernel_launches{0};
+std::atomic<long long> g_devbuf_epoch{0};
 
 Ctx::Ctx(const double *coords, int64_t nv, const int32_t *tris, int64_t nt, const double *meas, int64_t nm, int dev,
          int threads)
@@ -27,26 +29,9 @@ Ctx::Ctx(const double *coords, int64_t nv, const int32_t *tris, int64_t nt, cons
     BAEMM_CUDA(cudaStreamCreateWithFlags(&own_stream, cudaStreamNonBlocking));
     stream = own_stream;
 
-    mesh.nv = nv;
-    mesh.nt = nt;
     mesh.nm = nm;
     meas_h.assign(meas, meas + 3 * nm);
-    BAEMM_CUDA(cudaMemcpyAsync(mesh.coords.reserve(3 * nv), coords, 3 * nv * sizeof(double), cudaMemcpyHostToDevice,
-                               stream));
-    BAEMM_CUDA(cudaMemcpyAsync(mesh.tris.reserve(3 * nt), tris, 3 * nt * sizeof(int32_t), cudaMemcpyHostToDevice,
-                               stream));
-    build_topology(tris);
-
-    mesh.mid_f.reserve(4 * nt); mesh.nrm_f.reserve(4 * nt);
-    mesh.area_f.reserve(nt); mesh.a3_f.reserve(nt); mesh.diag_f.reserve(nt);
-    mesh.mid_d.reserve(4 * nt); mesh.nrm_d.reserve(4 * nt);
-    mesh.area_d.reserve(nt); mesh.a3_d.reserve(nt); mesh.diag_d.reserve(nt);
-    mesh.mass_f.reserve(mass_inner_h.size()); mesh.mass_d.reserve(mass_inner_h.size());
-    mesh.lumped_f.reserve(nv); mesh.lumped_d.reserve(nv);
-    launch_geometry(mesh, false, stream);
-    launch_geometry(mesh, true, stream);
-    launch_mass_values(mesh, false, stream);
-    launch_mass_values(mesh, true, stream);
+    init_mesh(coords, nv, tris, nt);
 
     // Measurement directions padded to 4 (InitializeBuffers.hpp:415-424).
     std::vector<float> mf(4 * std::max<int64_t>(nm, 1), 0.f);
@@ -66,8 +51,114 @@ Ctx::Ctx(const double *coords, int64_t nv, const int32_t *tris, int64_t nt, cons
     sync();
 }
 
+// Mesh-dependent state (Initialize.hpp:57-353): coordinates and triangles on
+// the device, the integer topology, geometry, mass values.  Device buffers
+// only grow, so a context re-meshed with a mesh no larger than one it held
+// before allocates nothing.
+void Ctx::init_mesh(const double *coords, int64_t nv, const int32_t *tris, int64_t nt)
+{
+    mesh.nv = nv;
+    mesh.nt = nt;
+    BAEMM_CUDA(cudaMemcpyAsync(mesh.coords.reserve(3 * nv), coords, 3 * nv * sizeof(double), cudaMemcpyHostToDevice,
+                               stream));
+    BAEMM_CUDA(cudaMemcpyAsync(mesh.tris.reserve(3 * nt), tris, 3 * nt * sizeof(int32_t), cudaMemcpyHostToDevice,
+                               stream));
+    build_topology(tris);   // ends with a stream synchronisation: the host arrays are free afterwards
+
+    mesh.mid_f.reserve(4 * nt); mesh.nrm_f.reserve(4 * nt);
+    mesh.area_f.reserve(nt); mesh.a3_f.reserve(nt); mesh.diag_f.reserve(nt);
+    mesh.mid_d.reserve(4 * nt); mesh.nrm_d.reserve(4 * nt);
+    mesh.area_d.reserve(nt); mesh.a3_d.reserve(nt); mesh.diag_d.reserve(nt);
+    mesh.mass_f.reserve(mass_inner_h.size()); mesh.mass_d.reserve(mass_inner_h.size());
+    mesh.lumped_f.reserve(nv); mesh.lumped_d.reserve(nv);
+    launch_geometry(mesh, false, stream);
+    launch_geometry(mesh, true, stream);
+    launch_mass_values(mesh, false, stream);
+    launch_mass_values(mesh, true, stream);
+    tc_geo_ready = false;
+    operators_loaded = false;
+    ++mesh_generation;
+    ++graph_state;
+}
+
+// Replaces the mesh of a live context (no reference counterpart: the
+// reference builds a new Helmholtz_OpenCL per mesh).
+void Ctx::set_mesh(const double *coords, int64_t nv, const int32_t *tris, int64_t nt)
+{
+    BAEMM_CUDA(cudaSetDevice(device));
+    sync();
+    init_mesh(coords, nv, tris, nt);
+    sync();
+}
+
+void Ctx::clear_graphs()
+{
+    for (auto &kv : graph_cache)
+        if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
+    graph_cache.clear();
+}
+
+void Ctx::run_graphed(const GraphKey &key, const std::function<void()> &enqueue)
+{
+    // Capture needs a stream of our own kind (not the legacy default stream)
+    // and nothing host-side inside the work (profiling reads events back).
+    if (!use_graphs || profiling || stream == nullptr || stream == cudaStreamLegacy)
+    {
+        enqueue();
+        return;
+    }
+    const long long epoch = g_devbuf_epoch.load(std::memory_order_relaxed);
+    if (epoch != graphs_epoch || graph_state != graphs_state)
+    {
+        clear_graphs();
+        graphs_epoch = epoch;
+        graphs_state = graph_state;
+    }
+    GraphEntry &e = graph_cache[key];
+    if (e.broken || (!e.exec && e.eager_runs == 0))
+    {
+        // first use of these operands (it may allocate), or not capturable
+        ++e.eager_runs;
+        enqueue();
+        return;
+    }
+    if (!e.exec)
+    {
+        BAEMM_CUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+        bool failed = false;
+        try
+        {
+            enqueue();
+        }
+        catch (const Error &)
+        {
+            failed = true;
+        }
+        cudaGraph_t g = nullptr;
+        const cudaError_t ec = cudaStreamEndCapture(stream, &g);
+        if (failed || ec != cudaSuccess || !g ||
+            g_devbuf_epoch.load(std::memory_order_relaxed) != graphs_epoch ||
+            cudaGraphInstantiate(&e.exec, g, 0) != cudaSuccess)
+        {
+            (void)cudaGetLastError();
+            if (e.exec) cudaGraphExecDestroy(e.exec);
+            e.exec = nullptr;
+            e.broken = true;
+            if (g) cudaGraphDestroy(g);
+            enqueue();   // run it uncaptured
+            return;
+        }
+        cudaGraphDestroy(g);
+        ++graph_captures;
+    }
+    BAEMM_CUDA(cudaGraphLaunch(e.exec, stream));
+    ++graph_replays;
+    if (apply_mode == BAEMM_APPLY_TC) tc_pending = true;   // the graph may hold the tensor-core kernel
+}
+
 Ctx::~Ctx()
 {
+    clear_graphs();
     if (tc_err_host) cudaFreeHost(tc_err_host);
     for (auto &e : prof_ev)
         if (e) cudaEventDestroy(e);
@@ -173,6 +264,7 @@ void Ctx::load_parameters(const double *kappa, const zc *coeff, int wc, int wcs,
     wave_chunk_size = wcs;
     wave_chunk_count = wc / wcs;
     const int wcc = wave_chunk_count;
+    ++graph_state;
     kappa_h.assign(kappa, kappa + wcc);
     coeff_h.assign(coeff, coeff + 4 * wcc);
     factor_h = factor;
@@ -392,7 +484,18 @@ bool Ctx::mass_inverse_real(const double *X, int64_t ldX, double *Y, int64_t ldY
 {
     int it = 0;
     // ApplyMassInverse.hpp:48: max_iter = 20
-    const bool ok = cg.solve_mass(mesh, mass_values_fp64(), X, ldX, Y, ldY, ncols, tol, 20, stream, &it);
+    const bool v64 = mass_values_fp64();
+    bool ok;
+    if (use_graphs)
+    {
+        long long tb = 0;
+        std::memcpy(&tb, &tol, sizeof(tb));
+        run_graphed(GraphKey{2, X, Y, ldX, ldY, 2LL * ncols + (v64 ? 1 : 0), tb},
+                    [&] { cg.enqueue_mass(mesh, v64, X, ldX, Y, ldY, ncols, tol, 20, stream); });
+        ok = cg.finish(stream, &it);
+    }
+    else
+        ok = cg.solve_mass(mesh, v64, X, ldX, Y, ldY, ncols, tol, 20, stream, &it);
     stats.cg_iterations = std::max(stats.cg_iterations, it);
     stats.cg_converged = stats.cg_converged && ok;
     return ok;

@@ -4,6 +4,8 @@
 // OpenCL objects replaced by device buffers on one CUDA stream.
 #pragma once
 #include <complex>
+#include <functional>
+#include <map>
 #include <string>
 #include <vector>
 
@@ -132,8 +134,51 @@ public:
     // Times the dense-kernel settings of `mode` on the loaded operators and
     // keeps the fastest (tune.cu).
     void autotune(int mode, int repeats, baemm_tune_result *out);
+    // ---- CUDA graphs of the solver's inner operators (baemm_set_graphs) --------
+    // The GMRES operator apply and the CG mass inverse are fixed launch
+    // sequences; with use_graphs on, the second call with the same operands is
+    // captured and later calls replay the graph.  Any device-buffer
+    // reallocation in the library (g_devbuf_epoch) or a change of the loaded
+    // operators, mesh, mode or tuning (graph_state) drops the graphs.
+    struct GraphKey
+    {
+        int kind;
+        const void *x;
+        const void *y;
+        int64_t ldx, ldy;
+        long long a, b;   // kind-specific (columns, tolerance bits, mode, ...)
+        bool operator<(const GraphKey &o) const
+        {
+            if (kind != o.kind) return kind < o.kind;
+            if (x != o.x) return x < o.x;
+            if (y != o.y) return y < o.y;
+            if (ldx != o.ldx) return ldx < o.ldx;
+            if (ldy != o.ldy) return ldy < o.ldy;
+            if (a != o.a) return a < o.a;
+            return b < o.b;
+        }
+    };
+    struct GraphEntry
+    {
+        cudaGraphExec_t exec = nullptr;
+        int eager_runs = 0;
+        bool broken = false;
+    };
+    bool use_graphs = false;
+    long long graph_state = 0;           // bumped when captured work would change
+    long long graphs_epoch = -1, graphs_state = -1;
+    long long graph_captures = 0, graph_replays = 0;
+    std::map<GraphKey, GraphEntry> graph_cache;
+    void clear_graphs();
+    // Runs `enqueue` (which only enqueues work on `stream`) through the cache.
+    void run_graphed(const GraphKey &key, const std::function<void()> &enqueue);
+
+    // Replace the mesh (same measurement directions); unloads the operators.
+    void set_mesh(const double *coords, int64_t nv, const int32_t *tris, int64_t nt);
+    long long mesh_generation = 0;   // bumped by every mesh set-up
 
 private:
+    void init_mesh(const double *coords, int64_t nv, const int32_t *tris, int64_t nt);
     void build_topology(const int32_t *tris);
     template <class R>
     void dense_apply(const cplx<R> *Btri, cplx<R> *Ctri);

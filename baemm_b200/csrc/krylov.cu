@@ -507,6 +507,20 @@ CgSolver::~CgSolver()
 bool CgSolver::solve_mass(const MeshDev &m, bool fp64_values, const double *b, int64_t ldb, double *y, int64_t ldy,
                           int c, double tol, int max_iter, cudaStream_t st, int *iterations)
 {
+    enqueue_mass(m, fp64_values, b, ldb, y, ldy, c, tol, max_iter, st);
+    return finish(st, iterations);
+}
+
+bool CgSolver::finish(cudaStream_t st, int *iterations)
+{
+    BAEMM_CUDA(cudaStreamSynchronize(st));
+    if (iterations) *iterations = host_flags_[1];
+    return host_flags_[0] != 0;
+}
+
+void CgSolver::enqueue_mass(const MeshDev &m, bool fp64_values, const double *b, int64_t ldb, double *y,
+                            int64_t ldy, int c, double tol, int max_iter, cudaStream_t st)
+{
     const int64_t n = m.nv;
     BAEMM_REQUIRE(c >= 1 && c <= kMaxKrylovColumns, BAEMM_ERR_SIZE, "CG column count out of range");
     const int64_t N = n * c;
@@ -539,9 +553,6 @@ bool CgSolver::solve_mass(const MeshDev &m, bool fp64_values, const double *b, i
     cg_output_kernel<<<eg(N), 256, 0, st>>>(n, c, x_.p, y, ldy);
     BAEMM_LAUNCH_CHECK();
     BAEMM_CUDA(cudaMemcpyAsync(host_flags_, flags_.p, 2 * sizeof(int), cudaMemcpyDeviceToHost, st));
-    BAEMM_CUDA(cudaStreamSynchronize(st));
-    if (iterations) *iterations = host_flags_[1];
-    return host_flags_[0] != 0;
 }
 
 // =================================== GMRES host ===================================

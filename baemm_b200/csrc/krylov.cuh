@@ -32,6 +32,13 @@ public:
     // Returns true when every column converged; *iterations = iterations run.
     bool solve_mass(const MeshDev &m, bool fp64_values, const double *b, int64_t ldb, double *y, int64_t ldy, int c,
                     double tol, int max_iter, cudaStream_t st, int *iterations);
+    // The same in two parts: enqueue_mass only enqueues work on `st` (a fixed
+    // launch sequence plus a copy of the convergence flags to pinned host
+    // memory, so it can be captured in a CUDA graph); finish synchronises `st`
+    // and reads the flags.
+    void enqueue_mass(const MeshDev &m, bool fp64_values, const double *b, int64_t ldb, double *y, int64_t ldy, int c,
+                      double tol, int max_iter, cudaStream_t st);
+    bool finish(cudaStream_t st, int *iterations);
 
 private:
     DevBuf<double> x_, r_, z_, p_, q_, col_, partial_;

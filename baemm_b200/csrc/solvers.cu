@@ -28,7 +28,8 @@ void Ctx::bie_solve(const double *kappa, const zc *coeff4, const double2 *rhs, d
     stats = baemm_solve_stats{};
     stats.cg_converged = 1;
     GmresSolver<double2>::Op A = [&](const double2 *x, double2 *y) {
-        apply_boundary<double2>(kOne, x, wc, kZero, y, wc);
+        run_graphed(GraphKey{1, x, y, wc, wc, apply_mode, wave_count},
+                    [&] { apply_boundary<double2>(kOne, x, wc, kZero, y, wc); });
     };
     GmresSolver<double2>::Op P = [&](const double2 *x, double2 *y) {
         mass_inverse_complex(x, wc, y, wc, wc, cg_tol);

@@ -84,6 +84,15 @@ class Helmholtz_CUDA:
         self._user_stream = None   # set by SetStream; otherwise torch tensors join torch's current stream
 
     # --- lifecycle ---------------------------------------------------------------
+    def SetMesh(self, vertex_coords, triangles):
+        """Replace the mesh, keeping device, stream, measurement directions and
+        settings (baemm_set_mesh); the boundary operators must be loaded again."""
+        coords = _f64(vertex_coords).reshape(-1, 3)
+        tris = np.ascontiguousarray(np.asarray(triangles, dtype=np.int64).reshape(-1, 3))
+        self._ck(self._lib.baemm_set_mesh(self._h, _dp(coords), coords.shape[0],
+                                          tris.ctypes.data_as(_capi.i64p), tris.shape[0]))
+        self._coords, self._tris = coords, tris
+
     def close(self):
         if getattr(self, "_h", None):
             self._lib.baemm_destroy(self._h)
@@ -181,6 +190,16 @@ class Helmholtz_CUDA:
 
     def SetRefinement(self, max_steps: int, inner_tol: float = 1e-4):
         self._ck(self._lib.baemm_set_refinement(self._h, int(max_steps), float(inner_tol)))
+
+    def SetGraphs(self, on: bool = True):
+        """Replay the solvers' inner operators as CUDA graphs (baemm_set_graphs)."""
+        self._ck(self._lib.baemm_set_graphs(self._h, 1 if on else 0))
+
+    def GraphStats(self) -> tuple:
+        """(captures, replays) since the context was created."""
+        a, b = C.c_int64(), C.c_int64()
+        self._ck(self._lib.baemm_graph_stats(self._h, C.byref(a), C.byref(b)))
+        return int(a.value), int(b.value)
 
     def Autotune(self, mode=APPLY_TC, repeats: int = 2) -> dict:
         """Time the dense-kernel settings of `mode` on the loaded operators and

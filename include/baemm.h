@@ -89,6 +89,15 @@ int baemm_create_i32(const double *coords, int64_t vertex_count,
                      const int32_t *triangles, int64_t simplex_count,
                      const double *meas_directions, int64_t meas_count,
                      int device, int cpu_threads, baemm_ctx **out);
+/* Replace the mesh of a context, keeping its device, stream, measurement
+ * directions and settings (no reference counterpart: the reference constructs
+ * a new Helmholtz_OpenCL per mesh).  Device buffers only grow, so a mesh no
+ * larger than one the context held before allocates nothing; a serving loop
+ * re-meshes pooled contexts instead of creating and destroying them (a
+ * cudaFree synchronises the whole device).  Unloads the boundary operators;
+ * synchronises the context's stream. */
+int baemm_set_mesh(baemm_ctx *ctx, const double *coords, int64_t vertex_count,
+                   const int64_t *triangles, int64_t simplex_count);
 /* ~Helmholtz_OpenCL (Helmholtz_OpenCL.hpp:251-282). */
 void baemm_destroy(baemm_ctx *ctx);
 const char *baemm_last_error(const baemm_ctx *ctx);
@@ -139,6 +148,19 @@ int baemm_get_apply_mode(const baemm_ctx *ctx);
 #define BAEMM_TUNE_TC_STAGGER    4
 int baemm_set_tuning(baemm_ctx *ctx, int key, int value);
 int baemm_get_tuning(const baemm_ctx *ctx, int key);
+/* CUDA graphs for the solvers' inner operators (no reference counterpart;
+ * default off).  When on, the GMRES operator apply and the CG mass inverse of
+ * BoundaryPotential / DirichletToNeumann / FarField and the derivative solves
+ * run as fixed launch sequences: the second call with the same operands is
+ * captured (thread-local capture mode, on the context's stream) and later
+ * calls replay the graph, which saves the launch overhead that dominates small
+ * meshes.  Graphs are dropped when the library reallocates a device buffer or
+ * when the mesh, the loaded operators, the apply mode or the tuning change;
+ * they are not used on the legacy default stream or while profiling.  Results
+ * are the same as without graphs.  baemm_graph_stats counts captures and
+ * replays since the context was created. */
+int baemm_set_graphs(baemm_ctx *ctx, int on);
+int baemm_graph_stats(const baemm_ctx *ctx, int64_t *captures, int64_t *replays);
 /* Autotuner (no reference counterpart): times the dense-kernel settings of
  * `mode` (BAEMM_APPLY_FP32: the three plain variants; BAEMM_APPLY_TC: the
  * tensor-core segment lengths 4/8/16/32) on the loaded operators, with the

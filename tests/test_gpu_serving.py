@@ -1,0 +1,97 @@
+"""GPU tests of the serving path: re-meshing a live context, CUDA-graph replay
+of the solver's inner operators, and the serving loop (a request gives the
+same result alone and in a mix of concurrent requests)."""
+import numpy as np
+import pytest
+
+from baemm_b200 import APPLY_FP32, APPLY_TC, Helmholtz_CUDA, WaveType, meshes
+from baemm_b200.serving import SolveRequest, SolveServer, make_stream, summarize
+from tests.helpers import crandn, relerr
+
+pytestmark = pytest.mark.gpu
+
+
+def _apply(H, B, kap, coeff, wc, wcs):
+    C = np.zeros_like(B)
+    H.ApplyBoundaryOperators_PL(1.0, B, 0.0, C, kap, coeff, wc, wcs)
+    return C
+
+
+def test_set_mesh_matches_a_fresh_context():
+    """A context re-meshed (to a larger, then a smaller mesh) computes exactly
+    what a context created on that mesh computes."""
+    meas = meshes.fibonacci_sphere(16)
+    small = meshes.sh_perturbed_sphere(2, 4, 0.1, seed=1)
+    large = meshes.sh_perturbed_sphere(3, 4, 0.1, seed=2)
+    kap = [3.0]
+    coeff = np.array([[0.5, -3j, 1.0, 0.25]])
+    with Helmholtz_CUDA(*small, meas) as H:
+        for coords, tris in (large, small):
+            H.SetMesh(coords, tris)
+            B = crandn(np.random.default_rng(coords.shape[0]), coords.shape[0], 16)
+            with Helmholtz_CUDA(coords, tris, meas) as F:
+                ref = _apply(F, B, kap, coeff, 16, 16)
+                assert np.array_equal(F.Areas(), H.Areas())
+            assert H.VertexCount() == coords.shape[0]
+            assert np.array_equal(_apply(H, B, kap, coeff, 16, 16), ref)
+
+
+@pytest.mark.parametrize("mode", [APPLY_FP32, APPLY_TC])
+def test_graphs_give_the_same_solve(mode):
+    """FarField with the GMRES apply and the CG mass inverse replayed as CUDA
+    graphs equals the solve without graphs (same kernels, same order)."""
+    coords, tris = meshes.icosphere(3)
+    meas = meshes.fibonacci_sphere(32)
+    inc = meshes.fibonacci_sphere(16)
+    kap = np.array([4.0])
+    with Helmholtz_CUDA(coords, tris, meas) as H:
+        H.SetApplyMode(mode)
+        F0 = np.zeros((32, 16), complex)
+        H.FarField(kap, inc, F0, WaveType.Plane, 1e-8, 1e-8)
+        H.SetGraphs(True)
+        for _ in range(2):
+            F1 = np.zeros((32, 16), complex)
+            H.FarField(kap, inc, F1, WaveType.Plane, 1e-8, 1e-8)
+            assert relerr(F1, F0) < 1e-12
+        captures, replays = H.GraphStats()
+        assert captures > 0 and replays > captures
+
+
+def _requests(n, seed):
+    reqs = make_stream(n, rate=0.0, levels=(2, 3), kappa_range=(1.0, 6.0), rhs_range=(1, 40), degree=4,
+                       seed=seed)
+    for r in reqs:
+        r.gmres_tol = 1e-8
+    return reqs
+
+
+def test_result_is_the_same_alone_and_in_the_mix():
+    """Each request's far field served concurrently with others equals the
+    same request served alone (tolerance 1e-10: the kernels are deterministic;
+    only the interleaving of other requests' work differs)."""
+    meas = meshes.fibonacci_sphere(24)
+    reqs = _requests(10, seed=7)
+    with SolveServer(meas, slots=4, graphs=True) as srv:
+        mix = srv.run(reqs, realtime=False)
+        assert srv.scheduler.peak_running > 1
+    for r in reqs[:4]:
+        with SolveServer(meas, slots=1, graphs=False) as alone:
+            one = alone.run([SolveRequest(r.rid, r.coords, r.triangles, r.kappa, r.directions,
+                                          gmres_tol=r.gmres_tol)], realtime=False)
+        assert one[r.rid].converged and mix[r.rid].converged
+        assert relerr(mix[r.rid].far_field, one[r.rid].far_field) < 1e-10
+    s = summarize(mix)
+    assert s["requests"] == 10 and s["converged"] == 10
+
+
+def test_served_tensor_core_matches_plain():
+    """Served tensor-core solves agree with plain FP32 solves at the solve
+    tolerance (the accuracy the serving comparison is stated at)."""
+    meas = meshes.fibonacci_sphere(24)
+    reqs = _requests(4, seed=11)
+    with SolveServer(meas, slots=2, apply_mode=APPLY_TC) as a, SolveServer(meas, slots=1, apply_mode=APPLY_FP32,
+                                                                          graphs=False) as b:
+        ra = a.run(reqs, realtime=False)
+        rb = b.run(reqs, realtime=False)
+    for r in reqs:
+        assert relerr(ra[r.rid].far_field, rb[r.rid].far_field) < 1e-5
