@@ -450,6 +450,72 @@ def run_solve_workload(args):
     return 0
 
 
+# ---------------------------------------------------------------------------
+# the serving workload (--workload serve): not the headline line
+# ---------------------------------------------------------------------------
+def run_serve_workload(args):
+    """Stream of scattering-solve requests (icosphere levels 4-6 radially
+    perturbed by a random degree-8 spherical-harmonic field of amplitude 0.1,
+    kappa ~ U[1, 10], 1-64 plane waves, GMRES to 1e-6, far field at 128
+    directions).  Three runs over the same requests:
+      sequential  the plain FP32 apply, one request at a time (the baseline);
+      capacity    the serving loop (slots of resident contexts, memory-budget
+                  admission, tensor-core apply, CUDA-graph replay) with every
+                  request queued at once: solves/s is its throughput;
+      latency     the serving loop with Poisson arrivals at 80 % of that
+                  capacity: p50 / p99 of finish - arrival.
+    The far fields of the served runs are compared with the sequential ones."""
+    from baemm_b200 import APPLY_FP32, APPLY_TC, meshes
+    from baemm_b200.serving import SolveServer, make_stream, summarize
+    meas = meshes.fibonacci_sphere(128)
+    reqs = make_stream(args.requests, rate=0.0, seed=args.serve_seed)
+    warm = make_stream(2, rate=0.0, levels=(4,), seed=12345)
+
+    def at_once():
+        for r in reqs:
+            r.arrival = 0.0
+        return reqs
+
+    with SolveServer(meas, slots=1, apply_mode=APPLY_FP32, graphs=False) as seq:
+        seq.run(warm, realtime=False)
+        t0 = time.perf_counter()
+        base = seq.run(at_once(), realtime=False)
+        t_seq = time.perf_counter() - t0
+    thr_plain = len(reqs) / t_seq
+    with SolveServer(meas, slots=args.slots, apply_mode=APPLY_TC, graphs=True) as srv:
+        srv.run(warm, realtime=False)
+        t0 = time.perf_counter()
+        cap = srv.run(at_once(), realtime=False)
+        t_cap = time.perf_counter() - t0
+        peak = srv.scheduler.peak_running
+        thr_served = len(reqs) / t_cap
+        rate = 0.8 * thr_served
+        rng = np.random.default_rng(args.serve_seed + 1)
+        t = 0.0
+        for r in reqs:
+            t += rng.exponential(1.0 / rate)
+            r.arrival = t
+        lat = srv.run(reqs, realtime=True)
+    s_lat = summarize(lat)
+    diff = max(max(float(np.linalg.norm(run[k].far_field - base[k].far_field) /
+                         max(np.linalg.norm(base[k].far_field), 1e-300)) for k in base) for run in (cap, lat))
+    line = {"metric": "served solves/s (scattering, FarField)", "value": thr_served, "unit": "solves/s",
+            "n_gpus": 1, "higher_is_better": True, "data": "synthetic",
+            "config": {"workload": "perturbed-icosphere scattering solves, levels 4-6, kappa U[1,10], 1-64 plane "
+                                   "waves, GMRES 1e-6, far field at 128 directions",
+                       "requests": len(reqs), "slots": args.slots, "seed": args.serve_seed},
+            "capacity": {"solves_per_s": thr_served, "seconds": t_cap, "peak_concurrent": peak,
+                         "converged": int(sum(r.converged for r in cap.values()))},
+            "latency_at_80pct_load": {"arrival_rate_per_s": rate, "p50_s": s_lat["p50_latency_s"],
+                                      "p99_s": s_lat["p99_latency_s"], "mean_s": s_lat["mean_latency_s"],
+                                      "solves_per_s": s_lat["solves_per_s"]},
+            "sequential_plain_fp32": {"solves_per_s": thr_plain, "seconds": t_seq},
+            "speedup_vs_sequential_plain": thr_served / thr_plain,
+            "max_far_field_rel_diff_served_vs_sequential": diff}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -460,8 +526,12 @@ def main(argv=None):
                     help="apply arithmetic: plain FP32, compensated tensor-core (default), FP64")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-compare", action="store_true", help="skip the plain-FP32 and FP64 comparison applies")
-    ap.add_argument("--workload", default="apply", choices=["apply", "solve"],
-                    help="apply: the headline operator-apply line; solve: the scattering-solve configuration")
+    ap.add_argument("--workload", default="apply", choices=["apply", "solve", "serve"],
+                    help="apply: the headline operator-apply line; solve: the scattering-solve configuration; "
+                         "serve: the request stream through the serving loop")
+    ap.add_argument("--requests", type=int, default=100, help="requests of --workload serve")
+    ap.add_argument("--slots", type=int, default=6, help="serving slots of --workload serve")
+    ap.add_argument("--serve-seed", type=int, default=0)
     ap.add_argument("--solve-level", type=int, default=6, help="icosphere level of --workload solve")
     ap.add_argument("--small", action="store_true", help="38400-triangle torus (profiling captures only)")
     args = ap.parse_args(argv)
@@ -472,6 +542,8 @@ def main(argv=None):
         return run_reference_arm(args, rank, world)
     if args.workload == "solve":
         return run_solve_workload(args) if rank == 0 else 0
+    if args.workload == "serve":
+        return run_serve_workload(args) if rank == 0 else 0
     if world > 1:
         import datetime
 
