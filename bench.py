@@ -212,6 +212,26 @@ def run_reference_arm(args, rank, world):
 
 
 # ---------------------------------------------------------------------------
+# replicas across ranks
+# ---------------------------------------------------------------------------
+def max_over_ranks(x: float, dist, device) -> float:
+    """The largest `x` over all ranks (the job takes as long as its slowest
+    replica); `dist` None means a single process."""
+    if not dist:
+        return float(x)
+    import torch
+    t = torch.tensor([x], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job_rate(world: int, interactions_per_step: int, steps: int, total_ms: float) -> float:
+    """GInteractions/s of the whole job: every rank applies the same workload
+    `steps` times (weak scaling) in at most `total_ms`."""
+    return world * interactions_per_step * steps / (total_ms * 1e-3) / 1e9
+
+
+# ---------------------------------------------------------------------------
 # the CUDA arm
 # ---------------------------------------------------------------------------
 def run_gpu_arm(args, rank, world, local_rank):
@@ -262,12 +282,8 @@ def run_gpu_arm(args, rank, world, local_rank):
         torch.cuda.synchronize()
     launches = H.KernelLaunchCount() - launches0 - 0  # library kernels only (flush is torch's)
     step_ms = [a.elapsed_time(b) for a, b in ev]
-    total_ms = float(np.sum(step_ms))
-    if dist:
-        t = torch.tensor([total_ms], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
-    value = world * inter * args.steps / (total_ms * 1e-3) / 1e9
+    total_ms = max_over_ranks(float(np.sum(step_ms)), dist, "cuda")
+    value = whole_job_rate(world, inter, args.steps, total_ms)
 
     # ---- e2e through the host-pointer C ABI (pinned host buffers) -----------------
     Bh = torch.from_numpy(B).pin_memory().numpy()
@@ -285,12 +301,8 @@ def run_gpu_arm(args, rank, world, local_rank):
         t0 = time.perf_counter()
         H.ApplyBoundaryOperators_PL(1.0, Bh, 0.0, Ch)   # H2D, apply, D2H, synchronised
         e2e_ms.append((time.perf_counter() - t0) * 1e3)
-    e2e_total = float(np.sum(e2e_ms))
-    if dist:
-        t = torch.tensor([e2e_total], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_total = float(t.item())
-    e2e_value = world * inter * args.steps / (e2e_total * 1e-3) / 1e9
+    e2e_total = max_over_ranks(float(np.sum(e2e_ms)), dist, "cuda")
+    e2e_value = whole_job_rate(world, inter, args.steps, e2e_total)
     # ---- plain FP32 form and accuracy against the FP64 apply (rank 0, untimed for value) ----
     compare = None
     if rank == 0 and not args.no_compare:
