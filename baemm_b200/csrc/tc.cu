@@ -386,7 +386,10 @@ struct PieceIter
     }
 };
 
-template <int CH, bool SL, bool DL, bool ADL>
+// RI: every chunk's single-layer coefficient is imaginary and its double- and
+// adjoint-double-layer coefficients are real (the mixed BIE and DtN tuples of
+// FarField.hpp), so the double-layer factor u below is real.
+template <int CH, bool SL, bool DL, bool ADL, bool RI>
 __global__ void __launch_bounds__(TC_THREADS, 1)
 boundary_tc_kernel(const float *__restrict__ mid4, const float *__restrict__ nrm4, const TcTileGeo *__restrict__ tgeo,
                    const float2 *__restrict__ Btri, float2 *__restrict__ Ctri, float2 *__restrict__ ws,
@@ -596,12 +599,25 @@ boundary_tc_kernel(const float *__restrict__ mid4, const float *__restrict__ nrm
                             __sincosf(kr.y, &sn1, &cs1);
                             const float2 cs = make_float2(cs0, cs1), sn = make_float2(sn0, sn1);
                             float2 hx = make_float2(0.f, 0.f), hy = make_float2(0.f, 0.f);
-                            if (SL)
+                            if (RI)
+                            {
+                                // c1 = i c1y, c2 and c3 real: u = (ux, 0), hx = ux, hy = c1y / r - k r ux
+                                if (SL) hy = __fmul2_rn(c1y, rinv[p]);
+                                if (DL || ADL)
+                                {
+                                    float2 ux = DL ? __fmul2_rn(nc2x, dmu[p]) : make_float2(0.f, 0.f);
+                                    if (ADL) ux = DL ? __ffma2_rn(c3x, dnu[p], ux) : __fmul2_rn(c3x, dnu[p]);
+                                    const float2 nkr = __fmul2_rn(nkap, r[p]);
+                                    hx = ux;
+                                    hy = SL ? __ffma2_rn(nkr, ux, hy) : __fmul2_rn(nkr, ux);
+                                }
+                            }
+                            else if (SL)
                             {
                                 hx = __fmul2_rn(c1x, rinv[p]);
                                 hy = __fmul2_rn(c1y, rinv[p]);
                             }
-                            if (DL || ADL)
+                            if (!RI && (DL || ADL))
                             {
                                 float2 ux = make_float2(0.f, 0.f), uy = make_float2(0.f, 0.f);
                                 if (DL) { ux = __fmul2_rn(nc2x, dmu[p]); uy = __fmul2_rn(nc2y, dmu[p]); }
@@ -920,7 +936,7 @@ __global__ void tc_fixup_kernel(const float2 *__restrict__ ws, float2 *__restric
     }
 }
 
-template <int CH, bool SL, bool DL, bool ADL>
+template <int CH, bool SL, bool DL, bool ADL, bool RI>
 void tc_launch(cudaStream_t st, const float *mid, const float *nrm, const TcTileGeo *tg, const float2 *B, float2 *C,
                float2 *ws, const ChunkParamsF *p, const TcPlan &plan, int *err)
 {
@@ -930,26 +946,26 @@ void tc_launch(cudaStream_t st, const float *mid, const float *nrm, const TcTile
     static std::once_flag once;
     static cudaError_t attr = cudaSuccess;
     std::call_once(once, [&] {
-        attr = cudaFuncSetAttribute(boundary_tc_kernel<CH, SL, DL, ADL>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        attr = cudaFuncSetAttribute(boundary_tc_kernel<CH, SL, DL, ADL, RI>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     (int)bytes);
     });
     BAEMM_CUDA(attr);
-    boundary_tc_kernel<CH, SL, DL, ADL><<<plan.ctas, TC_THREADS, bytes, st>>>(mid, nrm, tg, B, C, ws, p, plan, err);
+    boundary_tc_kernel<CH, SL, DL, ADL, RI><<<plan.ctas, TC_THREADS, bytes, st>>>(mid, nrm, tg, B, C, ws, p, plan, err);
 }
 
-template <int CH>
+template <int CH, bool RI>
 void tc_flags(int code, cudaStream_t st, const float *mid, const float *nrm, const TcTileGeo *tg, const float2 *B,
               float2 *C, float2 *ws, const ChunkParamsF *p, const TcPlan &plan, int *err)
 {
     switch (code)
     {
-        case 1: tc_launch<CH, true, false, false>(st, mid, nrm, tg, B, C, ws, p, plan, err); break;
-        case 2: tc_launch<CH, false, true, false>(st, mid, nrm, tg, B, C, ws, p, plan, err); break;
-        case 3: tc_launch<CH, true, true, false>(st, mid, nrm, tg, B, C, ws, p, plan, err); break;
-        case 4: tc_launch<CH, false, false, true>(st, mid, nrm, tg, B, C, ws, p, plan, err); break;
-        case 5: tc_launch<CH, true, false, true>(st, mid, nrm, tg, B, C, ws, p, plan, err); break;
-        case 6: tc_launch<CH, false, true, true>(st, mid, nrm, tg, B, C, ws, p, plan, err); break;
-        case 7: tc_launch<CH, true, true, true>(st, mid, nrm, tg, B, C, ws, p, plan, err); break;
+        case 1: tc_launch<CH, true, false, false, RI>(st, mid, nrm, tg, B, C, ws, p, plan, err); break;
+        case 2: tc_launch<CH, false, true, false, RI>(st, mid, nrm, tg, B, C, ws, p, plan, err); break;
+        case 3: tc_launch<CH, true, true, false, RI>(st, mid, nrm, tg, B, C, ws, p, plan, err); break;
+        case 4: tc_launch<CH, false, false, true, RI>(st, mid, nrm, tg, B, C, ws, p, plan, err); break;
+        case 5: tc_launch<CH, true, false, true, RI>(st, mid, nrm, tg, B, C, ws, p, plan, err); break;
+        case 6: tc_launch<CH, false, true, true, RI>(st, mid, nrm, tg, B, C, ws, p, plan, err); break;
+        case 7: tc_launch<CH, true, true, true, RI>(st, mid, nrm, tg, B, C, ws, p, plan, err); break;
         default: break;
     }
 }
@@ -1016,9 +1032,20 @@ void launch_boundary_tc(const MeshDev &m, const OpFlags &f, const void *chunk_pa
     const float *mid = m.mid_f, *nrm = m.nrm_f;
     const auto *tg = reinterpret_cast<const TcTileGeo *>(tgeo);
     BAEMM_REQUIRE(tg, BAEMM_ERR_ARG, "tensor-core tile geometry missing");
-    if (CH == 4) tc_flags<4>(code, st, mid, nrm, tg, Btri, Ctri, ws, p, plan, err);
-    else if (CH == 2) tc_flags<2>(code, st, mid, nrm, tg, Btri, Ctri, ws, p, plan, err);
-    else tc_flags<1>(code, st, mid, nrm, tg, Btri, Ctri, ws, p, plan, err);
+    // the real / imaginary coefficient structure of the BIE solves (see boundary_tc_kernel)
+    const bool ri = !f.re_sl && !f.im_dl && !f.im_adl && (f.dl() || f.adl());
+    if (ri)
+    {
+        if (CH == 4) tc_flags<4, true>(code, st, mid, nrm, tg, Btri, Ctri, ws, p, plan, err);
+        else if (CH == 2) tc_flags<2, true>(code, st, mid, nrm, tg, Btri, Ctri, ws, p, plan, err);
+        else tc_flags<1, true>(code, st, mid, nrm, tg, Btri, Ctri, ws, p, plan, err);
+    }
+    else
+    {
+        if (CH == 4) tc_flags<4, false>(code, st, mid, nrm, tg, Btri, Ctri, ws, p, plan, err);
+        else if (CH == 2) tc_flags<2, false>(code, st, mid, nrm, tg, Btri, Ctri, ws, p, plan, err);
+        else tc_flags<1, false>(code, st, mid, nrm, tg, Btri, Ctri, ws, p, plan, err);
+    }
     BAEMM_LAUNCH_CHECK();
     if (plan.tail_blocks > 0)
     {

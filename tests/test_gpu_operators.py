@@ -113,7 +113,7 @@ def test_apply_boundary_fp64(env, cname, wname):
     assert relerr(Cg, C64) < FP64_TOL
 
 
-@pytest.mark.parametrize("cname", ["sl", "dl", "adl", "bie", "all"])
+@pytest.mark.parametrize("cname", ["sl", "dl", "adl", "bie", "dtn", "all"])
 @pytest.mark.parametrize("wname", ["w16", "w32", "w64"])
 def test_apply_boundary_tensor_core(env, cname, wname):
     """Compensated tensor-core form (TF32 hi/lo, FP32 accumulation): within
