@@ -528,6 +528,82 @@ def run_serve_workload(args):
     return 0
 
 
+# ---------------------------------------------------------------------------
+# the Gauss-Newton workload (--workload gauss-newton): not the headline line
+# ---------------------------------------------------------------------------
+def run_gn_workload(args):
+    """One Gauss-Newton shape step (GaussNewtonSolve, FarField.hpp:457-604) on
+    the configuration: initial shape the icosphere level 5 (10242 V, 20480 T),
+    synthetic far-field data from a target shape perturbed by a degree-6
+    spherical-harmonic field of amplitude 0.05, 2 wavenumbers {2, 4} x 32
+    Fibonacci plane-wave directions, 128 far-field directions.  The right-hand
+    side is the adjoint derivative of the far-field residual; the system
+    (regpar M + DF* DF) X = B is solved by CG (outer tolerance 1e-8) with
+    M = regpar x mass and the lumped-mass preconditioner (the reference's
+    tangent-point metric lives in an unvendored library).  Runs: plain FP32,
+    tensor-core, tensor-core inside FP64 iterative refinement, FP64; error of X
+    against the FP64 run."""
+    from baemm_b200 import APPLY_FP32, APPLY_FP64, APPLY_TC, Helmholtz_CUDA, WaveType, meshes
+    coords, tris = meshes.icosphere(args.gn_level)
+    tcoords, ttris = meshes.sh_perturbed_sphere(args.gn_level, 6, 0.05, seed=5)
+    meas = meshes.fibonacci_sphere(128)
+    inc = meshes.fibonacci_sphere(32)
+    kap = np.array([2.0, 4.0])
+    wc = 64
+    regpar = 0.1
+    with Helmholtz_CUDA(tcoords, ttris, meas) as T:
+        T.SetApplyMode(APPLY_FP64)
+        F_data = np.zeros((meas.shape[0], wc), complex)
+        T.FarField(kap, inc, F_data, WaveType.Plane, 1e-12, 1e-12)
+    H = Helmholtz_CUDA(coords, tris, meas)
+    H.gmres_max_restarts = 10     # caps the outer CG at 30 x 10 iterations (and the inner GMRES at 10 cycles)
+    nv = coords.shape[0]
+
+    def Mop(x, y):
+        H.MassDot(regpar, x, 0.0, y)
+
+    def Pop(x, y):
+        H.ApplyLumpedMassInverse(x, y)
+        y /= regpar
+
+    def step(mode, ir_steps=0):
+        H.SetApplyMode(mode)
+        H.SetRefinement(ir_steps, 1e-6)
+        t0 = time.perf_counter()
+        F0 = np.zeros((meas.shape[0], wc), complex)
+        H.FarField(kap, inc, F0, WaveType.Plane, 1e-12, 1e-10)
+        du = np.zeros((nv, wc), complex)
+        H.Derivative_FF_Helper(kap, inc, du, WaveType.Plane, 1e-12, 1e-10)
+        B = np.zeros((nv, 3))
+        H.AdjointDerivative_FF(kap, inc, F0 - F_data, B, du, WaveType.Plane, 1e-12, 1e-10)
+        X = np.zeros((nv, 3))
+        ok = H.GaussNewtonSolve(kap, inc, Mop, Pop, 1.0, B, 0.0, X, du, WaveType.Plane, 1e-12, 1e-10, 1e-8,
+                                solver=1)
+        dt = time.perf_counter() - t0
+        st = H.LastSolveStats()
+        H.SetRefinement(0)
+        H.SetApplyMode(APPLY_FP32)
+        return X, dt, bool(ok), int(st["gmres_iterations"]), float(st["gmres_relative_residual"])
+
+    r64 = step(APPLY_FP64)
+    X64 = r64[0]
+    runs = {"fp64": r64, "fp32": step(APPLY_FP32), "tc": step(APPLY_TC), "tc_fp64ir": step(APPLY_TC, ir_steps=6)}
+    n64 = float(np.linalg.norm(X64))
+    res = {k: {"seconds": v[1], "converged": v[2], "cg_iterations": v[3], "cg_relative_residual": v[4],
+               "rel_err_vs_fp64": float(np.linalg.norm(v[0] - X64) / n64)}
+           for k, v in runs.items()}
+    line = {"metric": "Gauss-Newton shape step (s)", "value": res["tc_fp64ir"]["seconds"], "unit": "s",
+            "n_gpus": 1, "higher_is_better": False, "data": "synthetic",
+            "config": {"workload": f"icosphere level {args.gn_level} ({nv} V, {tris.shape[0]} T), kappa {{2,4}} x 32 "
+                                   "plane waves, 128 far-field directions, CG to 1e-8 on regpar M + DF*DF, regpar 0.1",
+                       "wave_count": wc},
+            "runs": res,
+            "note": "each run: far field, du/dn, adjoint-derivative gradient, GaussNewtonSolve (wall time)"}
+    print(json.dumps(line), flush=True)
+    H.close()
+    return 0
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -538,12 +614,13 @@ def main(argv=None):
                     help="apply arithmetic: plain FP32, compensated tensor-core (default), FP64")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-compare", action="store_true", help="skip the plain-FP32 and FP64 comparison applies")
-    ap.add_argument("--workload", default="apply", choices=["apply", "solve", "serve"],
+    ap.add_argument("--workload", default="apply", choices=["apply", "solve", "serve", "gauss-newton"],
                     help="apply: the headline operator-apply line; solve: the scattering-solve configuration; "
                          "serve: the request stream through the serving loop")
     ap.add_argument("--requests", type=int, default=100, help="requests of --workload serve")
     ap.add_argument("--slots", type=int, default=6, help="serving slots of --workload serve")
     ap.add_argument("--serve-seed", type=int, default=0)
+    ap.add_argument("--gn-level", type=int, default=5, help="icosphere level of --workload gauss-newton")
     ap.add_argument("--solve-level", type=int, default=6, help="icosphere level of --workload solve")
     ap.add_argument("--small", action="store_true", help="38400-triangle torus (profiling captures only)")
     args = ap.parse_args(argv)
@@ -556,6 +633,8 @@ def main(argv=None):
         return run_solve_workload(args) if rank == 0 else 0
     if args.workload == "serve":
         return run_serve_workload(args) if rank == 0 else 0
+    if args.workload == "gauss-newton":
+        return run_gn_workload(args) if rank == 0 else 0
     if world > 1:
         import datetime
 

@@ -116,6 +116,28 @@ public:
     void UseDiagonal(bool use_it) { check(baemm_use_diagonal(ctx_, use_it ? 1 : 0), "UseDiagonal"); }
     void SetApplyMode(int mode) { check(baemm_set_apply_mode(ctx_, mode), "SetApplyMode"); }
     void SetRefinement(int steps, double inner_tol) { check(baemm_set_refinement(ctx_, steps, inner_tol), "SetRefinement"); }
+    // Additions without reference counterpart (see include/baemm.h).
+    void SetTuning(int key, int value) { check(baemm_set_tuning(ctx_, key, value), "SetTuning"); }
+    int GetTuning(int key) const { return baemm_get_tuning(ctx_, key); }
+    baemm_tune_result Autotune(int mode, int repeats = 2)
+    {
+        baemm_tune_result r{};
+        check(baemm_autotune(ctx_, mode, repeats, &r), "Autotune");
+        return r;
+    }
+    void SetGraphs(bool on) { check(baemm_set_graphs(ctx_, on ? 1 : 0), "SetGraphs"); }
+    template <typename ExtReal, typename ExtInt>
+    void SetMesh(const ExtReal *coords, ExtInt nv, const ExtInt *tris, ExtInt nt)
+    {
+        auto c = to_d(coords, 3 * (size_t)nv);
+        std::vector<int64_t> t(3 * (size_t)nt);
+        for (size_t e = 0; e < t.size(); ++e) t[e] = (int64_t)tris[e];
+        if (check(baemm_set_mesh(ctx_, c.data(), (int64_t)nv, t.data(), (int64_t)nt), "SetMesh"))
+        {
+            areas_.clear(); normals_.clear(); midpoints_.clear(); diag_.clear();
+            mass_ = MassMatrix_T{};
+        }
+    }
 
     const Real *Areas() { return tri_field(areas_, baemm_get_areas, 1); }
     const Real *TriangleAreas() { return Areas(); }

@@ -36,5 +36,12 @@ int main()
                                        w.data(), du_dn, WaveType::Plane, Real(1e-5), Real(1e-4));
     std::printf("%s |F| = %g\n", H.ClassName().c_str(), std::abs(F[0]));
     std::free(du_dn);
+    // additions: re-mesh the context in place, graphs, tuning
+    H.SetMesh(coords.data(), Int(6), tris.data(), Int(8));
+    H.SetGraphs(true);
+    H.SetTuning(BAEMM_TUNE_TC_SEGMENT, 8);
+    H.SetApplyMode(BAEMM_APPLY_TC);
+    H.FarField<wave_count>(kappa.data(), wave_chunk_count, inc.data(), wave_chunk_size, F.data(), WaveType::Plane,
+                           Real(1e-5), Real(1e-4));
     return 0;
 }
