@@ -448,7 +448,8 @@ boundary_tc_kernel(const float *__restrict__ mid4, const float *__restrict__ nrm
     if (tid < TC_GEN_THREADS)
     {
         // ------------------------------ generators ------------------------------
-        constexpr int CC = CH >= 2 ? 2 : 1;   // chunks evaluated together (independent work for latency hiding)
+        constexpr int CC = 1;                 // A stages published together
+        uint32_t hiA[16], loA[16], hiB[16], loB[16];   // alternating register buffers of consecutive chunks
         const int q = warp & 3, g = warp >> 2;
         const int row = q * 32 + lane;
         const uint32_t lane_addr = tbase + ((uint32_t)(q * 32) << 16);
@@ -565,119 +566,104 @@ boundary_tc_kernel(const float *__restrict__ mid4, const float *__restrict__ nrm
                     }
                 }
                 mbar_arrive(&sm.r_empty[rs]);
-                // not unrolled: the step body is large, and two copies of it
-                // overflow the instruction cache
-                #pragma unroll 1
-                for (int c0 = 0; c0 < CH; c0 += CC)
-                {
-                    // test the A stages this step fills now; the answer arrives during the math
-                    int stage[CC];
-                    bool ready[CC];
+                // One chunk: evaluate its kernel entries into (hi, lo), publish the
+                // previous chunk's A stage, store this one.  Consecutive chunks use
+                // the two register buffers alternately, so the math of a chunk never
+                // writes registers the previous chunk's TMEM stores still read.
+                auto do_chunk = [&](int c, uint32_t (&hi)[16], uint32_t (&lo)[16]) -> bool {
+                    const int u = T * CH + c;
+                    const int stage = u % TC_ASTAGES;
+                    // test the A stage now; the answer arrives during the math
+                    bool ready = u < TC_ASTAGES ||
+                                 mbar_test_wait(&sm.a_empty[stage], (uint32_t)((u / TC_ASTAGES) - 1) & 1u);
+                    const float2 *P = sm.prm[cg * CH + c];
+                    const float2 kap = P[0], nkap = P[1], c1x = P[2], c1y = P[3];
+                    const float2 nc2x = P[4], nc2y = P[5], c3x = P[6], c3y = P[7];
                     #pragma unroll
-                    for (int k = 0; k < CC; ++k)
+                    for (int p = 0; p < 4; ++p)
                     {
-                        const int u = T * CH + c0 + k;
-                        stage[k] = u % TC_ASTAGES;
-                        ready[k] = u < TC_ASTAGES ||
-                                   mbar_test_wait(&sm.a_empty[stage[k]], (uint32_t)((u / TC_ASTAGES) - 1) & 1u);
-                    }
-                    uint32_t hi[CC][16], lo[CC][16];
-                    #pragma unroll
-                    for (int k = 0; k < CC; ++k)
-                    {
-                        const float2 *P = sm.prm[cg * CH + c0 + k];
-                        const float2 kap = P[0], nkap = P[1], c1x = P[2], c1y = P[3];
-                        const float2 nc2x = P[4], nc2y = P[5], c3x = P[6], c3y = P[7];
-                        #pragma unroll
-                        for (int p = 0; p < 4; ++p)
+                        // A = e^{i k r} h,  h = c1 / r + w (i k r - 1) = c1 / r + u + i k r (-u),  u = -w
+                        //   hx = c1x / r + ux + k r uy,   hy = c1y / r + uy - k r ux
+                        const float2 kr = __fmul2_rn(kap, r[p]);
+                        float sn0, cs0, sn1, cs1;
+                        __sincosf(kr.x, &sn0, &cs0);
+                        __sincosf(kr.y, &sn1, &cs1);
+                        const float2 cs = make_float2(cs0, cs1), sn = make_float2(sn0, sn1);
+                        float2 hx = make_float2(0.f, 0.f), hy = make_float2(0.f, 0.f);
+                        if (RI)
                         {
-                            // A = e^{i k r} h,  h = c1 / r + w (i k r - 1) = c1 / r + u + i k r (-u),  u = -w
-                            //   hx = c1x / r + ux + k r uy,   hy = c1y / r + uy - k r ux
-                            const float2 kr = __fmul2_rn(kap, r[p]);
-                            float sn0, cs0, sn1, cs1;
-                            __sincosf(kr.x, &sn0, &cs0);
-                            __sincosf(kr.y, &sn1, &cs1);
-                            const float2 cs = make_float2(cs0, cs1), sn = make_float2(sn0, sn1);
-                            float2 hx = make_float2(0.f, 0.f), hy = make_float2(0.f, 0.f);
-                            if (RI)
+                            // c1 = i c1y, c2 and c3 real: u = (ux, 0), hx = ux, hy = c1y / r - k r ux
+                            if (SL) hy = __fmul2_rn(c1y, rinv[p]);
+                            if (DL || ADL)
                             {
-                                // c1 = i c1y, c2 and c3 real: u = (ux, 0), hx = ux, hy = c1y / r - k r ux
-                                if (SL) hy = __fmul2_rn(c1y, rinv[p]);
-                                if (DL || ADL)
-                                {
-                                    float2 ux = DL ? __fmul2_rn(nc2x, dmu[p]) : make_float2(0.f, 0.f);
-                                    if (ADL) ux = DL ? __ffma2_rn(c3x, dnu[p], ux) : __fmul2_rn(c3x, dnu[p]);
-                                    const float2 nkr = __fmul2_rn(nkap, r[p]);
-                                    hx = ux;
-                                    hy = SL ? __ffma2_rn(nkr, ux, hy) : __fmul2_rn(nkr, ux);
-                                }
-                            }
-                            else if (SL)
-                            {
-                                hx = __fmul2_rn(c1x, rinv[p]);
-                                hy = __fmul2_rn(c1y, rinv[p]);
-                            }
-                            if (!RI && (DL || ADL))
-                            {
-                                float2 ux = make_float2(0.f, 0.f), uy = make_float2(0.f, 0.f);
-                                if (DL) { ux = __fmul2_rn(nc2x, dmu[p]); uy = __fmul2_rn(nc2y, dmu[p]); }
-                                if (ADL) { ux = __ffma2_rn(c3x, dnu[p], ux); uy = __ffma2_rn(c3y, dnu[p], uy); }
+                                float2 ux = DL ? __fmul2_rn(nc2x, dmu[p]) : make_float2(0.f, 0.f);
+                                if (ADL) ux = DL ? __ffma2_rn(c3x, dnu[p], ux) : __fmul2_rn(c3x, dnu[p]);
                                 const float2 nkr = __fmul2_rn(nkap, r[p]);
-                                hx = __ffma2_rn(kr, uy, __fadd2_rn(hx, ux));
-                                hy = __ffma2_rn(nkr, ux, __fadd2_rn(hy, uy));
+                                hx = ux;
+                                hy = SL ? __ffma2_rn(nkr, ux, hy) : __fmul2_rn(nkr, ux);
                             }
-                            // (ax, ay) = (hx cs - hy sn, hx sn + hy cs)
-                            const float2 msn = __fmul2_rn(m1, sn);
-                            const float2 ax = __ffma2_rn(hy, msn, __fmul2_rn(hx, cs));
-                            const float2 ay = __ffma2_rn(hy, cs, __fmul2_rn(hx, sn));
-                            // hi = the FP32 bits (read as TF32 by the tensor core), lo = x - trunc_tf32(x)
-                            const float2 tx = make_float2(__uint_as_float(__float_as_uint(ax.x) & 0xffffe000u),
-                                                          __uint_as_float(__float_as_uint(ax.y) & 0xffffe000u));
-                            const float2 ty = make_float2(__uint_as_float(__float_as_uint(ay.x) & 0xffffe000u),
-                                                          __uint_as_float(__float_as_uint(ay.y) & 0xffffe000u));
-                            const float2 lx = __ffma2_rn(tx, m1, ax), ly = __ffma2_rn(ty, m1, ay);
-                            hi[k][4 * p + 0] = __float_as_uint(ax.x);
-                            hi[k][4 * p + 1] = __float_as_uint(ax.y);
-                            hi[k][4 * p + 2] = __float_as_uint(ay.x);
-                            hi[k][4 * p + 3] = __float_as_uint(ay.y);
-                            lo[k][4 * p + 0] = __float_as_uint(lx.x);
-                            lo[k][4 * p + 1] = __float_as_uint(lx.y);
-                            lo[k][4 * p + 2] = __float_as_uint(ly.x);
-                            lo[k][4 * p + 3] = __float_as_uint(ly.y);
                         }
-                    }
-                    // publish the previous step's stages now that their stores had this step's math to land
-                    publish();
-                    #pragma unroll
-                    for (int k = 0; k < CC; ++k)
-                        if (!ready[k])
+                        else if (SL)
                         {
-                            const int u = T * CH + c0 + k;
-                            ready[k] = wait_bar(&sm.a_empty[stage[k]], (uint32_t)((u / TC_ASTAGES) - 1) & 1u,
-                                                abort_flag, err, 3);
+                            hx = __fmul2_rn(c1x, rinv[p]);
+                            hy = __fmul2_rn(c1y, rinv[p]);
                         }
-                    // the tcgen05 stores below are warp-collective: the warp agrees on the outcome
-                    bool all = true;
-                    #pragma unroll
-                    for (int k = 0; k < CC; ++k) all = all && ready[k];
-                    if (!__all_sync(0xffffffffu, all)) { ok = false; break; }
-                    tc_fence_after();
-                    #pragma unroll
-                    for (int k = 0; k < CC; ++k)
-                    {
-                        const uint32_t acol = TC_ACOL + (uint32_t)stage[k] * 64u + (uint32_t)g * 16u;
-                        tmem_st16(lane_addr + acol, hi[k]);
-                        tmem_st16(lane_addr + acol + 32u, lo[k]);
-                        pending[k] = stage[k];
+                        if (!RI && (DL || ADL))
+                        {
+                            float2 ux = make_float2(0.f, 0.f), uy = make_float2(0.f, 0.f);
+                            if (DL) { ux = __fmul2_rn(nc2x, dmu[p]); uy = __fmul2_rn(nc2y, dmu[p]); }
+                            if (ADL) { ux = __ffma2_rn(c3x, dnu[p], ux); uy = __ffma2_rn(c3y, dnu[p], uy); }
+                            const float2 nkr = __fmul2_rn(nkap, r[p]);
+                            hx = __ffma2_rn(kr, uy, __fadd2_rn(hx, ux));
+                            hy = __ffma2_rn(nkr, ux, __fadd2_rn(hy, uy));
+                        }
+                        // (ax, ay) = (hx cs - hy sn, hx sn + hy cs)
+                        const float2 msn = __fmul2_rn(m1, sn);
+                        const float2 ax = __ffma2_rn(hy, msn, __fmul2_rn(hx, cs));
+                        const float2 ay = __ffma2_rn(hy, cs, __fmul2_rn(hx, sn));
+                        // hi = the FP32 bits (read as TF32 by the tensor core), lo = x - trunc_tf32(x)
+                        const float2 tx = make_float2(__uint_as_float(__float_as_uint(ax.x) & 0xffffe000u),
+                                                      __uint_as_float(__float_as_uint(ax.y) & 0xffffe000u));
+                        const float2 ty = make_float2(__uint_as_float(__float_as_uint(ay.x) & 0xffffe000u),
+                                                      __uint_as_float(__float_as_uint(ay.y) & 0xffffe000u));
+                        const float2 lx = __ffma2_rn(tx, m1, ax), ly = __ffma2_rn(ty, m1, ay);
+                        hi[4 * p + 0] = __float_as_uint(ax.x);
+                        hi[4 * p + 1] = __float_as_uint(ax.y);
+                        hi[4 * p + 2] = __float_as_uint(ay.x);
+                        hi[4 * p + 3] = __float_as_uint(ay.y);
+                        lo[4 * p + 0] = __float_as_uint(lx.x);
+                        lo[4 * p + 1] = __float_as_uint(lx.y);
+                        lo[4 * p + 2] = __float_as_uint(ly.x);
+                        lo[4 * p + 3] = __float_as_uint(ly.y);
                     }
-                    npending = CC;
+                    // publish the previous chunk's stage now that its stores had this math to land
+                    publish();
+                    if (!ready)
+                        ready = wait_bar(&sm.a_empty[stage], (uint32_t)((u / TC_ASTAGES) - 1) & 1u, abort_flag, err, 3);
+                    // the tcgen05 stores below are warp-collective: the warp agrees on the outcome
+                    if (!__all_sync(0xffffffffu, ready)) return false;
+                    tc_fence_after();
+                    const uint32_t acol = TC_ACOL + (uint32_t)stage * 64u + (uint32_t)g * 16u;
+                    tmem_st16(lane_addr + acol, hi);
+                    tmem_st16(lane_addr + acol + 32u, lo);
+                    pending[0] = stage;
+                    npending = 1;
                     if (drain_due >= 0)
                     {
                         publish();
-                        if (!drain(drain_due, first_drain)) { ok = false; break; }
+                        if (!drain(drain_due, first_drain)) return false;
                         first_drain = false;
                         drain_due = -1;
                     }
+                    return true;
+                };
+                // pairs of chunks: two copies of the chunk body (more would overflow the
+                // instruction cache)
+                #pragma unroll 1
+                for (int c0 = 0; c0 < CH; c0 += 2)
+                {
+                    if (!do_chunk(c0, hiA, loA)) { ok = false; break; }
+                    if (c0 + 1 < CH && !do_chunk(c0 + 1, hiB, loB)) { ok = false; break; }
                 }
                 if (!ok) break;
                 const int lt = t - tb;
