@@ -25,18 +25,18 @@
 // tail piece of a CTA) writes its partial sums to a workspace slot, and
 // tc_fixup_kernel adds the slots of each split block in CTA order
 // (deterministic).
-// Warp roles (384 threads):
-//   warps 0-7   generators: thread (lane quarter q = warp % 4, half g = warp / 4)
-//               owns target row 32 q + lane and sources 8 g .. 8 g + 7 of each
+// Warp roles (640 threads):
+//   warps 0-15  generators: thread (lane quarter q = warp % 4, group g = warp / 4)
+//               owns target row 32 q + lane and sources 4 g .. 4 g + 3 of each
 //               16-source K tile; it evaluates the kernel entries in registers,
 //               two sources per FP32x2 instruction (geometry shared by all
 //               chunks), splits them into hi / lo and writes them straight into
 //               TMEM (tcgen05.st), so the A operand never touches shared memory;
-//   warps 8-9   expanders: expand the tile's 16 B_tri rows into hi / lo K-major
+//   warps 16-17 expanders: expand the tile's 16 B_tri rows into hi / lo K-major
 //               SWIZZLE_128B images in shared memory;
-//   warp 10     bulk-copy producer: cp.async.bulk of the raw tile (B_tri rows,
+//   warp 18     bulk-copy producer: cp.async.bulk of the raw tile (B_tri rows,
 //               midpoints, normals) into shared memory;
-//   warp 11     MMA issuer: 8 tcgen05.mma (kind::tf32, A from TMEM, B from
+//   warp 19     MMA issuer: 8 tcgen05.mma (kind::tf32, A from TMEM, B from
 //               shared memory, M 128, K 8) per chunk and tile.
 // Pipelines use mbarriers (A stages in TMEM, B stages in shared memory).
 // Every wait is bounded: on time-out the CTA raises a shared abort flag, writes
@@ -58,7 +58,21 @@ constexpr int TC_SRC = 16;         // sources per K tile
 constexpr int TC_N = 32;           // MMA N: 16 columns as (re | im)
 constexpr int TC_CHMAX = 4;        // chunks per work unit
 constexpr int TC_MAXCHUNKS = 32;   // wave_count <= 512 with wave_chunk_size 16
-constexpr int TC_GEN_THREADS = 256;
+// Generator warps: 16 (4 per SM sub-partition, 4 sources per thread and tile,
+// <= 96 registers at 640 threads) hide the latency of the entry evaluation
+// better than 8 (8 sources per thread): 146 vs 159 ms on the 153,600-triangle
+// torus with 64 right-hand sides.
+#ifndef BAEMM_TC_GEN_WARPS
+#define BAEMM_TC_GEN_WARPS 16
+#endif
+constexpr int TC_GEN_WARPS = BAEMM_TC_GEN_WARPS;   // 8 or 16
+constexpr int TC_GEN_THREADS = 32 * TC_GEN_WARPS;
+constexpr int TC_GROUPS = TC_GEN_WARPS / 4;        // source groups of a tile (4 warps cover the 128 rows)
+constexpr int TC_SPT = 16 / TC_GROUPS;             // sources per generator thread and tile
+constexpr int TC_PPT = TC_SPT / 2;                 // their pairs
+constexpr int TC_KPT = 2 * TC_SPT;                 // their K columns of an A stage
+constexpr int TC_CPG = 16 / TC_GROUPS;             // right-hand sides per thread in the drain
+static_assert(TC_GEN_WARPS == 8 || TC_GEN_WARPS == 16, "8 or 16 generator warps");
 constexpr int TC_EXP_THREADS = 64;
 constexpr int TC_THREADS = TC_GEN_THREADS + TC_EXP_THREADS + 64;   // + TMA producer warp + MMA warp
 constexpr int TC_ASTAGES = 4;      // A stages in TMEM (one chunk of one tile each)
@@ -259,12 +273,41 @@ __device__ __forceinline__ void tmem_st16(uint32_t taddr, const uint32_t (&v)[16
                  : "memory");
 }
 
+__device__ __forceinline__ void tmem_st8(uint32_t taddr, const uint32_t (&v)[8])
+{
+    asm volatile("tcgen05.st.sync.aligned.32x32b.x8.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8};" ::"r"(taddr),
+                 "r"(v[0]), "r"(v[1]), "r"(v[2]), "r"(v[3]), "r"(v[4]), "r"(v[5]), "r"(v[6]), "r"(v[7])
+                 : "memory");
+}
+
+template <int N>
+__device__ __forceinline__ void tmem_st(uint32_t taddr, const uint32_t (&v)[N])
+{
+    if constexpr (N == 16) tmem_st16(taddr, v);
+    else tmem_st8(taddr, v);
+}
+
+__device__ __forceinline__ void tmem_ld4(uint32_t taddr, uint32_t (&v)[4])
+{
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x4.b32 {%0, %1, %2, %3}, [%4];"
+                 : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3])
+                 : "r"(taddr)
+                 : "memory");
+}
+
 __device__ __forceinline__ void tmem_ld8(uint32_t taddr, uint32_t (&v)[8])
 {
     asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
                  : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7])
                  : "r"(taddr)
                  : "memory");
+}
+
+template <int N>
+__device__ __forceinline__ void tmem_ld(uint32_t taddr, uint32_t (&v)[N])
+{
+    if constexpr (N == 8) tmem_ld8(taddr, v);
+    else tmem_ld4(taddr, v);
 }
 
 // Shared-memory matrix descriptor: K-major, SWIZZLE_128B, 8-row groups 1024 B apart.
@@ -449,11 +492,11 @@ boundary_tc_kernel(const float *__restrict__ mid4, const float *__restrict__ nrm
     {
         // ------------------------------ generators ------------------------------
         constexpr int CC = 1;                 // A stages published together
-        uint32_t hiA[16], loA[16], hiB[16], loB[16];   // alternating register buffers of consecutive chunks
+        uint32_t hiA[TC_KPT], loA[TC_KPT], hiB[TC_KPT], loB[TC_KPT];   // alternating register buffers of consecutive chunks
         const int q = warp & 3, g = warp >> 2;
         const int row = q * 32 + lane;
         const uint32_t lane_addr = tbase + ((uint32_t)(q * 32) << 16);
-        float2 *acc_row = &sm.acc[row][g * 8];
+        float2 *acc_row = &sm.acc[row][g * TC_CPG];
         bool ok = true;
         int pending[CC];    // A stages written but not yet published
         int npending = 0;
@@ -478,16 +521,16 @@ boundary_tc_kernel(const float *__restrict__ mid4, const float *__restrict__ nrm
             #pragma unroll
             for (int c = 0; c < CH; ++c)
             {
-                uint32_t re[8], im[8], cre[8], cim[8];
-                const uint32_t col = (uint32_t)(c * TC_DCOLS + g * 8);
-                tmem_ld8(lane_addr + col, re);
-                tmem_ld8(lane_addr + col + 16u, im);
-                tmem_ld8(lane_addr + col + (uint32_t)TC_N, cre);
-                tmem_ld8(lane_addr + col + (uint32_t)TC_N + 16u, cim);
+                uint32_t re[TC_CPG], im[TC_CPG], cre[TC_CPG], cim[TC_CPG];
+                const uint32_t col = (uint32_t)(c * TC_DCOLS + g * TC_CPG);
+                tmem_ld<TC_CPG>(lane_addr + col, re);
+                tmem_ld<TC_CPG>(lane_addr + col + 16u, im);
+                tmem_ld<TC_CPG>(lane_addr + col + (uint32_t)TC_N, cre);
+                tmem_ld<TC_CPG>(lane_addr + col + (uint32_t)TC_N + 16u, cim);
                 asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
                 float4 *a4 = reinterpret_cast<float4 *>(acc_row + c * 16);
                 #pragma unroll
-                for (int k = 0; k < 4; ++k)
+                for (int k = 0; k < TC_CPG / 2; ++k)
                 {
                     float4 v = first ? make_float4(0.f, 0.f, 0.f, 0.f) : a4[k];
                     v.x += __uint_as_float(re[2 * k]) + __uint_as_float(cre[2 * k]);
@@ -532,15 +575,15 @@ boundary_tc_kernel(const float *__restrict__ mid4, const float *__restrict__ nrm
                     if (!__all_sync(0xffffffffu, got)) { ok = false; break; }
                 }
                 // per source pair: 1/r, r, (z.mu_j)/r^3, (z.nu_i)/r^3; shared by every chunk
-                float2 rinv[4], r[4], dmu[4], dnu[4];
+                float2 rinv[TC_PPT], r[TC_PPT], dmu[TC_PPT], dnu[TC_PPT];
                 {
                     const TcTileGeo &G = sm.raw[rs].geo;
                     // tiles that hold the target itself or padding past the end need masks
                     const bool special = (ts == ntiles - 1) || (ts * TC_SRC < blk * TC_M + TC_M && ts * TC_SRC + TC_SRC > blk * TC_M);
                     #pragma unroll
-                    for (int p = 0; p < 4; ++p)
+                    for (int p = 0; p < TC_PPT; ++p)
                     {
-                        const int sl = g * 8 + 2 * p;
+                        const int sl = g * TC_SPT + 2 * p;
                         const float2 zx = __fadd2_rn(*reinterpret_cast<const float2 *>(&G.x[sl]), nx0);
                         const float2 zy = __fadd2_rn(*reinterpret_cast<const float2 *>(&G.y[sl]), nx1);
                         const float2 zz = __fadd2_rn(*reinterpret_cast<const float2 *>(&G.z[sl]), nx2);
@@ -570,7 +613,7 @@ boundary_tc_kernel(const float *__restrict__ mid4, const float *__restrict__ nrm
                 // previous chunk's A stage, store this one.  Consecutive chunks use
                 // the two register buffers alternately, so the math of a chunk never
                 // writes registers the previous chunk's TMEM stores still read.
-                auto do_chunk = [&](int c, uint32_t (&hi)[16], uint32_t (&lo)[16]) -> bool {
+                auto do_chunk = [&](int c, uint32_t (&hi)[TC_KPT], uint32_t (&lo)[TC_KPT]) -> bool {
                     const int u = T * CH + c;
                     const int stage = u % TC_ASTAGES;
                     // test the A stage now; the answer arrives during the math
@@ -580,7 +623,7 @@ boundary_tc_kernel(const float *__restrict__ mid4, const float *__restrict__ nrm
                     const float2 kap = P[0], nkap = P[1], c1x = P[2], c1y = P[3];
                     const float2 nc2x = P[4], nc2y = P[5], c3x = P[6], c3y = P[7];
                     #pragma unroll
-                    for (int p = 0; p < 4; ++p)
+                    for (int p = 0; p < TC_PPT; ++p)
                     {
                         // A = e^{i k r} h,  h = c1 / r + w (i k r - 1) = c1 / r + u + i k r (-u),  u = -w
                         //   hx = c1x / r + ux + k r uy,   hy = c1y / r + uy - k r ux
@@ -643,9 +686,9 @@ boundary_tc_kernel(const float *__restrict__ mid4, const float *__restrict__ nrm
                     // the tcgen05 stores below are warp-collective: the warp agrees on the outcome
                     if (!__all_sync(0xffffffffu, ready)) return false;
                     tc_fence_after();
-                    const uint32_t acol = TC_ACOL + (uint32_t)stage * 64u + (uint32_t)g * 16u;
-                    tmem_st16(lane_addr + acol, hi);
-                    tmem_st16(lane_addr + acol + 32u, lo);
+                    const uint32_t acol = TC_ACOL + (uint32_t)stage * 64u + (uint32_t)(g * TC_KPT);
+                    tmem_st<TC_KPT>(lane_addr + acol, hi);
+                    tmem_st<TC_KPT>(lane_addr + acol + 32u, lo);
                     pending[0] = stage;
                     npending = 1;
                     if (drain_due >= 0)
@@ -697,9 +740,9 @@ boundary_tc_kernel(const float *__restrict__ mid4, const float *__restrict__ nrm
                 for (int c = 0; c < CH; ++c)
                 {
                     const float4 *a4 = reinterpret_cast<const float4 *>(acc_row + c * 16);
-                    float4 *out = reinterpret_cast<float4 *>(dst + c * 16 + g * 8);
+                    float4 *out = reinterpret_cast<float4 *>(dst + c * 16 + g * TC_CPG);
                     #pragma unroll
-                    for (int k = 0; k < 4; ++k) out[k] = a4[k];
+                    for (int k = 0; k < TC_CPG / 2; ++k) out[k] = a4[k];
                 }
             }
         }
