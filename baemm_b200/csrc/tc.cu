@@ -38,7 +38,10 @@
 //               midpoints, normals) into shared memory;
 //   warp 19     MMA issuer: 8 tcgen05.mma (kind::tf32, A from TMEM, B from
 //               shared memory, M 128, K 8) per chunk and tile.
-// Pipelines use mbarriers (A stages in TMEM, B stages in shared memory).
+// Pipelines use mbarriers (A stages in TMEM, B stages in shared memory).  All
+// roles wait with mbarrier.try_wait, which suspends the warp in hardware (on
+// the torus this measured 1 % faster than polling the producer's and the
+// expanders' barriers with __nanosleep in between).
 // Every wait is bounded: on time-out the CTA raises a shared abort flag, writes
 // an error code for the host, waits (bounded) for its issued MMAs and frees
 // its TMEM before returning.
@@ -191,33 +194,6 @@ __device__ __forceinline__ bool mbar_test_wait(uint64_t *bar, uint32_t parity)
                  : "r"(smem_u32(bar)), "r"(parity)
                  : "memory");
     return ok != 0;
-}
-
-// Bounded wait for the roles that run ahead of the generators (producer,
-// expanders): they poll with a growing __nanosleep between tests, so that
-// their waiting takes few issue slots from the generator warps that share
-// their SM sub-partition.  The MMA issuer is on the critical path and uses
-// wait_bar.  Same contract as wait_bar.
-__device__ __forceinline__ bool wait_bar_sleepy(uint64_t *bar, uint32_t parity, volatile int *abort_flag, int *err,
-                                                int code, bool honour_abort = true)
-{
-    if (mbar_test_wait(bar, parity)) return true;
-    const uint64_t t0 = global_ns();
-    uint32_t ns = 32;
-    for (uint32_t it = 1;; ++it)
-    {
-        __nanosleep(ns);
-        if (mbar_test_wait(bar, parity)) return true;
-        ns = ns < 256u ? 2u * ns : 256u;
-        if ((it & 15u) == 0)
-        {
-            if (honour_abort && (*abort_flag || *(volatile int *)err)) return false;
-            if (global_ns() - t0 > kWaitNs) break;
-        }
-    }
-    *abort_flag = 1;
-    atomicExch(err, code);
-    return false;
 }
 
 // One lane of a converged warp (the lowest), for the single-thread
@@ -764,9 +740,9 @@ boundary_tc_kernel(const float *__restrict__ mid4, const float *__restrict__ nrm
             for (int t = tb; t < te; ++t, ++T)
             {
                 const int rs = T % TC_RSTAGES, b = T % TC_BSTAGES;
-                if (!wait_bar_sleepy(&sm.r_full[rs], (uint32_t)(T / TC_RSTAGES) & 1u, abort_flag, err, 4)) { ok = false; break; }
+                if (!wait_bar(&sm.r_full[rs], (uint32_t)(T / TC_RSTAGES) & 1u, abort_flag, err, 4)) { ok = false; break; }
                 if (T >= TC_BSTAGES &&
-                    !wait_bar_sleepy(&sm.b_empty[b], (uint32_t)((T / TC_BSTAGES) - 1) & 1u, abort_flag, err, 5))
+                    !wait_bar(&sm.b_empty[b], (uint32_t)((T / TC_BSTAGES) - 1) & 1u, abort_flag, err, 5))
                 {
                     ok = false;
                     break;
@@ -816,7 +792,7 @@ boundary_tc_kernel(const float *__restrict__ mid4, const float *__restrict__ nrm
                 if (T >= TC_RSTAGES)
                 {
                     const bool got =
-                        wait_bar_sleepy(&sm.r_empty[rs], (uint32_t)((T / TC_RSTAGES) - 1) & 1u, abort_flag, err, 6);
+                        wait_bar(&sm.r_empty[rs], (uint32_t)((T / TC_RSTAGES) - 1) & 1u, abort_flag, err, 6);
                     if (!__all_sync(0xffffffffu, got)) { ok = false; break; }
                 }
                 if (elect_one())
