@@ -157,6 +157,36 @@ static void farfield_host(Ctx &c, const double *alpha, const double *B, int64_t 
     c.sync();
 }
 
+// ApplyNearFieldOperators.hpp:56-122 with host blocks: B (nv x wc, ld ldB) in,
+// C (npts x wc, ld ldC) in/out, points npts x 3 (real type S).
+template <class T, class S>
+static void nearfield_host(Ctx &c, const S *alpha, const S *B, int64_t ldB, const S *beta, S *C, int64_t ldC,
+                           const S *points, int64_t npts)
+{
+    BAEMM_REQUIRE(B && C, BAEMM_ERR_ARG, "null block");
+    const int wc = c.wave_count;
+    if (c.wave_chunk_count < 1 || !(c.flags.sl() || c.flags.dl())) return;
+    BAEMM_REQUIRE(ldB >= wc && ldC >= wc, BAEMM_ERR_ARG, "leading dimension smaller than wave_count");
+    BAEMM_REQUIRE(npts >= 0, BAEMM_ERR_ARG, "negative evaluation point count");
+    if (npts == 0) return;
+    BAEMM_REQUIRE(points, BAEMM_ERR_ARG, "null evaluation points");
+    static_assert(sizeof(T) == 2 * sizeof(S), "complex layout");
+    const int64_t nv = c.mesh.nv;
+    T *dB = reinterpret_cast<T *>(c.io_a.reserve((nv * wc * sizeof(T) + 15) / 16));
+    T *dC = reinterpret_cast<T *>(c.io_b.reserve((npts * wc * sizeof(T) + 15) / 16));
+    double *dP = c.io_r1.reserve(3 * npts);
+    std::vector<double> pts(points, points + 3 * npts);   // widened; the kernels take their own precision
+    BAEMM_CUDA(cudaMemcpyAsync(dP, pts.data(), 3 * npts * sizeof(double), cudaMemcpyHostToDevice, c.stream));
+    h2d_block<T>(c, dB, reinterpret_cast<const T *>(B), nv, wc, ldB);
+    if (!is_zero(beta)) h2d_block<T>(c, dC, reinterpret_cast<const T *>(C), npts, wc, ldC);
+    T al, be;
+    al.x = alpha ? alpha[0] : 0; al.y = alpha ? alpha[1] : 0;
+    be.x = beta ? beta[0] : 0; be.y = beta ? beta[1] : 0;
+    c.apply_nearfield<T>(al, dB, wc, be, dC, wc, dP, npts);
+    d2h_block<T>(c, reinterpret_cast<T *>(C), ldC, dC, npts, wc);
+    c.sync();   // pts is a host temporary
+}
+
 static void mass_inverse_host(Ctx &c, const double *X, int64_t ldX, double *Y, int64_t ldY, int cols, double tol,
                               bool lumped)
 {
@@ -523,6 +553,47 @@ int baemm_apply_far_field_operators_dev_z(baemm_ctx *ctx, const double alpha[2],
         BAEMM_REQUIRE(B && C, BAEMM_ERR_ARG, "null block");
         c.apply_farfield(zz(alpha), reinterpret_cast<const double2 *>(B), ldB, zz(beta),
                          reinterpret_cast<double2 *>(C), ldC);
+    });
+}
+
+int baemm_apply_near_field_operators_z(baemm_ctx *ctx, const double alpha[2], const double *B, int64_t ldB,
+                                       const double beta[2], double *C, int64_t ldC, const double *points,
+                                       int64_t npts)
+{
+    return guarded(ctx, [&](Ctx &c) { nearfield_host<double2, double>(c, alpha, B, ldB, beta, C, ldC, points, npts); });
+}
+int baemm_apply_near_field_operators_c(baemm_ctx *ctx, const float alpha[2], const float *B, int64_t ldB,
+                                       const float beta[2], float *C, int64_t ldC, const float *points, int64_t npts)
+{
+    return guarded(ctx, [&](Ctx &c) { nearfield_host<float2, float>(c, alpha, B, ldB, beta, C, ldC, points, npts); });
+}
+int baemm_apply_near_field_operators_full_z(baemm_ctx *ctx, const double alpha[2], const double *B, int64_t ldB,
+                                            const double beta[2], double *C, int64_t ldC, const double *kappa,
+                                            const double *coeff, int wc, int wcs, const double *points, int64_t npts)
+{
+    return guarded(ctx, [&](Ctx &c) {
+        c.load_parameters(kappa, reinterpret_cast<const zc *>(coeff), wc, wcs, 1.0);
+        nearfield_host<double2, double>(c, alpha, B, ldB, beta, C, ldC, points, npts);
+    });
+}
+int baemm_apply_near_field_operators_dev_z(baemm_ctx *ctx, const double alpha[2], const double *B, int64_t ldB,
+                                           const double beta[2], double *C, int64_t ldC, const double *points,
+                                           int64_t npts)
+{
+    return guarded(ctx, [&](Ctx &c) {
+        BAEMM_REQUIRE(B && C, BAEMM_ERR_ARG, "null block");
+        c.apply_nearfield<double2>(z2(alpha), reinterpret_cast<const double2 *>(B), ldB, z2(beta),
+                                   reinterpret_cast<double2 *>(C), ldC, points, npts);
+    });
+}
+int baemm_apply_near_field_operators_dev_c(baemm_ctx *ctx, const float alpha[2], const float *B, int64_t ldB,
+                                           const float beta[2], float *C, int64_t ldC, const double *points,
+                                           int64_t npts)
+{
+    return guarded(ctx, [&](Ctx &c) {
+        BAEMM_REQUIRE(B && C, BAEMM_ERR_ARG, "null block");
+        c.apply_nearfield<float2>(c2(alpha), reinterpret_cast<const float2 *>(B), ldB, c2(beta),
+                                  reinterpret_cast<float2 *>(C), ldC, points, npts);
     });
 }
 

@@ -391,6 +391,78 @@ void Ctx::apply_boundary(Text alpha, const Text *B, int64_t ldB, Text beta, Text
     prof_valid = profiling;
 }
 
+template <class Text>
+void Ctx::apply_nearfield(Text alpha, const Text *B, int64_t ldB, Text beta, Text *C, int64_t ldC, const double *pts3,
+                          int64_t npts)
+{
+    if (wave_chunk_count < 1) return;
+    // the near-field kernel reads the single- and double-layer coefficients only
+    // (NearFieldOperatorKernel.cl:105-149); without either C is left untouched
+    OpFlags nf;
+    nf.re_sl = flags.re_sl;
+    nf.im_sl = flags.im_sl;
+    nf.re_dl = flags.re_dl;
+    nf.im_dl = flags.im_dl;
+    if (!nf.any_layer()) return;
+    BAEMM_REQUIRE(ldB >= wave_count && ldC >= wave_count, BAEMM_ERR_ARG, "leading dimension smaller than wave_count");
+    BAEMM_REQUIRE(npts >= 0, BAEMM_ERR_ARG, "negative evaluation point count");
+    if (npts == 0) return;
+    BAEMM_REQUIRE(pts3, BAEMM_ERR_ARG, "null evaluation points");
+    const int64_t tri_elems = mesh.nt * wave_count, pt_elems = npts * wave_count;
+    if (profiling)
+    {
+        for (auto &e : prof_ev)
+            if (!e) BAEMM_CUDA(cudaEventCreate(&e));
+        BAEMM_CUDA(cudaEventRecord(prof_ev[0], stream));
+    }
+    auto mark = [&](int q) {
+        if (profiling) BAEMM_CUDA(cudaEventRecord(prof_ev[q], stream));
+    };
+    const double2 al = make_double2((double)alpha.x, (double)alpha.y), be = make_double2((double)beta.x, (double)beta.y);
+    if (apply_mode == BAEMM_APPLY_FP64)
+    {
+        double2 *Bt = Btri_d.reserve(tri_elems), *Cp = Cpts_d.reserve(pt_elems);
+        double *p4 = pts_d.reserve(4 * npts);
+        launch_avop<Text, double>(mesh, B, ldB, wave_count, Bt, stream);
+        launch_pack_points<double>(npts, pts3, p4, stream);
+        mark(1);
+        launch_nearfield_dense<double>(mesh, nf, prm_d.p, wave_count, wave_chunk_size, p4, npts, Bt, Cp, stream);
+        mark(2);
+        launch_combine<Text, double>(npts, wave_count, al, Cp, be, C, ldC, stream);
+    }
+    else
+    {
+        float2 *Bt = Btri_f.reserve(tri_elems), *Cp = Cpts_f.reserve(pt_elems);
+        float *p4 = pts_f.reserve(4 * npts);
+        launch_avop<Text, float>(mesh, B, ldB, wave_count, Bt, stream);
+        launch_pack_points<float>(npts, pts3, p4, stream);
+        mark(1);
+        if (apply_mode == BAEMM_APPLY_TC && tc_supported(wave_count, wave_chunk_size))
+        {
+            if (!tc_geo_ready)
+            {
+                launch_tc_tile_geometry(mesh, mesh.tgeo_f.reserve(tc_tile_geometry_floats(mesh.nt)), stream);
+                tc_geo_ready = true;
+            }
+            const size_t ws_elems = tc_workspace_elems(tc_ctas);
+            launch_nearfield_tc(mesh, nf, prm16_f.p, wave_count, wave_chunk_size, mesh.tgeo_f.p, p4, npts, Bt, Cp,
+                                tc_ws.reserve(ws_elems), ws_elems, tc_err.p, stream, tc_seg_tiles, tc_ctas, tc_stagger);
+            tc_pending = true;
+        }
+        else
+            launch_nearfield_dense<float>(mesh, nf, prm_f.p, wave_count, wave_chunk_size, p4, npts, Bt, Cp, stream,
+                                          dense_variant);
+        mark(2);
+        launch_combine<Text, float>(npts, wave_count, al, Cp, be, C, ldC, stream);
+    }
+    mark(3);
+    prof_valid = profiling;
+}
+
+template void Ctx::apply_nearfield<double2>(double2, const double2 *, int64_t, double2, double2 *, int64_t,
+                                            const double *, int64_t);
+template void Ctx::apply_nearfield<float2>(float2, const float2 *, int64_t, float2, float2 *, int64_t, const double *,
+                                           int64_t);
 template void Ctx::dense_apply<float>(const float2 *, float2 *);
 template void Ctx::apply_boundary<double2>(double2, const double2 *, int64_t, double2, double2 *, int64_t);
 template void Ctx::apply_boundary<float2>(float2, const float2 *, int64_t, float2, float2 *, int64_t);

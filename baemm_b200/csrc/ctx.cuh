@@ -73,6 +73,10 @@ public:
     DevBuf<double2> Btri_d, Ctri_d, ff_partial_d;
     DevBuf<float> dirs_f;
     DevBuf<double> dirs_d;
+    DevBuf<float> pts_f;                // near field: evaluation points, npts x 4
+    DevBuf<double> pts_d;
+    DevBuf<float2> Cpts_f;              // near field: values at the points, npts x wc
+    DevBuf<double2> Cpts_d;
     DevBuf<double2> io_a, io_b, io_c;   // host-API staging
     DevBuf<double> io_r1, io_r2, tri_r;
     // solver scratch (one buffer per role; the compositions nest)
@@ -92,6 +96,12 @@ public:
     void apply_boundary(Text alpha, const Text *B, int64_t ldB, Text beta, Text *C, int64_t ldC);
     // Far field: C (nm x wc) = alpha FF B + beta C   (ApplyFarFieldOperators.hpp:356-412)
     void apply_farfield(zc alpha, const double2 *B, int64_t ldB, zc beta, double2 *C, int64_t ldC);
+    // ApplyNearFieldOperators.hpp:56-122 on device blocks: C (npts x wc) =
+    // alpha K(points) AvOp B + beta C at the points pts3 (npts x 3 doubles,
+    // device), in the apply arithmetic (FP32, tensor-core or FP64).
+    template <class Text>
+    void apply_nearfield(Text alpha, const Text *B, int64_t ldB, Text beta, Text *C, int64_t ldC, const double *pts3,
+                         int64_t npts);
     // Incident wave: C = alpha wave + beta C (CreateIncidentWave.hpp:54-127), dirs on host (wcs x 3)
     void incident(zc alpha, const double *dirs, zc beta, double2 *C, int64_t ldC, int type);
     // Herglotz wave of g (device, nm x ld): C = alpha HW + beta C (CreateHerglotzWave.hpp:50-95)

@@ -3,6 +3,8 @@
 //   boundary  C_i = sum_{j != i} A_ij(kappa) B_j     BoundaryOperatorKernel.cl:5-239
 //             A_ij = c1 e^{i k r}/r + (c2 (z.mu_j) - c3 (z.nu_i)) (i k r - 1) e^{i k r}/r^3,
 //             z = y_j - x_i, r = |z|; c1..c3 already carry 1/(4 pi).
+//   near field  the same sum with c3 = 0 at arbitrary points x_i, no pair
+//             excluded                               NearFieldOperatorKernel.cl:5-194
 //   far field F_i = sum_j (c1 - i k c2 (x_i.mu_j)) e^{-i k x_i.y_j} B_j     FarFieldOperatorKernel.cl:85-133
 //   Herglotz  C_i = sum_j (c1 - i k c2 (nu_i.d_j)) e^{-i k x_i.d_j} conj(g_j) HerglotzWaveKernel.cl:85-160
 //   incident  plane / radial waves at the midpoints                          IncidentWaveKernel_*.hpp
@@ -81,19 +83,22 @@ __device__ __forceinline__ void stage_tile(Tile<R, COLS> &t, const R *__restrict
 
 template <class R, int COLS, bool SL, bool DL, bool ADL>
 __global__ void __launch_bounds__(kTargets)
-boundary_dense_kernel(const R *__restrict__ mid4, const R *__restrict__ nrm4, const cplx<R> *__restrict__ B,
-                      cplx<R> *__restrict__ C, const typename Prm<R>::type *__restrict__ prm, int n, int wc, int wcs)
+boundary_dense_kernel(DenseTargets<R> tg, const R *__restrict__ mid4, const R *__restrict__ nrm4,
+                      const cplx<R> *__restrict__ B, cplx<R> *__restrict__ C,
+                      const typename Prm<R>::type *__restrict__ prm, int n, int wc, int wcs)
 {
     __shared__ Tile<R, COLS> tile;
     const int i = blockIdx.x * kTargets + threadIdx.x;
+    const int iself = tg.self ? i : -1;   // the source index excluded for this target (none: -1)
     const int col0 = blockIdx.y * COLS;
     const int ch = col0 / wcs;
     const R kap = prm[ch].kappa;
     const cplx<R> c1 = prm[ch].c[1], c2 = prm[ch].c[2], c3 = prm[ch].c[3];
     R x0 = R(0), x1 = R(0), x2 = R(0), n0 = R(0), n1 = R(0), n2 = R(0);
-    if (i < n)
+    if (i < tg.m)
     {
-        x0 = mid4[4 * (int64_t)i]; x1 = mid4[4 * (int64_t)i + 1]; x2 = mid4[4 * (int64_t)i + 2];
+        const R *x = tg.pts4;
+        x0 = x[4 * (int64_t)i]; x1 = x[4 * (int64_t)i + 1]; x2 = x[4 * (int64_t)i + 2];
         if (ADL) { n0 = nrm4[4 * (int64_t)i]; n1 = nrm4[4 * (int64_t)i + 1]; n2 = nrm4[4 * (int64_t)i + 2]; }
     }
     cplx<R> acc[COLS];
@@ -111,7 +116,7 @@ boundary_dense_kernel(const R *__restrict__ mid4, const R *__restrict__ nrm4, co
         {
             const R zx = tile.y[s][0] - x0, zy = tile.y[s][1] - x1, zz = tile.y[s][2] - x2;
             const R r2 = zx * zx + zy * zy + zz * zz;
-            const R rinv = (j0 + s == i) ? R(0) : drsqrt(r2);
+            const R rinv = (j0 + s == iself) ? R(0) : drsqrt(r2);
             const R r = r2 * rinv;
             const R kr = kap * r;
             R sn, cs;
@@ -150,7 +155,7 @@ boundary_dense_kernel(const R *__restrict__ mid4, const R *__restrict__ nrm4, co
             for (int k = 0; k < COLS; ++k) cfma(acc[k], A, tile.B[s][k]);
         }
     }
-    if (i < n)
+    if (i < tg.m)
     {
         cplx<R> *out = &C[(int64_t)i * wc + col0];
         #pragma unroll
@@ -178,25 +183,27 @@ struct PackedTile
 
 template <int TT, bool SL, bool DL, bool ADL>
 __global__ void __launch_bounds__(kTargets, TT == 1 ? 4 : 3)
-boundary_packed_kernel(const float *__restrict__ mid4, const float *__restrict__ nrm4, const float2 *__restrict__ B,
-                       float2 *__restrict__ C, const ChunkParamsF *__restrict__ prm, int n, int wc, int wcs)
+boundary_packed_kernel(DenseTargets<float> tg, const float *__restrict__ mid4, const float *__restrict__ nrm4,
+                       const float2 *__restrict__ B, float2 *__restrict__ C, const ChunkParamsF *__restrict__ prm,
+                       int n, int wc, int wcs)
 {
     __shared__ PackedTile tile;
     const int col0 = blockIdx.y * kPackedCols;
     const int ch = col0 / wcs;
     const float kap = prm[ch].kappa;
     const float2 c1 = prm[ch].c[1], c2 = prm[ch].c[2], c3 = prm[ch].c[3];
-    int ti[TT];
+    int ti[TT], tself[TT];
     float3 x[TT], nu[TT];
     #pragma unroll
     for (int t = 0; t < TT; ++t)
     {
         ti[t] = blockIdx.x * (kTargets * TT) + t * kTargets + threadIdx.x;
+        tself[t] = tg.self ? ti[t] : -1;
         x[t] = make_float3(0.f, 0.f, 0.f);
         nu[t] = make_float3(0.f, 0.f, 0.f);
-        if (ti[t] < n)
+        if (ti[t] < tg.m)
         {
-            const float4 m = reinterpret_cast<const float4 *>(mid4)[ti[t]];
+            const float4 m = reinterpret_cast<const float4 *>(tg.pts4)[ti[t]];
             x[t] = make_float3(m.x, m.y, m.z);
             if (ADL)
             {
@@ -247,7 +254,7 @@ boundary_packed_kernel(const float *__restrict__ mid4, const float *__restrict__
             {
                 const float zx = yv.x - x[t].x, zy = yv.y - x[t].y, zz = yv.z - x[t].z;
                 const float r2 = zx * zx + zy * zy + zz * zz;
-                const float rinv = (j0 + s == ti[t]) ? 0.f : rsqrtf(r2);
+                const float rinv = (j0 + s == tself[t]) ? 0.f : rsqrtf(r2);
                 const float r = r2 * rinv;
                 const float kr = kap * r;
                 float sn, cs;
@@ -298,7 +305,7 @@ boundary_packed_kernel(const float *__restrict__ mid4, const float *__restrict__
     }
     #pragma unroll
     for (int t = 0; t < TT; ++t)
-        if (ti[t] < n)
+        if (ti[t] < tg.m)
         {
             float4 *out = reinterpret_cast<float4 *>(&C[(int64_t)ti[t] * wc + col0]);
             #pragma unroll
@@ -495,13 +502,26 @@ __global__ void incident_kernel(int64_t nt, const R *__restrict__ mid4, const R 
     C[idx] = cmul(f, e);
 }
 
+// Evaluation points (m x 3 doubles) as m x 4 reals, w = 0
+// (ApplyNearFieldOperators.hpp:96-107 pads them the same way).
+template <class R>
+__global__ void pack_points_kernel(int64_t m, const double *__restrict__ pts3, R *__restrict__ pts4)
+{
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= m) return;
+    pts4[4 * i + 0] = (R)pts3[3 * i + 0];
+    pts4[4 * i + 1] = (R)pts3[3 * i + 1];
+    pts4[4 * i + 2] = (R)pts3[3 * i + 2];
+    pts4[4 * i + 3] = R(0);
+}
+
 // ---- dispatch helpers -----------------------------------------------------------
 template <class R, int COLS>
-void boundary_cols(const OpFlags &f, dim3 grid, cudaStream_t st, const R *mid, const R *nrm, const cplx<R> *B,
-                   cplx<R> *C, const typename Prm<R>::type *p, int n, int wc, int wcs)
+void boundary_cols(const OpFlags &f, dim3 grid, cudaStream_t st, DenseTargets<R> tg, const R *mid, const R *nrm,
+                   const cplx<R> *B, cplx<R> *C, const typename Prm<R>::type *p, int n, int wc, int wcs)
 {
     const int code = (f.sl() ? 1 : 0) | (f.dl() ? 2 : 0) | (f.adl() ? 4 : 0);
-#define BAEMM_BK(SL, DL, ADL) boundary_dense_kernel<R, COLS, SL, DL, ADL><<<grid, kTargets, 0, st>>>(mid, nrm, B, C, p, n, wc, wcs)
+#define BAEMM_BK(SL, DL, ADL) boundary_dense_kernel<R, COLS, SL, DL, ADL><<<grid, kTargets, 0, st>>>(tg, mid, nrm, B, C, p, n, wc, wcs)
     switch (code)
     {
         case 1: BAEMM_BK(true, false, false); break;
@@ -555,11 +575,11 @@ template <> const double *geo_meas<double>(const MeshDev &m) { return m.meas_d; 
 inline int cols_for(int wcs) { return wcs < 16 ? wcs : 16; }
 
 template <int TT>
-void packed_dispatch(int code, int n, int wc, int wcs, const float *mid, const float *nrm, const float2 *B, float2 *C,
-                     const ChunkParamsF *p, cudaStream_t st)
+void packed_dispatch(int code, DenseTargets<float> tg, int n, int wc, int wcs, const float *mid, const float *nrm,
+                     const float2 *B, float2 *C, const ChunkParamsF *p, cudaStream_t st)
 {
-    dim3 grid(ceil_div(n, kTargets * TT), wc / kPackedCols);
-#define BAEMM_PK(SL, DL, ADL) boundary_packed_kernel<TT, SL, DL, ADL><<<grid, kTargets, 0, st>>>(mid, nrm, B, C, p, n, wc, wcs)
+    dim3 grid(ceil_div(tg.m, kTargets * TT), wc / kPackedCols);
+#define BAEMM_PK(SL, DL, ADL) boundary_packed_kernel<TT, SL, DL, ADL><<<grid, kTargets, 0, st>>>(tg, mid, nrm, B, C, p, n, wc, wcs)
     switch (code)
     {
         case 1: BAEMM_PK(true, false, false); break;
@@ -574,16 +594,15 @@ void packed_dispatch(int code, int n, int wc, int wcs, const float *mid, const f
 #undef BAEMM_PK
 }
 
-} // namespace
-
+// Ctri (tg.m x wc) = K Btri over all nt sources for the targets tg.
 template <class R>
-void launch_boundary_dense(const MeshDev &m, const OpFlags &f, const void *chunk_params, int wc, int wcs,
-                           const cplx<R> *Btri, cplx<R> *Ctri, cudaStream_t st, int variant)
+void dense_dispatch(const MeshDev &m, const OpFlags &f, const void *chunk_params, int wc, int wcs,
+                    DenseTargets<R> tg, const cplx<R> *Btri, cplx<R> *Ctri, cudaStream_t st, int variant)
 {
-    if (!f.any_layer() || m.nt == 0) return;
+    if (!f.any_layer() || m.nt == 0 || tg.m == 0) return;
     const int n = (int)m.nt;
     const int cols = cols_for(wcs);
-    dim3 grid(ceil_div(n, kTargets), wc / cols);
+    dim3 grid(ceil_div(tg.m, kTargets), wc / cols);
     const auto *p = static_cast<const typename Prm<R>::type *>(chunk_params);
     const R *mid = geo_mid<R>(m), *nrm = geo_nrm<R>(m);
     if constexpr (std::is_same<R, float>::value)
@@ -591,21 +610,49 @@ void launch_boundary_dense(const MeshDev &m, const OpFlags &f, const void *chunk
         if (cols == kPackedCols && variant > 0)
         {
             const int code = (f.sl() ? 1 : 0) | (f.dl() ? 2 : 0) | (f.adl() ? 4 : 0);
-            if (variant == 2) packed_dispatch<2>(code, n, wc, wcs, mid, nrm, Btri, Ctri, p, st);
-            else packed_dispatch<1>(code, n, wc, wcs, mid, nrm, Btri, Ctri, p, st);
+            if (variant == 2) packed_dispatch<2>(code, tg, n, wc, wcs, mid, nrm, Btri, Ctri, p, st);
+            else packed_dispatch<1>(code, tg, n, wc, wcs, mid, nrm, Btri, Ctri, p, st);
             BAEMM_LAUNCH_CHECK();
             return;
         }
     }
     switch (cols)
     {
-        case 1: boundary_cols<R, 1>(f, grid, st, mid, nrm, Btri, Ctri, p, n, wc, wcs); break;
-        case 2: boundary_cols<R, 2>(f, grid, st, mid, nrm, Btri, Ctri, p, n, wc, wcs); break;
-        case 4: boundary_cols<R, 4>(f, grid, st, mid, nrm, Btri, Ctri, p, n, wc, wcs); break;
-        case 8: boundary_cols<R, 8>(f, grid, st, mid, nrm, Btri, Ctri, p, n, wc, wcs); break;
-        case 16: boundary_cols<R, 16>(f, grid, st, mid, nrm, Btri, Ctri, p, n, wc, wcs); break;
+        case 1: boundary_cols<R, 1>(f, grid, st, tg, mid, nrm, Btri, Ctri, p, n, wc, wcs); break;
+        case 2: boundary_cols<R, 2>(f, grid, st, tg, mid, nrm, Btri, Ctri, p, n, wc, wcs); break;
+        case 4: boundary_cols<R, 4>(f, grid, st, tg, mid, nrm, Btri, Ctri, p, n, wc, wcs); break;
+        case 8: boundary_cols<R, 8>(f, grid, st, tg, mid, nrm, Btri, Ctri, p, n, wc, wcs); break;
+        case 16: boundary_cols<R, 16>(f, grid, st, tg, mid, nrm, Btri, Ctri, p, n, wc, wcs); break;
         default: throw Error(BAEMM_ERR_SIZE, "wave_chunk_size must be a power of two <= 64");
     }
+    BAEMM_LAUNCH_CHECK();
+}
+
+} // namespace
+
+template <class R>
+void launch_boundary_dense(const MeshDev &m, const OpFlags &f, const void *chunk_params, int wc, int wcs,
+                           const cplx<R> *Btri, cplx<R> *Ctri, cudaStream_t st, int variant)
+{
+    dense_dispatch<R>(m, f, chunk_params, wc, wcs, DenseTargets<R>{geo_mid<R>(m), (int)m.nt, 1}, Btri, Ctri, st,
+                      variant);
+}
+
+template <class R>
+void launch_nearfield_dense(const MeshDev &m, const OpFlags &f, const void *chunk_params, int wc, int wcs,
+                            const R *pts4, int64_t npts, const cplx<R> *Btri, cplx<R> *Cpts, cudaStream_t st,
+                            int variant)
+{
+    BAEMM_REQUIRE(!f.adl() && !f.mass(), BAEMM_ERR_ARG, "near field: single and double layer only");
+    BAEMM_REQUIRE(npts <= INT32_MAX, BAEMM_ERR_SIZE, "too many evaluation points");
+    dense_dispatch<R>(m, f, chunk_params, wc, wcs, DenseTargets<R>{pts4, (int)npts, 0}, Btri, Cpts, st, variant);
+}
+
+template <class R>
+void launch_pack_points(int64_t m, const double *pts3, R *pts4, cudaStream_t st)
+{
+    if (m == 0) return;
+    pack_points_kernel<R><<<ceil_div(m, 256), 256, 0, st>>>(m, pts3, pts4);
     BAEMM_LAUNCH_CHECK();
 }
 
@@ -690,6 +737,12 @@ void launch_incident(const MeshDev &m, const void *chunk_params, int wc, int wcs
 
 template void launch_boundary_dense<float>(const MeshDev &, const OpFlags &, const void *, int, int, const float2 *,
                                            float2 *, cudaStream_t, int);
+template void launch_pack_points<float>(int64_t, const double *, float *, cudaStream_t);
+template void launch_pack_points<double>(int64_t, const double *, double *, cudaStream_t);
+template void launch_nearfield_dense<float>(const MeshDev &, const OpFlags &, const void *, int, int, const float *,
+                                            int64_t, const float2 *, float2 *, cudaStream_t, int);
+template void launch_nearfield_dense<double>(const MeshDev &, const OpFlags &, const void *, int, int, const double *,
+                                             int64_t, const double2 *, double2 *, cudaStream_t, int);
 template void launch_boundary_dense<double>(const MeshDev &, const OpFlags &, const void *, int, int, const double2 *,
                                             double2 *, cudaStream_t, int);
 template void launch_farfield<float>(const MeshDev &, const OpFlags &, const void *, int, int, const float2 *, float2 *,

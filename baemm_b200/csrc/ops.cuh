@@ -26,6 +26,17 @@ struct MeshDev
     DevBuf<double> mid_d, nrm_d, area_d, a3_d, diag_d, mass_d, lumped_d, meas_d;
 };
 
+// Target points of a dense launch: the triangle midpoints with the pair i == j
+// excluded (self = 1, boundary operators) or arbitrary points with no pair
+// excluded (self = 0, near field).  pts4: m x 4 reals (xyz, w unused).
+template <class R>
+struct DenseTargets
+{
+    const R *pts4;
+    int m;
+    int self;
+};
+
 // ---- mesh.cu -------------------------------------------------------------------
 // Initialize.hpp:57-302 (geometry and single-layer diagonal) in precision R.
 void launch_geometry(const MeshDev &m, bool fp64, cudaStream_t st);
@@ -70,6 +81,12 @@ void launch_mass_dot_real(const MeshDev &m, bool fp64_values, double alpha, cons
 // Lumped inverse on real columns: Y = L X.
 void launch_lumped_real(const MeshDev &m, bool fp64_values, const double *X, int64_t ldX, double *Y, int64_t ldY,
                         int ncols, cudaStream_t st);
+// Cout[r, k] = alpha Cin[r, k] + beta Cout[r, k] over rows x wc, Cin packed
+// (ld wc, internal precision R), arithmetic in double; beta == 0 overwrites
+// (combine_matrices as called at ApplyNearFieldOperators.hpp:112-116).
+template <class Text, class R>
+void launch_combine(int64_t rows, int wc, double2 alpha, const cplx<R> *Cin, double2 beta, Text *Cout, int64_t ldC,
+                    cudaStream_t st);
 // Strided copies / conversions of external blocks.
 template <class Tsrc, class Tdst>
 void launch_copy_block(int64_t rows, int cols, const Tsrc *src, int64_t lds, Tdst *dst, int64_t ldd, cudaStream_t st);
@@ -86,6 +103,16 @@ constexpr int kDenseVariants = 3;
 template <class R>
 void launch_boundary_dense(const MeshDev &m, const OpFlags &f, const void *chunk_params, int wc, int wcs,
                            const cplx<R> *Btri, cplx<R> *Ctri, cudaStream_t st, int variant = 2);
+// Near-field kernel (NearFieldOperatorKernel.cl:5-194): Cpts (npts x wc) =
+// K(kappa) Btri at the points pts4 (npts x 4 reals), single and double layer
+// (c1, c2) only, no pair excluded.  Same kernels and variants as the boundary form.
+template <class R>
+void launch_nearfield_dense(const MeshDev &m, const OpFlags &f, const void *chunk_params, int wc, int wcs,
+                            const R *pts4, int64_t npts, const cplx<R> *Btri, cplx<R> *Cpts, cudaStream_t st,
+                            int variant = 2);
+// Evaluation points (m x 3 doubles, device) -> m x 4 reals, w = 0.
+template <class R>
+void launch_pack_points(int64_t m, const double *pts3, R *pts4, cudaStream_t st);
 // Compensated tensor-core dense kernel (tc.cu): TF32 hi/lo split, three
 // tcgen05 MMAs per K step, FP32 accumulation in TMEM.  wave_chunk_size 16.
 // `err` (device int) receives a non-zero code when a bounded wait gave up.
@@ -95,6 +122,12 @@ bool tc_supported(int wc, int wcs);
 void launch_boundary_tc(const MeshDev &m, const OpFlags &f, const void *chunk_params, int wc, int wcs,
                         const float *tgeo, const float2 *Btri, float2 *Ctri, float2 *ws, size_t ws_elems, int *err,
                         cudaStream_t st, int seg_tiles = 16, int ctas = 0, int stagger = 0);
+// The tensor-core form of the near field: targets pts4 (npts x 4 floats), no
+// pair excluded, flags without the adjoint double layer.
+void launch_nearfield_tc(const MeshDev &m, const OpFlags &f, const void *chunk_params, int wc, int wcs,
+                         const float *tgeo, const float *pts4, int64_t npts, const float2 *Btri, float2 *Cpts,
+                         float2 *ws, size_t ws_elems, int *err, cudaStream_t st, int seg_tiles = 16, int ctas = 0,
+                         int stagger = 0);
 // Source geometry of the tensor-core form, per 16-source tile (built once per mesh).
 size_t tc_tile_geometry_floats(int64_t nt);
 void launch_tc_tile_geometry(const MeshDev &m, float *tgeo, cudaStream_t st);

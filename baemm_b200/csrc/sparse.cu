@@ -267,6 +267,29 @@ __global__ void axpby_kernel(int64_t rows, int cols, T a, const T *__restrict__ 
     *o = isZero(b) ? ax : addT(ax, mulT(b, *o));
 }
 
+// Cout = alpha Cin + beta Cout (keep = false: beta == 0, overwrite, so stale
+// NaNs do not survive), in double, Cin packed with ld wc.
+template <class Text, class R>
+__global__ void combine_kernel(int64_t rows, int wc, double2 alpha, const cplx<R> *__restrict__ Cin, double2 beta,
+                               Text *__restrict__ Cout, int64_t ldC, bool keep)
+{
+    const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= rows * wc) return;
+    const int64_t r = idx / wc;
+    const int c = (int)(idx - r * wc);
+    const cplx<R> x = Cin[idx];
+    double2 v = dmul(alpha, make_double2((double)x.x, (double)x.y));
+    Text *o = &Cout[r * ldC + c];
+    if (keep)
+    {
+        const Text yo = *o;   // read and written by this thread only
+        const double2 y = dmul(beta, make_double2((double)yo.x, (double)yo.y));
+        v.x += y.x;
+        v.y += y.y;
+    }
+    *o = st2<Text>(v);
+}
+
 constexpr int kT = 256;
 inline int grid_for(int64_t n) { return ceil_div(n, kT); }
 
@@ -384,6 +407,16 @@ void launch_lumped_real(const MeshDev &m, bool fp64_values, const double *X, int
     BAEMM_LAUNCH_CHECK();
 }
 
+template <class Text, class R>
+void launch_combine(int64_t rows, int wc, double2 alpha, const cplx<R> *Cin, double2 beta, Text *Cout, int64_t ldC,
+                    cudaStream_t st)
+{
+    if (rows * wc == 0) return;
+    const bool keep = !(beta.x == 0.0 && beta.y == 0.0);
+    combine_kernel<Text, R><<<grid_for(rows * wc), kT, 0, st>>>(rows, wc, alpha, Cin, beta, Cout, ldC, keep);
+    BAEMM_LAUNCH_CHECK();
+}
+
 template <class Tsrc, class Tdst>
 void launch_copy_block(int64_t rows, int cols, const Tsrc *src, int64_t lds, Tdst *dst, int64_t ldd, cudaStream_t st)
 {
@@ -417,6 +450,14 @@ template void launch_epilogue<double2, double>(const MeshDev &, const EpilogueAr
 template void launch_epilogue<float2, double>(const MeshDev &, const EpilogueArgs &, const double2 *, const double2 *,
                                               const void *, const float2 *, int64_t, float2, float2, float2 *,
                                               int64_t, cudaStream_t);
+template void launch_combine<double2, float>(int64_t, int, double2, const float2 *, double2, double2 *, int64_t,
+                                            cudaStream_t);
+template void launch_combine<double2, double>(int64_t, int, double2, const double2 *, double2, double2 *, int64_t,
+                                             cudaStream_t);
+template void launch_combine<float2, float>(int64_t, int, double2, const float2 *, double2, float2 *, int64_t,
+                                           cudaStream_t);
+template void launch_combine<float2, double>(int64_t, int, double2, const double2 *, double2, float2 *, int64_t,
+                                            cudaStream_t);
 template void launch_copy_block<double2, double2>(int64_t, int, const double2 *, int64_t, double2 *, int64_t,
                                                   cudaStream_t);
 template void launch_copy_block<double2, float2>(int64_t, int, const double2 *, int64_t, float2 *, int64_t,

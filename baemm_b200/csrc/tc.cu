@@ -349,6 +349,8 @@ __device__ __forceinline__ uint32_t img_off16(int row, int sp) { return (uint32_
 struct TcPlan
 {
     int n, wc, nblk, ntiles, ncg, seg_tiles;
+    int m;             // targets (rows of C): n for the boundary operators, the point count for the near field
+    int self;          // 1: target i is source i and the pair is excluded (boundary); 0: no pair excluded
     int ctas;          // grid size
     int full_waves;    // whole blocks per CTA before the tail
     int tail_blocks;   // ncg * nblk - full_waves * ctas
@@ -420,7 +422,7 @@ boundary_tc_kernel(const float *__restrict__ mid4, const float *__restrict__ nrm
     TcSmem &sm = *reinterpret_cast<TcSmem *>(smem_raw + ((1024u - (smem_u32(smem_raw) & 1023u)) & 1023u));
     const int tid = threadIdx.x;
     const int warp = tid >> 5, lane = tid & 31;
-    const int n = plan.n, wc = plan.wc, ntiles = plan.ntiles;
+    const int n = plan.n, mt = plan.m, wc = plan.wc, ntiles = plan.ntiles;
     const int S = plan.seg_tiles;   // tiles per TMEM partial sum
     const int k_cta = blockIdx.x;
     volatile int *abort_flag = &sm.abort_flag;
@@ -526,9 +528,10 @@ boundary_tc_kernel(const float *__restrict__ mid4, const float *__restrict__ nrm
         while (ok && it.next(plan, cg, blk, tb, te, slot, rot))
         {
             const int i = blk * TC_M + row;
+            const int iself = plan.self ? i : -1;   // the source excluded for this target (none: -1)
             // -x_i and nu_i as broadcast pairs
             float2 nx0 = make_float2(0.f, 0.f), nx1 = nx0, nx2 = nx0, tn0 = nx0, tn1 = nx0, tn2 = nx0;
-            if (i < n)
+            if (i < mt)
             {
                 const float4 m = reinterpret_cast<const float4 *>(mid4)[i];
                 nx0 = make_float2(-m.x, -m.x); nx1 = make_float2(-m.y, -m.y); nx2 = make_float2(-m.z, -m.z);
@@ -555,7 +558,8 @@ boundary_tc_kernel(const float *__restrict__ mid4, const float *__restrict__ nrm
                 {
                     const TcTileGeo &G = sm.raw[rs].geo;
                     // tiles that hold the target itself or padding past the end need masks
-                    const bool special = (ts == ntiles - 1) || (ts * TC_SRC < blk * TC_M + TC_M && ts * TC_SRC + TC_SRC > blk * TC_M);
+                    const bool special = (ts == ntiles - 1) ||
+                                         (plan.self && ts * TC_SRC < blk * TC_M + TC_M && ts * TC_SRC + TC_SRC > blk * TC_M);
                     #pragma unroll
                     for (int p = 0; p < TC_PPT; ++p)
                     {
@@ -568,8 +572,8 @@ boundary_tc_kernel(const float *__restrict__ mid4, const float *__restrict__ nrm
                         if (special)
                         {
                             const int j = ts * TC_SRC + sl;
-                            if (!(j < n && j != i)) ri0 = 0.f;
-                            if (!(j + 1 < n && j + 1 != i)) ri1 = 0.f;
+                            if (!(j < n && j != iself)) ri0 = 0.f;
+                            if (!(j + 1 < n && j + 1 != iself)) ri1 = 0.f;
                         }
                         rinv[p] = make_float2(ri0, ri1);
                         r[p] = __fmul2_rn(r2, rinv[p]);
@@ -706,7 +710,7 @@ boundary_tc_kernel(const float *__restrict__ mid4, const float *__restrict__ nrm
             float2 *dst = nullptr;
             if (tb == 0 && te == ntiles)
             {
-                if (i < n) dst = &Ctri[(int64_t)i * wc + cg * cw];
+                if (i < mt) dst = &Ctri[(int64_t)i * wc + cg * cw];
             }
             else
                 dst = &ws[((int64_t)(k_cta * 2 + slot) * TC_M + row) * (TC_CHMAX * 16)];
@@ -926,7 +930,7 @@ __global__ void tc_fixup_kernel(const float2 *__restrict__ ws, float2 *__restric
     {
         const int row = e / cw, col = e - row * cw;
         const int i = blk * TC_M + row;
-        if (i >= plan.n) continue;
+        if (i >= plan.m) continue;
         float2 acc = make_float2(0.f, 0.f);
         for (int k = k_first; k <= k_last; ++k)
         {
@@ -1009,19 +1013,27 @@ void launch_tc_tile_geometry(const MeshDev &m, float *tgeo, cudaStream_t st)
     BAEMM_LAUNCH_CHECK();
 }
 
-void launch_boundary_tc(const MeshDev &m, const OpFlags &f, const void *chunk_params, int wc, int wcs,
-                        const float *tgeo, const float2 *Btri, float2 *Ctri, float2 *ws, size_t ws_elems, int *err,
-                        cudaStream_t st, int seg_tiles, int ctas, int stagger)
+namespace
+{
+// One launch of the tensor-core form over the targets (pts4, m_targets) and all
+// nt sources of the mesh; self = 1 excludes the pair i == j (targets are the
+// midpoints).
+void tc_run(const MeshDev &m, const OpFlags &f, const void *chunk_params, int wc, int wcs, const float *tgeo,
+            const float *pts4, int64_t m_targets, int self, const float2 *Btri, float2 *Ctri, float2 *ws,
+            size_t ws_elems, int *err, cudaStream_t st, int seg_tiles, int ctas, int stagger)
 {
     BAEMM_REQUIRE(tc_supported(wc, wcs), BAEMM_ERR_SIZE,
                   "tensor-core apply needs wave_chunk_size a multiple of 16 and wave_count <= 512");
-    if (!f.any_layer() || m.nt == 0) return;
+    BAEMM_REQUIRE(m_targets <= INT32_MAX - TC_M, BAEMM_ERR_SIZE, "too many targets");
+    if (!f.any_layer() || m.nt == 0 || m_targets == 0) return;
     TcPlan plan;
     plan.n = (int)m.nt;
+    plan.m = (int)m_targets;
+    plan.self = self;
     plan.wc = wc;
     const int CH = (wc % 64 == 0) ? 4 : (wc % 32 == 0) ? 2 : 1;
     plan.ncg = wc / (16 * CH);
-    plan.nblk = ceil_div(plan.n, TC_M);
+    plan.nblk = ceil_div(plan.m, TC_M);
     plan.ntiles = ceil_div(plan.n, TC_SRC);
     plan.seg_tiles = std::max(1, seg_tiles);
     const int blocks = plan.ncg * plan.nblk;
@@ -1034,22 +1046,22 @@ void launch_boundary_tc(const MeshDev &m, const OpFlags &f, const void *chunk_pa
     BAEMM_REQUIRE(ws && ws_elems >= tc_workspace_elems(plan.ctas), BAEMM_ERR_ARG, "tensor-core workspace too small");
     const int code = (f.sl() ? 1 : 0) | (f.dl() ? 2 : 0) | (f.adl() ? 4 : 0);
     const auto *p = static_cast<const ChunkParamsF *>(chunk_params);
-    const float *mid = m.mid_f, *nrm = m.nrm_f;
+    const float *nrm = m.nrm_f;   // target normals: read only with the adjoint double layer (targets = midpoints)
     const auto *tg = reinterpret_cast<const TcTileGeo *>(tgeo);
     BAEMM_REQUIRE(tg, BAEMM_ERR_ARG, "tensor-core tile geometry missing");
     // the real / imaginary coefficient structure of the BIE solves (see boundary_tc_kernel)
     const bool ri = !f.re_sl && !f.im_dl && !f.im_adl && (f.dl() || f.adl());
     if (ri)
     {
-        if (CH == 4) tc_flags<4, true>(code, st, mid, nrm, tg, Btri, Ctri, ws, p, plan, err);
-        else if (CH == 2) tc_flags<2, true>(code, st, mid, nrm, tg, Btri, Ctri, ws, p, plan, err);
-        else tc_flags<1, true>(code, st, mid, nrm, tg, Btri, Ctri, ws, p, plan, err);
+        if (CH == 4) tc_flags<4, true>(code, st, pts4, nrm, tg, Btri, Ctri, ws, p, plan, err);
+        else if (CH == 2) tc_flags<2, true>(code, st, pts4, nrm, tg, Btri, Ctri, ws, p, plan, err);
+        else tc_flags<1, true>(code, st, pts4, nrm, tg, Btri, Ctri, ws, p, plan, err);
     }
     else
     {
-        if (CH == 4) tc_flags<4, false>(code, st, mid, nrm, tg, Btri, Ctri, ws, p, plan, err);
-        else if (CH == 2) tc_flags<2, false>(code, st, mid, nrm, tg, Btri, Ctri, ws, p, plan, err);
-        else tc_flags<1, false>(code, st, mid, nrm, tg, Btri, Ctri, ws, p, plan, err);
+        if (CH == 4) tc_flags<4, false>(code, st, pts4, nrm, tg, Btri, Ctri, ws, p, plan, err);
+        else if (CH == 2) tc_flags<2, false>(code, st, pts4, nrm, tg, Btri, Ctri, ws, p, plan, err);
+        else tc_flags<1, false>(code, st, pts4, nrm, tg, Btri, Ctri, ws, p, plan, err);
     }
     BAEMM_LAUNCH_CHECK();
     if (plan.tail_blocks > 0)
@@ -1057,6 +1069,24 @@ void launch_boundary_tc(const MeshDev &m, const OpFlags &f, const void *chunk_pa
         tc_fixup_kernel<<<plan.tail_blocks, 256, 0, st>>>(ws, Ctri, plan, CH * 16);
         BAEMM_LAUNCH_CHECK();
     }
+}
+} // namespace
+
+void launch_boundary_tc(const MeshDev &m, const OpFlags &f, const void *chunk_params, int wc, int wcs,
+                        const float *tgeo, const float2 *Btri, float2 *Ctri, float2 *ws, size_t ws_elems, int *err,
+                        cudaStream_t st, int seg_tiles, int ctas, int stagger)
+{
+    tc_run(m, f, chunk_params, wc, wcs, tgeo, m.mid_f, m.nt, 1, Btri, Ctri, ws, ws_elems, err, st, seg_tiles, ctas,
+           stagger);
+}
+
+void launch_nearfield_tc(const MeshDev &m, const OpFlags &f, const void *chunk_params, int wc, int wcs,
+                         const float *tgeo, const float *pts4, int64_t npts, const float2 *Btri, float2 *Cpts,
+                         float2 *ws, size_t ws_elems, int *err, cudaStream_t st, int seg_tiles, int ctas, int stagger)
+{
+    BAEMM_REQUIRE(!f.adl() && !f.mass(), BAEMM_ERR_ARG, "near field: single and double layer only");
+    tc_run(m, f, chunk_params, wc, wcs, tgeo, pts4, npts, 0, Btri, Cpts, ws, ws_elems, err, st, seg_tiles, ctas,
+           stagger);
 }
 
 } // namespace baemm

@@ -371,6 +371,70 @@ class Helmholtz_CUDA:
                 _dp(C_out.view(np.float64)), C_out.shape[1]))
         return C_out
 
+    def ApplyNearFieldOperators_PL(self, alpha, B_in, beta, C_out, *args):
+        """C_out (points x wc) = alpha (c1 SL + c2 DL)(points) AvOp B_in + beta C_out
+        (ApplyNearFieldOperators.hpp:27-122), the boundary potential at points
+        off the surface.
+
+        The reference's two overloads:
+            ApplyNearFieldOperators_PL(alpha, B_in, beta, C_out, kappa, coeff, wave_count,
+                                       wave_chunk_size, evaluation_points)
+            ApplyNearFieldOperators_PL(alpha, B_in, beta, C_out, evaluation_points)
+        (the second uses the loaded parameters).  evaluation_points: m x 3.
+        numpy complex128 / complex64 host blocks or torch CUDA complex tensors
+        (then the points may be a torch CUDA float64 tensor or host array).
+        """
+        if len(args) == 5:
+            kappa, coeff, wave_count, wave_chunk_size, points = args
+        elif len(args) == 1:
+            kappa = coeff = wave_count = wave_chunk_size = None
+            points = args[0]
+        else:
+            raise TypeError("ApplyNearFieldOperators_PL(alpha, B_in, beta, C_out, [kappa, coeff, wave_count, "
+                            "wave_chunk_size,] evaluation_points)")
+        if _is_torch_cuda(B_in):
+            import torch
+            if kappa is not None:
+                self.LoadParameters(kappa, coeff, wave_count, wave_chunk_size)
+            if B_in.dtype == torch.complex128:
+                fn, cs, ptr = self._lib.baemm_apply_near_field_operators_dev_z, _cz, _dp
+            elif B_in.dtype == torch.complex64:
+                fn, cs, ptr = self._lib.baemm_apply_near_field_operators_dev_c, _cc, _fp
+            else:
+                raise TypeError("B_in must be complex64 or complex128")
+            if _is_torch_cuda(points):
+                P = points.to(torch.float64).reshape(-1, 3).contiguous()
+            else:
+                P = torch.from_numpy(_f64(points).reshape(-1, 3)).to(B_in.device)
+            with self._on_torch_stream(B_in):
+                self._ck(fn(self._h, ptr(cs(alpha)), C.c_void_p(B_in.data_ptr()), B_in.stride(0), ptr(cs(beta)),
+                            C.c_void_p(C_out.data_ptr()), C_out.stride(0), C.c_void_p(P.data_ptr()), P.shape[0]))
+            return C_out
+        if isinstance(B_in, np.ndarray) and B_in.dtype == np.complex64:
+            if kappa is not None:
+                self.LoadParameters(kappa, coeff, wave_count, wave_chunk_size)
+            _check_out(C_out, np.complex64, "C_out")
+            B = np.ascontiguousarray(B_in)
+            P = np.ascontiguousarray(points, dtype=np.float32).reshape(-1, 3)
+            self._ck(self._lib.baemm_apply_near_field_operators_c(
+                self._h, _fp(_cc(alpha)), _fp(B.view(np.float32)), B.shape[1], _fp(_cc(beta)),
+                _fp(C_out.view(np.float32)), C_out.shape[1], _fp(P), P.shape[0]))
+            return C_out
+        _check_out(C_out, np.complex128, "C_out")
+        B = np.ascontiguousarray(B_in, dtype=np.complex128)
+        P = _f64(points).reshape(-1, 3)
+        if kappa is not None:
+            k, c = _f64(kappa), _coeff(coeff)
+            self._ck(self._lib.baemm_apply_near_field_operators_full_z(
+                self._h, _dp(_cz(alpha)), _dp(B.view(np.float64)), B.shape[1], _dp(_cz(beta)),
+                _dp(C_out.view(np.float64)), C_out.shape[1], _dp(k), _dp(c.view(np.float64)), int(wave_count),
+                int(wave_chunk_size), _dp(P), P.shape[0]))
+        else:
+            self._ck(self._lib.baemm_apply_near_field_operators_z(
+                self._h, _dp(_cz(alpha)), _dp(B.view(np.float64)), B.shape[1], _dp(_cz(beta)),
+                _dp(C_out.view(np.float64)), C_out.shape[1], _dp(P), P.shape[0]))
+        return C_out
+
     def CreateIncidentWave_PL(self, alpha, incident_directions, beta, C_out, kappa, coeff, wave_count,
                               wave_chunk_size, wave_type=WaveType.Plane):
         """C_out = alpha * wave + beta * C_out (CreateIncidentWave.hpp:21-50)."""

@@ -147,6 +147,29 @@ def torus(major: float = 1.0, minor: float = 0.4, n_minor: int = 160, n_major: i
     return coords, tris
 
 
+def points_off_torus(n: int, major: float = 1.0, minor: float = 0.4, min_dist: float = 0.05, seed: int = 0,
+                     box=((-1.6, 1.6), (-1.6, 1.6), (-0.6, 0.6))) -> np.ndarray:
+    """``n`` seeded points, uniform in ``box``, whose distance to the torus
+    surface is at least ``min_dist`` (inside the tube and outside), float64 n x 3.
+
+    Evaluation points for near-field potentials: closer to the surface the
+    rounding of z = y - x in single precision is amplified by 1 / r^3.
+    """
+    rng = np.random.default_rng(seed)
+    lo = np.array([b[0] for b in box])
+    hi = np.array([b[1] for b in box])
+    out = []
+    have = 0
+    while have < n:
+        p = lo + (hi - lo) * rng.random((2 * (n - have) + 64, 3))
+        rho = np.hypot(p[:, 0], p[:, 1])
+        d = np.abs(np.hypot(rho - major, p[:, 2]) - minor)
+        p = p[d >= min_dist]
+        out.append(p)
+        have += p.shape[0]
+    return np.concatenate(out)[:n]
+
+
 def fibonacci_sphere(n: int) -> np.ndarray:
     """``n`` quasi-uniform unit vectors (golden-angle spiral), float64 n x 3."""
     i = np.arange(n, dtype=np.float64) + 0.5

@@ -255,6 +255,37 @@ public:
             copy_block(C.data(), wc, C_out, ldC_out, GetMeasCount(), wc);
     }
 
+    // ---- near field (ApplyNearFieldOperators.hpp) ------------------------------------------
+    template <typename R_ext, typename C_ext, typename I_ext>
+    void ApplyNearFieldOperators_PL(const C_ext alpha, const C_ext *B_in, const I_ext ldB_in, const C_ext beta,
+                                    C_ext *C_out, const I_ext ldC_out, const R_ext *kappa_list,
+                                    const C_ext *coeff_list, const I_ext wave_count_, const I_ext wave_chunk_size_,
+                                    const R_ext *evaluation_points, const I_ext evaluation_count)
+    {
+        LoadParameters(kappa_list, coeff_list, wave_count_, wave_chunk_size_);
+        ApplyNearFieldOperators_PL(alpha, B_in, ldB_in, beta, C_out, ldC_out, evaluation_points, evaluation_count);
+    }
+
+    // C_out (evaluation_count x wave_count, ld ldC_out) = alpha (c1 SL + c2 DL)(points) B_in + beta C_out
+    template <typename R_ext, typename C_ext, typename I_ext>
+    void ApplyNearFieldOperators_PL(const C_ext alpha, const C_ext *B_in, const I_ext ldB_in, const C_ext beta,
+                                    C_ext *C_out, const I_ext ldC_out, const R_ext *evaluation_points,
+                                    const I_ext evaluation_count)
+    {
+        const Int wc = GetWaveCount();
+        const Int m = (Int)evaluation_count;
+        auto B = to_z_block(B_in, VertexCount(), wc, ldB_in);
+        std::vector<std::complex<double>> C((size_t)m * wc);
+        copy_block(C_out, ldC_out, C.data(), wc, m, wc);
+        auto P = to_d(evaluation_points, 3 * (size_t)m);
+        const double a[2] = {(double)alpha.real(), (double)alpha.imag()};
+        const double b[2] = {(double)beta.real(), (double)beta.imag()};
+        if (check(baemm_apply_near_field_operators_z(ctx_, a, dd(B.data()), wc, b, dd(C.data()), wc, P.data(),
+                                                     (int64_t)m),
+                  "ApplyNearFieldOperators_PL"))
+            copy_block(C.data(), wc, C_out, ldC_out, m, wc);
+    }
+
     // ---- waves (CreateIncidentWave.hpp, CreateHerglotzWave.hpp) ---------------------------
     template <typename R_ext, typename C_ext, typename I_ext>
     void CreateIncidentWave_PL(const C_ext alpha, const R_ext *incident_directions, const I_ext inc_count,

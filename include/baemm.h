@@ -254,6 +254,42 @@ int baemm_apply_far_field_operators_loaded_z(baemm_ctx *ctx, const double alpha[
 int baemm_apply_far_field_operators_dev_z(baemm_ctx *ctx, const double alpha[2], const double *B_in, int64_t ldB,
                                           const double beta[2], double *C_out, int64_t ldC);
 
+/* ApplyNearFieldOperators_PL (ApplyNearFieldOperators.hpp:56-122, kernel
+ * NearFieldOperatorKernel.cl:5-194): the boundary potential of the vertex
+ * values B_in (vertex_count x wave_count) at evaluation points,
+ *   C_out (point_count x wave_count) = alpha * (c1 SL + c2 DL)(points) AvOp B_in
+ *                                      + beta * C_out,
+ * no pair excluded, c0 (mass) and c3 (adjoint double layer) not used.
+ * evaluation_points: point_count x 3.  Uses the loaded parameters (the
+ * reference's overload without kappa_list); returns without touching C_out
+ * when none are loaded or neither layer is present, as the reference does.
+ * The arithmetic is the context's apply mode (FP32, tensor-core, FP64).
+ * The reference writes C_out with leading dimension wave_count whatever ldC_out
+ * is (ApplyNearFieldOperators.hpp:76,112-116); here ldC is honoured (the same
+ * when ldC == wave_count).  A point that coincides with a triangle midpoint
+ * gives non-finite values in its row, as in the reference (r = 0). */
+int baemm_apply_near_field_operators_z(baemm_ctx *ctx, const double alpha[2], const double *B_in, int64_t ldB,
+                                       const double beta[2], double *C_out, int64_t ldC,
+                                       const double *evaluation_points, int64_t point_count);
+int baemm_apply_near_field_operators_c(baemm_ctx *ctx, const float alpha[2], const float *B_in, int64_t ldB,
+                                       const float beta[2], float *C_out, int64_t ldC,
+                                       const float *evaluation_points, int64_t point_count);
+/* The overload with kappa_list / coeff_list (ApplyNearFieldOperators.hpp:27-50):
+ * loads the parameters first, as LoadParameters does. */
+int baemm_apply_near_field_operators_full_z(baemm_ctx *ctx, const double alpha[2], const double *B_in, int64_t ldB,
+                                            const double beta[2], double *C_out, int64_t ldC, const double *kappa,
+                                            const double *coeff, int wave_count, int wave_chunk_size,
+                                            const double *evaluation_points, int64_t point_count);
+/* Device-pointer forms (no reference counterpart): B_in, C_out and
+ * evaluation_points (point_count x 3 doubles) in device memory; enqueued on the
+ * context's stream without host synchronisation. */
+int baemm_apply_near_field_operators_dev_z(baemm_ctx *ctx, const double alpha[2], const double *B_in, int64_t ldB,
+                                           const double beta[2], double *C_out, int64_t ldC,
+                                           const double *evaluation_points, int64_t point_count);
+int baemm_apply_near_field_operators_dev_c(baemm_ctx *ctx, const float alpha[2], const float *B_in, int64_t ldB,
+                                           const float beta[2], float *C_out, int64_t ldC,
+                                           const double *evaluation_points, int64_t point_count);
+
 /* CreateIncidentWave_PL (CreateIncidentWave.hpp:21-50): weak-form incident
  * waves, C_out (vertex_count x wave_count) = alpha * wave + beta * C_out.
  * incident_directions: inc_count x 3 (plane directions or point sources). */

@@ -293,6 +293,8 @@ struct Base
     virtual void farfield_kernel() = 0;                                        // B_tri -> F (nm x wc)
     virtual void farfield_out(cd alpha, cd beta, cd *C, int64_t ldC) = 0;
     virtual void herglotz_kernel(const cd *g, int64_t ldg) = 0;                // g -> C_tri
+    virtual void nearfield_kernel(const double *pts, int64_t m) = 0;           // B_tri -> P (m x wc)
+    virtual void nearfield_out(cd alpha, cd beta, cd *C, int64_t ldC, int64_t m) = 0;
     virtual void incident_kernel(const double *dirs, int type) = 0;            // -> C_tri
     virtual void get_geometry(double *mid, double *nrm, double *areas, double *diag) = 0;
     // real-typed PL->PC / PC->PL helpers used by the normal-field helpers
@@ -385,6 +387,19 @@ struct Base
             avop(B, ldB, wave_count);
             farfield_kernel();
             farfield_out(alpha, beta, C, ldC);
+        }
+    }
+    // ApplyNearFieldOperators.hpp:56-122 (output written with ldC; the
+    // reference uses wave_count, the same when ldC == wave_count)
+    void apply_nearfield(cd alpha, const cd *B, int64_t ldB, cd beta, cd *C, int64_t ldC, const double *pts,
+                         int64_t m)
+    {
+        if (wave_chunk_count < 1) return;
+        if (any_sl_dl())
+        {
+            avop(B, ldB, wave_count);
+            nearfield_kernel(pts, m);
+            nearfield_out(alpha, beta, C, ldC, m);
         }
     }
     // CreateHerglotzWave.hpp:50-95
@@ -546,6 +561,7 @@ struct Ctx : Base
     std::vector<Real> kappa;
     std::vector<C> c;                                // wcc x 4
     std::vector<C> Btri, Ctri, F;                    // nt x wc, nt x wc, nm x wc
+    std::vector<C> P;                                // near field: m x wc
     static constexpr bool fp32 = std::is_same<Real, float>::value;
 
     void init(const double *coords, int64_t nv_, const int32_t *tris, int64_t nt_,
@@ -857,6 +873,53 @@ struct Ctx : Base
         }
     }
 
+    // NearFieldOperatorKernel.cl:86-149: z = y_j - x_i at the evaluation points
+    // (converted to Real, ApplyNearFieldOperators.hpp:98-107), no pair excluded,
+    // A = c1 e^{ikr}/r + c2 (z.mu_j) (ikr - 1) e^{ikr}/r^3.
+    void nearfield_kernel(const double *pts, int64_t m) override
+    {
+        P.assign(m * wave_count, C(0));
+        std::vector<Real> x4(4 * m, Real(0));
+        for (int64_t i = 0; i < m; ++i)
+            for (int d = 0; d < 3; ++d) x4[4 * i + d] = (Real)pts[3 * i + d];
+        const int kcc = wave_count / wave_chunk_size;
+        const bool sl = Re_sl || Im_sl, dl = Re_dl || Im_dl;
+        for (int ch = 0; ch < kcc; ++ch)
+        {
+            const Real kap = kappa[ch];
+            const C c1 = c[4 * ch + 1], c2 = c[4 * ch + 2];
+            dense_rows(m, nt, Btri.data(), P.data(), ch, [&](int64_t i, int64_t j) -> C {
+                const Real *x = &x4[4 * i];
+                const Real zx = mid[4 * j] - x[0], zy = mid[4 * j + 1] - x[1], zz = mid[4 * j + 2] - x[2];
+                const Real r = std::sqrt(zx * zx + zy * zy + zz * zz);
+                const Real rinv = Real(1) / r;
+                const Real kr = kap * r;
+                const Real sn = std::sin(kr), cs = std::cos(kr);
+                C A(0);
+                if (sl) A = c1 * C(cs * rinv, sn * rinv);
+                if (dl)
+                {
+                    const Real r3 = rinv * rinv * rinv;
+                    const C g(-(kr * sn + cs) * r3, (kr * cs - sn) * r3);
+                    A += c2 * (zx * nrm[4 * j] + zy * nrm[4 * j + 1] + zz * nrm[4 * j + 2]) * g;
+                }
+                return A;
+            });
+        }
+    }
+    // combine_matrices(alpha, C_ptr, ..., beta, C_out, ...) with the external
+    // alpha (ApplyNearFieldOperators.hpp:112-116); beta == 0 overwrites.
+    void nearfield_out(cd alpha, cd beta, cd *Cout, int64_t ldC, int64_t m) override
+    {
+        for (int64_t i = 0; i < m; ++i)
+            for (int k = 0; k < wave_count; ++k)
+            {
+                cd &o = Cout[i * ldC + k];
+                const cd v = alpha * cd(P[i * wave_count + k]);
+                o = (beta == cd(0)) ? v : v + beta * o;
+            }
+    }
+
     // IncidentWaveKernel_Plane.hpp:189-233 (type 201), IncidentWaveKernel_Radial.hpp:5-57 (type 202)
     void incident_kernel(const double *dirs, int type) override
     {
@@ -1054,6 +1117,26 @@ void orc_apply_farfield(void *h, const double *alpha, const double *B, int64_t l
 {
     static_cast<Base *>(h)->apply_farfield(cd(alpha[0], alpha[1]), reinterpret_cast<const cd *>(B), ldB,
                                            cd(beta[0], beta[1]), reinterpret_cast<cd *>(C), ldC);
+}
+void orc_apply_nearfield(void *h, const double *alpha, const double *B, int64_t ldB, const double *beta, double *C,
+                         int64_t ldC, const double *pts, int64_t m)
+{
+    static_cast<Base *>(h)->apply_nearfield(cd(alpha[0], alpha[1]), reinterpret_cast<const cd *>(B), ldB,
+                                            cd(beta[0], beta[1]), reinterpret_cast<cd *>(C), ldC, pts, m);
+}
+// Raw near-field kernel on triangle data (B_tri: nt x wc -> P: m x wc), no AvOp / combine.
+void orc_nearfield_kernel_tri(void *h, const double *Btri, const double *pts, int64_t m, double *P)
+{
+    auto run = [&](auto *c) {
+        using Cx = typename std::remove_reference<decltype(c->Btri[0])>::type;
+        const int64_t N = c->nt * c->wave_count;
+        c->Btri.resize(N);
+        for (int64_t e = 0; e < N; ++e) c->Btri[e] = Cx(Btri[2 * e], Btri[2 * e + 1]);
+        c->nearfield_kernel(pts, m);
+        for (int64_t e = 0; e < m * c->wave_count; ++e) { P[2 * e] = c->P[e].real(); P[2 * e + 1] = c->P[e].imag(); }
+    };
+    auto *b = static_cast<Base *>(h);
+    if (auto *c = dynamic_cast<Ctx<float> *>(b)) run(c); else run(static_cast<Ctx<double> *>(b));
 }
 void orc_create_herglotz(void *h, const double *alpha, const double *g, int64_t ldg,
                          const double *beta, double *C, int64_t ldC)

@@ -6,6 +6,7 @@
 #   src/Helmholtz_OpenCL/BoundaryOperatorKernel.cl
 #   src/Helmholtz_OpenCL/FarFieldOperatorKernel.cl
 #   src/Helmholtz_OpenCL/HerglotzWaveKernel.cl
+#   src/Helmholtz_OpenCL/NearFieldOperatorKernel.cl
 # Each .cl file is a C++ raw-string literal: its first line `R"(` and last line
 # `)"` are stripped and the remainder is streamed to g++ on stdin, so no copy of
 # the reference source is written anywhere.  One namespace per k_chunk_size in
@@ -18,7 +19,7 @@ HERE="$(cd "$(dirname "${BASH_SOURCE[0]}")" && pwd)"
 OUT="$HERE/_ref"
 KDIR="$REF/src/Helmholtz_OpenCL"
 
-for f in BoundaryOperatorKernel FarFieldOperatorKernel HerglotzWaveKernel; do
+for f in BoundaryOperatorKernel FarFieldOperatorKernel HerglotzWaveKernel NearFieldOperatorKernel; do
     if [ ! -f "$KDIR/$f.cl" ]; then
         echo "build_ref.sh: $KDIR/$f.cl not found" >&2
         exit 1
@@ -31,7 +32,8 @@ emit() {
     for K in 1 2 4 8 16 32 64; do
         echo "namespace refcl_k$K {"
         echo "#define k_chunk_size $K"
-        for pair in bok:BoundaryOperatorKernel ffk:FarFieldOperatorKernel hwk:HerglotzWaveKernel; do
+        for pair in bok:BoundaryOperatorKernel ffk:FarFieldOperatorKernel hwk:HerglotzWaveKernel \
+                    nfk:NearFieldOperatorKernel; do
             ns="${pair%%:*}"; f="${pair#*:}"
             echo "namespace $ns {"
             echo "#line 2 \"$f.cl\""

@@ -4,6 +4,7 @@
 //   src/Helmholtz_OpenCL/BoundaryOperatorKernel.cl
 //   src/Helmholtz_OpenCL/FarFieldOperatorKernel.cl
 //   src/Helmholtz_OpenCL/HerglotzWaveKernel.cl
+//   src/Helmholtz_OpenCL/NearFieldOperatorKernel.cl
 // compile as host C++ with block_size == 1 (one work item per work group).
 // With block_size == 1 every work item accumulates its row C_i over the
 // sources j strictly in increasing j order, exactly as the reference does for

@@ -2,12 +2,13 @@
 //
 // Host driver for the shim-compiled reference kernels (see cl_shim.h).  It is
 // appended after the kernel sources by build_ref.sh, so the namespaces
-// refcl_k<K>::{bok,ffk,hwk} (K = k_chunk_size) are visible here.
+// refcl_k<K>::{bok,ffk,hwk,nfk} (K = k_chunk_size) are visible here.
 //
 // Each entry point runs the reference kernel once per target row in
 // [row_begin, row_end) on an OpenMP team: the same NDRange the reference
 // launches (BoundaryOperatorKernel.hpp:16-18, FarFieldOperatorKernel.hpp:287-289,
-// HerglotzWaveKernel.hpp), with block_size == 1.  Coefficients must already be
+// HerglotzWaveKernel.hpp, NearFieldOperatorKernel.hpp:98-101), with
+// block_size == 1.  Coefficients must already be
 // scaled as LoadParameters.hpp:65-79 does (c1..c3 times factor/(4 pi)).
 // Not reentrant: the specialisation flags are process globals.
 #include <omp.h>
@@ -107,6 +108,22 @@ int refcl_herglotz(const float4 *mid, const float4 *nrm, const float4 *meas,
     REFCL_DISPATCH(wave_chunk_size,
         refcl_driver::run_rows(row_begin, row_end, nthreads, [&] {
             ns::hwk::HerglotzWaveKernel(mid, nrm, meas, B, C, kappa, coeff, &n, &m, &wave_count);
+        }))
+    return 0;
+}
+
+// NearFieldOperatorKernel.cl:5-194.  B: n x wave_count (triangle values),
+// points: m evaluation points (xyz, w = 0), C: m x wave_count.
+int refcl_nearfield(const float4 *mid, const float4 *nrm, const float2 *B, const float4 *points, float2 *C,
+                    const float *kappa, const float2 *coeff,
+                    int n, int m, int wave_count, int wave_chunk_size,
+                    int row_begin, int row_end, int nthreads)
+{
+    const int chunk_count = wave_count / wave_chunk_size;
+    refcl_driver::set_flags(coeff, chunk_count);
+    REFCL_DISPATCH(wave_chunk_size,
+        refcl_driver::run_rows(row_begin, row_end, nthreads, [&] {
+            ns::nfk::NearFieldOperatorKernel(mid, nrm, B, points, C, kappa, coeff, &n, &wave_count, &m);
         }))
     return 0;
 }

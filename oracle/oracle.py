@@ -68,6 +68,8 @@ def lib():
             "orc_farfield_kernel_tri": [V, _dp, _dp],
             "orc_herglotz_kernel_tri": [V, _dp, _dp],
             "orc_apply_farfield": [V, _dp, _dp, I64, _dp, _dp, I64],
+            "orc_apply_nearfield": [V, _dp, _dp, I64, _dp, _dp, I64, _dp, I64],
+            "orc_nearfield_kernel_tri": [V, _dp, _dp, I64, _dp],
             "orc_create_herglotz": [V, _dp, _dp, I64, _dp, _dp, I64],
             "orc_create_incident": [V, _dp, _dp, _dp, _dp, I64, I],
             "orc_mass_dot": [V, _dp, _dp, I64, _dp, _dp, I64, I],
@@ -108,6 +110,7 @@ def reflib():
         _ref.refcl_boundary.argtypes = [F, F, F, F, F, F, I, I, I, I, I, I]
         _ref.refcl_farfield.argtypes = [F, F, F, F, F, F, F, I, I, I, I, I, I, I]
         _ref.refcl_herglotz.argtypes = [F, F, F, F, F, F, F, I, I, I, I, I, I, I]
+        _ref.refcl_nearfield.argtypes = [F, F, F, F, F, F, F, I, I, I, I, I, I, I]
     return _ref
 
 
@@ -220,6 +223,26 @@ class Oracle:
         lib().orc_apply_farfield(self._h, _p(a.view(np.float64)), _p(B.view(np.float64)), B.shape[1],
                                  _p(b.view(np.float64)), _p(Cout.view(np.float64)), Cout.shape[1])
         return Cout
+
+    def ApplyNearFieldOperators_PL(self, alpha, B, beta, Cout, kappa, coeff, wave_count, wave_chunk_size,
+                                   evaluation_points):
+        """ApplyNearFieldOperators.hpp:27-122: Cout (m x wc) = alpha K(points) AvOp B + beta Cout."""
+        self.LoadParameters(kappa, coeff, wave_count, wave_chunk_size)
+        B = _c128(B); pts = _f64(evaluation_points).reshape(-1, 3)
+        assert Cout.dtype == np.complex128 and Cout.flags.c_contiguous
+        a = np.array([complex(alpha)], np.complex128); b = np.array([complex(beta)], np.complex128)
+        lib().orc_apply_nearfield(self._h, _p(a.view(np.float64)), _p(B.view(np.float64)), B.shape[1],
+                                  _p(b.view(np.float64)), _p(Cout.view(np.float64)), Cout.shape[1], _p(pts),
+                                  pts.shape[0])
+        return Cout
+
+    def nearfield_kernel_tri(self, Btri, kappa, coeff, wave_count, wave_chunk_size, evaluation_points):
+        self.LoadParameters(kappa, coeff, wave_count, wave_chunk_size)
+        Btri = _c128(Btri); pts = _f64(evaluation_points).reshape(-1, 3)
+        P = np.zeros((pts.shape[0], wave_count), np.complex128)
+        lib().orc_nearfield_kernel_tri(self._h, _p(Btri.view(np.float64)), _p(pts), pts.shape[0],
+                                       _p(P.view(np.float64)))
+        return P
 
     def CreateHerglotzWave_PL(self, alpha, g, beta, Cout, kappa, coeff, wave_count, wave_chunk_size):
         self.LoadParameters(kappa, coeff, wave_count, wave_chunk_size, 4.0 * np.pi / self.nm)
@@ -396,4 +419,25 @@ def ref_herglotz(mid4, nrm4, meas4, G, kappa, coeff_scaled, wave_chunk_size, thr
                                  n, m, wc, int(wave_chunk_size), 0, n, int(threads))
     if rc != 0:
         raise ValueError("refcl_herglotz: unsupported wave_chunk_size")
+    return Cout
+
+
+def ref_nearfield(mid4, nrm4, Btri, points, kappa, coeff_scaled, wave_chunk_size, row_begin=0, row_end=None,
+                  threads=0):
+    """The reference's NearFieldOperatorKernel.cl on triangle data: P (m x wc) at points (m x 3)."""
+    mid4 = np.ascontiguousarray(mid4, np.float32); nrm4 = np.ascontiguousarray(nrm4, np.float32)
+    Btri = np.ascontiguousarray(Btri, np.complex64)
+    pts = np.asarray(points, np.float64).reshape(-1, 3)
+    pts4 = np.zeros((pts.shape[0], 4), np.float32)
+    pts4[:, :3] = pts.astype(np.float32)   # ApplyNearFieldOperators.hpp:98-107
+    n, wc = Btri.shape
+    m = pts4.shape[0]
+    Cout = np.zeros((m, wc), np.complex64)
+    kap = np.ascontiguousarray(kappa, np.float32); co = np.ascontiguousarray(coeff_scaled, np.complex64)
+    row_end = m if row_end is None else row_end
+    rc = reflib().refcl_nearfield(_p(mid4, _fp), _p(nrm4, _fp), _p(Btri.view(np.float32), _fp), _p(pts4, _fp),
+                                  _p(Cout.view(np.float32), _fp), _p(kap, _fp), _p(co.view(np.float32), _fp),
+                                  n, m, wc, int(wave_chunk_size), int(row_begin), int(row_end), int(threads))
+    if rc != 0:
+        raise ValueError("refcl_nearfield: unsupported wave_chunk_size")
     return Cout

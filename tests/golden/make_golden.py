@@ -1,8 +1,10 @@
 """Generate tests/golden/refcl_small.npz from the reference's own kernels.
 
 The dense kernels come from oracle/_ref/libbaemm_refcl.so: the reference's
-BoundaryOperatorKernel.cl, FarFieldOperatorKernel.cl and HerglotzWaveKernel.cl
-compiled as C++ by oracle/build_ref.sh (block_size 1).  Inputs are seeded and
+BoundaryOperatorKernel.cl, FarFieldOperatorKernel.cl, HerglotzWaveKernel.cl and
+NearFieldOperatorKernel.cl compiled as C++ by oracle/build_ref.sh (block_size 1).
+The near-field cases evaluate at 45 seeded points inside, near and outside the
+sphere (none on a midpoint).  Inputs are seeded and
 small (icosphere level 2: 162 vertices / 320 triangles, 32 far-field
 directions), so the fixture is a few hundred KB.  Geometry inputs are the
 float32 midpoints/normals of the FP32 oracle restatement, which the CPU tests
@@ -31,6 +33,12 @@ BOUNDARY_CASES = [
     ("bie_dl", [0.5, -2.0j, 1, 0], [2.0], 16, 16),
     ("mix_2k", [0, 1 + 0.5j, 1 - 2j, 0.3j], [3.0, 7.5], 32, 16),
     ("wcs4", [0, 0.25j, 1, 1], [1.0, 2.0, 4.0, 8.0], 16, 4),
+]
+NF_CASES = [
+    ("nf_sl", [0, 1, 0, 0], [2.0], 16, 16),
+    ("nf_dl", [0, 0, 1, 0], [2.0], 16, 16),
+    ("nf_mix", [0.7, 1 + 0.5j, 1 - 2j, 0.3j], [3.0, 7.5], 32, 16),
+    ("nf_wcs4", [0, 0.25j, 1, 1], [1.0, 2.0, 4.0, 8.0], 16, 4),
 ]
 FF_CASES = [
     ("ff_sl", [0, 1, 0, 0], [2.0], 16, 16),
@@ -74,6 +82,21 @@ def main(out_path: str | None = None) -> str:
     G = (rng.standard_normal((meas.shape[0], 32)) + 1j * rng.standard_normal((meas.shape[0], 32))).astype(np.complex64)
     C = O.ref_herglotz(mid32, nrm32, meas4, G, kap, O.scaled_coefficients(coeff, 4 * np.pi / meas.shape[0]), 16)
     out.update({"hw_G": G, "hw_C": C, "hw_coeff": coeff, "hw_kappa": kap, "hw_wcs": np.array(16)})
+    # near field (appended last: the cases above keep their random inputs)
+    dirs = rng.standard_normal((45, 3))
+    dirs /= np.linalg.norm(dirs, axis=1, keepdims=True)
+    radii = np.tile([0.3, 0.6, 0.9, 1.1, 1.5, 2.5, 4.0, 8.0, 0.05], 5)
+    pts = dirs * radii[:, None]
+    out["nf_points"] = pts
+    for name, co, kap, wc, wcs in NF_CASES:
+        B = (rng.standard_normal((n, wc)) + 1j * rng.standard_normal((n, wc))).astype(np.complex64)
+        coeff = np.array([co] * len(kap), np.complex128)
+        C = O.ref_nearfield(mid32, nrm32, B, pts, np.array(kap), O.scaled_coefficients(coeff), wcs)
+        out[f"{name}_B"] = B
+        out[f"{name}_C"] = C
+        out[f"{name}_coeff"] = coeff
+        out[f"{name}_kappa"] = np.array(kap)
+        out[f"{name}_wcs"] = np.array(wcs)
     path = out_path or os.path.join(os.path.dirname(os.path.abspath(__file__)), "refcl_small.npz")
     np.savez_compressed(path, **out)
     return path

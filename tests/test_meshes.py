@@ -50,3 +50,14 @@ def test_fibonacci_and_sh_perturbation():
     c, t = meshes.sh_perturbed_sphere(3, 8, 0.1, seed=0)
     r = np.linalg.norm(c, axis=1)
     assert abs(np.abs(r - 1).max() - 0.1) < 1e-9
+
+
+def test_points_off_torus_keep_their_distance():
+    p = meshes.points_off_torus(5000, 1.0, 0.4, min_dist=0.05, seed=3)
+    assert p.shape == (5000, 3)
+    d = np.abs(np.hypot(np.hypot(p[:, 0], p[:, 1]) - 1.0, p[:, 2]) - 0.4)
+    assert d.min() >= 0.05
+    assert np.all(np.abs(p[:, 2]) <= 0.6) and np.all(np.abs(p[:, :2]) <= 1.6)
+    inside = np.hypot(np.hypot(p[:, 0], p[:, 1]) - 1.0, p[:, 2]) < 0.4
+    assert 0.1 < inside.mean() < 0.4                      # both sides of the surface
+    assert np.array_equal(p, meshes.points_off_torus(5000, 1.0, 0.4, min_dist=0.05, seed=3))

@@ -53,6 +53,100 @@ def test_oracle_herglotz_kernel_pinned_to_reference(golden):
     assert relerr(Cref, h64) < 2e-5
 
 
+@pytest.mark.parametrize("name", ["nf_sl", "nf_dl", "nf_mix", "nf_wcs4"])
+def test_oracle_nearfield_kernel_pinned_to_reference(golden, name):
+    B, Cref, pts = golden[f"{name}_B"], golden[f"{name}_C"], golden["nf_points"]
+    coeff, kappa, wcs = golden[f"{name}_coeff"], golden[f"{name}_kappa"], int(golden[f"{name}_wcs"])
+    wc = B.shape[1]
+    p32 = _oracle_for(golden, 32).nearfield_kernel_tri(B, kappa, coeff, wc, wcs, pts)
+    p64 = _oracle_for(golden, 64).nearfield_kernel_tri(B, kappa, coeff, wc, wcs, pts)
+    assert relerr(p32, Cref) < 2e-6
+    assert relerr(Cref, p64) < 2e-5
+
+
+def test_oracle_nearfield_apply_is_kernel_of_avop(golden):
+    """ApplyNearFieldOperators_PL = alpha * kernel(AvOp B) + beta * C, written with ldC."""
+    o = _oracle_for(golden, 64)
+    rng = np.random.default_rng(3)
+    nv = golden["coords"].shape[0]
+    pts = golden["nf_points"]
+    coeff = np.array([[0.5, 1 - 1j, 0.25 + 2j, 3.0]] * 2)
+    kappa = np.array([2.0, 5.0])
+    B = crandn(rng, nv, 32)
+    C0 = crandn(rng, pts.shape[0], 40)
+    C = C0.copy()
+    alpha, beta = 0.5 - 2j, 1.5 + 0.25j
+    o.ApplyNearFieldOperators_PL(alpha, B, beta, C, kappa, coeff, 32, 16, pts)
+    # the same through the raw kernel on the triangle values (AvOp = area / 3 per vertex)
+    mid, nrm, area, _ = o.geometry()
+    tris = golden["tris"]
+    Btri = (area / 3.0)[:, None] * B[tris].sum(axis=1)
+    P = o.nearfield_kernel_tri(Btri, kappa, coeff, 32, 16, pts)
+    assert relerr(C[:, :32], alpha * P + beta * C0[:, :32]) < 1e-13
+    assert np.array_equal(C[:, 32:], C0[:, 32:])     # columns past wave_count untouched
+    # beta == 0 overwrites (NaNs in C do not survive)
+    Cn = np.full((pts.shape[0], 32), np.nan, np.complex128)
+    o.ApplyNearFieldOperators_PL(alpha, B, 0.0, Cn, kappa, coeff, 32, 16, pts)
+    assert relerr(Cn, alpha * P) < 1e-13
+
+
+def test_oracle_nearfield_ignores_mass_and_adjoint_layer(golden):
+    o = _oracle_for(golden, 64)
+    rng = np.random.default_rng(4)
+    nv = golden["coords"].shape[0]
+    pts = golden["nf_points"]
+    B = crandn(rng, nv, 16)
+    C = crandn(rng, pts.shape[0], 16)
+    C0 = C.copy()
+    # only mass and adjoint double layer: the reference leaves C_out untouched
+    o.ApplyNearFieldOperators_PL(1.0, B, 0.0, C, [2.0], np.array([[1.0, 0, 0, 1.0]]), 16, 16, pts)
+    assert np.array_equal(C, C0)
+    a = o.ApplyNearFieldOperators_PL(1.0, B, 0.0, np.zeros_like(C), [2.0], np.array([[0, 1.0, 2.0, 0]]), 16, 16, pts)
+    b = o.ApplyNearFieldOperators_PL(1.0, B, 0.0, np.zeros_like(C), [2.0], np.array([[5.0, 1.0, 2.0, 7.0]]), 16, 16,
+                                     pts)
+    assert np.array_equal(a, b)
+
+
+def test_oracle_nearfield_potential_known_answers(sphere3):
+    """Closed forms on the unit sphere (kappa = 0, density 1): the double-layer
+    potential is -1 inside and 0 outside (Gauss: the solid angle of the
+    surface, with z = y - x and outward normals), the single-layer potential is
+    R = 1 inside and R^2 / |x| outside.  Midpoint rule on level 3 (1280 T)."""
+    coords, tris = sphere3
+    o = O.Oracle(coords, tris, np.eye(3), precision=64)
+    nv = coords.shape[0]
+    rng = np.random.default_rng(5)
+    d = rng.standard_normal((12, 3))
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    r_in, r_out = 0.4, 2.5
+    pts = np.concatenate([d * r_in, d * r_out])
+    ones = np.ones((nv, 1), np.complex128)
+    dl = o.ApplyNearFieldOperators_PL(1.0, ones, 0.0, np.zeros((24, 1), np.complex128), [0.0],
+                                      np.array([[0, 0, 1.0, 0]]), 1, 1, pts)[:, 0]
+    sl = o.ApplyNearFieldOperators_PL(1.0, ones, 0.0, np.zeros((24, 1), np.complex128), [0.0],
+                                      np.array([[0, 1.0, 0, 0]]), 1, 1, pts)[:, 0]
+    # midpoint-rule error O(h^2): 2.9e-3 inside at level 3
+    assert np.max(np.abs(dl[:12] + 1.0)) < 5e-3
+    assert np.max(np.abs(dl[12:])) < 5e-3
+    # the flat triangles lie inside the sphere: area 0.9959 of 4 pi at level 3
+    assert np.max(np.abs(sl[:12] - 1.0)) < 1e-2
+    assert np.max(np.abs(sl[12:] - 1.0 / r_out)) < 1e-2
+
+
+@pytest.mark.skipif(not O.ref_available(), reason="oracle/_ref not built here")
+def test_oracle_nearfield_vs_live_reference_kernel(sphere3):
+    coords, tris = sphere3
+    rng = np.random.default_rng(8)
+    o = O.Oracle(coords, tris, np.eye(3), precision=32)
+    mid, nrm, _, _ = o.geometry()
+    B = crandn(rng, tris.shape[0], 32, dtype=np.complex64)
+    pts = rng.uniform(-2.0, 2.0, (200, 3))
+    kappa = np.array([6.0, 11.0])
+    coeff = np.array([[0, 0.3 - 1j, 2.0 + 0.5j, -1.0j]] * 2)
+    Cref = O.ref_nearfield(mid, nrm, B, pts, kappa, O.scaled_coefficients(coeff), 16)
+    assert relerr(o.nearfield_kernel_tri(B, kappa, coeff, 32, 16, pts), Cref) < 3e-6
+
+
 @pytest.mark.skipif(not O.ref_available(), reason="oracle/_ref not built here")
 def test_oracle_vs_live_reference_kernel(sphere3):
     coords, tris = sphere3
