@@ -231,6 +231,32 @@ def whole_job_rate(world: int, interactions_per_step: int, steps: int, total_ms:
     return world * interactions_per_step * steps / (total_ms * 1e-3) / 1e9
 
 
+def roofline_model(n_targets, n_sources, n_k, inter, mode, peaks, clk_mhz, n_sm, kernel_ms):
+    """Roofline model of one dense launch (algorithmic work per launch):
+    W = 8 I contraction FLOPs, G = N_t N_s n_k kernel evaluations (2 MUFU sincos
+    + 20 FP32 FLOPs each) and N_t N_s rsqrt;
+    plain form T* = (W + 20 G) / P_fp32,
+    tensor-core form T* = max(W / P_tf32, (2 G + N_t N_s) / P_mufu, 20 G / P_fp32)."""
+    G = float(n_targets) * n_sources * n_k
+    f_hz = (clk_mhz or 1965.0) * 1e6
+    p_fp32 = n_sm * 128 * 2 * f_hz               # FFMA: 128 lanes/SM/clk
+    p_mufu = n_sm * 16 * f_hz                    # MUFU: 16 lanes/SM/clk
+    p_tf32 = peaks["bf16_tflops"] * 1e12 / 2.0   # dense TF32 = half the measured dense BF16 rate
+    terms = {"tensor_tf32_ms": 8.0 * inter / p_tf32 * 1e3,
+             "mufu_ms": (2 * G + float(n_targets) * n_sources) / p_mufu * 1e3,
+             "fp32_ms": 20.0 * G / p_fp32 * 1e3}
+    if mode == "tc":
+        t_star = max(terms.values())
+        limiter = max(terms, key=terms.get)
+    else:
+        t_star = (8.0 * inter + 20.0 * G) / p_fp32 * 1e3
+        limiter = "fp32_ms"
+    return {"T_star_ms": t_star, "limiter": limiter, "terms_ms": terms, "frac": t_star / kernel_ms,
+            "clock_mhz": clk_mhz or 1965.0,
+            "peaks": "P_fp32 = SMs x 256 FLOP/clk, P_mufu = SMs x 16/clk at the sampled SM clock; "
+                     "P_tf32 = measured dense BF16 / 2"}
+
+
 # ---------------------------------------------------------------------------
 # the CUDA arm
 # ---------------------------------------------------------------------------
@@ -348,34 +374,10 @@ def run_gpu_arm(args, rank, world, local_rank):
     cpu = None
     if world == 1 and not args.no_cpu_baseline:
         cpu = reference_rows_rate(coords, tris, B, target_seconds=float(os.environ.get("BAEMM_REF_SECONDS", "12")))
-    # Roofline model of the apply (algorithmic work per launch):
-    #   W = 8 I contraction FLOPs, G = N_t N_s n_k kernel evaluations (2 MUFU sincos
-    #   + 20 FP32 FLOPs each) and N_t N_s rsqrt;
-    #   plain form T* = (W + 20 G) / P_fp32,
-    #   tensor-core form T* = max(W / P_tf32, (2 G + N_t N_s) / P_mufu, 20 G / P_fp32).
-    n_k = len(KAPPA)
-    G = float(nt) * nt * n_k
-    clk_mhz = None
     cs = clk.summary()
-    if cs.get("sm_mhz"):
-        clk_mhz = cs["sm_mhz"]
-    f_hz = (clk_mhz or 1965.0) * 1e6
+    clk_mhz = cs.get("sm_mhz") or None
     n_sm = torch.cuda.get_device_properties(torch.cuda.current_device()).multi_processor_count
-    p_fp32 = n_sm * 128 * 2 * f_hz               # FFMA: 128 lanes/SM/clk
-    p_mufu = n_sm * 16 * f_hz                    # MUFU: 16 lanes/SM/clk
-    p_tf32 = peaks["bf16_tflops"] * 1e12 / 2.0   # dense TF32 = half the measured dense BF16 rate
-    terms = {"tensor_tf32_ms": 8.0 * inter / p_tf32 * 1e3, "mufu_ms": (2 * G + float(nt) * nt) / p_mufu * 1e3,
-             "fp32_ms": 20.0 * G / p_fp32 * 1e3}
-    if args.mode == "tc":
-        t_star = max(terms.values())
-        limiter = max(terms, key=terms.get)
-    else:
-        t_star = (8.0 * inter + 20.0 * G) / p_fp32 * 1e3
-        limiter = "fp32_ms"
-    model = {"T_star_ms": t_star, "limiter": limiter, "terms_ms": terms, "frac": t_star / dense_avg,
-             "clock_mhz": clk_mhz or 1965.0,
-             "peaks": "P_fp32 = SMs x 256 FLOP/clk, P_mufu = SMs x 16/clk at the sampled SM clock; "
-                      "P_tf32 = measured dense BF16 / 2"}
+    model = roofline_model(nt, nt, len(KAPPA), inter, args.mode, peaks, clk_mhz, n_sm, dense_avg)
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
@@ -400,6 +402,144 @@ def run_gpu_arm(args, rank, world, local_rank):
     if cpu is not None:
         line["cpu_baseline"] = {"value": cpu["value"], "unit": UNIT, "cores": cpu["cores"], "kind": cpu["kind"],
                                 "sample": cpu["sample"]}
+    print(json.dumps(line), flush=True)
+    H.close()
+    return 0
+
+
+# ---------------------------------------------------------------------------
+# the near-field workload (--workload nearfield): not the headline line
+# ---------------------------------------------------------------------------
+NF_WORKLOAD = ("torus R1.0 r0.4 160x480 grid (76800 V, 153600 T), 64 RHS = kappa {2,4,8,16} x 16, SL+DL potential "
+               "(ApplyNearFieldOperators_PL) at 153600 seeded points in [-1.6,1.6]^2 x [-0.6,0.6], at least 0.05 "
+               "from the surface")
+
+
+def nearfield_points(small=False):
+    """Seeded evaluation points around the torus (small: 38400, with the small torus)."""
+    from baemm_b200 import meshes
+    return meshes.points_off_torus(38400 if small else 153600, seed=0)
+
+
+def reference_nearfield_rate(coords, tris, B_vertex, pts, target_seconds=10.0, threads=0):
+    """GInteractions/s of the reference NearFieldOperatorKernel.cl (compiled as
+    C++, oracle/_ref) on a contiguous block of points against all sources
+    (cost is separable per point)."""
+    from oracle import oracle as O
+    if not O.ref_available():
+        return None
+    orc = O.Oracle(coords, tris, np.eye(3), precision=32, threads=threads)
+    mid, nrm, area, _ = orc.geometry()
+    n = tris.shape[0]
+    Btri = ((area / 3.0)[:, None] * B_vertex[tris].sum(axis=1)).astype(np.complex64)
+    cs = O.scaled_coefficients(coefficients(KAPPA))
+    nthreads = threads or O.reflib().refcl_max_threads()
+    rows = max(nthreads, 8)
+    t0 = time.perf_counter()
+    O.ref_nearfield(mid, nrm, Btri, pts[:rows], KAPPA, cs, WCS, threads=threads)
+    dt = time.perf_counter() - t0
+    rows2 = int(min(pts.shape[0] - rows, max(rows, rows * target_seconds / max(dt, 1e-3))))
+    t0 = time.perf_counter()
+    O.ref_nearfield(mid, nrm, Btri, pts[rows:rows + rows2], KAPPA, cs, WCS, threads=threads)
+    dt = time.perf_counter() - t0
+    return {"value": rows2 * n * WC / dt / 1e9, "unit": UNIT, "cores": int(nthreads), "kind": "reference",
+            "sample": f"reference NearFieldOperatorKernel.cl (oracle/_ref, compiled as C++) on {rows2} points x "
+                      f"all {n} sources x 64 RHS, OpenMP over points; scaled per interaction"}
+
+
+def run_nearfield_workload(args):
+    """ApplyNearFieldOperators_PL (ApplyNearFieldOperators.hpp:56-122) on the
+    torus: device-resident blocks, CUDA-event times over `steps` evaluations
+    after `warmup` (L2 flushed before each), for the tensor-core, plain FP32
+    and FP64 arithmetic; errors against the FP64 evaluation; the end-to-end
+    rate through the host-pointer C ABI; the reference kernel on the host."""
+    import torch
+    from baemm_b200 import APPLY_FP32, APPLY_FP64, APPLY_TC, Helmholtz_CUDA
+    coords, tris, B = build_workload(seed=0, small=args.small)
+    pts = nearfield_points(args.small)
+    nt, m = tris.shape[0], pts.shape[0]
+    inter = m * nt * WC
+    H = Helmholtz_CUDA(coords, tris, np.eye(3))
+    H.LoadParameters(KAPPA, coefficients(KAPPA), WC, WCS)
+    stream = torch.cuda.Stream()
+    H.SetStream(stream.cuda_stream)
+    H.SetProfiling(True)
+    Bd = torch.from_numpy(B).cuda()
+    Pd = torch.from_numpy(pts).cuda()
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+
+    def timed(mode, steps, warmup):
+        H.SetApplyMode(mode)
+        Bm = Bd.to(torch.complex128) if mode == APPLY_FP64 else Bd
+        Cd = torch.zeros((m, WC), dtype=Bm.dtype, device="cuda")
+        with torch.cuda.stream(stream):
+            for _ in range(warmup):
+                flush.fill_(1.0)
+                H.ApplyNearFieldOperators_PL(1.0, Bm, 0.0, Cd, Pd)
+        torch.cuda.synchronize()
+        evs, kern = [], []
+        with torch.cuda.stream(stream):
+            for k in range(steps):
+                flush.fill_(float(k))
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                H.ApplyNearFieldOperators_PL(1.0, Bm, 0.0, Cd, Pd)
+                e1.record(stream)
+                evs.append((e0, e1))
+                kern.append(H.LastApplyTimes()[1])
+        torch.cuda.synchronize()
+        return (Cd.cpu().numpy().astype(np.complex128), float(np.mean([a.elapsed_time(b) for a, b in evs])),
+                float(np.mean(kern)))
+
+    launches0 = H.KernelLaunchCount()
+    with ClockSampler(torch.cuda.current_device()) as clk:
+        C_tc, ms_tc, k_tc = timed(APPLY_TC, args.steps, args.warmup)
+    launches = H.KernelLaunchCount() - launches0
+    C_32, ms_32, k_32 = timed(APPLY_FP32, 2, 1)
+    C_64, ms_64, k_64 = timed(APPLY_FP64, 1, 1)
+    nref = float(np.linalg.norm(C_64))
+    err = lambda C: float(np.linalg.norm(C - C_64) / nref)
+    # end to end through the host-pointer C ABI (pinned host blocks, copies inside)
+    H.SetStream(None)
+    H.SetApplyMode(APPLY_TC)
+    Bh = torch.from_numpy(B).pin_memory().numpy()
+    Ch = torch.zeros((m, WC), dtype=torch.complex64).pin_memory().numpy()
+    P32 = pts.astype(np.float32)
+    H.ApplyNearFieldOperators_PL(1.0, Bh, 0.0, Ch, P32)
+    e2e = []
+    for k in range(args.steps):
+        flush.fill_(float(k))
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        H.ApplyNearFieldOperators_PL(1.0, Bh, 0.0, Ch, P32)
+        e2e.append((time.perf_counter() - t0) * 1e3)
+    e2e_ms = float(np.mean(e2e))
+    peaks = load_peaks()
+    cs = clk.summary()
+    n_sm = torch.cuda.get_device_properties(torch.cuda.current_device()).multi_processor_count
+    model = roofline_model(m, nt, len(KAPPA), inter, "tc", peaks, cs.get("sm_mhz") or None, n_sm, k_tc)
+    rate = lambda ms: inter / (ms * 1e-3) / 1e9
+    cpu = None
+    if not args.no_cpu_baseline:
+        cpu = reference_nearfield_rate(coords, tris, B, pts, float(os.environ.get("BAEMM_REF_SECONDS", "10")))
+    line = {"metric": "GInteractions/s per near-field evaluation", "value": rate(ms_tc), "unit": UNIT,
+            "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_tc, "higher_is_better": True,
+            "dtype": "tc", "data": "synthetic",
+            "config": {"workload": NF_WORKLOAD if not args.small else "SMALL torus 80x240, 38400 points (profiling)",
+                       "points": m, "interactions_per_step": inter, "wave_count": WC,
+                       "l2": "flushed (256 MiB write) before every timed step"},
+            "runs": {"tc": {"ms": ms_tc, "kernel_ms": k_tc, "GInteractions_per_s": rate(ms_tc),
+                            "rel_err_vs_fp64": err(C_tc)},
+                     "fp32": {"ms": ms_32, "kernel_ms": k_32, "GInteractions_per_s": rate(ms_32),
+                              "rel_err_vs_fp64": err(C_32)},
+                     "fp64": {"ms": ms_64, "kernel_ms": k_64, "GInteractions_per_s": rate(ms_64)}},
+            "speedup_tc_vs_fp32": ms_32 / ms_tc,
+            "roofline": {"kernel": "boundary_tc_kernel (targets = points)", "model": model},
+            "e2e": {"value": rate(e2e_ms), "unit": UNIT, "ms_per_step": e2e_ms,
+                    "h2d_bytes_per_step": int(B.nbytes + P32.nbytes), "d2h_bytes_per_step": int(m * WC * 8)},
+            "gpu_launches": int(launches), "clocks": cs}
+    if cpu is not None:
+        line["cpu_baseline"] = cpu
     print(json.dumps(line), flush=True)
     H.close()
     return 0
@@ -614,7 +754,7 @@ def main(argv=None):
                     help="apply arithmetic: plain FP32, compensated tensor-core (default), FP64")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-compare", action="store_true", help="skip the plain-FP32 and FP64 comparison applies")
-    ap.add_argument("--workload", default="apply", choices=["apply", "solve", "serve", "gauss-newton"],
+    ap.add_argument("--workload", default="apply", choices=["apply", "nearfield", "solve", "serve", "gauss-newton"],
                     help="apply: the headline operator-apply line; solve: the scattering-solve configuration; "
                          "serve: the request stream through the serving loop")
     ap.add_argument("--requests", type=int, default=100, help="requests of --workload serve")
@@ -629,6 +769,8 @@ def main(argv=None):
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         return run_reference_arm(args, rank, world)
+    if args.workload == "nearfield":
+        return run_nearfield_workload(args) if rank == 0 else 0
     if args.workload == "solve":
         return run_solve_workload(args) if rank == 0 else 0
     if args.workload == "serve":
