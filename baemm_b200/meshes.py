@@ -5,6 +5,9 @@ Host-side data preparation only (numpy); nothing here computes operators.
 * ``read_mesh_txt`` / ``write_mesh_txt`` follow the text format read by
   ReadMeshFromFile.hpp:3-102 (``dom_dim``, ``amb_dim``, ``vertex_count``,
   ``simplex_count`` headers, then vertex rows and 0-based simplex rows).
+* ``read_mesh_stl`` / ``write_mesh_stl`` read and write STL (ASCII or binary)
+  for ReadMeshFromSTL.hpp:5-44, with the vertex merging of the stl_reader
+  library the reference calls (restated in include/BAEMM_Meshes.hpp).
 * ``icosphere`` builds the unit sphere from an icosahedron subdivided ``level``
   times and projected to radius 1 (level 3: 642 vertices / 1280 triangles).
 * ``torus`` builds the parametric torus of the large-block apply workload.
@@ -21,6 +24,9 @@ import numpy as np
 __all__ = [
     "read_mesh_txt",
     "write_mesh_txt",
+    "read_mesh_stl",
+    "write_mesh_stl",
+    "points_off_torus",
     "icosphere",
     "torus",
     "fibonacci_sphere",
@@ -68,6 +74,67 @@ def write_mesh_txt(path: str | os.PathLike, coords: np.ndarray, simplices: np.nd
             f.write(" ".join(repr(float(x)) for x in row) + "\n")
         for row in simplices:
             f.write(" ".join(str(int(x)) for x in row) + "\n")
+
+
+def read_mesh_stl(path: str | os.PathLike):
+    """Read an STL file (ASCII or binary) as ``(coords, triangles)``, float64
+    n x 3 and int64 m x 3 (ReadMeshFromSTL.hpp:5-44).
+
+    Vertices with bit-identical float32 coordinates are merged and numbered in
+    lexicographic (x, y, z) order; triangles keep their file order.  Raises
+    ``ValueError`` on a file that is neither form (the reference prints the
+    reader's exception and returns false).
+    """
+    data = open(path, "rb").read()
+    raw = None
+    if len(data) >= 84:
+        count = int(np.frombuffer(data[80:84], dtype="<u4")[0])
+        if len(data) == 84 + 50 * count:
+            rec = np.dtype([("n", "<f4", 3), ("v", "<f4", 9), ("attr", "<u2")])
+            raw = np.frombuffer(data, dtype=rec, count=count, offset=84)["v"].reshape(-1, 3)
+    if raw is None:
+        tokens = data.decode("ascii", errors="replace").split()
+        if not tokens or tokens[0] != "solid":
+            raise ValueError(f"read_mesh_stl: {path} is neither binary STL nor ASCII STL")
+        vals = []
+        for k, t in enumerate(tokens):
+            if t == "vertex":
+                if k + 3 >= len(tokens):
+                    raise ValueError(f"read_mesh_stl: {path}: malformed vertex")
+                vals.extend(tokens[k + 1:k + 4])
+        raw = np.array(vals, dtype=np.float32).reshape(-1, 3)
+        if raw.shape[0] % 3:
+            raise ValueError(f"read_mesh_stl: {path}: vertex count is not a multiple of 3")
+    uniq, inv = np.unique(np.ascontiguousarray(raw, np.float32), axis=0, return_inverse=True)
+    return uniq.astype(np.float64), inv.reshape(-1, 3).astype(np.int64)
+
+
+def write_mesh_stl(path: str | os.PathLike, coords: np.ndarray, triangles: np.ndarray, binary: bool = True,
+                   name: str = "baemm") -> None:
+    """Write a triangle mesh as STL (float32 coordinates, facet normals from
+    the vertex order)."""
+    p = np.asarray(coords, np.float64)[np.asarray(triangles, np.int64)]
+    n = np.cross(p[:, 1] - p[:, 0], p[:, 2] - p[:, 0])
+    n /= np.maximum(np.linalg.norm(n, axis=1, keepdims=True), 1e-300)
+    if binary:
+        rec = np.dtype([("n", "<f4", 3), ("v", "<f4", 9), ("attr", "<u2")])
+        out = np.zeros(p.shape[0], dtype=rec)
+        out["n"] = n
+        out["v"] = p.reshape(-1, 9)
+        with open(path, "wb") as f:
+            f.write(name.encode("ascii")[:80].ljust(80, b" "))
+            f.write(np.array([p.shape[0]], "<u4").tobytes())
+            f.write(out.tobytes())
+        return
+    p32, n32 = p.astype(np.float32), n.astype(np.float32)
+    with open(path, "w") as f:
+        f.write(f"solid {name}\n")
+        for t in range(p.shape[0]):
+            f.write("  facet normal {:.9e} {:.9e} {:.9e}\n    outer loop\n".format(*n32[t]))
+            for q in range(3):
+                f.write("      vertex {:.9e} {:.9e} {:.9e}\n".format(*p32[t, q]))
+            f.write("    endloop\n  endfacet\n")
+        f.write(f"endsolid {name}\n")
 
 
 def icosphere(level: int):
