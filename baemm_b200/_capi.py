@@ -109,6 +109,8 @@ SIGNATURES = {
     "baemm_apply_far_field_operators_z": (I, [vp, dp, dp, I64, dp, dp, I64, dp, dp, I, I]),
     "baemm_apply_far_field_operators_loaded_z": (I, [vp, dp, dp, I64, dp, dp, I64]),
     "baemm_apply_far_field_operators_dev_z": (I, [vp, dp, vp, I64, dp, vp, I64]),
+    "baemm_apply_boundary_operators_rows_dev_z": (I, [vp, dp, vp, I64, dp, vp, I64, I64, I64, I]),
+    "baemm_apply_boundary_operators_rows_dev_c": (I, [vp, fp, vp, I64, fp, vp, I64, I64, I64, I]),
     "baemm_apply_near_field_operators_z": (I, [vp, dp, dp, I64, dp, dp, I64, dp, I64]),
     "baemm_apply_near_field_operators_c": (I, [vp, fp, fp, I64, fp, fp, I64, fp, I64]),
     "baemm_apply_near_field_operators_full_z": (I, [vp, dp, dp, I64, dp, dp, I64, dp, dp, I, I, dp, I64]),

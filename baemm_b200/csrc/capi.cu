@@ -508,6 +508,29 @@ int baemm_apply_boundary_operators_dev_c(baemm_ctx *ctx, const float alpha[2], c
 
 
 
+int baemm_apply_boundary_operators_rows_dev_z(baemm_ctx *ctx, const double alpha[2], const double *B, int64_t ldB,
+                                              const double beta[2], double *C, int64_t ldC, int64_t row_begin,
+                                              int64_t row_end, int with_mass)
+{
+    return guarded(ctx, [&](Ctx &c) {
+        c.require_loaded();
+        BAEMM_REQUIRE(B && C, BAEMM_ERR_ARG, "null block");
+        c.apply_boundary_rows<double2>(z2(alpha), reinterpret_cast<const double2 *>(B), ldB, z2(beta),
+                                       reinterpret_cast<double2 *>(C), ldC, row_begin, row_end, with_mass != 0);
+    });
+}
+int baemm_apply_boundary_operators_rows_dev_c(baemm_ctx *ctx, const float alpha[2], const float *B, int64_t ldB,
+                                              const float beta[2], float *C, int64_t ldC, int64_t row_begin,
+                                              int64_t row_end, int with_mass)
+{
+    return guarded(ctx, [&](Ctx &c) {
+        c.require_loaded();
+        BAEMM_REQUIRE(B && C, BAEMM_ERR_ARG, "null block");
+        c.apply_boundary_rows<float2>(c2(alpha), reinterpret_cast<const float2 *>(B), ldB, c2(beta),
+                                      reinterpret_cast<float2 *>(C), ldC, row_begin, row_end, with_mass != 0);
+    });
+}
+
 int baemm_apply_boundary_operators_z(baemm_ctx *ctx, const double alpha[2], const double *B, int64_t ldB,
                                      const double beta[2], double *C, int64_t ldC)
 {

@@ -324,10 +324,11 @@ void Ctx::require_loaded() const
 }
 
 template <class R>
-void Ctx::dense_apply(const cplx<R> *Btri, cplx<R> *Ctri)
+void Ctx::dense_apply(const cplx<R> *Btri, cplx<R> *Ctri, int64_t r0, int64_t r1)
 {
     if constexpr (std::is_same<R, double>::value)
-        launch_boundary_dense<double>(mesh, flags, prm_d.p, wave_count, wave_chunk_size, Btri, Ctri, stream);
+        launch_boundary_dense<double>(mesh, flags, prm_d.p, wave_count, wave_chunk_size, Btri, Ctri, stream, 2, r0,
+                                      r1);
     else if (apply_mode == BAEMM_APPLY_TC && tc_supported(wave_count, wave_chunk_size))
     {
         if (!tc_geo_ready)
@@ -337,28 +338,40 @@ void Ctx::dense_apply(const cplx<R> *Btri, cplx<R> *Ctri)
         }
         const size_t ws_elems = tc_workspace_elems(tc_ctas);
         launch_boundary_tc(mesh, flags, prm16_f.p, wave_count, wave_chunk_size, mesh.tgeo_f.p, Btri, Ctri,
-                           tc_ws.reserve(ws_elems), ws_elems, tc_err.p, stream, tc_seg_tiles, tc_ctas, tc_stagger);
+                           tc_ws.reserve(ws_elems), ws_elems, tc_err.p, stream, tc_seg_tiles, tc_ctas, tc_stagger, r0,
+                           r1);
         tc_pending = true;
     }
     else
         launch_boundary_dense<float>(mesh, flags, prm_f.p, wave_count, wave_chunk_size, Btri, Ctri, stream,
-                                     dense_variant);
+                                     dense_variant, r0, r1);
 }
 
 // ApplyBoundaryOperators.hpp:289-391 on device blocks.
 template <class Text>
 void Ctx::apply_boundary(Text alpha, const Text *B, int64_t ldB, Text beta, Text *C, int64_t ldC)
 {
+    apply_boundary_rows<Text>(alpha, B, ldB, beta, C, ldC, 0, mesh.nt, true);
+}
+
+template <class Text>
+void Ctx::apply_boundary_rows(Text alpha, const Text *B, int64_t ldB, Text beta, Text *C, int64_t ldC, int64_t r0,
+                              int64_t r1, bool with_mass)
+{
     if (wave_chunk_count < 1) return;
+    BAEMM_REQUIRE(r0 >= 0 && r0 <= r1 && r1 <= mesh.nt, BAEMM_ERR_ARG, "row range outside [0, simplex_count]");
     BAEMM_REQUIRE(ldB >= wave_count && ldC >= wave_count, BAEMM_ERR_ARG, "leading dimension smaller than wave_count");
     const bool layers = flags.any_layer();
     if (!layers && !flags.mass()) return;   // the reference leaves C_out untouched
     EpilogueArgs ea;
     ea.layers = layers;
     ea.sl_diag = layers && use_diagonal && flags.sl();
-    ea.mass = flags.mass();
+    ea.mass = flags.mass() && with_mass;
     ea.wc = wave_count;
     ea.wcs = wave_chunk_size;
+    ea.t_begin = r0;
+    ea.t_end = r1;
+    const bool rows = r1 > r0;
     const int64_t tri_elems = mesh.nt * wave_count;
     if (profiling)
     {
@@ -374,7 +387,7 @@ void Ctx::apply_boundary(Text alpha, const Text *B, int64_t ldB, Text beta, Text
         double2 *Bt = Btri_d.reserve(tri_elems), *Ct = Ctri_d.reserve(tri_elems);
         if (layers) launch_avop<Text, double>(mesh, B, ldB, wave_count, Bt, stream);
         mark(1);
-        if (layers) dense_apply<double>(Bt, Ct);
+        if (layers && rows) dense_apply<double>(Bt, Ct, r0, r1);
         mark(2);
         launch_epilogue<Text, double>(mesh, ea, Ct, Bt, prm_d.p, B, ldB, alpha, beta, C, ldC, stream);
     }
@@ -383,7 +396,7 @@ void Ctx::apply_boundary(Text alpha, const Text *B, int64_t ldB, Text beta, Text
         float2 *Bt = Btri_f.reserve(tri_elems), *Ct = Ctri_f.reserve(tri_elems);
         if (layers) launch_avop<Text, float>(mesh, B, ldB, wave_count, Bt, stream);
         mark(1);
-        if (layers) dense_apply<float>(Bt, Ct);
+        if (layers && rows) dense_apply<float>(Bt, Ct, r0, r1);
         mark(2);
         launch_epilogue<Text, float>(mesh, ea, Ct, Bt, prm_f.p, B, ldB, alpha, beta, C, ldC, stream);
     }
@@ -463,7 +476,11 @@ template void Ctx::apply_nearfield<double2>(double2, const double2 *, int64_t, d
                                             const double *, int64_t);
 template void Ctx::apply_nearfield<float2>(float2, const float2 *, int64_t, float2, float2 *, int64_t, const double *,
                                            int64_t);
-template void Ctx::dense_apply<float>(const float2 *, float2 *);
+template void Ctx::dense_apply<float>(const float2 *, float2 *, int64_t, int64_t);
+template void Ctx::apply_boundary_rows<double2>(double2, const double2 *, int64_t, double2, double2 *, int64_t,
+                                                int64_t, int64_t, bool);
+template void Ctx::apply_boundary_rows<float2>(float2, const float2 *, int64_t, float2, float2 *, int64_t, int64_t,
+                                               int64_t, bool);
 template void Ctx::apply_boundary<double2>(double2, const double2 *, int64_t, double2, double2 *, int64_t);
 template void Ctx::apply_boundary<float2>(float2, const float2 *, int64_t, float2, float2 *, int64_t);
 

@@ -94,6 +94,12 @@ public:
     // ---- operators on device blocks (async on `stream`) --------------------------
     template <class Text>
     void apply_boundary(Text alpha, const Text *B, int64_t ldB, Text beta, Text *C, int64_t ldC);
+    // One row shard of the apply: C = alpha AvOp^T|[r0,r1) (K[r0,r1) + diag) AvOp B
+    // [+ alpha c0 M B if with_mass] + beta C.  The shards of a partition of the
+    // triangles, with the mass term and beta on one of them, sum to the apply.
+    template <class Text>
+    void apply_boundary_rows(Text alpha, const Text *B, int64_t ldB, Text beta, Text *C, int64_t ldC, int64_t r0,
+                             int64_t r1, bool with_mass);
     // Far field: C (nm x wc) = alpha FF B + beta C   (ApplyFarFieldOperators.hpp:356-412)
     void apply_farfield(zc alpha, const double2 *B, int64_t ldB, zc beta, double2 *C, int64_t ldC);
     // ApplyNearFieldOperators.hpp:56-122 on device blocks: C (npts x wc) =
@@ -191,7 +197,7 @@ private:
     void init_mesh(const double *coords, int64_t nv, const int32_t *tris, int64_t nt);
     void build_topology(const int32_t *tris);
     template <class R>
-    void dense_apply(const cplx<R> *Btri, cplx<R> *Ctri);
+    void dense_apply(const cplx<R> *Btri, cplx<R> *Ctri, int64_t r0 = 0, int64_t r1 = -1);
 };
 
 } // namespace baemm

@@ -89,7 +89,7 @@ boundary_dense_kernel(DenseTargets<R> tg, const R *__restrict__ mid4, const R *_
 {
     __shared__ Tile<R, COLS> tile;
     const int i = blockIdx.x * kTargets + threadIdx.x;
-    const int iself = tg.self ? i : -1;   // the source index excluded for this target (none: -1)
+    const int iself = tg.self ? tg.off + i : -1;   // the source index excluded for this target (none: -1)
     const int col0 = blockIdx.y * COLS;
     const int ch = col0 / wcs;
     const R kap = prm[ch].kappa;
@@ -99,7 +99,11 @@ boundary_dense_kernel(DenseTargets<R> tg, const R *__restrict__ mid4, const R *_
     {
         const R *x = tg.pts4;
         x0 = x[4 * (int64_t)i]; x1 = x[4 * (int64_t)i + 1]; x2 = x[4 * (int64_t)i + 2];
-        if (ADL) { n0 = nrm4[4 * (int64_t)i]; n1 = nrm4[4 * (int64_t)i + 1]; n2 = nrm4[4 * (int64_t)i + 2]; }
+        if (ADL)
+        {
+            const int64_t gi = (int64_t)tg.off + i;   // the target's triangle (ADL: targets are midpoints)
+            n0 = nrm4[4 * gi]; n1 = nrm4[4 * gi + 1]; n2 = nrm4[4 * gi + 2];
+        }
     }
     cplx<R> acc[COLS];
     #pragma unroll
@@ -198,7 +202,7 @@ boundary_packed_kernel(DenseTargets<float> tg, const float *__restrict__ mid4, c
     for (int t = 0; t < TT; ++t)
     {
         ti[t] = blockIdx.x * (kTargets * TT) + t * kTargets + threadIdx.x;
-        tself[t] = tg.self ? ti[t] : -1;
+        tself[t] = tg.self ? tg.off + ti[t] : -1;
         x[t] = make_float3(0.f, 0.f, 0.f);
         nu[t] = make_float3(0.f, 0.f, 0.f);
         if (ti[t] < tg.m)
@@ -207,7 +211,7 @@ boundary_packed_kernel(DenseTargets<float> tg, const float *__restrict__ mid4, c
             x[t] = make_float3(m.x, m.y, m.z);
             if (ADL)
             {
-                const float4 q = reinterpret_cast<const float4 *>(nrm4)[ti[t]];
+                const float4 q = reinterpret_cast<const float4 *>(nrm4)[tg.off + ti[t]];
                 nu[t] = make_float3(q.x, q.y, q.z);
             }
         }
@@ -632,10 +636,13 @@ void dense_dispatch(const MeshDev &m, const OpFlags &f, const void *chunk_params
 
 template <class R>
 void launch_boundary_dense(const MeshDev &m, const OpFlags &f, const void *chunk_params, int wc, int wcs,
-                           const cplx<R> *Btri, cplx<R> *Ctri, cudaStream_t st, int variant)
+                           const cplx<R> *Btri, cplx<R> *Ctri, cudaStream_t st, int variant, int64_t row_begin,
+                           int64_t row_end)
 {
-    dense_dispatch<R>(m, f, chunk_params, wc, wcs, DenseTargets<R>{geo_mid<R>(m), (int)m.nt, 1}, Btri, Ctri, st,
-                      variant);
+    const int64_t r0 = std::max<int64_t>(0, row_begin), r1 = row_end < 0 ? m.nt : std::min<int64_t>(row_end, m.nt);
+    if (r1 <= r0) return;
+    dense_dispatch<R>(m, f, chunk_params, wc, wcs, DenseTargets<R>{geo_mid<R>(m) + 4 * r0, (int)(r1 - r0), 1, (int)r0},
+                      Btri, Ctri + r0 * wc, st, variant);
 }
 
 template <class R>
@@ -645,7 +652,7 @@ void launch_nearfield_dense(const MeshDev &m, const OpFlags &f, const void *chun
 {
     BAEMM_REQUIRE(!f.adl() && !f.mass(), BAEMM_ERR_ARG, "near field: single and double layer only");
     BAEMM_REQUIRE(npts <= INT32_MAX, BAEMM_ERR_SIZE, "too many evaluation points");
-    dense_dispatch<R>(m, f, chunk_params, wc, wcs, DenseTargets<R>{pts4, (int)npts, 0}, Btri, Cpts, st, variant);
+    dense_dispatch<R>(m, f, chunk_params, wc, wcs, DenseTargets<R>{pts4, (int)npts, 0, 0}, Btri, Cpts, st, variant);
 }
 
 template <class R>
@@ -736,7 +743,7 @@ void launch_incident(const MeshDev &m, const void *chunk_params, int wc, int wcs
 }
 
 template void launch_boundary_dense<float>(const MeshDev &, const OpFlags &, const void *, int, int, const float2 *,
-                                           float2 *, cudaStream_t, int);
+                                           float2 *, cudaStream_t, int, int64_t, int64_t);
 template void launch_pack_points<float>(int64_t, const double *, float *, cudaStream_t);
 template void launch_pack_points<double>(int64_t, const double *, double *, cudaStream_t);
 template void launch_nearfield_dense<float>(const MeshDev &, const OpFlags &, const void *, int, int, const float *,
@@ -744,7 +751,7 @@ template void launch_nearfield_dense<float>(const MeshDev &, const OpFlags &, co
 template void launch_nearfield_dense<double>(const MeshDev &, const OpFlags &, const void *, int, int, const double *,
                                              int64_t, const double2 *, double2 *, cudaStream_t, int);
 template void launch_boundary_dense<double>(const MeshDev &, const OpFlags &, const void *, int, int, const double2 *,
-                                            double2 *, cudaStream_t, int);
+                                            double2 *, cudaStream_t, int, int64_t, int64_t);
 template void launch_farfield<float>(const MeshDev &, const OpFlags &, const void *, int, int, const float2 *, float2 *,
                                      size_t, double2, double2, double2 *, int64_t, cudaStream_t);
 template void launch_farfield<double>(const MeshDev &, const OpFlags &, const void *, int, int, const double2 *,

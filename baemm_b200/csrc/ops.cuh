@@ -28,13 +28,16 @@ struct MeshDev
 
 // Target points of a dense launch: the triangle midpoints with the pair i == j
 // excluded (self = 1, boundary operators) or arbitrary points with no pair
-// excluded (self = 0, near field).  pts4: m x 4 reals (xyz, w unused).
+// excluded (self = 0, near field).  pts4: m x 4 reals (xyz, w unused).  With
+// self = 1 the targets may be a row range of the midpoints: target i is
+// triangle off + i (pts4 = midpoints + 4 off).
 template <class R>
 struct DenseTargets
 {
     const R *pts4;
     int m;
     int self;
+    int off;
 };
 
 // ---- mesh.cu -------------------------------------------------------------------
@@ -55,6 +58,9 @@ struct EpilogueArgs
     bool sl_diag = false;     // SL diagonal (ApplySingleLayerDiagonal.hpp:397-454)
     bool mass = false;        // add alpha * c0 * M Bin (ApplyBoundaryOperators.hpp:363-387)
     int wc = 0, wcs = 1;
+    // AvOp^T over the triangles [t_begin, t_end) only (a row shard of the
+    // apply); the other rows of Ctri are not read
+    int64_t t_begin = 0, t_end = INT64_MAX;
 };
 // C_out[v,k] = [layers] alpha * sum_{t ∋ v} a3_t (Ctri[t,k] + diag-term) + [mass] alpha c0 (M Bin)[v,k]
 //              + beta * C_out[v,k]   (beta == 0 overwrites)
@@ -98,11 +104,14 @@ void launch_axpby(int64_t rows, int cols, T a, const T *x, int64_t ldx, T b, T *
 // Dense boundary kernel (BoundaryOperatorKernel.cl:5-239): Ctri = K(kappa) Btri
 // chunk by chunk, the self pair excluded.  R = float (plain FP32) or double.
 // variant (FP32, 16-column groups): 0 scalar FMA kernel, 1 / 2 packed FP32x2
-// kernel with 1 / 2 targets per thread.
+// kernel with 1 / 2 targets per thread.  [row_begin, row_end) restricts the
+// targets to those triangles (rows of Ctri outside are not written; row_end
+// < 0: all).
 constexpr int kDenseVariants = 3;
 template <class R>
 void launch_boundary_dense(const MeshDev &m, const OpFlags &f, const void *chunk_params, int wc, int wcs,
-                           const cplx<R> *Btri, cplx<R> *Ctri, cudaStream_t st, int variant = 2);
+                           const cplx<R> *Btri, cplx<R> *Ctri, cudaStream_t st, int variant = 2,
+                           int64_t row_begin = 0, int64_t row_end = -1);
 // Near-field kernel (NearFieldOperatorKernel.cl:5-194): Cpts (npts x wc) =
 // K(kappa) Btri at the points pts4 (npts x 4 reals), single and double layer
 // (c1, c2) only, no pair excluded.  Same kernels and variants as the boundary form.
@@ -121,7 +130,8 @@ bool tc_supported(int wc, int wcs);
 // added to FP32 registers (bounds the tensor-core accumulation chain).
 void launch_boundary_tc(const MeshDev &m, const OpFlags &f, const void *chunk_params, int wc, int wcs,
                         const float *tgeo, const float2 *Btri, float2 *Ctri, float2 *ws, size_t ws_elems, int *err,
-                        cudaStream_t st, int seg_tiles = 16, int ctas = 0, int stagger = 0);
+                        cudaStream_t st, int seg_tiles = 16, int ctas = 0, int stagger = 0, int64_t row_begin = 0,
+                        int64_t row_end = -1);
 // The tensor-core form of the near field: targets pts4 (npts x 4 floats), no
 // pair excluded, flags without the adjoint double layer.
 void launch_nearfield_tc(const MeshDev &m, const OpFlags &f, const void *chunk_params, int wc, int wcs,

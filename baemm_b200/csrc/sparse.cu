@@ -59,7 +59,7 @@ __global__ void epilogue_kernel(int64_t nv, int wc, int wcs, bool layers, bool s
                                 const int32_t *__restrict__ m_outer, const int32_t *__restrict__ m_inner,
                                 const R *__restrict__ m_val,
                                 const Text *__restrict__ Bin, int64_t ldB, double2 alpha, double2 beta,
-                                Text *__restrict__ Cout, int64_t ldC)
+                                Text *__restrict__ Cout, int64_t ldC, int64_t t_begin, int64_t t_end)
 {
     const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (idx >= nv * wc) return;
@@ -80,6 +80,7 @@ __global__ void epilogue_kernel(int64_t nv, int wc, int wcs, bool layers, bool s
         for (int32_t e = avt_outer[v]; e < avt_outer[v + 1]; ++e)
         {
             const int64_t t = avt_inner[e];
+            if (t < t_begin || t >= t_end) continue;   // a row shard: triangles of other shards
             cplx<R> ct = Ctri[t * wc + k];
             if (sl_diag)
             {
@@ -321,7 +322,7 @@ void launch_epilogue(const MeshDev &m, const EpilogueArgs &a, const cplx<R> *Ctr
     epilogue_kernel<Text, R><<<grid_for(n), kT, 0, st>>>(
         m.nv, a.wc, a.wcs, a.layers, a.sl_diag, a.mass, m.avt_outer, m.avt_inner, a3, diag, Ctri, Btri,
         static_cast<const typename PrmOf<R>::type *>(chunk_params), m.mass_outer, m.mass_inner, mv, Bin, ldB, al, be,
-        Cout, ldC);
+        Cout, ldC, a.t_begin, a.t_end);
     BAEMM_LAUNCH_CHECK();
 }
 

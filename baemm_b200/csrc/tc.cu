@@ -350,7 +350,8 @@ struct TcPlan
 {
     int n, wc, nblk, ntiles, ncg, seg_tiles;
     int m;             // targets (rows of C): n for the boundary operators, the point count for the near field
-    int self;          // 1: target i is source i and the pair is excluded (boundary); 0: no pair excluded
+    int self;          // 1: target i is source off + i and the pair is excluded (boundary); 0: no pair excluded
+    int off;           // with self: the triangle of target 0 (a row shard of the boundary apply)
     int ctas;          // grid size
     int full_waves;    // whole blocks per CTA before the tail
     int tail_blocks;   // ncg * nblk - full_waves * ctas
@@ -528,7 +529,7 @@ boundary_tc_kernel(const float *__restrict__ mid4, const float *__restrict__ nrm
         while (ok && it.next(plan, cg, blk, tb, te, slot, rot))
         {
             const int i = blk * TC_M + row;
-            const int iself = plan.self ? i : -1;   // the source excluded for this target (none: -1)
+            const int iself = plan.self ? plan.off + i : -1;   // the source excluded for this target (none: -1)
             // -x_i and nu_i as broadcast pairs
             float2 nx0 = make_float2(0.f, 0.f), nx1 = nx0, nx2 = nx0, tn0 = nx0, tn1 = nx0, tn2 = nx0;
             if (i < mt)
@@ -559,7 +560,8 @@ boundary_tc_kernel(const float *__restrict__ mid4, const float *__restrict__ nrm
                     const TcTileGeo &G = sm.raw[rs].geo;
                     // tiles that hold the target itself or padding past the end need masks
                     const bool special = (ts == ntiles - 1) ||
-                                         (plan.self && ts * TC_SRC < blk * TC_M + TC_M && ts * TC_SRC + TC_SRC > blk * TC_M);
+                                         (plan.self && ts * TC_SRC < plan.off + blk * TC_M + TC_M &&
+                                          ts * TC_SRC + TC_SRC > plan.off + blk * TC_M);
                     #pragma unroll
                     for (int p = 0; p < TC_PPT; ++p)
                     {
@@ -1016,10 +1018,10 @@ void launch_tc_tile_geometry(const MeshDev &m, float *tgeo, cudaStream_t st)
 namespace
 {
 // One launch of the tensor-core form over the targets (pts4, m_targets) and all
-// nt sources of the mesh; self = 1 excludes the pair i == j (targets are the
-// midpoints).
+// nt sources of the mesh; self = 1: the targets are the midpoints of triangles
+// off .. off + m_targets - 1 and the pair i == j is excluded.
 void tc_run(const MeshDev &m, const OpFlags &f, const void *chunk_params, int wc, int wcs, const float *tgeo,
-            const float *pts4, int64_t m_targets, int self, const float2 *Btri, float2 *Ctri, float2 *ws,
+            const float *pts4, int64_t m_targets, int self, int64_t off, const float2 *Btri, float2 *Ctri, float2 *ws,
             size_t ws_elems, int *err, cudaStream_t st, int seg_tiles, int ctas, int stagger)
 {
     BAEMM_REQUIRE(tc_supported(wc, wcs), BAEMM_ERR_SIZE,
@@ -1030,6 +1032,7 @@ void tc_run(const MeshDev &m, const OpFlags &f, const void *chunk_params, int wc
     plan.n = (int)m.nt;
     plan.m = (int)m_targets;
     plan.self = self;
+    plan.off = (int)off;
     plan.wc = wc;
     const int CH = (wc % 64 == 0) ? 4 : (wc % 32 == 0) ? 2 : 1;
     plan.ncg = wc / (16 * CH);
@@ -1046,7 +1049,7 @@ void tc_run(const MeshDev &m, const OpFlags &f, const void *chunk_params, int wc
     BAEMM_REQUIRE(ws && ws_elems >= tc_workspace_elems(plan.ctas), BAEMM_ERR_ARG, "tensor-core workspace too small");
     const int code = (f.sl() ? 1 : 0) | (f.dl() ? 2 : 0) | (f.adl() ? 4 : 0);
     const auto *p = static_cast<const ChunkParamsF *>(chunk_params);
-    const float *nrm = m.nrm_f;   // target normals: read only with the adjoint double layer (targets = midpoints)
+    const float *nrm = m.nrm_f + 4 * off;   // target normals: read only with the adjoint double layer (targets = midpoints)
     const auto *tg = reinterpret_cast<const TcTileGeo *>(tgeo);
     BAEMM_REQUIRE(tg, BAEMM_ERR_ARG, "tensor-core tile geometry missing");
     // the real / imaginary coefficient structure of the BIE solves (see boundary_tc_kernel)
@@ -1074,10 +1077,12 @@ void tc_run(const MeshDev &m, const OpFlags &f, const void *chunk_params, int wc
 
 void launch_boundary_tc(const MeshDev &m, const OpFlags &f, const void *chunk_params, int wc, int wcs,
                         const float *tgeo, const float2 *Btri, float2 *Ctri, float2 *ws, size_t ws_elems, int *err,
-                        cudaStream_t st, int seg_tiles, int ctas, int stagger)
+                        cudaStream_t st, int seg_tiles, int ctas, int stagger, int64_t row_begin, int64_t row_end)
 {
-    tc_run(m, f, chunk_params, wc, wcs, tgeo, m.mid_f, m.nt, 1, Btri, Ctri, ws, ws_elems, err, st, seg_tiles, ctas,
-           stagger);
+    const int64_t r0 = std::max<int64_t>(0, row_begin), r1 = row_end < 0 ? m.nt : std::min<int64_t>(row_end, m.nt);
+    if (r1 <= r0) return;
+    tc_run(m, f, chunk_params, wc, wcs, tgeo, m.mid_f + 4 * r0, r1 - r0, 1, r0, Btri, Ctri + r0 * wc, ws, ws_elems,
+           err, st, seg_tiles, ctas, stagger);
 }
 
 void launch_nearfield_tc(const MeshDev &m, const OpFlags &f, const void *chunk_params, int wc, int wcs,
@@ -1085,7 +1090,7 @@ void launch_nearfield_tc(const MeshDev &m, const OpFlags &f, const void *chunk_p
                          float2 *ws, size_t ws_elems, int *err, cudaStream_t st, int seg_tiles, int ctas, int stagger)
 {
     BAEMM_REQUIRE(!f.adl() && !f.mass(), BAEMM_ERR_ARG, "near field: single and double layer only");
-    tc_run(m, f, chunk_params, wc, wcs, tgeo, pts4, npts, 0, Btri, Cpts, ws, ws_elems, err, st, seg_tiles, ctas,
+    tc_run(m, f, chunk_params, wc, wcs, tgeo, pts4, npts, 0, 0, Btri, Cpts, ws, ws_elems, err, st, seg_tiles, ctas,
            stagger);
 }
 

@@ -371,6 +371,26 @@ class Helmholtz_CUDA:
                 _dp(C_out.view(np.float64)), C_out.shape[1]))
         return C_out
 
+    def ApplyBoundaryOperatorsRows(self, alpha, B_in, beta, C_out, row_begin, row_end, with_mass=True):
+        """One row shard of the loaded apply on torch CUDA tensors (no reference
+        counterpart): C_out = alpha AvOp^T|rows (K[rows, :] + diag) AvOp B_in
+        [+ alpha c0 M B_in if with_mass] + beta C_out, rows = triangles
+        [row_begin, row_end).  See baemm_b200.sharded for the multi-GPU apply."""
+        import torch
+        if not _is_torch_cuda(B_in):
+            raise TypeError("ApplyBoundaryOperatorsRows takes torch CUDA tensors")
+        if B_in.dtype == torch.complex128:
+            fn, cs, ptr = self._lib.baemm_apply_boundary_operators_rows_dev_z, _cz, _dp
+        elif B_in.dtype == torch.complex64:
+            fn, cs, ptr = self._lib.baemm_apply_boundary_operators_rows_dev_c, _cc, _fp
+        else:
+            raise TypeError("B_in must be complex64 or complex128")
+        with self._on_torch_stream(B_in):
+            self._ck(fn(self._h, ptr(cs(alpha)), C.c_void_p(B_in.data_ptr()), B_in.stride(0), ptr(cs(beta)),
+                        C.c_void_p(C_out.data_ptr()), C_out.stride(0), int(row_begin), int(row_end),
+                        1 if with_mass else 0))
+        return C_out
+
     def ApplyNearFieldOperators_PL(self, alpha, B_in, beta, C_out, *args):
         """C_out (points x wc) = alpha (c1 SL + c2 DL)(points) AvOp B_in + beta C_out
         (ApplyNearFieldOperators.hpp:27-122), the boundary potential at points

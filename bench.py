@@ -19,12 +19,14 @@ singular SL diagonal.  Interactions per apply I = N_t * N_s * wave_count.
          (baemm_apply_boundary_operators_c) from pinned host memory,
          host->device and device->host copies inside the timed region
 
-  python bench.py [--gpus N] [--steps K] [--warmup W] [--mode tc|fp32|fp64]
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--mode tc|fp32|fp64] [--shard]
   python bench.py --impl reference ...   # the reference's own kernel on the host cores
 
 Multi-GPU (torchrun, one process per GPU): independent replicas of the same
 workload per rank (the operator apply does not exchange data); value = all
-ranks' interactions / the max over ranks of the timed device time.
+ranks' interactions / the max over ranks of the timed device time.  --shard:
+one apply per step split by target rows over the ranks, shards summed by an
+NCCL all-reduce (strong scaling).
 """
 from __future__ import annotations
 
@@ -282,9 +284,18 @@ def run_gpu_arm(args, rank, world, local_rank):
     Cd = torch.zeros_like(Bd)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
     H.LoadBoundaryOperators_PL(kap, coeff, WC, WCS)
+    S = None
+    if args.shard:
+        # one apply split by target rows over the ranks, shards summed by an all-reduce
+        from baemm_b200.sharded import ShardedBoundaryApply
+        S = ShardedBoundaryApply(H)
+    inter_kernel = (S.r1 - S.r0) * nt * WC if S is not None else inter   # this rank's dense-kernel interactions
 
     def step():
-        H.ApplyBoundaryOperators_PL(1.0, Bd, 0.0, Cd)
+        if S is not None:
+            S(1.0, Bd, 0.0, Cd)
+        else:
+            H.ApplyBoundaryOperators_PL(1.0, Bd, 0.0, Cd)
 
     with torch.cuda.stream(stream):
         for _ in range(args.warmup):
@@ -309,14 +320,26 @@ def run_gpu_arm(args, rank, world, local_rank):
     launches = H.KernelLaunchCount() - launches0 - 0  # library kernels only (flush is torch's)
     step_ms = [a.elapsed_time(b) for a, b in ev]
     total_ms = max_over_ranks(float(np.sum(step_ms)), dist, "cuda")
-    value = whole_job_rate(world, inter, args.steps, total_ms)
+    jobs = 1 if S is not None else world   # sharded: one apply per step for the whole job; replicas: one per rank
+    value = whole_job_rate(jobs, inter, args.steps, total_ms)
 
     # ---- e2e through the host-pointer C ABI (pinned host buffers) -----------------
-    Bh = torch.from_numpy(B).pin_memory().numpy()
-    Ch = torch.zeros(B.shape, dtype=torch.complex64).pin_memory().numpy()
+    Bp = torch.from_numpy(B).pin_memory()
+    Cp = torch.zeros(B.shape, dtype=torch.complex64).pin_memory()
+    Bh, Ch = Bp.numpy(), Cp.numpy()
     H.SetStream(None)
+
+    def e2e_step():
+        if S is not None:   # host blocks through the sharded apply (copies on torch's stream)
+            Bd.copy_(Bp, non_blocking=True)
+            S(1.0, Bd, 0.0, Cd)
+            Cp.copy_(Cd, non_blocking=True)
+            torch.cuda.synchronize()
+        else:
+            H.ApplyBoundaryOperators_PL(1.0, Bh, 0.0, Ch)   # H2D, apply, D2H, synchronised
+
     for _ in range(max(1, args.warmup // 2)):
-        H.ApplyBoundaryOperators_PL(1.0, Bh, 0.0, Ch)
+        e2e_step()
     torch.cuda.synchronize()
     if dist:
         dist.barrier()
@@ -325,13 +348,13 @@ def run_gpu_arm(args, rank, world, local_rank):
         flush.fill_(float(k))
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        H.ApplyBoundaryOperators_PL(1.0, Bh, 0.0, Ch)   # H2D, apply, D2H, synchronised
+        e2e_step()
         e2e_ms.append((time.perf_counter() - t0) * 1e3)
     e2e_total = max_over_ranks(float(np.sum(e2e_ms)), dist, "cuda")
-    e2e_value = whole_job_rate(world, inter, args.steps, e2e_total)
+    e2e_value = whole_job_rate(jobs, inter, args.steps, e2e_total)
     # ---- plain FP32 form and accuracy against the FP64 apply (rank 0, untimed for value) ----
     compare = None
-    if rank == 0 and not args.no_compare:
+    if rank == 0 and not args.no_compare and S is None:
         H.SetStream(stream.cuda_stream)
         with torch.cuda.stream(stream):
             C_mode = Cd.clone()
@@ -367,7 +390,7 @@ def run_gpu_arm(args, rank, world, local_rank):
         return 0
     peaks = load_peaks()
     dense_avg = float(np.mean(dense_ms))
-    flops = 8.0 * inter
+    flops = 8.0 * inter_kernel
     achieved = flops / (dense_avg * 1e-3) / 1e12
     traffic = load_traffic(args.mode)
     kernel_name = {"tc": "boundary_tc_kernel", "fp32": "boundary_dense_kernel", "fp64": "boundary_dense_kernel<double>"}[args.mode]
@@ -377,20 +400,24 @@ def run_gpu_arm(args, rank, world, local_rank):
     cs = clk.summary()
     clk_mhz = cs.get("sm_mhz") or None
     n_sm = torch.cuda.get_device_properties(torch.cuda.current_device()).multi_processor_count
-    model = roofline_model(nt, nt, len(KAPPA), inter, args.mode, peaks, clk_mhz, n_sm, dense_avg)
+    n_tgt = (S.r1 - S.r0) if S is not None else nt
+    model = roofline_model(n_tgt, nt, len(KAPPA), inter_kernel, args.mode, peaks, clk_mhz, n_sm, dense_avg)
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": args.mode, "data": "synthetic",
+        "scaling": "strong" if S is not None else "weak", "vs_baseline": None, "dtype": args.mode,
+        "data": "synthetic",
         "config": {"workload": WORKLOAD if not args.small else "SMALL torus 80x240 (profiling only)", "interactions_per_step": inter, "wave_count": WC,
                    "wave_chunk_size": WCS, "kappa": KAPPA.tolist(), "apply_mode": args.mode,
-                   "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+                   "parallelism": (f"target rows x{world} + all-reduce" if S is not None else
+                                   f"replicas x{world}" if world > 1 else "single GPU"),
                    "l2": "flushed (256 MiB write) before every timed step",
                    "phase_ms_last": list(H.LastApplyTimes()) if False else None},
         "roofline": {"bound": "tensor", "kernel": kernel_name, "achieved": achieved,
                      "peak": peaks["bf16_tflops"], "unit": "TFLOP/s", "frac": achieved / peaks["bf16_tflops"],
                      "peak_source": peaks["source"] + " (dense bf16 burst)",
-                     "algorithmic": "8 * N_t * N_s * wave_count FLOPs per launch (complex MACs), counted once",
+                     "algorithmic": "8 * N_t * N_s * wave_count FLOPs per launch (complex MACs), counted once; "
+                                    "N_t = this rank's target rows",
                      "dense_kernel_ms": dense_avg, "traffic": traffic, "model": model},
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(B.nbytes),
                 "d2h_bytes_per_step": int(B.nbytes), "ms_per_step": e2e_total / args.steps},
@@ -763,6 +790,8 @@ def main(argv=None):
     ap.add_argument("--gn-level", type=int, default=5, help="icosphere level of --workload gauss-newton")
     ap.add_argument("--solve-level", type=int, default=6, help="icosphere level of --workload solve")
     ap.add_argument("--small", action="store_true", help="38400-triangle torus (profiling captures only)")
+    ap.add_argument("--shard", action="store_true",
+                    help="split each apply by target rows over the ranks (strong scaling; default: replicas)")
     args = ap.parse_args(argv)
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))

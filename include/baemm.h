@@ -254,6 +254,22 @@ int baemm_apply_far_field_operators_loaded_z(baemm_ctx *ctx, const double alpha[
 int baemm_apply_far_field_operators_dev_z(baemm_ctx *ctx, const double alpha[2], const double *B_in, int64_t ldB,
                                           const double beta[2], double *C_out, int64_t ldC);
 
+/* One row shard of ApplyBoundaryOperators_PL for an apply split by target
+ * triangles over several GPUs (no reference counterpart; the reference runs on
+ * one device).  On device blocks:
+ *   C_out = alpha * AvOp^T|rows (K[rows, :] + SL diagonal) AvOp B_in
+ *           [+ alpha * c0 * Mass B_in  if with_mass]  + beta * C_out,
+ * rows = triangles [row_begin, row_end), every source included.  For a
+ * partition of [0, simplex_count) into shards, with with_mass and beta on one
+ * shard only (beta = 0 on the others), the shards' C_out sum to the full apply;
+ * one all-reduce of the vertex block combines them (baemm_b200.sharded). */
+int baemm_apply_boundary_operators_rows_dev_z(baemm_ctx *ctx, const double alpha[2], const double *B_in, int64_t ldB,
+                                              const double beta[2], double *C_out, int64_t ldC, int64_t row_begin,
+                                              int64_t row_end, int with_mass);
+int baemm_apply_boundary_operators_rows_dev_c(baemm_ctx *ctx, const float alpha[2], const float *B_in, int64_t ldB,
+                                              const float beta[2], float *C_out, int64_t ldC, int64_t row_begin,
+                                              int64_t row_end, int with_mass);
+
 /* ApplyNearFieldOperators_PL (ApplyNearFieldOperators.hpp:56-122, kernel
  * NearFieldOperatorKernel.cl:5-194): the boundary potential of the vertex
  * values B_in (vertex_count x wave_count) at evaluation points,
