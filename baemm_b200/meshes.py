@@ -16,6 +16,7 @@ Host-side data preparation only (numpy); nothing here computes operators.
 """
 from __future__ import annotations
 
+import functools
 import math
 import os
 
@@ -138,6 +139,20 @@ def write_mesh_stl(path: str | os.PathLike, coords: np.ndarray, triangles: np.nd
 
 
 def icosphere(level: int):
+    """Unit icosphere: an icosahedron subdivided ``level`` times, projected to
+    radius 1 and oriented outward; float64 coordinates and int64 triangles
+    (level 3: 642 vertices / 1280 triangles).  The subdivision is cached per
+    level; the arrays returned are fresh copies."""
+    coords, tris = _icosphere_cached(int(level))
+    return coords.copy(), tris.copy()
+
+
+@functools.lru_cache(maxsize=8)
+def _icosphere_cached(level: int):
+    return _icosphere_build(level)
+
+
+def _icosphere_build(level: int):
     """Unit icosphere: icosahedron, ``level`` midpoint subdivisions, projected.
 
     Outward-oriented triangles.  V = 10*4^level + 2, T = 20*4^level.
