@@ -96,6 +96,7 @@ SIGNATURES = {
     "baemm_get_triangle_midpoints": (I, [vp, fp]),
     "baemm_get_single_layer_diagonal": (I, [vp, fp]),
     "baemm_get_mass_matrix": (I, [vp, i64p, i32p, fp, i64p]),
+    "baemm_get_curl_operator": (I, [vp, i64p, i32p, fp, i64p]),
     "baemm_last_solve_stats": (I, [vp, C.POINTER(SolveStats)]),
     "baemm_load_parameters": (I, [vp, dp, dp, I, I, D]),
     "baemm_load_boundary_operators": (I, [vp, dp, dp, I, I]),

@@ -456,6 +456,22 @@ int baemm_get_mass_matrix(baemm_ctx *ctx, int64_t *outer, int32_t *inner, float 
         }
     });
 }
+int baemm_get_curl_operator(baemm_ctx *ctx, int64_t *outer, int32_t *inner, float *values, int64_t *nnz)
+{
+    return guarded(ctx, [&](Ctx &c) {
+        const int64_t nt = c.mesh.nt, z = 9 * nt;
+        if (nnz) *nnz = z;
+        if (!outer) return;
+        for (int64_t r = 0; r <= 3 * nt; ++r) outer[r] = 3 * r;
+        if (!inner && !values) return;
+        DevBuf<int32_t> di;
+        DevBuf<float> dv;
+        launch_curl(c.mesh, di.reserve(z), dv.reserve(z), c.stream);
+        if (inner) BAEMM_CUDA(cudaMemcpyAsync(inner, di.p, z * sizeof(int32_t), cudaMemcpyDeviceToHost, c.stream));
+        if (values) BAEMM_CUDA(cudaMemcpyAsync(values, dv.p, z * sizeof(float), cudaMemcpyDeviceToHost, c.stream));
+        c.sync();
+    });
+}
 int baemm_last_solve_stats(const baemm_ctx *ctx, baemm_solve_stats *out)
 {
     if (!ctx || !ctx->impl || !out) return BAEMM_ERR_ARG;

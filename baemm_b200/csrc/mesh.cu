@@ -108,7 +108,82 @@ __global__ void mass_values_kernel(int64_t nv, const int32_t *__restrict__ tris,
     lumped[v] = R(1) / lump;
 }
 
+// CurlOp (Initialize.hpp:146-211): per triangle three rows (x, y, z) of
+// area-weighted nu x grad of the three P1 basis functions, in FP32 (the
+// reference's Real).  grad comes from the pseudo-inverse of the edge frame
+// (df0, df1): df^+ = g^-1 df^T with g the 2 x 2 Gram matrix.  The row's three
+// entries are written with their vertex columns in ascending order (the
+// reference sorts each row, Initialize.hpp:317-323).
+__global__ void curl_kernel(const double *__restrict__ coords, const int32_t *__restrict__ tris, int64_t nt,
+                            int32_t *__restrict__ inner, float *__restrict__ vals)
+{
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nt) return;
+    int32_t v[3];
+    float x[3][3];
+    #pragma unroll
+    for (int a = 0; a < 3; ++a)
+    {
+        v[a] = tris[3 * i + a];
+        #pragma unroll
+        for (int d = 0; d < 3; ++d) x[a][d] = (float)coords[3 * (int64_t)v[a] + d];
+    }
+    float df0[3], df1[3], anu[3];
+    #pragma unroll
+    for (int d = 0; d < 3; ++d)
+    {
+        df0[d] = x[1][d] - x[0][d];
+        df1[d] = x[2][d] - x[0][d];
+    }
+    anu[0] = 0.5f * (df0[1] * df1[2] - df0[2] * df1[1]);
+    anu[1] = 0.5f * (df0[2] * df1[0] - df0[0] * df1[2]);
+    anu[2] = 0.5f * (df0[0] * df1[1] - df0[1] * df1[0]);
+    const float g00 = df0[0] * df0[0] + df0[1] * df0[1] + df0[2] * df0[2];
+    const float g01 = df0[0] * df1[0] + df0[1] * df1[1] + df0[2] * df1[2];
+    const float g11 = df1[0] * df1[0] + df1[1] * df1[1] + df1[2] * df1[2];
+    const float dinv = 1.0f / (g00 * g11 - g01 * g01);
+    const float i00 = g11 * dinv, i01 = -g01 * dinv, i11 = g00 * dinv;
+    float grad[3][3];   // grad[component][corner]
+    #pragma unroll
+    for (int k = 0; k < 3; ++k)
+    {
+        const float p0 = i00 * df0[k] + i01 * df1[k];
+        const float p1 = i01 * df0[k] + i11 * df1[k];
+        grad[k][0] = -p0 - p1;
+        grad[k][1] = p0;
+        grad[k][2] = p1;
+    }
+    float curl[3][3];   // curl[row][corner] = (anu x grad)[row]
+    #pragma unroll
+    for (int a = 0; a < 3; ++a)
+    {
+        curl[0][a] = anu[1] * grad[2][a] - anu[2] * grad[1][a];
+        curl[1][a] = anu[2] * grad[0][a] - anu[0] * grad[2][a];
+        curl[2][a] = anu[0] * grad[1][a] - anu[1] * grad[0][a];
+    }
+    // corners in ascending vertex order
+    int p[3] = {0, 1, 2};
+    if (v[p[1]] < v[p[0]]) { const int t = p[0]; p[0] = p[1]; p[1] = t; }
+    if (v[p[2]] < v[p[1]]) { const int t = p[1]; p[1] = p[2]; p[2] = t; }
+    if (v[p[1]] < v[p[0]]) { const int t = p[0]; p[0] = p[1]; p[1] = t; }
+    #pragma unroll
+    for (int d = 0; d < 3; ++d)
+        #pragma unroll
+        for (int k = 0; k < 3; ++k)
+        {
+            inner[9 * i + 3 * d + k] = v[p[k]];
+            vals[9 * i + 3 * d + k] = curl[d][p[k]];
+        }
+}
+
 } // namespace
+
+void launch_curl(const MeshDev &m, int32_t *inner, float *vals, cudaStream_t st)
+{
+    if (m.nt == 0) return;
+    curl_kernel<<<ceil_div(m.nt, 128), 128, 0, st>>>(m.coords, m.tris, m.nt, inner, vals);
+    BAEMM_LAUNCH_CHECK();
+}
 
 void launch_geometry(const MeshDev &m, bool fp64, cudaStream_t st)
 {

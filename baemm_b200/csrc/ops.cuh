@@ -47,6 +47,10 @@ void launch_geometry(const MeshDev &m, bool fp64, cudaStream_t st);
 // (Initialize.hpp:339-353), after launch_geometry.
 void launch_mass_values(const MeshDev &m, bool fp64, cudaStream_t st);
 
+// CurlOp values (Initialize.hpp:146-211, FP32): rows 3 t + d of triangle t,
+// 9 entries per triangle, columns ascending within each row.
+void launch_curl(const MeshDev &m, int32_t *inner, float *vals, cudaStream_t st);
+
 // ---- sparse.cu -----------------------------------------------------------------
 // AvOp (PL -> PC): Btri[t,k] = a3_t * sum_q Bin[v_q, k]; Text = float2/double2, R = internal.
 template <class Text, class R>

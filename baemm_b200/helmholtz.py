@@ -243,6 +243,19 @@ class Helmholtz_CUDA:
                                                  inner.ctypes.data_as(_capi.i32p), _fp(vals), C.byref(nnz)))
         return outer, inner, vals
 
+    def CurlOperator(self):
+        """CSR (outer, inner, values) of CurlOp (Initialize.hpp:146-211): rows
+        3 t + d, the triangle's vertex columns ascending, values (area nu x
+        grad phi)[d] in FP32."""
+        nnz = C.c_int64()
+        self._ck(self._lib.baemm_get_curl_operator(self._h, None, None, None, C.byref(nnz)))
+        outer = np.zeros(3 * self.SimplexCount() + 1, np.int64)
+        inner = np.zeros(nnz.value, np.int32)
+        vals = np.zeros(nnz.value, np.float32)
+        self._ck(self._lib.baemm_get_curl_operator(self._h, outer.ctypes.data_as(_capi.i64p),
+                                                   inner.ctypes.data_as(_capi.i32p), _fp(vals), C.byref(nnz)))
+        return outer, inner, vals
+
     def SetProfiling(self, on: bool):
         self._ck(self._lib.baemm_set_profiling(self._h, int(bool(on))))
 

@@ -194,6 +194,13 @@ int baemm_get_single_layer_diagonal(baemm_ctx *ctx, float *out);
 /* MassMatrix (GetSetters.hpp:113-116) as CSR: outer (nv+1), inner (nnz),
  * values (nnz).  Call with outer == NULL to query *nnz only. */
 int baemm_get_mass_matrix(baemm_ctx *ctx, int64_t *outer, int32_t *inner, float *values, int64_t *nnz);
+/* CurlOp (Initialize.hpp:146-211; the reference builds it as a member and no
+ * public method uses it): 3 simplex_count x vertex_count CSR, rows 3 t + d
+ * (d = x, y, z) of triangle t, the three vertex columns of the triangle in
+ * ascending order; value = (area * nu_t x grad phi_v)[d] in FP32, phi_v the P1
+ * basis function of vertex v.  outer: 3 simplex_count + 1, inner and values:
+ * 9 simplex_count.  Call with outer == NULL to query *nnz only. */
+int baemm_get_curl_operator(baemm_ctx *ctx, int64_t *outer, int32_t *inner, float *values, int64_t *nnz);
 /* Statistics of the last solve on this context. */
 int baemm_last_solve_stats(const baemm_ctx *ctx, baemm_solve_stats *out);
 

@@ -281,6 +281,8 @@ struct Base
     CSR AvOp, AvOpT, Mass;
     std::vector<double> lumped_inv;
     std::vector<double> meas_d;         // nm x 3 (as given)
+    std::vector<double> coords_d;       // nv x 3 (as given)
+    std::vector<int32_t> tris_i;        // nt x 3 (as given)
 
     bool any_layer() const { return Re_sl || Im_sl || Re_dl || Im_dl || Re_adl || Im_adl; }
     bool any_sl_dl() const { return Re_sl || Im_sl || Re_dl || Im_dl; }
@@ -570,6 +572,7 @@ struct Ctx : Base
         nv = nv_; nt = nt_; nm = nm_; threads = threads_ > 0 ? threads_ : omp_get_max_threads();
         mid.assign(4 * nt, 0); nrm.assign(4 * nt, 0); area.assign(nt, 0); diag.assign(nt, 0);
         meas4.assign(4 * nm, 0); meas_d.assign(meas, meas + 3 * nm);
+        coords_d.assign(coords, coords + 3 * nv); tris_i.assign(tris, tris + 3 * nt);
         // InitializeBuffers.hpp:415-424
         for (int64_t i = 0; i < nm; ++i)
             for (int d = 0; d < 3; ++d) meas4[4 * i + d] = (Real)meas[3 * i + d];
@@ -1020,6 +1023,59 @@ struct Ctx : Base
 
 using namespace orc;
 
+// CurlOp (Initialize.hpp:146-211) restated in the precision of the context:
+// rows 3 t + d, columns the triangle's vertices ascending (SortInner,
+// Initialize.hpp:317-323), values (a_nu x grad_f)[d] with a_nu the half cross
+// product of the edges and grad_f the P1 gradient operator from the
+// pseudo-inverse g^-1 df^T of the edge frame.
+template <class Real>
+static void curl_csr(const std::vector<double> &coords, const std::vector<int32_t> &tris, int64_t nt, int64_t *outer,
+                     int32_t *inner, double *val)
+{
+    for (int64_t r = 0; r <= 3 * nt; ++r) outer[r] = 3 * r;
+    for (int64_t i = 0; i < nt; ++i)
+    {
+        int32_t v[3];
+        Real x[3][3];
+        for (int a = 0; a < 3; ++a)
+        {
+            v[a] = tris[3 * i + a];
+            for (int d = 0; d < 3; ++d) x[a][d] = (Real)coords[3 * (int64_t)v[a] + d];
+        }
+        Real df0[3], df1[3], anu[3];
+        for (int d = 0; d < 3; ++d) { df0[d] = x[1][d] - x[0][d]; df1[d] = x[2][d] - x[0][d]; }
+        const Real half = Real(1) / Real(2);
+        anu[0] = half * (df0[1] * df1[2] - df0[2] * df1[1]);
+        anu[1] = half * (df0[2] * df1[0] - df0[0] * df1[2]);
+        anu[2] = half * (df0[0] * df1[1] - df0[1] * df1[0]);
+        Real g00 = 0, g01 = 0, g11 = 0;
+        for (int d = 0; d < 3; ++d) { g00 += df0[d] * df0[d]; g01 += df0[d] * df1[d]; g11 += df1[d] * df1[d]; }
+        const Real det_inv = Real(1) / (g00 * g11 - g01 * g01);
+        const Real i00 = g11 * det_inv, i01 = -g01 * det_inv, i11 = g00 * det_inv;
+        Real grad[3][3];
+        for (int k = 0; k < 3; ++k)
+        {
+            const Real p0 = i00 * df0[k] + i01 * df1[k], p1 = i01 * df0[k] + i11 * df1[k];
+            grad[k][0] = -p0 - p1; grad[k][1] = p0; grad[k][2] = p1;
+        }
+        Real curl[3][3];
+        for (int a = 0; a < 3; ++a)
+        {
+            curl[0][a] = anu[1] * grad[2][a] - anu[2] * grad[1][a];
+            curl[1][a] = anu[2] * grad[0][a] - anu[0] * grad[2][a];
+            curl[2][a] = anu[0] * grad[1][a] - anu[1] * grad[0][a];
+        }
+        int p[3] = {0, 1, 2};
+        std::sort(p, p + 3, [&](int a, int b) { return v[a] < v[b]; });
+        for (int d = 0; d < 3; ++d)
+            for (int k = 0; k < 3; ++k)
+            {
+                inner[9 * i + 3 * d + k] = v[p[k]];
+                val[9 * i + 3 * d + k] = (double)curl[d][p[k]];
+            }
+    }
+}
+
 extern "C" {
 
 // precision: 32 -> reference arithmetic (FP32 inside), 64 -> FP64 twin.
@@ -1051,6 +1107,12 @@ void orc_mass_csr(void *h, int64_t *outer, int32_t *inner, double *val)
     std::copy(M.outer.begin(), M.outer.end(), outer);
     std::copy(M.inner.begin(), M.inner.end(), inner);
     std::copy(M.val_d.begin(), M.val_d.end(), val);
+}
+void orc_curl_csr(void *h, int64_t *outer, int32_t *inner, double *val)
+{
+    auto *b = static_cast<Base *>(h);
+    if (dynamic_cast<Ctx<float> *>(b)) curl_csr<float>(b->coords_d, b->tris_i, b->nt, outer, inner, val);
+    else curl_csr<double>(b->coords_d, b->tris_i, b->nt, outer, inner, val);
 }
 void orc_lumped_inv(void *h, double *out)
 {

@@ -62,6 +62,7 @@ def lib():
             "orc_mass_nnz": [V],
             "orc_mass_csr": [V, _i64p, _i32p, _dp],
             "orc_lumped_inv": [V, _dp],
+            "orc_curl_csr": [V, _i64p, _i32p, _dp],
             "orc_load_parameters": [V, _dp, _dp, I, I, D],
             "orc_apply_boundary": [V, _dp, _dp, I64, _dp, _dp, I64],
             "orc_boundary_kernel_tri": [V, _dp, _dp],
@@ -161,6 +162,14 @@ class Oracle:
         nnz = L.orc_mass_nnz(self._h)
         outer = np.zeros(self.nv + 1, np.int64); inner = np.zeros(nnz, np.int32); val = np.zeros(nnz)
         L.orc_mass_csr(self._h, _p(outer, _i64p), _p(inner, _i32p), _p(val))
+        return outer, inner, val
+
+    def curl_operator(self):
+        """CurlOp CSR (Initialize.hpp:146-211): (outer, inner, values)."""
+        outer = np.zeros(3 * self.nt + 1, np.int64)
+        inner = np.zeros(9 * self.nt, np.int32)
+        val = np.zeros(9 * self.nt, np.float64)
+        lib().orc_curl_csr(self._h, outer.ctypes.data_as(_i64p), inner.ctypes.data_as(_i32p), _p(val))
         return outer, inner, val
 
     def lumped_inverse_diag(self):

@@ -433,3 +433,19 @@ def test_error_statuses(env):
     C = np.zeros_like(B)
     H.ApplyBoundaryOperators_PL(1.0, B + 1, 0.0, C, [1.0], [[0, 1, 0, 0]], 16, 16)
     assert np.isfinite(C).all() and np.abs(C).max() > 0
+
+
+def test_curl_operator_matches_oracle(env):
+    """CurlOp (Initialize.hpp:146-211) built on the device: same CSR structure
+    as the oracle, values within FP32 rounding, and area * nu x g on the vertex
+    values of a linear field g . x."""
+    coords, tris, meas, H, o32, o64 = env
+    go, gi, gv = H.CurlOperator()
+    oo, oi, ov = o32.curl_operator()
+    assert np.array_equal(go, oo) and np.array_equal(gi, oi)
+    assert relerr(gv, ov) < 1e-6
+    _, nrm, area, _ = o64.geometry()
+    g = np.array([-0.4, 0.9, 1.3])
+    rows = np.add.reduceat(gv.astype(np.float64) * (coords @ g)[gi], go[:-1]).reshape(-1, 3)
+    want = area[:, None] * np.cross(nrm[:, :3], g)
+    assert np.max(np.abs(rows - want)) < 2e-5 * np.max(np.abs(want))

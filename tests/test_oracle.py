@@ -235,3 +235,23 @@ def test_mass_inverse_restatement(sphere2):
     # 20 CG iterations (ApplyMassInverse.hpp:48) reach ~1e-9 on this mesh
     assert o.ApplyMassInverse(X, Y, 1e-8)
     assert relerr(M @ Y, X) < 1e-8
+
+
+@pytest.mark.parametrize("precision,tol", [(64, 1e-12), (32, 2e-5)])
+def test_oracle_curl_operator_known_answer(sphere2, precision, tol):
+    """CurlOp (Initialize.hpp:146-211) applied to the vertex values of a linear
+    field f(x) = g . x gives, per triangle, area * nu x g (P1 interpolation of a
+    linear field is exact, and nu x grad_tan f = nu x g); rows of a triangle
+    hold its three vertices in ascending order."""
+    coords, tris = sphere2
+    o = O.Oracle(coords, tris, np.eye(3), precision=precision)
+    outer, inner, val = o.curl_operator()
+    nt = tris.shape[0]
+    assert np.array_equal(outer, 3 * np.arange(3 * nt + 1))
+    assert np.array_equal(inner.reshape(nt, 3, 3), np.repeat(np.sort(tris, axis=1)[:, None, :], 3, axis=1))
+    _, nrm, area, _ = o.geometry()
+    g = np.array([0.3, -1.2, 0.7])
+    f = coords @ g
+    rows = np.add.reduceat(val * f[inner], outer[:-1])
+    want = area[:, None] * np.cross(nrm[:, :3], g)
+    assert np.max(np.abs(rows.reshape(nt, 3) - want)) < tol * np.max(np.abs(want))
