@@ -136,6 +136,7 @@ public:
         {
             areas_.clear(); normals_.clear(); midpoints_.clear(); diag_.clear();
             mass_ = MassMatrix_T{};
+            curl_ = MassMatrix_T{};
         }
     }
 
@@ -159,6 +160,25 @@ public:
                   "MassMatrix");
         }
         return mass_;
+    }
+
+    // CurlOp (Initialize.hpp:146-211; a member of the reference class that no
+    // method uses): 3 SimplexCount() x VertexCount() CSR in FP32.
+    const MassMatrix_T &CurlOperator()
+    {
+        if (curl_.rows == 0)
+        {
+            int64_t nnz = 0;
+            check(baemm_get_curl_operator(ctx_, nullptr, nullptr, nullptr, &nnz), "CurlOperator");
+            curl_.rows = 3 * (int64_t)SimplexCount();
+            curl_.cols = VertexCount();
+            curl_.outer.resize(curl_.rows + 1);
+            curl_.inner.resize(nnz);
+            curl_.values.resize(nnz);
+            check(baemm_get_curl_operator(ctx_, curl_.outer.data(), curl_.inner.data(), curl_.values.data(), &nnz),
+                  "CurlOperator");
+        }
+        return curl_;
     }
 
     baemm_solve_stats LastSolveStats() const
@@ -501,6 +521,7 @@ private:
     baemm_ctx *ctx_ = nullptr;
     std::vector<Real> areas_, normals_, midpoints_, diag_;
     MassMatrix_T mass_;
+    MassMatrix_T curl_;
 
     template <typename ExtReal, typename ExtInt>
     void init(const ExtReal *coords, ExtInt nv, const ExtInt *tris, ExtInt nt, const ExtReal *meas, ExtInt nm,

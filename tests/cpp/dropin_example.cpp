@@ -3,6 +3,7 @@
 // Helmholtz_CUDA.  Run on a GPU box it computes a small far field and its
 // derivative; without a device every call reports an error and returns.
 #include "Helmholtz_CUDA.hpp"
+#include "BAEMM_Meshes.hpp"
 
 #include <cmath>
 #include <complex>
@@ -43,5 +44,17 @@ int main()
     H.SetApplyMode(BAEMM_APPLY_TC);
     H.FarField<wave_count>(kappa.data(), wave_chunk_count, inc.data(), wave_chunk_size, F.data(), WaveType::Plane,
                            Real(1e-5), Real(1e-4));
+    // the near-field potential of a density at two points, CurlOp, the mesh readers
+    std::vector<Complex> B(6 * wave_count, Complex(1.0, 0.0)), P(2 * wave_count);
+    std::vector<Real> pts = {0.1, 0.0, 0.0, 3.0, 0.0, 0.0};
+    std::vector<Complex> coeff = {Complex(0), Complex(1), Complex(1), Complex(0)};
+    H.ApplyNearFieldOperators_PL(Complex(1), B.data(), wave_count, Complex(0), P.data(), wave_count, kappa.data(),
+                                 coeff.data(), wave_count, wave_chunk_size, pts.data(), Int(2));
+    const auto &curl = H.CurlOperator();
+    std::printf("near field %g, CurlOp rows %lld\n", std::abs(P[0]), (long long)curl.rows);
+    std::vector<double> mesh_coords;
+    std::vector<int64_t> mesh_tris;
+    if (BAEMM::ReadMeshFromFile("Sphere_00001280T.txt", mesh_coords, mesh_tris))
+        std::printf("read %zu triangles\n", mesh_tris.size() / 3);
     return 0;
 }
