@@ -307,7 +307,7 @@ def run_gpu_arm(args, rank, world, local_rank):
     torch.cuda.synchronize()
     launches0 = H.KernelLaunchCount()
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
-    dense_ms = []
+    dense_ms, phase_ms = [], []
     with ClockSampler(torch.cuda.current_device()) as clk:
         with torch.cuda.stream(stream):
             for k in range(args.steps):
@@ -315,7 +315,8 @@ def run_gpu_arm(args, rank, world, local_rank):
                 ev[k][0].record(stream)
                 step()
                 ev[k][1].record(stream)
-                dense_ms.append(H.LastApplyTimes()[1])
+                phase_ms.append(H.LastApplyTimes())
+                dense_ms.append(phase_ms[-1][1])
         torch.cuda.synchronize()
     launches = H.KernelLaunchCount() - launches0 - 0  # library kernels only (flush is torch's)
     step_ms = [a.elapsed_time(b) for a, b in ev]
@@ -424,6 +425,20 @@ def run_gpu_arm(args, rank, world, local_rank):
         "gpu_launches": int(launches),
         "clocks": clk.summary(),
     }
+    # HBM-bound sparse steps of the apply (device times of the same steps):
+    #   AvOp:     reads AvOp (3 int32 + a3 per triangle) and the vertex block, writes B_tri;
+    #   epilogue: reads the AvOp^T CSR, a3, diag, C_tri and B_tri (SL diagonal), writes the vertex block.
+    cb = 8 if args.mode != "fp64" else 16            # bytes per complex of the internal blocks
+    nnz = 3 * nt
+    avop_bytes = nt * 16 + nv * WC * B.itemsize + nt * WC * cb
+    epi_bytes = (nv + 1) * 4 + nnz * 4 + nt * 8 + 2 * nt * WC * cb + nv * WC * B.itemsize
+    if S is None:
+        ph = np.mean(np.array(phase_ms), axis=0)
+        line["sparse_steps"] = {
+            name: {"ms": float(ms), "algorithmic_bytes": int(nb), "GB_s": nb / (ms * 1e-3) / 1e9,
+                   "frac_of_hbm_peak": nb / (ms * 1e-3) / 1e9 / peaks["hbm_gbs"],
+                   "peak_source": peaks["source"] + " (copy bandwidth)"}
+            for name, ms, nb in (("avop", ph[0], avop_bytes), ("avopT_epilogue", ph[2], epi_bytes))}
     if compare is not None:
         line["compare"] = compare
     if cpu is not None:
