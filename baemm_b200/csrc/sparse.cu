@@ -23,14 +23,19 @@ template <> __device__ __forceinline__ double2 st2<double2>(double2 v) { return 
 
 __device__ __forceinline__ double2 dmul(double2 a, double2 b) { return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x); }
 
+// 2-D grid: threadIdx.x / blockIdx.y run over the columns (a warp reads 32
+// consecutive columns of a row), threadIdx.y / blockIdx.x over the rows.
+constexpr int kRowsPerBlock = 8;
+
 template <class Text, class R>
-__global__ void avop_kernel(int64_t nt, int wc, const int32_t *__restrict__ tri_sorted, const R *__restrict__ a3,
-                            const Text *__restrict__ Bin, int64_t ldB, cplx<R> *__restrict__ Btri)
+__global__ void __launch_bounds__(32 * kRowsPerBlock)
+avop_kernel(int64_t nt, int wc, const int32_t *__restrict__ tri_sorted, const R *__restrict__ a3,
+            const Text *__restrict__ Bin, int64_t ldB, cplx<R> *__restrict__ Btri)
 {
-    const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (idx >= nt * wc) return;
-    const int64_t t = idx / wc;
-    const int k = (int)(idx - t * wc);
+    const int64_t t = (int64_t)blockIdx.x * kRowsPerBlock + threadIdx.y;
+    const int k = blockIdx.y * 32 + threadIdx.x;
+    if (t >= nt || k >= wc) return;
+    const int64_t idx = t * wc + k;
     const double a = (double)a3[t];
     double2 s = make_double2(0.0, 0.0);
     #pragma unroll
@@ -51,7 +56,8 @@ template <> struct PrmOf<float> { using type = ChunkParamsF; };
 template <> struct PrmOf<double> { using type = ChunkParamsD; };
 
 template <class Text, class R>
-__global__ void epilogue_kernel(int64_t nv, int wc, int wcs, bool layers, bool sl_diag, bool mass,
+__global__ void __launch_bounds__(32 * kRowsPerBlock)
+epilogue_kernel(int64_t nv, int wc, int wcs, bool layers, bool sl_diag, bool mass,
                                 const int32_t *__restrict__ avt_outer, const int32_t *__restrict__ avt_inner,
                                 const R *__restrict__ a3, const R *__restrict__ diag,
                                 const cplx<R> *__restrict__ Ctri, const cplx<R> *__restrict__ Btri,
@@ -61,10 +67,9 @@ __global__ void epilogue_kernel(int64_t nv, int wc, int wcs, bool layers, bool s
                                 const Text *__restrict__ Bin, int64_t ldB, double2 alpha, double2 beta,
                                 Text *__restrict__ Cout, int64_t ldC, int64_t t_begin, int64_t t_end)
 {
-    const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (idx >= nv * wc) return;
-    const int64_t v = idx / wc;
-    const int k = (int)(idx - v * wc);
+    const int64_t v = (int64_t)blockIdx.x * kRowsPerBlock + threadIdx.y;
+    const int k = blockIdx.y * 32 + threadIdx.x;
+    if (v >= nv || k >= wc) return;
     const int ch = k / wcs;
     double2 out = make_double2(0.0, 0.0);
     if (layers)
@@ -303,7 +308,8 @@ void launch_avop(const MeshDev &m, const Text *Bin, int64_t ldB, int wc, cplx<R>
     if (n == 0) return;
     const R *a3;
     if constexpr (std::is_same<R, float>::value) a3 = m.a3_f; else a3 = m.a3_d;
-    avop_kernel<Text, R><<<grid_for(n), kT, 0, st>>>(m.nt, wc, m.tri_sorted, a3, Bin, ldB, Btri);
+    const dim3 grid(ceil_div(m.nt, kRowsPerBlock), ceil_div(wc, 32)), block(32, kRowsPerBlock);
+    avop_kernel<Text, R><<<grid, block, 0, st>>>(m.nt, wc, m.tri_sorted, a3, Bin, ldB, Btri);
     BAEMM_LAUNCH_CHECK();
 }
 
@@ -319,7 +325,8 @@ void launch_epilogue(const MeshDev &m, const EpilogueArgs &a, const cplx<R> *Ctr
     else { a3 = m.a3_d; diag = m.diag_d; mv = m.mass_d; }
     const double2 al = make_double2((double)alpha.x, (double)alpha.y);
     const double2 be = make_double2((double)beta.x, (double)beta.y);
-    epilogue_kernel<Text, R><<<grid_for(n), kT, 0, st>>>(
+    const dim3 grid(ceil_div(m.nv, kRowsPerBlock), ceil_div(a.wc, 32)), block(32, kRowsPerBlock);
+    epilogue_kernel<Text, R><<<grid, block, 0, st>>>(
         m.nv, a.wc, a.wcs, a.layers, a.sl_diag, a.mass, m.avt_outer, m.avt_inner, a3, diag, Ctri, Btri,
         static_cast<const typename PrmOf<R>::type *>(chunk_params), m.mass_outer, m.mass_inner, mv, Bin, ldB, al, be,
         Cout, ldC, a.t_begin, a.t_end);
