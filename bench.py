@@ -112,6 +112,11 @@ class ClockSampler:
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
+            # the first sample before the timed region starts: nvidia-smi's start-up
+            # (NVML initialisation on a fresh machine) must not fall inside it
+            t0 = time.time()
+            while not self.lines and self.proc.poll() is None and time.time() - t0 < 15.0:
+                time.sleep(0.01)
         except Exception:
             self.proc = None
         return self
