@@ -109,14 +109,33 @@ __global__ void cg_init_kernel(int64_t n, int c, int cp, int rp, int64_t rpb, co
     block_reduce_store(bb, sm, tr, tc, cp, rp, active, out + c + k);
 }
 
+
+// Sum of one column of the per-block partial sums, partial[q * ld + off] over
+// q < nblk, by one warp: lane l takes q = l, l + 32, ..., a shuffle tree adds
+// the lanes in a fixed order and every lane returns lane 0's total (so the
+// result does not depend on timing).  The finalize kernels below give each
+// column its own warp, instead of one thread summing all nblk values in turn.
+__device__ __forceinline__ double warp_sum_partials(const double *__restrict__ partial, int64_t ld, int64_t off,
+                                                    int nblk)
+{
+    const int lane = threadIdx.x & 31;
+    double s = 0.0;
+    for (int q = lane; q < nblk; q += 32) s += partial[(int64_t)q * ld + off];
+    #pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+    return __shfl_sync(0xffffffffu, s, 0);
+}
+
 __global__ void cg_finalize_init_kernel(int c, int nblk, const double *__restrict__ partial, double *__restrict__ col,
                                         int *__restrict__ flags, double tol)
 {
     int all = 1;
-    for (int k = threadIdx.x; k < c; k += blockDim.x)
+    const int warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5, lane = threadIdx.x & 31;
+    for (int k = warp; k < c; k += nwarps)
     {
-        double rz = 0.0, bb = 0.0;
-        for (int q = 0; q < nblk; ++q) { rz += partial[(int64_t)q * 2 * c + k]; bb += partial[(int64_t)q * 2 * c + c + k]; }
+        const double rz = warp_sum_partials(partial, 2 * c, k, nblk);
+        const double bb = warp_sum_partials(partial, 2 * c, c + k, nblk);
+        if (lane != 0) continue;
         const double bn = sqrt(bb);
         col[k] = rz;
         col[c + k] = bn;
@@ -159,11 +178,11 @@ __global__ void cg_finalize_alpha_kernel(int c, int nblk, const double *__restri
                                          const int *__restrict__ flags)
 {
     if (flags[0]) return;
-    for (int k = threadIdx.x; k < c; k += blockDim.x)
+    const int warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5, lane = threadIdx.x & 31;
+    for (int k = warp; k < c; k += nwarps)
     {
-        double pq = 0.0;
-        for (int q = 0; q < nblk; ++q) pq += partial[(int64_t)q * c + k];
-        col[2 * c + k] = (flags[2 + k] || pq == 0.0) ? 0.0 : col[k] / pq;
+        const double pq = warp_sum_partials(partial, c, k, nblk);
+        if (lane == 0) col[2 * c + k] = (flags[2 + k] || pq == 0.0) ? 0.0 : col[k] / pq;
     }
 }
 
@@ -205,10 +224,12 @@ __global__ void cg_finalize_beta_kernel(int c, int nblk, const double *__restric
 {
     if (flags[0]) return;
     int all = 1;
-    for (int k = threadIdx.x; k < c; k += blockDim.x)
+    const int warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5, lane = threadIdx.x & 31;
+    for (int k = warp; k < c; k += nwarps)
     {
-        double rzn = 0.0, rr = 0.0;
-        for (int q = 0; q < nblk; ++q) { rzn += partial[(int64_t)q * 2 * c + k]; rr += partial[(int64_t)q * 2 * c + c + k]; }
+        const double rzn = warp_sum_partials(partial, 2 * c, k, nblk);
+        const double rr = warp_sum_partials(partial, 2 * c, c + k, nblk);
+        if (lane != 0) continue;
         const int was = flags[2 + k];
         col[3 * c + k] = (was || col[k] == 0.0) ? 0.0 : rzn / col[k];
         col[k] = rzn;
@@ -297,16 +318,14 @@ template <class S>
 __global__ void gs_finalize_kernel(int c, int nblk, int nvec, const double *__restrict__ partial, S *__restrict__ h,
                                    S *__restrict__ H, int m, int j, int accumulate)
 {
-    const int item = blockIdx.x * blockDim.x + threadIdx.x;
-    if (item >= nvec * c) return;
+    // one warp per item (a basis vector's dot product with one column)
+    const int item = (int)(((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+    if (item >= nvec * c) return;   // warp-uniform
     constexpr int W = kWords<S>;
-    double sx = 0.0, sy = 0.0;
-    for (int q = 0; q < nblk; ++q)
-    {
-        const double *src = partial + ((int64_t)q * nvec * c + item) * W;
-        sx += src[0];
-        if (W == 2) sy += src[1];
-    }
+    const int64_t ld = (int64_t)nvec * c * W;
+    const double sx = warp_sum_partials(partial, ld, (int64_t)item * W, nblk);
+    const double sy = W == 2 ? warp_sum_partials(partial, ld, (int64_t)item * W + 1, nblk) : 0.0;
+    if ((threadIdx.x & 31) != 0) return;
     const S v = mkS<S>(sx, sy);
     h[item] = v;
     const int i = item / c, k = item - i * c;
@@ -351,11 +370,13 @@ __global__ void norm_finalize_kernel(int c, int nblk, const double *__restrict__
                                      S *__restrict__ g, double *__restrict__ bnorm, int *__restrict__ flags, double tol)
 {
     int all = 1;
-    for (int k = threadIdx.x; k < c; k += blockDim.x)
+    const int warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5, lane = threadIdx.x & 31;
+    for (int k = warp; k < c; k += nwarps)
     {
-        double s = 0.0;
-        for (int q = 0; q < nblk; ++q) s += partial[(int64_t)q * c + k];
-        const double nv = sqrt(s);
+        const double nv = sqrt(warp_sum_partials(partial, c, k, nblk));
+        if (mode != 0)
+            for (int i = lane; i <= m; i += 32) g[(int64_t)i * c + k] = mkS<S>(i == 0 ? nv : 0.0, 0.0);
+        if (lane != 0) continue;
         hn[k] = nv;
         if (mode == 0)
             H[((int64_t)(j + 1) * m + j) * c + k] = mkS<S>(nv, 0.0);
@@ -363,7 +384,6 @@ __global__ void norm_finalize_kernel(int c, int nblk, const double *__restrict__
         {
             if (mode == 2) bnorm[k] = nv;   // first cycle: ||P b||
             res[k] = nv;
-            for (int i = 0; i <= m; ++i) g[(int64_t)i * c + k] = mkS<S>(i == 0 ? nv : 0.0, 0.0);
             all &= (nv <= tol * bnorm[k]) ? 1 : 0;
         }
     }
@@ -531,7 +551,7 @@ void CgSolver::enqueue_mass(const MeshDev &m, bool fp64_values, const double *b,
     partial_.reserve((size_t)L.nblk * 2 * c);
     if (!host_flags_) BAEMM_CUDA(cudaMallocHost(&host_flags_, 2 * sizeof(int)));
     dim3 grid(L.nblk, L.nchunk);
-    const int fin = std::min(1024, ((c + 31) / 32) * 32);
+    const int fin = std::min(1024, 32 * c);   // finalize kernels: one warp per column
     auto run = [&](auto Lv, auto Mv) {
         cg_init_kernel<<<grid, RT, 0, st>>>(n, c, L.cp, L.rp, L.rows_per_block, b, ldb, Lv, x_.p, r_.p, z_.p, p_.p,
                                             partial_.p);
@@ -600,7 +620,8 @@ typename GmresSolver<S>::Stats GmresSolver<S>::solve(int64_t n, int c, int resta
         host_cap_ = c;
     }
     dim3 grid(L.nblk, L.nchunk);
-    const int fin = std::min(1024, ((c + 31) / 32) * 32);
+    const int fin = std::min(1024, ((c + 31) / 32) * 32);   // givens: one thread per column
+    const int fin_w = std::min(1024, 32 * c);                // norm finalize: one warp per column
 
     auto read_flag = [&]() {
         BAEMM_CUDA(cudaMemcpyAsync(host_flags_, flags_.p, sizeof(int), cudaMemcpyDeviceToHost, st));
@@ -610,7 +631,7 @@ typename GmresSolver<S>::Stats GmresSolver<S>::solve(int64_t n, int c, int resta
     // hn = ||w|| columnwise, with `mode` as in norm_finalize_kernel
     auto norms = [&](const S *w, int j, int mode) {
         norm_partial_kernel<S><<<grid, RT, 0, st>>>(n, c, L.cp, L.rp, L.rows_per_block, w, partial_.p);
-        norm_finalize_kernel<S><<<1, fin, 0, st>>>(c, L.nblk, partial_.p, hn_.p, H_.p, m, j, mode, res_.p, g_.p,
+        norm_finalize_kernel<S><<<1, fin_w, 0, st>>>(c, L.nblk, partial_.p, hn_.p, H_.p, m, j, mode, res_.p, g_.p,
                                                    bnorm_.p, flags_.p, tol);
         BAEMM_LAUNCH_CHECK();
     };
@@ -644,7 +665,7 @@ typename GmresSolver<S>::Stats GmresSolver<S>::solve(int64_t n, int c, int resta
             A(Vj, tmp_.p);
             P(tmp_.p, w_.p);
             const int nvec = j + 1;
-            const int fg = ceil_div((int64_t)nvec * c, 256);
+            const int fg = ceil_div((int64_t)nvec * c * 32, 256);   // one warp per item
             for (int pass = 0; pass < 2; ++pass)
             {
                 gs_dot_kernel<S><<<grid, RT, 0, st>>>(n, c, L.cp, L.rp, L.rows_per_block, V_.p, nvec, w_.p,
