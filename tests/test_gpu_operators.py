@@ -420,6 +420,29 @@ def test_mass_inverse_and_lumped(env, mode):
     assert relerr(Lg, Lo) < (1e-6 if mode == APPLY_FP32 else 1e-14)
 
 
+@pytest.mark.parametrize("ncols,cplx", [(1, False), (31, False), (33, False), (100, False), (1024, False),
+                                        (512, True)])
+def test_mass_inverse_column_counts(env, ncols, cplx):
+    """FP64 CG on 1 ... 1024 real columns (512 complex = 1024 real): the
+    finalizers give each column one warp of a block of at most 1024 threads,
+    so above 32 columns each warp takes several.  Column 0 is zero and
+    converges at once while the others iterate."""
+    coords, tris, meas, H, o32, o64 = env
+    rng = np.random.default_rng(40 + ncols)
+    nv = coords.shape[0]
+    X = crandn(rng, nv, ncols) if cplx else rng.standard_normal((nv, ncols))
+    X[:, 0] = 0
+    Yg, Yo = np.zeros_like(X), np.zeros_like(X)
+    H.SetApplyMode(APPLY_FP64)
+    try:
+        H.ApplyMassInverse(X, Yg, 1e-10)
+    finally:
+        H.SetApplyMode(APPLY_FP32)
+    o64.ApplyMassInverse(X, Yo, 1e-10)
+    assert np.all(Yg[:, 0] == 0)
+    assert relerr(Yg, Yo) < 1e-11
+
+
 def test_error_statuses(env):
     coords, tris, meas, H, o32, o64 = env
     B = np.zeros((coords.shape[0], 16), complex)

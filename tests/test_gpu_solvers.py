@@ -123,6 +123,27 @@ def test_boundary_potential_and_dtn_match_oracle(env):
     assert relerr(dn_g, dn_o) < 1e-5
 
 
+@pytest.mark.parametrize("nk", [1, 3, 5])
+def test_boundary_potential_fp64_column_counts(env, nk):
+    """FP64 GMRES on 16 nk columns (16, 48, 80): the column sums of the Krylov
+    reductions are finished by one warp per column, so counts that are not
+    multiples of 32 (and more columns than a warp loop covers once) are
+    checked against the FP64 oracle."""
+    coords, tris, meas, inc, H, o32, o64 = env
+    rng = np.random.default_rng(30 + nk)
+    kap = np.linspace(2.0, 6.0, nk)
+    wave = crandn(rng, coords.shape[0], 16 * nk)
+    coeff = np.zeros((nk, 4), complex)
+    phi_g, phi_o = np.zeros_like(wave), np.zeros_like(wave)
+    H.SetApplyMode(APPLY_FP64)
+    try:
+        H.BoundaryPotential(kap, coeff, wave, phi_g, 16, 1e-12, 1e-12)
+    finally:
+        H.SetApplyMode(APPLY_FP32)
+    o64.BoundaryPotential(kap, wave, phi_o, 16, 1e-12, 1e-12)
+    assert relerr(phi_g, phi_o) < 1e-9
+
+
 def test_derivative_and_adjoint_match_oracle(env):
     coords, tris, meas, inc, H, o32, o64 = env
     kap = np.array([2.0])
