@@ -627,23 +627,58 @@ def run_solve_workload(args):
         H.SetApplyMode(APPLY_FP32)
         return F, dt, st
 
-    F64, t64, s64 = solve(APPLY_FP64, 1e-10)
-    runs = {"fp64_tol1e-10": (F64, t64, s64)}
-    runs["fp32_tol1e-6"] = solve(APPLY_FP32, 1e-6)
-    runs["tc_tol1e-6"] = solve(APPLY_TC, 1e-6)
-    runs["tc_fp64ir_tol1e-10"] = solve(APPLY_TC, 1e-10, ir_steps=8, inner=1e-5)
-    n64 = float(np.linalg.norm(F64))
+    def apply_ms(mode):
+        """One boundary apply of the solve's operator (BIE coefficients, 32
+        right-hand sides), CUDA events, minimum of 3 after a warm-up."""
+        dt = torch.complex128 if mode == APPLY_FP64 else torch.complex64
+        coeff = np.array([[0.5, -1j * k, 1, 0] for k in kap], np.complex128)
+        rng = np.random.default_rng(0)
+        B = torch.from_numpy(rng.standard_normal((coords.shape[0], 32)) +
+                             1j * rng.standard_normal((coords.shape[0], 32))).to(dt).cuda()
+        C = torch.zeros_like(B)
+        H.LoadBoundaryOperators_PL(kap, coeff, 32, 16)
+        H.SetApplyMode(mode)
+        try:
+            ts = []
+            for _ in range(4):
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record()
+                H.ApplyBoundaryOperators_PL(1.0, B, 0.0, C)
+                e1.record()
+                torch.cuda.synchronize()
+                ts.append(e0.elapsed_time(e1))
+        finally:
+            H.SetApplyMode(APPLY_FP32)
+            H.UnloadBoundaryOperators_PL()
+        return min(ts[1:])
+
+    modes = [m.strip() for m in args.solve_modes.split(",") if m.strip()]
+    known = {"fp64": ("fp64_tol1e-10", APPLY_FP64, 1e-10, 0), "fp32": ("fp32_tol1e-6", APPLY_FP32, 1e-6, 0),
+             "tc": ("tc_tol1e-6", APPLY_TC, 1e-6, 0), "tc_ir": ("tc_fp64ir_tol1e-10", APPLY_TC, 1e-10, 8)}
+    bad = [m for m in modes if m not in known]
+    if bad:
+        raise SystemExit(f"--solve-modes: unknown {bad}; choose from {sorted(known)}")
+    runs = {}
+    for m in modes:
+        name, mode, tol, ir = known[m]
+        runs[name] = solve(mode, tol, ir_steps=ir, inner=1e-5)
+    F64 = runs["fp64_tol1e-10"][0] if "fp64" in modes else None
+    n64 = float(np.linalg.norm(F64)) if F64 is not None else None
     res = {}
     for name, (F, dt, st) in runs.items():
         res[name] = {"seconds": dt, "solves_per_s": 1.0 / dt, "gmres_iterations": st["gmres_iterations"],
                      "refinement_steps": st["refinement_steps"],
                      "gmres_relative_residual": st["gmres_relative_residual"],
-                     "far_field_rel_err_vs_fp64": float(np.linalg.norm(F - F64) / n64)}
-    line = {"metric": "scattering solves/s (FarField)", "value": res["tc_fp64ir_tol1e-10"]["solves_per_s"],
+                     "far_field_rel_err_vs_fp64": (float(np.linalg.norm(F - F64) / n64) if F64 is not None
+                                                   else None)}
+    apply = {name.split("_")[0]: apply_ms(mode) for m in ("tc", "fp32", "fp64") if m in modes
+             for name, mode, _, _ in [known[m]]}
+    head = "tc_fp64ir_tol1e-10" if "tc_fp64ir_tol1e-10" in res else next(iter(res))
+    line = {"metric": "scattering solves/s (FarField)", "value": res[head]["solves_per_s"],
             "unit": "solves/s", "n_gpus": 1, "higher_is_better": True, "data": "synthetic",
             "config": {"workload": SOLVE_WORKLOAD if args.solve_level == 6 else f"icosphere level {args.solve_level}",
-                       "triangles": int(tris.shape[0]), "wave_count": 32, "meas_count": 256},
-            "runs": res}
+                       "triangles": int(tris.shape[0]), "wave_count": 32, "meas_count": 256, "value_run": head},
+            "runs": res, "apply_ms": apply}
     print(json.dumps(line), flush=True)
     H.close()
     return 0
@@ -813,6 +848,9 @@ def main(argv=None):
                     help="--workload serve: run the sequential baseline on the first N requests only (0: all)")
     ap.add_argument("--gn-level", type=int, default=5, help="icosphere level of --workload gauss-newton")
     ap.add_argument("--solve-level", type=int, default=6, help="icosphere level of --workload solve")
+    ap.add_argument("--solve-modes", default="fp64,fp32,tc,tc_ir",
+                    help="--workload solve: the runs to make (fp64 is the error reference; without it the errors "
+                         "are null)")
     ap.add_argument("--small", action="store_true", help="38400-triangle torus (profiling captures only)")
     ap.add_argument("--shard", action="store_true",
                     help="split each apply by target rows over the ranks (strong scaling; default: replicas)")
