@@ -875,21 +875,21 @@ int baemm_gauss_newton_solve(baemm_ctx *ctx, const double *kappa, int wcc, const
             BAEMM_CUDA(cudaMemcpyAsync(r.p, dB.p, n3 * sizeof(double), cudaMemcpyDeviceToDevice, c.stream));
             Pop(r.p, z.p);
             BAEMM_CUDA(cudaMemcpyAsync(p.p, z.p, n3 * sizeof(double), cudaMemcpyDeviceToDevice, c.stream));
-            double rz = baemm::device_dot(r.p, z.p, n3, c.stream);
-            const double bn = std::sqrt(baemm::device_dot(dB.p, dB.p, n3, c.stream));
+            double rz = baemm::device_dot(r.p, z.p, n3, c.reduce_scratch, c.stream);
+            const double bn = std::sqrt(baemm::device_dot(dB.p, dB.p, n3, c.reduce_scratch, c.stream));
             double rn = bn;
             const int max_it = c.gmres_max_iter * c.gmres_max_restarts;
             while (!(rn <= gmres_tol_outer * bn) && iters < max_it)
             {
                 Aop(p.p, q.p);
-                const double pq = baemm::device_dot(p.p, q.p, n3, c.stream);
+                const double pq = baemm::device_dot(p.p, q.p, n3, c.reduce_scratch, c.stream);
                 if (pq == 0.0) break;
                 const double a = rz / pq;
                 baemm::launch_axpby<double>(n3, 1, a, p.p, 1, 1.0, dX.p, 1, c.stream);
                 baemm::launch_axpby<double>(n3, 1, -a, q.p, 1, 1.0, r.p, 1, c.stream);
                 Pop(r.p, z.p);
-                const double rzn = baemm::device_dot(r.p, z.p, n3, c.stream);
-                rn = std::sqrt(baemm::device_dot(r.p, r.p, n3, c.stream));
+                const double rzn = baemm::device_dot(r.p, z.p, n3, c.reduce_scratch, c.stream);
+                rn = std::sqrt(baemm::device_dot(r.p, r.p, n3, c.reduce_scratch, c.stream));
                 baemm::launch_axpby<double>(n3, 1, 1.0, z.p, 1, rz != 0.0 ? rzn / rz : 0.0, p.p, 1, c.stream);
                 rz = rzn;
                 ++iters;

@@ -60,6 +60,7 @@ public:
     double ir_inner_tol = 1e-4;
     baemm_solve_stats stats{};
     DevBuf<int> tc_err;               // error word of the tensor-core kernel's bounded waits
+    DevBuf<double> reduce_scratch;    // per-block partial sums of device_dot / device_colnorms
     int *tc_err_host = nullptr;
     bool tc_pending = false;          // a tensor-core launch since the last error check
     bool profiling = false;

@@ -717,10 +717,9 @@ __global__ void dot_partial_kernel(const double *__restrict__ a, const double *_
 }
 } // namespace
 
-double device_dot(const double *a, const double *b, int64_t n, cudaStream_t st)
+double device_dot(const double *a, const double *b, int64_t n, DevBuf<double> &partial, cudaStream_t st)
 {
     constexpr int nb = 256;
-    static thread_local DevBuf<double> partial;
     std::vector<double> h(nb);
     dot_partial_kernel<<<nb, RT, 0, st>>>(a, b, n, partial.reserve(nb));
     BAEMM_LAUNCH_CHECK();
@@ -731,10 +730,10 @@ double device_dot(const double *a, const double *b, int64_t n, cudaStream_t st)
     return s;
 }
 
-void device_colnorms(const double2 *w, int64_t n, int c, double *out_host, cudaStream_t st)
+void device_colnorms(const double2 *w, int64_t n, int c, double *out_host, DevBuf<double> &partial,
+                     cudaStream_t st)
 {
     const Layout L = make_layout(n, c);
-    static thread_local DevBuf<double> partial;
     partial.reserve((size_t)L.nblk * c);
     norm_partial_kernel<double2><<<dim3(L.nblk, L.nchunk), RT, 0, st>>>(n, c, L.cp, L.rp, L.rows_per_block, w,
                                                                         partial.p);

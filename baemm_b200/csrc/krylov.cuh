@@ -67,9 +67,12 @@ private:
     int host_cap_ = 0;
 };
 
-// Helpers with a host result (they synchronise `st`).
-double device_dot(const double *a, const double *b, int64_t n, cudaStream_t st);
+// Helpers with a host result (they synchronise `st`).  `scratch` holds the
+// per-block partial sums; it belongs to the caller's context, so it lives on
+// the device the stream runs on.
+double device_dot(const double *a, const double *b, int64_t n, DevBuf<double> &scratch, cudaStream_t st);
 // out_host[k] = ||w[:,k]||_2 for an n x c complex block (ld c)
-void device_colnorms(const double2 *w, int64_t n, int c, double *out_host, cudaStream_t st);
+void device_colnorms(const double2 *w, int64_t n, int c, double *out_host, DevBuf<double> &scratch,
+                     cudaStream_t st);
 
 } // namespace baemm

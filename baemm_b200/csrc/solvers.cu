@@ -48,7 +48,7 @@ void Ctx::bie_solve(const double *kappa, const zc *coeff4, const double2 *rhs, d
         double2 *r = sv_res.reserve(N), *d = sv_d.reserve(N), *pr = sv_tmp.reserve(N);
         std::vector<double> pb(wc), prn(wc);
         P(rhs, pr);
-        device_colnorms(pr, nv, wc, pb.data(), stream);
+        device_colnorms(pr, nv, wc, pb.data(), reduce_scratch, stream);
         BAEMM_CUDA(cudaMemsetAsync(sol, 0, N * sizeof(double2), stream));
         BAEMM_CUDA(cudaMemcpyAsync(r, rhs, N * sizeof(double2), cudaMemcpyDeviceToDevice, stream));
         const int mode = apply_mode;
@@ -66,7 +66,7 @@ void Ctx::bie_solve(const double *kappa, const zc *coeff4, const double2 *rhs, d
             apply_boundary<double2>(make_double2(-1.0, 0.0), sol, wc, kOne, r, wc);
             apply_mode = mode;
             P(r, pr);
-            device_colnorms(pr, nv, wc, prn.data(), stream);
+            device_colnorms(pr, nv, wc, prn.data(), reduce_scratch, stream);
             rel = 0.0;
             conv = true;
             for (int k = 0; k < wc; ++k)

@@ -954,13 +954,21 @@ void tc_launch(cudaStream_t st, const float *mid, const float *nrm, const TcTile
     // More than half of the SM's shared memory, so one CTA per SM: the CTA
     // allocates all 512 TMEM columns and a second resident CTA would only wait.
     const size_t bytes = std::max(sizeof(TcSmem) + 1024, (size_t)(116 * 1024));
-    static std::once_flag once;
-    static cudaError_t attr = cudaSuccess;
-    std::call_once(once, [&] {
-        attr = cudaFuncSetAttribute(boundary_tc_kernel<CH, SL, DL, ADL, RI>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    (int)bytes);
-    });
-    BAEMM_CUDA(attr);
+    // The shared-memory limit is a per-device attribute of the function: set
+    // it once on every device this instantiation is launched on.
+    int dev = 0;
+    BAEMM_CUDA(cudaGetDevice(&dev));
+    static std::mutex mu;
+    static bool done[64] = {};
+    {
+        std::lock_guard<std::mutex> lock(mu);
+        if (dev < 0 || dev >= 64 || !done[dev])
+        {
+            BAEMM_CUDA(cudaFuncSetAttribute(boundary_tc_kernel<CH, SL, DL, ADL, RI>,
+                                            cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+            if (dev >= 0 && dev < 64) done[dev] = true;
+        }
+    }
     boundary_tc_kernel<CH, SL, DL, ADL, RI><<<plan.ctas, TC_THREADS, bytes, st>>>(mid, nrm, tg, B, C, ws, p, plan, err);
 }
 
