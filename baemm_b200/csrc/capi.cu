@@ -3,6 +3,7 @@
 // converts exceptions into a baemm_status plus a message for baemm_last_error.
 #include <cstdlib>
 #include <cstring>
+#include <memory>
 #include <new>
 
 #include "ctx.cuh"
@@ -17,12 +18,35 @@ namespace
 
 thread_local std::string g_create_error;
 
+// Makes the context's device current for one call and restores the caller's
+// device afterwards, so contexts on different GPUs can be driven from one
+// thread (allocations, streams and launches all belong to the context's device).
+struct DeviceScope
+{
+    int prev = -1;
+    explicit DeviceScope(int dev)   // dev < 0: only restore the caller's device at the end
+    {
+        if (cudaGetDevice(&prev) != cudaSuccess)
+        {
+            (void)cudaGetLastError();
+            prev = -1;
+        }
+        if (dev >= 0 && prev != dev) BAEMM_CUDA(cudaSetDevice(dev));
+    }
+    ~DeviceScope()
+    {
+        int cur = -1;
+        if (prev >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != prev) (void)cudaSetDevice(prev);
+    }
+};
+
 template <class F>
 int guarded(baemm_ctx *ctx, F &&f)
 {
     if (!ctx || !ctx->impl) return BAEMM_ERR_ARG;
     try
     {
+        DeviceScope scope(ctx->impl->device);
         f(*ctx->impl);
         ctx->impl->last_error.clear();
         return BAEMM_OK;
@@ -90,9 +114,10 @@ int create_impl(const double *coords, int64_t nv, const int32_t *tris, int64_t n
         }
     try
     {
-        auto *c = new baemm_ctx();
+        DeviceScope keep(-1);   // the constructor selects its device; the caller's is restored
+        std::unique_ptr<baemm_ctx> c(new baemm_ctx());
         c->impl = new Ctx(coords, nv, tris, nt, meas, nm, device, threads);
-        *out = c;
+        *out = c.release();
         g_create_error.clear();
         return BAEMM_OK;
     }
@@ -105,6 +130,11 @@ int create_impl(const double *coords, int64_t nv, const int32_t *tris, int64_t n
     {
         g_create_error = "host allocation failed";
         return BAEMM_ERR_ALLOC;
+    }
+    catch (const std::exception &e)
+    {
+        g_create_error = e.what();
+        return BAEMM_ERR_ARG;
     }
 }
 
@@ -277,7 +307,15 @@ int baemm_set_mesh(baemm_ctx *ctx, const double *coords, int64_t nv, const int64
 void baemm_destroy(baemm_ctx *ctx)
 {
     if (!ctx) return;
-    try { delete ctx->impl; } catch (...) {}
+    try
+    {
+        if (ctx->impl)
+        {
+            DeviceScope scope(ctx->impl->device);
+            delete ctx->impl;
+        }
+    }
+    catch (...) {}
     delete ctx;
 }
 

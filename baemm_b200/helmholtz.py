@@ -59,6 +59,24 @@ def _f64(a) -> np.ndarray:
     return np.ascontiguousarray(np.asarray(a, dtype=np.float64))
 
 
+def _check_dev(t, dtype, rows, cols, device, name):
+    """A torch CUDA block handed to a device-pointer entry point: the kernels
+    read or write rows x cols entries at t.data_ptr() with leading dimension
+    t.stride(0), on the context's device, so the tensor must hold them there."""
+    import torch
+    if not (isinstance(t, torch.Tensor) and t.is_cuda):
+        raise TypeError(f"{name} must be a torch CUDA tensor")
+    if t.dtype != dtype:
+        raise TypeError(f"{name} must be {dtype}, got {t.dtype}")
+    if t.device.index != device:
+        raise ValueError(f"{name} is on {t.device}, the context on cuda:{device}")
+    if t.dim() != 2 or (t.shape[1] > 1 and t.stride(1) != 1):
+        raise ValueError(f"{name} must be a 2-D tensor with unit column stride")
+    if t.shape[0] < rows or t.shape[1] < cols or (rows > 1 and t.stride(0) < cols):
+        raise ValueError(f"{name} must hold {rows} x {cols} entries (got shape {tuple(t.shape)}, "
+                         f"row stride {t.stride(0)})")
+
+
 def _check_out(a, dtype, name):
     if not (isinstance(a, np.ndarray) and a.dtype == dtype and a.ndim == 2 and a.flags.c_contiguous):
         raise TypeError(f"{name} must be a C-contiguous 2-D numpy array of dtype {np.dtype(dtype).name}")
@@ -81,7 +99,20 @@ class Helmholtz_CUDA:
             raise BaemmError(st, L.baemm_last_error(None).decode())
         self._h = h
         self._lib = L
+        self._device = int(device)   # resolved on first use (an out-of-range number means device 0)
         self._user_stream = None   # set by SetStream; otherwise torch tensors join torch's current stream
+
+    def _dev_index(self) -> int:
+        import torch
+        d = self._device
+        return d if 0 <= d < torch.cuda.device_count() else 0
+
+    def _check_pair(self, B, Cout, rows_c):
+        """B (vertices x wave_count) and C (rows_c x wave_count) for a device call."""
+        wc = self.GetWaveCount()
+        dev = self._dev_index()
+        _check_dev(B, B.dtype, self.VertexCount(), wc, dev, "B_in")
+        _check_dev(Cout, B.dtype, rows_c, wc, dev, "C_out")
 
     # --- lifecycle ---------------------------------------------------------------
     def SetMesh(self, vertex_coords, triangles):
@@ -338,6 +369,7 @@ class Helmholtz_CUDA:
                     fn, cs, ptr = self._lib.baemm_apply_boundary_operators_dev_c, _cc, _fp
                 else:
                     raise TypeError("B_in must be complex64 or complex128")
+                self._check_pair(B_in, C_out, self.VertexCount())
                 with self._on_torch_stream(B_in):
                     self._ck(fn(self._h, ptr(cs(alpha)), C.c_void_p(B_in.data_ptr()), B_in.stride(0),
                                 ptr(cs(beta)), C.c_void_p(C_out.data_ptr()), C_out.stride(0)))
@@ -363,8 +395,12 @@ class Helmholtz_CUDA:
         """C_out (meas x wc) = alpha (c1 FF_SL + c2 FF_DL) B_in + beta C_out
         (ApplyFarFieldOperators.hpp:334-412)."""
         if _is_torch_cuda(B_in):
+            import torch
             if kappa is not None:
                 self.LoadParameters(kappa, coeff, wave_count, wave_chunk_size)
+            if B_in.dtype != torch.complex128:
+                raise TypeError("the far field on torch tensors takes complex128")
+            self._check_pair(B_in, C_out, self.GetMeasCount())
             with self._on_torch_stream(B_in):
                 self._ck(self._lib.baemm_apply_far_field_operators_dev_z(
                     self._h, _dp(_cz(alpha)), C.c_void_p(B_in.data_ptr()), B_in.stride(0), _dp(_cz(beta)),
@@ -398,6 +434,7 @@ class Helmholtz_CUDA:
             fn, cs, ptr = self._lib.baemm_apply_boundary_operators_rows_dev_c, _cc, _fp
         else:
             raise TypeError("B_in must be complex64 or complex128")
+        self._check_pair(B_in, C_out, self.VertexCount())
         with self._on_torch_stream(B_in):
             self._ck(fn(self._h, ptr(cs(alpha)), C.c_void_p(B_in.data_ptr()), B_in.stride(0), ptr(cs(beta)),
                         C.c_void_p(C_out.data_ptr()), C_out.stride(0), int(row_begin), int(row_end),
@@ -436,9 +473,10 @@ class Helmholtz_CUDA:
             else:
                 raise TypeError("B_in must be complex64 or complex128")
             if _is_torch_cuda(points):
-                P = points.to(torch.float64).reshape(-1, 3).contiguous()
+                P = points.to(device=B_in.device, dtype=torch.float64).reshape(-1, 3).contiguous()
             else:
                 P = torch.from_numpy(_f64(points).reshape(-1, 3)).to(B_in.device)
+            self._check_pair(B_in, C_out, P.shape[0])
             with self._on_torch_stream(B_in):
                 self._ck(fn(self._h, ptr(cs(alpha)), C.c_void_p(B_in.data_ptr()), B_in.stride(0), ptr(cs(beta)),
                             C.c_void_p(C_out.data_ptr()), C_out.stride(0), C.c_void_p(P.data_ptr()), P.shape[0]))

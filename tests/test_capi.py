@@ -53,3 +53,40 @@ def test_null_context_is_rejected():
     assert L.baemm_vertex_count(None) == -1
     assert L.baemm_autotune(None, 1, 1, None) == 1
     L.baemm_destroy(None)   # no-op
+
+
+def test_device_block_check_refuses_host_tensors_and_bad_shapes():
+    """The torch-block check of the Python mirror runs before any device call:
+    host tensors are refused, and (through a stand-in with a CUDA device) too
+    few rows or columns, a column stride and another dtype are refused."""
+    import torch
+    from baemm_b200.helmholtz import _check_dev
+    with pytest.raises(TypeError):
+        _check_dev(torch.zeros((4, 2), dtype=torch.complex64), torch.complex64, 4, 2, 0, "B")
+
+    class Fake(torch.Tensor):
+        """A CPU tensor that reports itself as living on cuda:0 (host logic only)."""
+        @property
+        def is_cuda(self):
+            return True
+
+        @property
+        def device(self):
+            return torch.device("cuda", 0)
+
+    def fake(t):
+        return t.as_subclass(Fake)
+
+    ok = fake(torch.zeros((10, 8), dtype=torch.complex64))
+    _check_dev(ok, torch.complex64, 10, 8, 0, "B")
+    _check_dev(fake(torch.zeros((10, 12), dtype=torch.complex64)[:, :8]), torch.complex64, 10, 8, 0, "B")
+    with pytest.raises(ValueError, match="hold"):
+        _check_dev(ok, torch.complex64, 11, 8, 0, "B")
+    with pytest.raises(ValueError, match="hold"):
+        _check_dev(ok, torch.complex64, 10, 9, 0, "B")
+    with pytest.raises(ValueError, match="unit column stride"):
+        _check_dev(fake(torch.zeros((8, 10), dtype=torch.complex64).t()), torch.complex64, 10, 8, 0, "B")
+    with pytest.raises(TypeError, match="must be"):
+        _check_dev(ok, torch.complex128, 10, 8, 0, "B")
+    with pytest.raises(ValueError, match="context on cuda:1"):
+        _check_dev(ok, torch.complex64, 10, 8, 1, "B")

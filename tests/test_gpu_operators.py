@@ -443,6 +443,61 @@ def test_mass_inverse_column_counts(env, ncols, cplx):
     assert relerr(Yg, Yo) < 1e-11
 
 
+def test_device_blocks_are_validated(env):
+    """Torch blocks with too few rows or columns, another dtype or a column
+    stride are refused by the Python mirror before any launch; a valid call
+    afterwards still runs."""
+    import torch
+    coords, tris, meas, H, o32, o64 = env
+    nv = coords.shape[0]
+    B = torch.zeros((nv, 16), dtype=torch.complex64, device="cuda")
+    H.LoadBoundaryOperators_PL([2.0], [[1, 1, 0, 0]], 16, 16)
+    try:
+        with pytest.raises(ValueError):
+            H.ApplyBoundaryOperators_PL(1.0, B, 0.0, torch.zeros((nv - 1, 16), dtype=torch.complex64, device="cuda"))
+        with pytest.raises(ValueError):
+            H.ApplyBoundaryOperators_PL(1.0, B[:, :8], 0.0, B.clone())
+        with pytest.raises(TypeError):
+            H.ApplyBoundaryOperators_PL(1.0, B, 0.0, B.to(torch.complex128))
+        with pytest.raises(ValueError):
+            H.ApplyBoundaryOperators_PL(1.0, B, 0.0,
+                                        torch.zeros((16, nv), dtype=torch.complex64, device="cuda").t())
+        with pytest.raises(TypeError):
+            H.ApplyFarFieldOperators_PL(1.0, B, 0.0,
+                                        torch.zeros((meas.shape[0], 16), dtype=torch.complex64, device="cuda"))
+        with pytest.raises(ValueError):
+            H.ApplyBoundaryOperatorsRows(1.0, B, 0.0, B[:10], 0, 10)
+        C = torch.zeros_like(B)
+        H.ApplyBoundaryOperators_PL(1.0, B, 0.0, C)
+        torch.cuda.synchronize()
+        assert torch.count_nonzero(C).item() == 0
+    finally:
+        H.UnloadBoundaryOperators_PL()
+
+
+def test_two_contexts_from_one_thread_keep_the_callers_device(env):
+    """Calls on two contexts interleaved from one thread give the results of
+    each alone, and leave the caller's current device as it was."""
+    import torch
+    coords, tris, meas, H, o32, o64 = env
+    before = torch.cuda.current_device()
+    H2 = Helmholtz_CUDA(*meshes.icosphere(2), meas)
+    try:
+        rng = np.random.default_rng(9)
+        nv2 = H2.VertexCount()
+        X1, X2 = crandn(rng, coords.shape[0], 4), crandn(rng, nv2, 4)
+        Y1, Y2 = np.zeros_like(X1), np.zeros_like(X2)
+        Y1b, Y2b = np.zeros_like(X1), np.zeros_like(X2)
+        H.ApplyMassInverse(X1, Y1, 1e-10)
+        H2.ApplyMassInverse(X2, Y2, 1e-10)
+        H.ApplyMassInverse(X1, Y1b, 1e-10)
+        H2.ApplyMassInverse(X2, Y2b, 1e-10)
+        assert np.array_equal(Y1, Y1b) and np.array_equal(Y2, Y2b)
+        assert torch.cuda.current_device() == before
+    finally:
+        H2.close()
+
+
 def test_error_statuses(env):
     coords, tris, meas, H, o32, o64 = env
     B = np.zeros((coords.shape[0], 16), complex)
