@@ -603,8 +603,9 @@ def run_solve_workload(args):
     """FarField (FarField.hpp:28-144) on the scattering-solve configuration:
     plain FP32 apply, compensated tensor-core apply, the tensor-core apply
     inside FP64 iterative refinement, and the FP64 path; errors of the far
-    field against the FP64 solve at residual 1e-10 (the FP64 device path is
-    held to 1e-11 of the FP64 oracle by the tests at smaller sizes)."""
+    field and of the boundary density phi against the FP64 solve at residual
+    1e-10 (the FP64 device path is held to 1e-11 of the FP64 oracle by the
+    tests at smaller sizes)."""
     import torch
     from baemm_b200 import APPLY_FP32, APPLY_FP64, APPLY_TC, Helmholtz_CUDA, WaveType, meshes
     coords, tris = meshes.icosphere(args.solve_level)
@@ -612,6 +613,10 @@ def run_solve_workload(args):
     inc = meshes.fibonacci_sphere(16)
     kap = np.array([4.0, 8.0])
     H = Helmholtz_CUDA(coords, tris, meas)
+
+    # the weak incident wave FarField solves for (c1 = -1 after the 1/(4 pi) scaling)
+    wave = np.zeros((coords.shape[0], 32), complex)
+    H.CreateIncidentWave_PL(1.0, inc, 0.0, wave, kap, [[0, -4 * np.pi, 0, 0]] * 2, 32, 16)
 
     def solve(mode, gmres_tol, ir_steps=0, inner=1e-5):
         H.SetApplyMode(mode)
@@ -623,9 +628,12 @@ def run_solve_workload(args):
         H.FarField(kap, inc, F, WaveType.Plane, 1e-10, gmres_tol)
         dt = time.perf_counter() - t0
         st = H.LastSolveStats()
+        # the boundary density phi of the same solve (not timed)
+        phi = np.zeros_like(wave)
+        H.BoundaryPotential(kap, np.zeros((2, 4), complex), wave, phi, 16, 1e-10, gmres_tol)
         H.SetRefinement(0)
         H.SetApplyMode(APPLY_FP32)
-        return F, dt, st
+        return F, dt, st, phi
 
     def apply_ms(mode):
         """One boundary apply of the solve's operator (BIE coefficients, 32
@@ -662,15 +670,17 @@ def run_solve_workload(args):
     for m in modes:
         name, mode, tol, ir = known[m]
         runs[name] = solve(mode, tol, ir_steps=ir, inner=1e-5)
-    F64 = runs["fp64_tol1e-10"][0] if "fp64" in modes else None
-    n64 = float(np.linalg.norm(F64)) if F64 is not None else None
+    F64, phi64 = (runs["fp64_tol1e-10"][0], runs["fp64_tol1e-10"][3]) if "fp64" in modes else (None, None)
+
+    def rel(x, ref):
+        return float(np.linalg.norm(x - ref) / np.linalg.norm(ref)) if ref is not None else None
+
     res = {}
-    for name, (F, dt, st) in runs.items():
+    for name, (F, dt, st, phi) in runs.items():
         res[name] = {"seconds": dt, "solves_per_s": 1.0 / dt, "gmres_iterations": st["gmres_iterations"],
                      "refinement_steps": st["refinement_steps"],
                      "gmres_relative_residual": st["gmres_relative_residual"],
-                     "far_field_rel_err_vs_fp64": (float(np.linalg.norm(F - F64) / n64) if F64 is not None
-                                                   else None)}
+                     "far_field_rel_err_vs_fp64": rel(F, F64), "phi_rel_err_vs_fp64": rel(phi, phi64)}
     apply = {name.split("_")[0]: apply_ms(mode) for m in ("tc", "fp32", "fp64") if m in modes
              for name, mode, _, _ in [known[m]]}
     head = "tc_fp64ir_tol1e-10" if "tc_fp64ir_tol1e-10" in res else next(iter(res))
