@@ -10,6 +10,7 @@
 
 using baemm::Ctx;
 using baemm::DevBuf;
+using baemm::DeviceScope;
 using baemm::Error;
 using baemm::zc;
 
@@ -17,28 +18,6 @@ namespace
 {
 
 thread_local std::string g_create_error;
-
-// Makes the context's device current for one call and restores the caller's
-// device afterwards, so contexts on different GPUs can be driven from one
-// thread (allocations, streams and launches all belong to the context's device).
-struct DeviceScope
-{
-    int prev = -1;
-    explicit DeviceScope(int dev)   // dev < 0: only restore the caller's device at the end
-    {
-        if (cudaGetDevice(&prev) != cudaSuccess)
-        {
-            (void)cudaGetLastError();
-            prev = -1;
-        }
-        if (dev >= 0 && prev != dev) BAEMM_CUDA(cudaSetDevice(dev));
-    }
-    ~DeviceScope()
-    {
-        int cur = -1;
-        if (prev >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != prev) (void)cudaSetDevice(prev);
-    }
-};
 
 template <class F>
 int guarded(baemm_ctx *ctx, F &&f)

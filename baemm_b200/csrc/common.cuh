@@ -44,6 +44,31 @@ extern std::atomic<long long> g_devbuf_epoch;
         if (!(cond)) throw ::baemm::Error((code), (msg));                                   \
     } while (0)
 
+// Makes a device current for one entry-point call and restores the caller's
+// device afterwards, so contexts on different GPUs can be driven from one
+// thread (allocations, streams and launches all belong to the context's
+// device) and a host framework's device selection is left as it was.
+struct DeviceScope
+{
+    int prev = -1;
+    explicit DeviceScope(int dev)   // dev < 0: only restore the caller's device at the end
+    {
+        if (cudaGetDevice(&prev) != cudaSuccess)
+        {
+            (void)cudaGetLastError();
+            prev = -1;
+        }
+        if (dev >= 0 && prev != dev) BAEMM_CUDA(cudaSetDevice(dev));
+    }
+    ~DeviceScope()
+    {
+        int cur = -1;
+        if (prev >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != prev) (void)cudaSetDevice(prev);
+    }
+    DeviceScope(const DeviceScope &) = delete;
+    DeviceScope &operator=(const DeviceScope &) = delete;
+};
+
 // Grow-only device buffer.
 template <class T>
 struct DevBuf

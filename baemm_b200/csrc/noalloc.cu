@@ -89,7 +89,7 @@ extern "C" int baemm_apply_boundary_operators_noalloc_dev_c(baemm_ctx *ctx, cons
                       "problem too large for the no-alloc scratch: 2 * simplex_count * wave_count * 8 bytes = " +
                           std::to_string(2 * tri_elems * sizeof(float2)) + " > " +
                           std::to_string(kNoAllocScratchBytes) + " bytes (use the allocating apply)");
-        BAEMM_CUDA(cudaSetDevice(c.device));
+        DeviceScope scope(c.device);   // restores the caller's device on return
         float2 *Bt = scratch_for(c.device);
         float2 *Ct = Bt + tri_elems;
         const bool layers = c.flags.any_layer();
