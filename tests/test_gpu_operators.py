@@ -498,6 +498,34 @@ def test_two_contexts_from_one_thread_keep_the_callers_device(env):
         H2.close()
 
 
+@pytest.mark.parametrize("mode", [APPLY_FP32, APPLY_TC, APPLY_FP64])
+def test_apply_at_the_maximum_wave_count(mode):
+    """wave_count 512, the largest the API takes (8 wavenumbers x 64 columns):
+    the tensor-core form runs its largest chunk count (32 groups of 16
+    columns, 8 passes of 4).  One more chunk is refused with ERR_SIZE."""
+    coords, tris = meshes.icosphere(2)
+    nv = coords.shape[0]
+    kap = np.linspace(1.0, 8.0, 8)
+    coeff = np.array([[0.25 + 1j, 1 + 0.5j, 1 - 2j, 0.3j]] * 8)
+    rng = np.random.default_rng(11)
+    B, C0 = crandn(rng, nv, 512), crandn(rng, nv, 512)
+    Cg = C0.copy()
+    H = Helmholtz_CUDA(coords, tris, np.eye(3))
+    try:
+        H.SetApplyMode(mode)
+        H.ApplyBoundaryOperators_PL(0.5 - 1j, B, 0.25, Cg, kap, coeff, 512, 64)
+        with pytest.raises(BaemmError, match="ERR_SIZE"):
+            Z = np.zeros((nv, 576), complex)
+            H.ApplyBoundaryOperators_PL(1.0, Z, 0.0, Z.copy(), np.linspace(1.0, 9.0, 9),
+                                        np.array([[0, 1, 0, 0]] * 9), 576, 64)
+    finally:
+        H.close()
+    o = O.Oracle(coords, tris, np.eye(3), precision=64)
+    Co = C0.copy()
+    o.ApplyBoundaryOperators_PL(0.5 - 1j, B, 0.25, Co, kap, coeff, 512, 64)
+    assert relerr(Cg, Co) < (1e-11 if mode == APPLY_FP64 else 3e-5)
+
+
 def test_error_statuses(env):
     coords, tris, meas, H, o32, o64 = env
     B = np.zeros((coords.shape[0], 16), complex)
