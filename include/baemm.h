@@ -54,7 +54,8 @@ typedef enum baemm_status
 #define BAEMM_APPLY_FP32 0   /* plain: FP32 generation and FP32 SIMT contraction */
 #define BAEMM_APPLY_TC   1   /* compensated: split hi+lo operands on the tensor cores, FP32 accumulate;
                               * needs wave_chunk_size a multiple of 16 and wave_count <= 512, other
-                              * shapes run the plain FP32 kernel */
+                              * shapes run the plain FP32 kernel; FP32 values below 1.2e-38 are
+                              * flushed to zero in this form */
 #define BAEMM_APPLY_FP64 2   /* FP64 generation and contraction */
 
 /* Solver statistics of the last GMRES / CG run (the reference discards them,
