@@ -9,7 +9,7 @@ import pytest
 
 from baemm_b200 import APPLY_FP32, APPLY_FP64, APPLY_TC, BaemmError, Helmholtz_CUDA, WaveType, _capi, meshes
 from oracle import oracle as O
-from tests.helpers import crandn, relerr
+from tests.helpers import crandn, relerr, tiny_meshes
 
 pytestmark = pytest.mark.gpu
 
@@ -526,25 +526,13 @@ def test_apply_at_the_maximum_wave_count(mode):
     assert relerr(Cg, Co) < (1e-11 if mode == APPLY_FP64 else 3e-5)
 
 
-def _tiny_meshes():
-    tri1 = (np.array([[0.0, 0, 0], [1, 0, 0], [0, 1, 0.2]]), np.array([[0, 1, 2]]))
-    quad2 = (np.array([[0.0, 0, 0], [1, 0, 0], [1, 1, 0.3], [0, 1, 0]]), np.array([[0, 1, 2], [0, 2, 3]]))
-    tetra = (np.array([[1.0, 1, 1], [1, -1, -1], [-1, 1, -1], [-1, -1, 1]]),
-             np.array([[0, 1, 2], [0, 3, 1], [0, 2, 3], [1, 3, 2]]))
-    # a strip of 17 triangles over 10 lower and 9 upper vertices (all used)
-    xs = np.arange(10, dtype=float)
-    strip_v = np.concatenate([np.stack([xs, 0 * xs, 0 * xs], 1), np.stack([xs[:9], 1 + 0 * xs[:9], 0.1 * xs[:9]], 1)])
-    strip_t = [[i, i + 1, 10 + i] for i in range(9)] + [[i + 1, 11 + i, 10 + i] for i in range(8)]
-    return {"tri1": tri1, "quad2": quad2, "tetra": tetra, "strip17": (strip_v, np.array(strip_t))}
-
-
 @pytest.mark.parametrize("mode", [APPLY_FP32, APPLY_TC, APPLY_FP64])
 @pytest.mark.parametrize("name", ["tri1", "quad2", "tetra", "strip17"])
 def test_apply_on_tiny_meshes(mode, name):
     """Meshes of 1, 2, 4 and 17 triangles: one partly filled source tile and
     target block, every row but a few past the end (masked), the self pair of
     each target inside the only tile."""
-    coords, tris = _tiny_meshes()[name]
+    coords, tris = tiny_meshes()[name]
     nv = coords.shape[0]
     coeff = np.array([[0.25 + 1j, 1 + 0.5j, 1 - 2j, 0.3j]])
     rng = np.random.default_rng(12)

@@ -5,7 +5,7 @@ import numpy as np
 import pytest
 
 from oracle import oracle as O
-from tests.helpers import crandn, relerr
+from tests.helpers import crandn, relerr, tiny_meshes
 
 
 def _oracle_for(golden, precision):
@@ -158,6 +158,26 @@ def test_oracle_vs_live_reference_kernel(sphere3):
     coeff = np.array([[0, 0.3 - 1j, 2.0 + 0.5j, -1.0j]] * 2)
     Cref = O.ref_boundary(mid, nrm, B, kappa, O.scaled_coefficients(coeff), 16)
     assert relerr(o.boundary_kernel_tri(B, kappa, coeff, 32, 16), Cref) < 3e-6
+
+
+@pytest.mark.skipif(not O.ref_available(), reason="oracle/_ref not built here")
+@pytest.mark.parametrize("name", ["tri1", "quad2", "tetra", "strip17"])
+def test_oracle_vs_live_reference_kernel_on_tiny_meshes(name):
+    """Meshes of 1, 2, 4 and 17 triangles (the GPU edge-case meshes): the FP32
+    restatement equals the reference's own kernel, and the FP64 twin agrees
+    to FP32 rounding, so the GPU tests on these meshes check against a pinned
+    oracle."""
+    coords, tris = tiny_meshes()[name]
+    rng = np.random.default_rng(13)
+    o32 = O.Oracle(coords, tris, np.eye(3), precision=32)
+    o64 = O.Oracle(coords, tris, np.eye(3), precision=64)
+    mid, nrm, _, _ = o32.geometry()
+    B = crandn(rng, tris.shape[0], 16, dtype=np.complex64)
+    kappa = np.array([3.0])
+    coeff = np.array([[0.25 + 1j, 1 + 0.5j, 1 - 2j, 0.3j]])
+    Cref = O.ref_boundary(mid, nrm, B, kappa, O.scaled_coefficients(coeff), 16)
+    assert relerr(o32.boundary_kernel_tri(B, kappa, coeff, 16, 16), Cref) < 3e-6
+    assert relerr(o64.boundary_kernel_tri(B.astype(np.complex128), kappa, coeff, 16, 16), Cref) < 1e-5
 
 
 def _self_integral_quadrature(p0, p1, p2, nq=4000):
