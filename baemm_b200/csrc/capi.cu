@@ -80,9 +80,9 @@ int create_impl(const double *coords, int64_t nv, const int32_t *tris, int64_t n
         g_create_error = "invalid mesh arguments";
         return BAEMM_ERR_ARG;
     }
-    if (nt > (int64_t)1 << 30 || nv > (int64_t)1 << 30)
+    if (nt > baemm::kMaxMeshSize || nv > baemm::kMaxMeshSize)
     {
-        g_create_error = "mesh too large";
+        g_create_error = "mesh too large (at most 2^28 triangles and vertices)";
         return BAEMM_ERR_SIZE;
     }
     for (int64_t e = 0; e < 3 * nt; ++e)
@@ -253,6 +253,12 @@ int baemm_create(const double *coords, int64_t nv, const int64_t *tris, int64_t 
                  int device, int cpu_threads, baemm_ctx **out)
 {
     if (!tris || nt <= 0) return create_impl(coords, nv, nullptr, nt, meas, nm, device, cpu_threads, out);
+    if (nt > baemm::kMaxMeshSize || nv > baemm::kMaxMeshSize)   // before any index is read
+    {
+        g_create_error = "mesh too large (at most 2^28 triangles and vertices)";
+        if (out) *out = nullptr;
+        return BAEMM_ERR_SIZE;
+    }
     std::vector<int32_t> t(3 * nt);
     for (int64_t e = 0; e < 3 * nt; ++e)
     {
@@ -271,7 +277,8 @@ int baemm_set_mesh(baemm_ctx *ctx, const double *coords, int64_t nv, const int64
 {
     return guarded(ctx, [&](Ctx &c) {
         BAEMM_REQUIRE(coords && tris && nv > 0 && nt > 0, BAEMM_ERR_ARG, "invalid mesh arguments");
-        BAEMM_REQUIRE(nt <= (int64_t)1 << 30 && nv <= (int64_t)1 << 30, BAEMM_ERR_SIZE, "mesh too large");
+        BAEMM_REQUIRE(nt <= baemm::kMaxMeshSize && nv <= baemm::kMaxMeshSize, BAEMM_ERR_SIZE,
+                      "mesh too large (at most 2^28 triangles and vertices)");
         std::vector<int32_t> t(3 * nt);
         for (int64_t e = 0; e < 3 * nt; ++e)
         {

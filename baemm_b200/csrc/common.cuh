@@ -44,6 +44,11 @@ extern std::atomic<long long> g_devbuf_epoch;
         if (!(cond)) throw ::baemm::Error((code), (msg));                                   \
     } while (0)
 
+// Largest mesh (triangles, vertices) a context takes.  The host topology and
+// the device sparse operators index with int32: AvOp^T holds 3 nt entries and
+// the mass matrix at most nv + 6 nt, both below 2^31 at this size.
+constexpr int64_t kMaxMeshSize = (int64_t)1 << 28;
+
 // Makes a device current for one entry-point call and restores the caller's
 // device afterwards, so contexts on different GPUs can be driven from one
 // thread (allocations, streams and launches all belong to the context's

@@ -47,6 +47,23 @@ def test_create_rejects_bad_mesh_on_host():
     assert st == 1
 
 
+def test_create_refuses_meshes_beyond_the_int32_sparse_limit():
+    """More than 2^28 triangles or vertices: BAEMM_ERR_SIZE from both index
+    widths, before any triangle index is read (the arrays here are tiny)."""
+    L = _capi.lib()
+    coords, tris = meshes.icosphere(0)
+    t32 = tris.astype(np.int32)
+    big = (1 << 28) + 1
+    for nv, nt in ((coords.shape[0], big), (big, tris.shape[0])):
+        h = C.c_void_p()
+        st = L.baemm_create(coords.ctypes.data_as(_capi.dp), nv, tris.ctypes.data_as(_capi.i64p), nt, None, 0, 0,
+                            1, C.byref(h))
+        assert st == 6 and not h.value and b"too large" in L.baemm_last_error(None)
+        st = L.baemm_create_i32(coords.ctypes.data_as(_capi.dp), nv, t32.ctypes.data_as(_capi.i32p), nt, None, 0,
+                                0, 1, C.byref(h))
+        assert st == 6 and not h.value
+
+
 def test_null_context_is_rejected():
     L = _capi.lib()
     assert L.baemm_synchronize(None) == 1
