@@ -177,6 +177,7 @@ static void nearfield_host(Ctx &c, const S *alpha, const S *B, int64_t ldB, cons
     if (c.wave_chunk_count < 1 || !(c.flags.sl() || c.flags.dl())) return;
     BAEMM_REQUIRE(ldB >= wc && ldC >= wc, BAEMM_ERR_ARG, "leading dimension smaller than wave_count");
     BAEMM_REQUIRE(npts >= 0, BAEMM_ERR_ARG, "negative evaluation point count");
+    BAEMM_REQUIRE(npts <= baemm::kMaxMeshSize, BAEMM_ERR_SIZE, "at most 2^28 evaluation points per call");
     if (npts == 0) return;
     BAEMM_REQUIRE(points, BAEMM_ERR_ARG, "null evaluation points");
     static_assert(sizeof(T) == 2 * sizeof(S), "complex layout");

@@ -419,6 +419,7 @@ void Ctx::apply_nearfield(Text alpha, const Text *B, int64_t ldB, Text beta, Tex
     if (!nf.any_layer()) return;
     BAEMM_REQUIRE(ldB >= wave_count && ldC >= wave_count, BAEMM_ERR_ARG, "leading dimension smaller than wave_count");
     BAEMM_REQUIRE(npts >= 0, BAEMM_ERR_ARG, "negative evaluation point count");
+    BAEMM_REQUIRE(npts <= kMaxMeshSize, BAEMM_ERR_SIZE, "at most 2^28 evaluation points per call");
     if (npts == 0) return;
     BAEMM_REQUIRE(pts3, BAEMM_ERR_ARG, "null evaluation points");
     const int64_t tri_elems = mesh.nt * wave_count, pt_elems = npts * wave_count;

@@ -293,7 +293,8 @@ int baemm_apply_boundary_operators_rows_dev_c(baemm_ctx *ctx, const float alpha[
  * The reference writes C_out with leading dimension wave_count whatever ldC_out
  * is (ApplyNearFieldOperators.hpp:76,112-116); here ldC is honoured (the same
  * when ldC == wave_count).  A point that coincides with a triangle midpoint
- * gives non-finite values in its row, as in the reference (r = 0). */
+ * gives non-finite values in its row, as in the reference (r = 0).  At most
+ * 2^28 points per call (BAEMM_ERR_SIZE beyond). */
 int baemm_apply_near_field_operators_z(baemm_ctx *ctx, const double alpha[2], const double *B_in, int64_t ldB,
                                        const double beta[2], double *C_out, int64_t ldC,
                                        const double *evaluation_points, int64_t point_count);
