@@ -80,9 +80,9 @@ int create_impl(const double *coords, int64_t nv, const int32_t *tris, int64_t n
         g_create_error = "invalid mesh arguments";
         return BAEMM_ERR_ARG;
     }
-    if (nt > baemm::kMaxMeshSize || nv > baemm::kMaxMeshSize)
+    if (nt > baemm::kMaxMeshSize || nv > baemm::kMaxMeshSize || nm > baemm::kMaxMeshSize)
     {
-        g_create_error = "mesh too large (at most 2^28 triangles and vertices)";
+        g_create_error = "mesh too large (at most 2^28 triangles, vertices and measurement directions)";
         return BAEMM_ERR_SIZE;
     }
     for (int64_t e = 0; e < 3 * nt; ++e)

@@ -82,8 +82,8 @@ typedef void (*baemm_real_op)(const double *x, double *y, void *user);
  * (Helmholtz_OpenCL.hpp:109-159; pass device = 0).  coords: nv x 3,
  * triangles: nt x 3 (0-based), meas_directions: nm x 3.  cpu_threads is
  * accepted for signature parity and bounds the host threads of set-up.
- * At most 2^28 triangles and 2^28 vertices (BAEMM_ERR_SIZE beyond: the sparse
- * operators index with int32). */
+ * At most 2^28 triangles, vertices and measurement directions each
+ * (BAEMM_ERR_SIZE beyond: the sparse operators and kernels index with int32). */
 int baemm_create(const double *coords, int64_t vertex_count,
                  const int64_t *triangles, int64_t simplex_count,
                  const double *meas_directions, int64_t meas_count,
