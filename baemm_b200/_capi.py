@@ -118,7 +118,9 @@ SIGNATURES = {
     "baemm_apply_near_field_operators_dev_z": (I, [vp, dp, vp, I64, dp, vp, I64, vp, I64]),
     "baemm_apply_near_field_operators_dev_c": (I, [vp, fp, vp, I64, fp, vp, I64, vp, I64]),
     "baemm_create_incident_wave_z": (I, [vp, dp, dp, I, dp, dp, I64, dp, dp, I, I, I]),
+    "baemm_create_incident_wave_loaded_z": (I, [vp, dp, dp, dp, dp, I64, I]),
     "baemm_create_herglotz_wave_z": (I, [vp, dp, dp, I64, dp, dp, I64, dp, dp, I, I]),
+    "baemm_create_herglotz_wave_loaded_z": (I, [vp, dp, dp, I64, dp, dp, I64]),
     "baemm_apply_mass_inverse_z": (I, [vp, dp, I64, dp, I64, I, D]),
     "baemm_apply_mass_inverse_d": (I, [vp, dp, I64, dp, I64, I, D]),
     "baemm_apply_lumped_mass_inverse_z": (I, [vp, dp, I64, dp, I64, I]),

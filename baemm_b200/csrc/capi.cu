@@ -242,6 +242,46 @@ static void ensure_du_dn(Ctx &c, const double *kappa, int wcc, const double *inc
     }
 }
 
+namespace
+{
+// The weak incident wave with the loaded parameters (CreateIncidentWave.hpp:55-124):
+// wave_chunk_size directions; C untouched without loaded chunks or without a
+// single- or double-layer coefficient, as in the reference.
+void incident_host(Ctx &c, const double alpha[2], const double *dirs, const double beta[2], double *C, int64_t ldC,
+                   int type)
+{
+    if (c.wave_chunk_count < 1) return;
+    const int wc = c.wave_count;
+    BAEMM_REQUIRE(ldC >= wc, BAEMM_ERR_ARG, "leading dimension smaller than wave_count");
+    if (!(c.flags.sl() || c.flags.dl())) return;
+    const int64_t nv = c.mesh.nv;
+    double2 *dC = c.io_b.reserve(nv * wc);
+    if (!is_zero(beta)) h2d_block<double2>(c, dC, reinterpret_cast<const double2 *>(C), nv, wc, ldC);
+    c.incident(zz(alpha), dirs, zz(beta), dC, wc, type);
+    d2h_block<double2>(c, reinterpret_cast<double2 *>(C), ldC, dC, nv, wc);
+    c.sync();
+}
+
+// The weak Herglotz wave of g (meas_count x wave_count) with the loaded
+// parameters (CreateHerglotzWave.hpp:51-95).
+void herglotz_host(Ctx &c, const double alpha[2], const double *g, int64_t ldg, const double beta[2], double *C,
+                   int64_t ldC)
+{
+    if (c.wave_chunk_count < 1) return;
+    BAEMM_REQUIRE(c.mesh.nm > 0, BAEMM_ERR_SIZE, "no measurement directions");
+    const int wc = c.wave_count;
+    BAEMM_REQUIRE(ldg >= wc && ldC >= wc, BAEMM_ERR_ARG, "leading dimension smaller than wave_count");
+    if (!(c.flags.sl() || c.flags.dl())) return;
+    const int64_t nv = c.mesh.nv, nm = c.mesh.nm;
+    double2 *dg = c.io_a.reserve(nm * wc), *dC = c.io_b.reserve(nv * wc);
+    h2d_block<double2>(c, dg, reinterpret_cast<const double2 *>(g), nm, wc, ldg);
+    if (!is_zero(beta)) h2d_block<double2>(c, dC, reinterpret_cast<const double2 *>(C), nv, wc, ldC);
+    c.herglotz(zz(alpha), dg, wc, zz(beta), dC, wc);
+    d2h_block<double2>(c, reinterpret_cast<double2 *>(C), ldC, dC, nv, wc);
+    c.sync();
+}
+} // namespace
+
 extern "C" {
 
 int baemm_create_i32(const double *coords, int64_t nv, const int32_t *tris, int64_t nt, const double *meas,
@@ -671,14 +711,16 @@ int baemm_create_incident_wave_z(baemm_ctx *ctx, const double alpha[2], const do
         BAEMM_REQUIRE(inc_count >= wcs, BAEMM_ERR_ARG,
                       "number of incident waves has to match the size of the wave chunks");
         c.load_parameters(kappa, reinterpret_cast<const zc *>(coeff), wc, wcs, 4.0 * M_PI);
-        BAEMM_REQUIRE(ldC >= wc, BAEMM_ERR_ARG, "leading dimension smaller than wave_count");
-        if (!(c.flags.sl() || c.flags.dl())) return;
-        const int64_t nv = c.mesh.nv;
-        double2 *dC = c.io_b.reserve(nv * wc);
-        if (!is_zero(beta)) h2d_block<double2>(c, dC, reinterpret_cast<const double2 *>(C), nv, wc, ldC);
-        c.incident(zz(alpha), dirs, zz(beta), dC, wc, type);
-        d2h_block<double2>(c, reinterpret_cast<double2 *>(C), ldC, dC, nv, wc);
-        c.sync();
+        incident_host(c, alpha, dirs, beta, C, ldC, type);
+    });
+}
+
+int baemm_create_incident_wave_loaded_z(baemm_ctx *ctx, const double alpha[2], const double *dirs,
+                                        const double beta[2], double *C, int64_t ldC, int type)
+{
+    return guarded(ctx, [&](Ctx &c) {
+        BAEMM_REQUIRE(dirs && C, BAEMM_ERR_ARG, "null argument");
+        incident_host(c, alpha, dirs, beta, C, ldC, type);
     });
 }
 
@@ -690,15 +732,16 @@ int baemm_create_herglotz_wave_z(baemm_ctx *ctx, const double alpha[2], const do
         BAEMM_REQUIRE(g && C, BAEMM_ERR_ARG, "null argument");
         BAEMM_REQUIRE(c.mesh.nm > 0, BAEMM_ERR_SIZE, "no measurement directions");
         c.load_parameters(kappa, reinterpret_cast<const zc *>(coeff), wc, wcs, 4.0 * M_PI / (double)c.mesh.nm);
-        BAEMM_REQUIRE(ldg >= wc && ldC >= wc, BAEMM_ERR_ARG, "leading dimension smaller than wave_count");
-        if (!(c.flags.sl() || c.flags.dl())) return;
-        const int64_t nv = c.mesh.nv, nm = c.mesh.nm;
-        double2 *dg = c.io_a.reserve(nm * wc), *dC = c.io_b.reserve(nv * wc);
-        h2d_block<double2>(c, dg, reinterpret_cast<const double2 *>(g), nm, wc, ldg);
-        if (!is_zero(beta)) h2d_block<double2>(c, dC, reinterpret_cast<const double2 *>(C), nv, wc, ldC);
-        c.herglotz(zz(alpha), dg, wc, zz(beta), dC, wc);
-        d2h_block<double2>(c, reinterpret_cast<double2 *>(C), ldC, dC, nv, wc);
-        c.sync();
+        herglotz_host(c, alpha, g, ldg, beta, C, ldC);
+    });
+}
+
+int baemm_create_herglotz_wave_loaded_z(baemm_ctx *ctx, const double alpha[2], const double *g, int64_t ldg,
+                                        const double beta[2], double *C, int64_t ldC)
+{
+    return guarded(ctx, [&](Ctx &c) {
+        BAEMM_REQUIRE(g && C, BAEMM_ERR_ARG, "null argument");
+        herglotz_host(c, alpha, g, ldg, beta, C, ldC);
     });
 }
 

@@ -506,27 +506,65 @@ class Helmholtz_CUDA:
                 _dp(C_out.view(np.float64)), C_out.shape[1], _dp(P), P.shape[0]))
         return C_out
 
-    def CreateIncidentWave_PL(self, alpha, incident_directions, beta, C_out, kappa, coeff, wave_count,
-                              wave_chunk_size, wave_type=WaveType.Plane):
-        """C_out = alpha * wave + beta * C_out (CreateIncidentWave.hpp:21-50)."""
+    def CreateIncidentWave_PL(self, alpha, incident_directions, beta, C_out, *args, wave_type=None):
+        """C_out = alpha * wave + beta * C_out, the weak incident waves.  The
+        reference's two overloads:
+            CreateIncidentWave_PL(alpha, directions, beta, C_out, kappa, coeff, wave_count,
+                                  wave_chunk_size[, wave_type])
+                (CreateIncidentWave.hpp:21-50; loads the parameters with factor 4 pi)
+            CreateIncidentWave_PL(alpha, directions, beta, C_out[, wave_type])
+                (CreateIncidentWave.hpp:55-124; the loaded parameters, wave_chunk_size directions)
+        wave_type defaults to WaveType.Plane."""
         _check_out(C_out, np.complex128, "C_out")
+        if C_out.shape[0] < self.VertexCount():
+            raise ValueError("C_out must hold vertex_count rows")
         d = _f64(incident_directions).reshape(-1, 3)
-        k, c = _f64(kappa), _coeff(coeff)
-        self._ck(self._lib.baemm_create_incident_wave_z(
-            self._h, _dp(_cz(alpha)), _dp(d), d.shape[0], _dp(_cz(beta)), _dp(C_out.view(np.float64)),
-            C_out.shape[1], _dp(k), _dp(c.view(np.float64)), int(wave_count), int(wave_chunk_size),
-            int(wave_type)))
+        if len(args) in (4, 5):
+            kappa, coeff, wave_count, wave_chunk_size = args[:4]
+            wt = args[4] if len(args) == 5 else (WaveType.Plane if wave_type is None else wave_type)
+            k, c = _f64(kappa), _coeff(coeff)
+            self._ck(self._lib.baemm_create_incident_wave_z(
+                self._h, _dp(_cz(alpha)), _dp(d), d.shape[0], _dp(_cz(beta)), _dp(C_out.view(np.float64)),
+                C_out.shape[1], _dp(k), _dp(c.view(np.float64)), int(wave_count), int(wave_chunk_size), int(wt)))
+        elif len(args) in (0, 1):
+            wt = args[0] if args else (WaveType.Plane if wave_type is None else wave_type)
+            if d.shape[0] < self.GetWaveChunkSize():
+                raise ValueError("the loaded-parameter overload reads wave_chunk_size incident directions")
+            self._ck(self._lib.baemm_create_incident_wave_loaded_z(
+                self._h, _dp(_cz(alpha)), _dp(d), _dp(_cz(beta)), _dp(C_out.view(np.float64)), C_out.shape[1],
+                int(wt)))
+        else:
+            raise TypeError("CreateIncidentWave_PL(alpha, directions, beta, C_out, [kappa, coeff, wave_count, "
+                            "wave_chunk_size,] [wave_type])")
         return C_out
 
-    def CreateHerglotzWave_PL(self, alpha, g, beta, C_out, kappa, coeff, wave_count, wave_chunk_size):
-        """C_out = alpha * HerglotzWave(g) + beta * C_out (CreateHerglotzWave.hpp:25-44)."""
+    def CreateHerglotzWave_PL(self, alpha, g, beta, C_out, *args):
+        """C_out = alpha * HerglotzWave(g) + beta * C_out, g meas_count x wave_count.
+        The reference's two overloads:
+            CreateHerglotzWave_PL(alpha, g, beta, C_out, kappa, coeff, wave_count, wave_chunk_size)
+                (CreateHerglotzWave.hpp:25-44; loads with factor 4 pi / meas_count)
+            CreateHerglotzWave_PL(alpha, g, beta, C_out)
+                (CreateHerglotzWave.hpp:51-95; the loaded parameters)"""
         _check_out(C_out, np.complex128, "C_out")
+        if C_out.shape[0] < self.VertexCount():
+            raise ValueError("C_out must hold vertex_count rows")
         G = np.ascontiguousarray(g, dtype=np.complex128)
-        k, c = _f64(kappa), _coeff(coeff)
-        self._ck(self._lib.baemm_create_herglotz_wave_z(
-            self._h, _dp(_cz(alpha)), _dp(G.view(np.float64)), G.shape[1], _dp(_cz(beta)),
-            _dp(C_out.view(np.float64)), C_out.shape[1], _dp(k), _dp(c.view(np.float64)), int(wave_count),
-            int(wave_chunk_size)))
+        if len(args) == 4:
+            kappa, coeff, wave_count, wave_chunk_size = args
+            k, c = _f64(kappa), _coeff(coeff)
+            self._ck(self._lib.baemm_create_herglotz_wave_z(
+                self._h, _dp(_cz(alpha)), _dp(G.view(np.float64)), G.shape[1], _dp(_cz(beta)),
+                _dp(C_out.view(np.float64)), C_out.shape[1], _dp(k), _dp(c.view(np.float64)), int(wave_count),
+                int(wave_chunk_size)))
+        elif not args:
+            if G.shape[0] < self.GetMeasCount():
+                raise ValueError("g must hold meas_count rows")
+            self._ck(self._lib.baemm_create_herglotz_wave_loaded_z(
+                self._h, _dp(_cz(alpha)), _dp(G.view(np.float64)), G.shape[1], _dp(_cz(beta)),
+                _dp(C_out.view(np.float64)), C_out.shape[1]))
+        else:
+            raise TypeError("CreateHerglotzWave_PL(alpha, g, beta, C_out[, kappa, coeff, wave_count, "
+                            "wave_chunk_size])")
         return C_out
 
     def ApplyMassInverse(self, X, Y, cg_tol, nrhs=None):

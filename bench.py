@@ -614,7 +614,7 @@ def run_solve_workload(args):
     kap = np.array([4.0, 8.0])
     H = Helmholtz_CUDA(coords, tris, meas)
 
-    # the weak incident wave FarField solves for (c1 = -1 after the 1/(4 pi) scaling)
+    # the weak incident wave of FarField, scaled by 4 pi (the boundary-density errors are relative)
     wave = np.zeros((coords.shape[0], 32), complex)
     H.CreateIncidentWave_PL(1.0, inc, 0.0, wave, kap, [[0, -4 * np.pi, 0, 0]] * 2, 32, 16)
 

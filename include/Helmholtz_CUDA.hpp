@@ -330,6 +330,24 @@ public:
             copy_block(C.data(), (Int)wave_count_, C_out, ldC_out, VertexCount(), (Int)wave_count_);
     }
 
+    // The overload with the loaded parameters (CreateIncidentWave.hpp:55-124): the
+    // parameters of the last LoadParameters call, wave_chunk_size directions.
+    template <typename R_ext, typename C_ext, typename I_ext>
+    void CreateIncidentWave_PL(const C_ext alpha, const R_ext *incident_directions, const C_ext beta, C_ext *C_out,
+                               const I_ext ldC_out, WaveType type)
+    {
+        const Int wc = GetWaveCount(), wcs = GetWaveChunkSize();
+        if (wc < 1) return;   // nothing loaded: C_out untouched, as in the reference
+        auto d = to_d(incident_directions, 3 * (size_t)wcs);
+        std::vector<std::complex<double>> C((size_t)VertexCount() * wc);
+        copy_block(C_out, ldC_out, C.data(), wc, VertexCount(), wc);
+        const double a[2] = {(double)alpha.real(), (double)alpha.imag()};
+        const double b[2] = {(double)beta.real(), (double)beta.imag()};
+        if (check(baemm_create_incident_wave_loaded_z(ctx_, a, d.data(), b, dd(C.data()), wc, (int)type),
+                  "CreateIncidentWave_PL"))
+            copy_block(C.data(), wc, C_out, ldC_out, VertexCount(), wc);
+    }
+
     template <typename R_ext, typename C_ext, typename I_ext>
     void CreateHerglotzWave_PL(const C_ext alpha, const C_ext *B_in, const I_ext ldB_in, const C_ext beta,
                                C_ext *C_out, const I_ext ldC_out, const R_ext *kappa_list, const C_ext *coeff_list,
@@ -348,6 +366,23 @@ public:
                                                (int)wave_chunk_size_),
                   "CreateHerglotzWave_PL"))
             copy_block(C.data(), (Int)wave_count_, C_out, ldC_out, VertexCount(), (Int)wave_count_);
+    }
+
+    // The overload with the loaded parameters (CreateHerglotzWave.hpp:51-95).
+    template <typename C_ext, typename I_ext>
+    void CreateHerglotzWave_PL(const C_ext alpha, const C_ext *B_in, const I_ext ldB_in, const C_ext beta,
+                               C_ext *C_out, const I_ext ldC_out)
+    {
+        const Int wc = GetWaveCount();
+        if (wc < 1) return;   // nothing loaded: C_out untouched, as in the reference
+        auto g = to_z_block(B_in, GetMeasCount(), wc, ldB_in);
+        std::vector<std::complex<double>> C((size_t)VertexCount() * wc);
+        copy_block(C_out, ldC_out, C.data(), wc, VertexCount(), wc);
+        const double a[2] = {(double)alpha.real(), (double)alpha.imag()};
+        const double b[2] = {(double)beta.real(), (double)beta.imag()};
+        if (check(baemm_create_herglotz_wave_loaded_z(ctx_, a, dd(g.data()), wc, b, dd(C.data()), wc),
+                  "CreateHerglotzWave_PL"))
+            copy_block(C.data(), wc, C_out, ldC_out, VertexCount(), wc);
     }
 
     // ---- mass inverse (ApplyMassInverse.hpp) --------------------------------------------

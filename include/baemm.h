@@ -324,12 +324,23 @@ int baemm_create_incident_wave_z(baemm_ctx *ctx, const double alpha[2], const do
                                  int inc_count, const double beta[2], double *C_out, int64_t ldC,
                                  const double *kappa, const double *coeff, int wave_count, int wave_chunk_size,
                                  int wave_type);
+/* The overload with the loaded parameters (CreateIncidentWave.hpp:55-124):
+ * the parameters of the last baemm_load_parameters call (factor as given
+ * there; the overload above loads with 4 pi), wave_chunk_size directions.
+ * C_out is left untouched when nothing is loaded or neither layer is present. */
+int baemm_create_incident_wave_loaded_z(baemm_ctx *ctx, const double alpha[2], const double *incident_directions,
+                                        const double beta[2], double *C_out, int64_t ldC, int wave_type);
 
 /* CreateHerglotzWave_PL (CreateHerglotzWave.hpp:25-44): weak-form Herglotz
  * waves of the kernel g (meas_count x wave_count). */
 int baemm_create_herglotz_wave_z(baemm_ctx *ctx, const double alpha[2], const double *g, int64_t ldg,
                                  const double beta[2], double *C_out, int64_t ldC,
                                  const double *kappa, const double *coeff, int wave_count, int wave_chunk_size);
+/* The overload with the loaded parameters (CreateHerglotzWave.hpp:51-95):
+ * the parameters of the last baemm_load_parameters call (the overload above
+ * loads with factor 4 pi / meas_count). */
+int baemm_create_herglotz_wave_loaded_z(baemm_ctx *ctx, const double alpha[2], const double *g, int64_t ldg,
+                                        const double beta[2], double *C_out, int64_t ldC);
 
 /* ApplyMassInverse (ApplyMassInverse.hpp:6-156): Y = M^-1 X by CG
  * (<= 20 iterations, lumped-mass preconditioner).  _z: nrhs complex columns,

@@ -50,6 +50,15 @@ int main()
     std::vector<Complex> coeff = {Complex(0), Complex(1), Complex(1), Complex(0)};
     H.ApplyNearFieldOperators_PL(Complex(1), B.data(), wave_count, Complex(0), P.data(), wave_count, kappa.data(),
                                  coeff.data(), wave_count, wave_chunk_size, pts.data(), Int(2));
+    // the waves, both overloads of each (the second form uses the loaded parameters)
+    std::vector<Complex> W(6 * wave_count), G(2 * wave_count, Complex(1.0, 0.0));
+    H.CreateIncidentWave_PL(Complex(1), inc.data(), wave_chunk_size, Complex(0), W.data(), wave_count, kappa.data(),
+                            coeff.data(), wave_count, wave_chunk_size, WaveType::Plane);
+    H.LoadParameters(kappa.data(), coeff.data(), wave_count, wave_chunk_size, Real(4 * M_PI));
+    H.CreateIncidentWave_PL(Complex(1), inc.data(), Complex(0), W.data(), wave_count, WaveType::Plane);
+    H.CreateHerglotzWave_PL(Complex(1), G.data(), wave_count, Complex(0), W.data(), wave_count, kappa.data(),
+                            coeff.data(), wave_count, wave_chunk_size);
+    H.CreateHerglotzWave_PL(Complex(1), G.data(), wave_count, Complex(0), W.data(), wave_count);
     const auto &curl = H.CurlOperator();
     std::printf("near field %g, CurlOp rows %lld\n", std::abs(P[0]), (long long)curl.rows);
     std::vector<double> mesh_coords;

@@ -392,6 +392,46 @@ def test_incident_wave(env, wtype, mode):
 
 
 @pytest.mark.parametrize("mode", [APPLY_FP32, APPLY_FP64])
+@pytest.mark.parametrize("wtype", [WaveType.Plane, WaveType.Radial])
+def test_wave_overloads_with_loaded_parameters(env, mode, wtype):
+    """The reference's second CreateIncidentWave_PL / CreateHerglotzWave_PL
+    overloads (CreateIncidentWave.hpp:55-124, CreateHerglotzWave.hpp:51-95) use
+    the loaded parameters; after LoadParameters with the factor the first
+    overloads use (4 pi, 4 pi / meas_count) they give the same blocks bit for
+    bit.  With nothing loaded they leave C_out untouched."""
+    coords, tris, meas, H, o32, o64 = env
+    nv = coords.shape[0]
+    wc, wcs, kap = WAVES["w32"]
+    coeff = np.array([[0, -1j * k, 1, 0] for k in kap])
+    rng = np.random.default_rng(14)
+    dirs = meshes.fibonacci_sphere(wcs) * (2.5 if wtype == WaveType.Radial else 1.0)
+    g = crandn(rng, meas.shape[0], wc)
+    C0 = crandn(rng, nv, wc)
+    H.SetApplyMode(mode)
+    try:
+        I1, I2 = C0.copy(), C0.copy()
+        H.CreateIncidentWave_PL(1.0 - 1j, dirs, 0.5, I1, kap, coeff, wc, wcs, wtype)
+        H.LoadParameters(kap, coeff, wc, wcs, 4 * np.pi)
+        H.CreateIncidentWave_PL(1.0 - 1j, dirs, 0.5, I2, wtype)
+        G1, G2 = C0.copy(), C0.copy()
+        H.CreateHerglotzWave_PL(0.5, g, -1.0, G1, kap, coeff, wc, wcs)
+        H.LoadParameters(kap, coeff, wc, wcs, 4 * np.pi / meas.shape[0])
+        H.CreateHerglotzWave_PL(0.5, g, -1.0, G2)
+    finally:
+        H.SetApplyMode(APPLY_FP32)
+    assert np.array_equal(I1, I2) and np.array_equal(G1, G2)
+    assert relerr(I1, C0) > 1e-3 and relerr(G1, C0) > 1e-3
+    fresh = Helmholtz_CUDA(coords, tris, meas)
+    try:
+        C = C0.copy()
+        fresh.CreateIncidentWave_PL(1.0, dirs, 0.0, C, wtype)
+        fresh.CreateHerglotzWave_PL(1.0, g, 0.0, C)
+        assert np.array_equal(C, C0)
+    finally:
+        fresh.close()
+
+
+@pytest.mark.parametrize("mode", [APPLY_FP32, APPLY_FP64])
 def test_mass_inverse_and_lumped(env, mode):
     """CG mass inverse (20 iterations max).  The FP32 path uses the float mass
     values of the reference (Sparse_T<float>), which differ from the oracle's in
