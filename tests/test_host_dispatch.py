@@ -1,0 +1,83 @@
+"""Host logic of the Python mirror without a GPU: which C entry point each
+call form of the reference's overloaded wave builders reaches, with which
+wave type, and which malformed calls are refused before any call.  The
+library is replaced by a recorder; nothing runs on a device."""
+import numpy as np
+import pytest
+
+from baemm_b200 import helmholtz
+from baemm_b200.helmholtz import Helmholtz_CUDA, WaveType
+
+
+class _Recorder:
+    def __init__(self):
+        self.calls = []
+
+    def __getattr__(self, name):
+        def entry(*args):
+            self.calls.append((name, args))
+            return 0
+        return entry
+
+
+def _mirror(nv=4, wcs=2, nm=3):
+    H = Helmholtz_CUDA.__new__(Helmholtz_CUDA)
+    H._lib, H._h, H._user_stream, H._device = _Recorder(), None, None, 0
+    H.VertexCount = lambda: nv
+    H.GetWaveChunkSize = lambda: wcs
+    H.GetMeasCount = lambda: nm
+    return H
+
+
+def _last(H):
+    name, args = H._lib.calls[-1]
+    return name, args
+
+
+def test_incident_wave_call_forms():
+    H = _mirror()
+    dirs = np.eye(3)[:2]
+    C = np.zeros((4, 4), complex)
+    H.CreateIncidentWave_PL(1.0, dirs, 0.0, C, [2.0, 3.0], [[0, 1, 0, 0]] * 2, 4, 2)
+    name, args = _last(H)
+    assert name == "baemm_create_incident_wave_z" and args[-1] == int(WaveType.Plane)
+    H.CreateIncidentWave_PL(1.0, dirs, 0.0, C, [2.0, 3.0], [[0, 1, 0, 0]] * 2, 4, 2, WaveType.Radial)
+    assert _last(H)[0] == "baemm_create_incident_wave_z" and _last(H)[1][-1] == int(WaveType.Radial)
+    H.CreateIncidentWave_PL(1.0, dirs, 0.0, C)
+    name, args = _last(H)
+    assert name == "baemm_create_incident_wave_loaded_z" and args[-1] == int(WaveType.Plane)
+    H.CreateIncidentWave_PL(1.0, dirs, 0.0, C, WaveType.Radial)
+    assert _last(H)[1][-1] == int(WaveType.Radial)
+    H.CreateIncidentWave_PL(1.0, dirs, 0.0, C, wave_type=WaveType.Radial)
+    assert _last(H)[1][-1] == int(WaveType.Radial)
+    n = len(H._lib.calls)
+    with pytest.raises(ValueError, match="wave_chunk_size incident directions"):
+        H.CreateIncidentWave_PL(1.0, dirs[:1], 0.0, C)
+    with pytest.raises(TypeError):
+        H.CreateIncidentWave_PL(1.0, dirs, 0.0, C, [2.0], [[0, 1, 0, 0]])
+    with pytest.raises(ValueError, match="vertex_count rows"):
+        H.CreateIncidentWave_PL(1.0, dirs, 0.0, np.zeros((3, 4), complex))
+    assert len(H._lib.calls) == n   # refused before any call
+
+
+def test_herglotz_wave_call_forms():
+    H = _mirror()
+    g = np.ones((3, 4), complex)
+    C = np.zeros((4, 4), complex)
+    H.CreateHerglotzWave_PL(1.0, g, 0.0, C, [2.0, 3.0], [[0, 1, 0, 0]] * 2, 4, 2)
+    assert _last(H)[0] == "baemm_create_herglotz_wave_z"
+    H.CreateHerglotzWave_PL(1.0, g, 0.0, C)
+    assert _last(H)[0] == "baemm_create_herglotz_wave_loaded_z"
+    n = len(H._lib.calls)
+    with pytest.raises(ValueError, match="meas_count rows"):
+        H.CreateHerglotzWave_PL(1.0, g[:2], 0.0, C)
+    with pytest.raises(TypeError):
+        H.CreateHerglotzWave_PL(1.0, g, 0.0, C, [2.0])
+    with pytest.raises(TypeError):
+        H.CreateHerglotzWave_PL(1.0, g, 0.0, C.astype(np.complex64))
+    assert len(H._lib.calls) == n
+
+
+def test_wave_type_values_match_the_c_header():
+    assert int(WaveType.Plane) == helmholtz._capi.WAVE_PLANE
+    assert int(WaveType.Radial) == helmholtz._capi.WAVE_RADIAL
