@@ -81,3 +81,34 @@ def test_herglotz_wave_call_forms():
 def test_wave_type_values_match_the_c_header():
     assert int(WaveType.Plane) == helmholtz._capi.WAVE_PLANE
     assert int(WaveType.Radial) == helmholtz._capi.WAVE_RADIAL
+
+
+def test_apply_call_forms():
+    """ApplyBoundaryOperators_PL / ApplyFarFieldOperators_PL /
+    ApplyNearFieldOperators_PL on host blocks: the overload with parameters
+    loads (and for the boundary apply unloads) around the loaded form."""
+    H = _mirror()
+    B = np.ones((4, 4), complex)
+    C = np.zeros((4, 4), complex)
+    kap, coeff = [2.0, 3.0], [[0, 1, 0, 0]] * 2
+    H.ApplyBoundaryOperators_PL(1.0, B, 0.0, C)
+    assert _last(H)[0] == "baemm_apply_boundary_operators_z"
+    H._lib.calls.clear()
+    H.ApplyBoundaryOperators_PL(1.0, B, 0.0, C, kap, coeff, 4, 2)
+    assert [c[0] for c in H._lib.calls] == ["baemm_load_boundary_operators", "baemm_apply_boundary_operators_z",
+                                            "baemm_unload_boundary_operators"]
+    H.ApplyBoundaryOperators_PL(1.0, B.astype(np.complex64), 0.0, C.astype(np.complex64))
+    assert _last(H)[0] == "baemm_apply_boundary_operators_c"
+    F = np.zeros((3, 4), complex)
+    H.ApplyFarFieldOperators_PL(1.0, B, 0.0, F)
+    assert _last(H)[0] == "baemm_apply_far_field_operators_loaded_z"
+    H.ApplyFarFieldOperators_PL(1.0, B, 0.0, F, kap, coeff, 4, 2)
+    assert _last(H)[0] == "baemm_apply_far_field_operators_z"
+    P = np.zeros((5, 4), complex)
+    pts = np.zeros((5, 3))
+    H.ApplyNearFieldOperators_PL(1.0, B, 0.0, P, pts)
+    assert _last(H)[0] == "baemm_apply_near_field_operators_z" and _last(H)[1][-1] == 5
+    H.ApplyNearFieldOperators_PL(1.0, B, 0.0, P, kap, coeff, 4, 2, pts)
+    assert _last(H)[0] == "baemm_apply_near_field_operators_full_z"
+    with pytest.raises(TypeError):
+        H.ApplyNearFieldOperators_PL(1.0, B, 0.0, P, kap, pts)
