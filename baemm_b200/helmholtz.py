@@ -77,6 +77,24 @@ def _check_dev(t, dtype, rows, cols, device, name):
                          f"row stride {t.stride(0)})")
 
 
+def _check_host(a, dtype, rows, name, cols=None, exact_cols=False, allow_1d=False):
+    """A host block the library writes in place (or reads without a copy): a
+    C-contiguous numpy array of `dtype` with at least `rows` rows and `cols`
+    columns, exactly `cols` where the entry point takes no leading dimension."""
+    ok_dim = a.ndim == 2 or (allow_1d and a.ndim == 1) if isinstance(a, np.ndarray) else False
+    if not (ok_dim and a.dtype == dtype and a.flags.c_contiguous):
+        raise TypeError(f"{name} must be a C-contiguous numpy array of dtype {np.dtype(dtype).name}")
+    c = a.shape[1] if a.ndim == 2 else 1
+    if a.shape[0] < rows or (cols is not None and (c != cols if exact_cols else c < cols)):
+        want = f"{rows} x {cols}" if cols is not None else f"{rows} rows of"
+        raise ValueError(f"{name} must hold {want} entries (got shape {a.shape})")
+
+
+def _need_rows(a, rows, name):
+    if a.shape[0] < rows:
+        raise ValueError(f"{name} must hold {rows} rows (got shape {a.shape})")
+
+
 def _check_out(a, dtype, name):
     if not (isinstance(a, np.ndarray) and a.dtype == dtype and a.ndim == 2 and a.flags.c_contiguous):
         raise TypeError(f"{name} must be a C-contiguous 2-D numpy array of dtype {np.dtype(dtype).name}")
@@ -376,12 +394,16 @@ class Helmholtz_CUDA:
             elif isinstance(B_in, np.ndarray) and B_in.dtype == np.complex64:
                 _check_out(C_out, np.complex64, "C_out")
                 B = np.ascontiguousarray(B_in)
+                _need_rows(B, self.VertexCount(), "B_in")
+                _need_rows(C_out, self.VertexCount(), "C_out")
                 self._ck(self._lib.baemm_apply_boundary_operators_c(
                     self._h, _fp(_cc(alpha)), _fp(B.view(np.float32)), B.shape[1], _fp(_cc(beta)),
                     _fp(C_out.view(np.float32)), C_out.shape[1]))
             else:
                 _check_out(C_out, np.complex128, "C_out")
                 B = np.ascontiguousarray(B_in, dtype=np.complex128)
+                _need_rows(B, self.VertexCount(), "B_in")
+                _need_rows(C_out, self.VertexCount(), "C_out")
                 self._ck(self._lib.baemm_apply_boundary_operators_z(
                     self._h, _dp(_cz(alpha)), _dp(B.view(np.float64)), B.shape[1], _dp(_cz(beta)),
                     _dp(C_out.view(np.float64)), C_out.shape[1]))
@@ -408,6 +430,8 @@ class Helmholtz_CUDA:
             return C_out
         _check_out(C_out, np.complex128, "C_out")
         B = np.ascontiguousarray(B_in, dtype=np.complex128)
+        _need_rows(B, self.VertexCount(), "B_in")
+        _need_rows(C_out, self.GetMeasCount(), "C_out")
         if kappa is not None:
             k, c = _f64(kappa), _coeff(coeff)
             self._ck(self._lib.baemm_apply_far_field_operators_z(
@@ -487,6 +511,8 @@ class Helmholtz_CUDA:
             _check_out(C_out, np.complex64, "C_out")
             B = np.ascontiguousarray(B_in)
             P = np.ascontiguousarray(points, dtype=np.float32).reshape(-1, 3)
+            _need_rows(B, self.VertexCount(), "B_in")
+            _need_rows(C_out, P.shape[0], "C_out")
             self._ck(self._lib.baemm_apply_near_field_operators_c(
                 self._h, _fp(_cc(alpha)), _fp(B.view(np.float32)), B.shape[1], _fp(_cc(beta)),
                 _fp(C_out.view(np.float32)), C_out.shape[1], _fp(P), P.shape[0]))
@@ -494,6 +520,8 @@ class Helmholtz_CUDA:
         _check_out(C_out, np.complex128, "C_out")
         B = np.ascontiguousarray(B_in, dtype=np.complex128)
         P = _f64(points).reshape(-1, 3)
+        _need_rows(B, self.VertexCount(), "B_in")
+        _need_rows(C_out, P.shape[0], "C_out")
         if kappa is not None:
             k, c = _f64(kappa), _coeff(coeff)
             self._ck(self._lib.baemm_apply_near_field_operators_full_z(
@@ -569,10 +597,12 @@ class Helmholtz_CUDA:
 
     def ApplyMassInverse(self, X, Y, cg_tol, nrhs=None):
         """Y = M^-1 X by CG (ApplyMassInverse.hpp:6-156); real or complex columns."""
+        nv = self.VertexCount()
         if np.iscomplexobj(X):
             Xc = np.ascontiguousarray(X, dtype=np.complex128)
-            _check_out(Y, np.complex128, "Y")
             n = Xc.shape[1] if nrhs is None else nrhs
+            _need_rows(Xc, nv, "X")
+            _check_host(Y, np.complex128, nv, "Y", n)
             self._ck(self._lib.baemm_apply_mass_inverse_z(self._h, _dp(Xc.view(np.float64)), Xc.shape[1],
                                                           _dp(Y.view(np.float64)), Y.shape[1], int(n),
                                                           float(cg_tol)))
@@ -580,21 +610,28 @@ class Helmholtz_CUDA:
             Xr = _f64(X)
             if Xr.ndim == 1:
                 Xr = Xr[:, None]
-            Yv = Y if Y.ndim == 2 else Y.reshape(-1, 1)
             n = Xr.shape[1] if nrhs is None else nrhs
+            _need_rows(Xr, nv, "X")
+            _check_host(Y, np.float64, nv, "Y", n, allow_1d=True)
+            Yv = Y if Y.ndim == 2 else Y.reshape(-1, 1)
             self._ck(self._lib.baemm_apply_mass_inverse_d(self._h, _dp(Xr), Xr.shape[1], _dp(Yv), Yv.shape[1],
                                                           int(n), float(cg_tol)))
         return Y
 
     def ApplyLumpedMassInverse(self, X, Y, nrhs=None):
+        nv = self.VertexCount()
         if np.iscomplexobj(X):
             Xc = np.ascontiguousarray(X, dtype=np.complex128)
             n = Xc.shape[1] if nrhs is None else nrhs
+            _need_rows(Xc, nv, "X")
+            _check_host(Y, np.complex128, nv, "Y", n)
             self._ck(self._lib.baemm_apply_lumped_mass_inverse_z(self._h, _dp(Xc.view(np.float64)), Xc.shape[1],
                                                                  _dp(Y.view(np.float64)), Y.shape[1], int(n)))
         else:
             Xr = _f64(X)
             n = Xr.shape[1] if nrhs is None else nrhs
+            _need_rows(Xr, nv, "X")
+            _check_host(Y, np.float64, nv, "Y", n)
             self._ck(self._lib.baemm_apply_lumped_mass_inverse_d(self._h, _dp(Xr), Xr.shape[1], _dp(Y), Y.shape[1],
                                                                  int(n)))
         return Y
@@ -602,6 +639,8 @@ class Helmholtz_CUDA:
     def MassDot(self, alpha, X, beta, Y):
         """Y = alpha M X + beta Y on real columns (MassMatrix().Dot)."""
         Xr = _f64(X)
+        _need_rows(Xr, self.VertexCount(), "X")
+        _check_host(Y, np.float64, self.VertexCount(), "Y", Xr.shape[1])
         self._ck(self._lib.baemm_mass_dot_d(self._h, float(alpha), _dp(Xr), Xr.shape[1], float(beta), _dp(Y),
                                             Y.shape[1], Xr.shape[1]))
         return Y
@@ -614,7 +653,7 @@ class Helmholtz_CUDA:
                             gmres_tol=1e-4):
         k = _f64(kappa)
         d = _f64(inc_directions).reshape(-1, 3)
-        _check_out(Y_out, np.complex128, "Y_out")
+        _check_host(Y_out, np.complex128, self.GetMeasCount(), "Y_out", k.size * d.shape[0], exact_cols=True)
         e = _f64(eta) if eta is not None else None
         self._ck(self._lib.baemm_far_field_parameters(self._h, _dp(k), k.size, _dp(d), d.shape[0],
                                                       _dp(Y_out.view(np.float64)), int(wave_type),
@@ -625,6 +664,10 @@ class Helmholtz_CUDA:
     def BoundaryPotential(self, kappa, coeff_out, wave, phi, wave_chunk_size, cg_tol, gmres_tol):
         k = _f64(kappa)
         W = np.ascontiguousarray(wave, dtype=np.complex128)
+        wc, nv = k.size * int(wave_chunk_size), self.VertexCount()
+        _check_host(W, np.complex128, nv, "wave", wc, exact_cols=True)
+        _check_host(phi, np.complex128, nv, "phi", wc, exact_cols=True)
+        _check_host(coeff_out, np.complex128, k.size, "coeff_out", 4, exact_cols=True)
         self._ck(self._lib.baemm_boundary_potential(self._h, _dp(k), _dp(coeff_out.view(np.float64)),
                                                     _dp(W.view(np.float64)), _dp(phi.view(np.float64)), k.size,
                                                     int(wave_chunk_size), float(cg_tol), float(gmres_tol)))
@@ -633,6 +676,9 @@ class Helmholtz_CUDA:
     def DirichletToNeumann(self, kappa, wave, neumann_trace, wave_chunk_size, cg_tol, gmres_tol):
         k = _f64(kappa)
         W = np.ascontiguousarray(wave, dtype=np.complex128)
+        wc, nv = k.size * int(wave_chunk_size), self.VertexCount()
+        _check_host(W, np.complex128, nv, "wave", wc, exact_cols=True)
+        _check_host(neumann_trace, np.complex128, nv, "neumann_trace", wc, exact_cols=True)
         self._ck(self._lib.baemm_dirichlet_to_neumann(self._h, _dp(k), _dp(W.view(np.float64)),
                                                       _dp(neumann_trace.view(np.float64)), k.size,
                                                       int(wave_chunk_size), float(cg_tol), float(gmres_tol)))
@@ -642,14 +688,17 @@ class Helmholtz_CUDA:
                              gmres_tol=1e-4):
         k = _f64(kappa)
         d = _f64(inc_directions).reshape(-1, 3)
+        _check_host(du_dn, np.complex128, self.VertexCount(), "du_dn", k.size * d.shape[0], exact_cols=True)
         self._ck(self._lib.baemm_derivative_ff_helper(self._h, _dp(k), k.size, _dp(d), d.shape[0],
                                                       _dp(du_dn.view(np.float64)), int(wave_type), float(cg_tol),
                                                       float(gmres_tol)))
         return du_dn
 
-    def _du_dn_ptr(self, du_dn):
+    def _du_dn_ptr(self, du_dn, wc=None):
         if du_dn is None:
             return _capi.dp()   # NULL: the library callocs and fills it
+        if wc is not None:
+            _check_host(du_dn, np.complex128, self.VertexCount(), "du_dn", wc, exact_cols=True)
         return du_dn.view(np.float64).ctypes.data_as(_capi.dp)
 
     def _take_du_dn(self, ptr, du_dn, wc):
@@ -666,7 +715,10 @@ class Helmholtz_CUDA:
         k = _f64(kappa)
         d = _f64(inc_directions).reshape(-1, 3)
         X = _f64(X_in).reshape(-1, 3)
-        ptr = self._du_dn_ptr(du_dn)
+        wc = k.size * d.shape[0]
+        _need_rows(X, self.VertexCount(), "X_in")
+        _check_host(Y_out, np.complex128, self.GetMeasCount(), "Y_out", wc, exact_cols=True)
+        ptr = self._du_dn_ptr(du_dn, wc)
         self._ck(self._lib.baemm_derivative_ff(self._h, _dp(k), k.size, _dp(d), d.shape[0], _dp(X),
                                                _dp(Y_out.view(np.float64)), C.byref(ptr), int(wave_type),
                                                float(cg_tol), float(gmres_tol)))
@@ -677,7 +729,10 @@ class Helmholtz_CUDA:
         k = _f64(kappa)
         d = _f64(inc_directions).reshape(-1, 3)
         G = np.ascontiguousarray(g, dtype=np.complex128)
-        ptr = self._du_dn_ptr(du_dn)
+        wc = k.size * d.shape[0]
+        _check_host(G, np.complex128, self.GetMeasCount(), "g", wc, exact_cols=True)
+        _check_host(Y_out, np.float64, self.VertexCount(), "Y_out", 3, exact_cols=True)
+        ptr = self._du_dn_ptr(du_dn, wc)
         self._ck(self._lib.baemm_adjoint_derivative_ff(self._h, _dp(k), k.size, _dp(d), d.shape[0],
                                                        _dp(G.view(np.float64)), _dp(Y_out), C.byref(ptr),
                                                        int(wave_type), float(cg_tol), float(gmres_tol)))
@@ -695,6 +750,8 @@ class Helmholtz_CUDA:
         d = _f64(inc_directions).reshape(-1, 3)
         n = self.VertexCount()
         B = _f64(B_in)
+        _check_host(B, np.float64, n, "B_in", 3)
+        _check_host(X_out, np.float64, n, "X_out", 3)
 
         def wrap(f):
             def cb(x, y, _user):
@@ -704,7 +761,7 @@ class Helmholtz_CUDA:
             return _capi.REAL_OP(cb)
 
         Mc, Pc = wrap(M), wrap(P)
-        ptr = self._du_dn_ptr(du_dn)
+        ptr = self._du_dn_ptr(du_dn, k.size * d.shape[0])
         ok = C.c_int(0)
         self._ck(self._lib.baemm_gauss_newton_solve(self._h, _dp(k), k.size, _dp(d), d.shape[0], Mc, None, Pc, None,
                                                     float(alpha), _dp(B), B.shape[1], float(beta), _dp(X_out),

@@ -112,3 +112,63 @@ def test_apply_call_forms():
     assert _last(H)[0] == "baemm_apply_near_field_operators_full_z"
     with pytest.raises(TypeError):
         H.ApplyNearFieldOperators_PL(1.0, B, 0.0, P, kap, pts)
+
+
+def test_host_blocks_are_checked_before_any_call():
+    """Blocks the library reads or writes through plain pointers must hold the
+    rows and columns it will touch: too few rows, another dtype, a strided
+    output, or (where the entry point has no leading dimension) another column
+    count is refused before any call; the shapes the reference uses pass."""
+    nv, nm = 4, 3
+    H = _mirror(nv=nv, nm=nm)
+    kap, inc = np.array([2.0, 3.0]), np.eye(3)[:2]          # wave_count 2 x 2 = 4
+    ok = [
+        lambda: H.ApplyMassInverse(np.ones((nv, 2), complex), np.zeros((nv, 2), complex), 1e-10),
+        lambda: H.ApplyMassInverse(np.ones((nv, 3)), np.zeros((nv, 3)), 1e-10),
+        lambda: H.ApplyMassInverse(np.ones(nv), np.zeros(nv), 1e-10),
+        lambda: H.ApplyLumpedMassInverse(np.ones((nv, 3)), np.zeros((nv, 3))),
+        lambda: H.MassDot(1.0, np.ones((nv, 3)), 0.0, np.zeros((nv, 3))),
+        lambda: H.FarField(kap, inc, np.zeros((nm, 4), complex)),
+        lambda: H.BoundaryPotential(kap, np.zeros((2, 4), complex), np.ones((nv, 4), complex),
+                                    np.zeros((nv, 4), complex), 2, 1e-10, 1e-10),
+        lambda: H.DirichletToNeumann(kap, np.ones((nv, 4), complex), np.zeros((nv, 4), complex), 2, 1e-10, 1e-10),
+        lambda: H.Derivative_FF_Helper(kap, inc, np.zeros((nv, 4), complex)),
+        lambda: H.Derivative_FF(kap, inc, np.ones((nv, 3)), np.zeros((nm, 4), complex), np.zeros((nv, 4), complex)),
+        lambda: H.AdjointDerivative_FF(kap, inc, np.ones((nm, 4), complex), np.zeros((nv, 3)),
+                                       np.zeros((nv, 4), complex)),
+        lambda: H.GaussNewtonSolve(kap, inc, None, None, 1.0, np.ones((nv, 3)), 0.0, np.zeros((nv, 3)),
+                                   np.zeros((nv, 4), complex)),
+    ]
+    for f in ok:
+        n = len(H._lib.calls)
+        f()
+        assert len(H._lib.calls) > n
+    bad = [
+        lambda: H.ApplyMassInverse(np.ones((nv, 2), complex), np.zeros((nv - 1, 2), complex), 1e-10),
+        lambda: H.ApplyMassInverse(np.ones((nv - 1, 2), complex), np.zeros((nv, 2), complex), 1e-10),
+        lambda: H.ApplyMassInverse(np.ones((nv, 3)), np.zeros((nv, 3), np.float32), 1e-10),
+        lambda: H.ApplyMassInverse(np.ones((nv, 3)), np.zeros((nv, 6))[:, ::2], 1e-10),
+        lambda: H.ApplyLumpedMassInverse(np.ones((nv, 3)), np.zeros((nv, 2))),
+        lambda: H.MassDot(1.0, np.ones((nv, 3)), 0.0, np.zeros((nv - 1, 3))),
+        lambda: H.FarField(kap, inc, np.zeros((nm, 5), complex)),
+        lambda: H.FarField(kap, inc, np.zeros((nm - 1, 4), complex)),
+        lambda: H.BoundaryPotential(kap, np.zeros((2, 4), complex), np.ones((nv, 4), complex),
+                                    np.zeros((nv, 3), complex), 2, 1e-10, 1e-10),
+        lambda: H.BoundaryPotential(kap, np.zeros((1, 4), complex), np.ones((nv, 4), complex),
+                                    np.zeros((nv, 4), complex), 2, 1e-10, 1e-10),
+        lambda: H.DirichletToNeumann(kap, np.ones((nv - 1, 4), complex), np.zeros((nv, 4), complex), 2, 1e-10,
+                                     1e-10),
+        lambda: H.Derivative_FF_Helper(kap, inc, np.zeros((nv, 3), complex)),
+        lambda: H.Derivative_FF(kap, inc, np.ones((nv - 1, 3)), np.zeros((nm, 4), complex)),
+        lambda: H.AdjointDerivative_FF(kap, inc, np.ones((nm, 4), complex), np.zeros((nv, 3), np.float32)),
+        lambda: H.GaussNewtonSolve(kap, inc, None, None, 1.0, np.ones((nv, 3)), 0.0, np.zeros((nv, 2)), None),
+        lambda: H.ApplyBoundaryOperators_PL(1.0, np.ones((nv - 1, 4), complex), 0.0, np.zeros((nv, 4), complex)),
+        lambda: H.ApplyFarFieldOperators_PL(1.0, np.ones((nv, 4), complex), 0.0, np.zeros((nm - 1, 4), complex)),
+        lambda: H.ApplyNearFieldOperators_PL(1.0, np.ones((nv, 4), complex), 0.0, np.zeros((2, 4), complex),
+                                             np.zeros((3, 3))),
+    ]
+    for f in bad:
+        n = len(H._lib.calls)
+        with pytest.raises((TypeError, ValueError)):
+            f()
+        assert len(H._lib.calls) == n
