@@ -68,7 +68,8 @@ def build(clean: bool = False, verbose: bool = False, ptxas_verbose: bool = Fals
     if todo:
         n = jobs or min(len(todo), os.cpu_count() or 4)
         with cf.ThreadPoolExecutor(max_workers=n) as ex:
-            futs = {ex.submit(_compile, s, o, extra + FILE_FLAGS.get(os.path.basename(s), [])): s for s, o in todo}
+            futs = {ex.submit(_compile, s, o, extra + FILE_FLAGS.get(os.path.basename(s), [])): s
+                    for s, o in todo}
             for f in cf.as_completed(futs):
                 msg = f.result()
                 if (verbose or ptxas_verbose) and msg:
