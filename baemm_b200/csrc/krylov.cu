@@ -485,9 +485,9 @@ __global__ void update_x_kernel(int64_t n, int c, int jend, const S *__restrict_
     x[e] = acc;
 }
 
-template <class S>
 // r = b - Ax; r may be Ax (the restart computes it in place), so those two
 // are not restrict-qualified.
+template <class S>
 __global__ void residual_kernel(int64_t total, const S *__restrict__ b, const S *Ax, S *r)
 {
     const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
