@@ -230,16 +230,6 @@ __device__ __forceinline__ void split_tf32(float x, uint32_t &hi, uint32_t &lo)
     lo = __float_as_uint(x - __uint_as_float(hi));
 }
 
-// Cheaper split for the generated kernel entries (two instructions): hi is x
-// itself, of which the tensor core reads the top 19 bits (x truncated to
-// TF32); lo = x - trunc(x) is exact, |lo| < 2^-10 |x|, and the bits of lo the
-// tensor core drops are below 2^-20 |x|.
-__device__ __forceinline__ void split_tf32_trunc(float x, uint32_t &hi, uint32_t &lo)
-{
-    hi = __float_as_uint(x);
-    lo = __float_as_uint(x - __uint_as_float(hi & 0xffffe000u));
-}
-
 __device__ __forceinline__ void tmem_st16(uint32_t taddr, const uint32_t (&v)[16])
 {
     asm volatile("tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, "
