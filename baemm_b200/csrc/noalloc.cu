@@ -1,16 +1,16 @@
 // An allocation-free variant of the device-pointer boundary-operator apply
 // (baemm_apply_boundary_operators_noalloc_dev_c in include/baemm.h).
 //
-// Who needs it: callers that must not call cudaMalloc while they run -- code
-// that enqueues the apply inside CUDA stream capture (a cudaMalloc during a
-// capture invalidates it), latency-critical loops for which cudaMalloc's
-// implicit device synchronisation is unacceptable, and host frameworks that
-// own all device memory through their own pool and forbid allocations behind
-// their back.  The regular apply keeps its triangle-level intermediate blocks
-// (B_tri = AvOp B and C_tri = K B_tri, 2 * simplex_count * wave_count complex64)
-// in grow-only cudaMalloc'ed buffers of the context; this variant places them
-// in one file-scope __device__ array of fixed size instead, so the call itself
-// allocates nothing and frees nothing.
+// Who needs it: callers that cannot call cudaMalloc while they run -- host
+// frameworks that own all device memory through their own pool or a fixed
+// budget and forbid allocations behind their back, long-running servers that
+// must not grow their device footprint after start-up, and latency-critical
+// loops for which cudaMalloc's and cudaFree's implicit device synchronisation
+// is unacceptable.  The regular apply keeps its triangle-level intermediate
+// blocks (B_tri = AvOp B and C_tri = K B_tri, 2 * simplex_count * wave_count
+// complex64) in grow-only cudaMalloc'ed buffers of the context; this variant
+// places them in one file-scope __device__ array of fixed size instead, so the
+// call itself allocates nothing and frees nothing.
 //
 // Costs and rules:
 //   * The array (kNoAllocScratchBytes = 32 MiB) is reserved on every GPU that
@@ -19,15 +19,19 @@
 //     2 * simplex_count * wave_count * 8 bytes must fit in 32 MiB.
 //   * The device address of the array is looked up (cudaGetSymbolAddress) the
 //     first time the entry point runs on a device, with that device current;
-//     make that first call before any stream capture begins.
+//     make that first call before any stream capture begins.  The address is
+//     cached per device ordinal for the life of the process, so
+//     cudaDeviceReset is not supported while the library is loaded.
 //   * All calls share the one array and it keeps the last call's contents.
 //     Both halves are fully overwritten by every call before they are read, so
 //     nothing needs clearing; but calls whose work overlaps on the GPU (two
 //     streams, two contexts on one device) race on the array and must be
 //     serialised by the caller.
 //   * Only the plain FP32 apply mode is offered; the operators must have been
-//     loaded with baemm_load_boundary_operators beforehand.
+//     loaded with baemm_load_boundary_operators beforehand.  The call records
+//     no phase timings (baemm_last_apply_times reports none after it).
 #include <mutex>
+#include <new>
 
 #include "ctx.cuh"
 
@@ -76,6 +80,7 @@ extern "C" int baemm_apply_boundary_operators_noalloc_dev_c(baemm_ctx *ctx, cons
     using namespace baemm;
     if (!ctx || !ctx->impl) return BAEMM_ERR_ARG;
     Ctx &c = *ctx->impl;
+    c.prof_valid = false;   // no phase timings for this call
     try
     {
         c.require_loaded();
@@ -120,5 +125,15 @@ extern "C" int baemm_apply_boundary_operators_noalloc_dev_c(baemm_ctx *ctx, cons
     {
         c.last_error = e.what();
         return e.code;
+    }
+    catch (const std::bad_alloc &)
+    {
+        c.last_error = "host allocation failed";
+        return BAEMM_ERR_ALLOC;
+    }
+    catch (const std::exception &e)   // e.g. std::system_error from the mutex
+    {
+        c.last_error = e.what();
+        return BAEMM_ERR_ARG;
     }
 }

@@ -232,16 +232,20 @@ int baemm_apply_boundary_operators_dev_z(baemm_ctx *ctx, const double alpha[2], 
 int baemm_apply_boundary_operators_dev_c(baemm_ctx *ctx, const float alpha[2], const float *B_in, int64_t ldB,
                                          const float beta[2], float *C_out, int64_t ldC);
 /* Allocation-free variant of baemm_apply_boundary_operators_dev_c.  No
- * counterpart in the reference.  For callers that must not allocate device
- * memory while they run (inside CUDA stream capture, latency-critical loops,
- * hosts that own all device memory): the triangle-level intermediate blocks
- * live in one fixed 32 MiB __device__ array of the library instead of
- * cudaMalloc'ed buffers, so the call allocates and frees nothing.
+ * counterpart in the reference.  For callers that cannot allocate device
+ * memory while they run (hosts that own all device memory through their own
+ * pool or budget, servers that must not grow their footprint after start-up,
+ * loops that cannot afford cudaMalloc's implicit synchronisation): the
+ * triangle-level intermediate blocks live in one fixed 32 MiB __device__
+ * array of the library instead of cudaMalloc'ed buffers, so the call
+ * allocates and frees nothing.
  * Limit: 2 * simplex_count * wave_count * 8 bytes <= 32 MiB, else
  * BAEMM_ERR_SIZE.  Plain FP32 apply mode only; operators loaded beforehand.
  * The array's device address is looked up on the first call on a device
- * (make it before any stream capture).  All calls share the array: calls
- * that overlap on the GPU race and must be serialised by the caller. */
+ * (make it before any stream capture) and cached for the process, so
+ * cudaDeviceReset is not supported while the library is loaded.  All calls
+ * share the array: calls that overlap on the GPU race and must be serialised
+ * by the caller.  The call records no phase timings. */
 int baemm_apply_boundary_operators_noalloc_dev_c(baemm_ctx *ctx, const float alpha[2], const float *B_in,
                                                  int64_t ldB, const float beta[2], float *C_out, int64_t ldC);
 /* The overload that loads, applies and unloads in one call
@@ -279,6 +283,19 @@ int baemm_apply_boundary_operators_rows_dev_z(baemm_ctx *ctx, const double alpha
 int baemm_apply_boundary_operators_rows_dev_c(baemm_ctx *ctx, const float alpha[2], const float *B_in, int64_t ldB,
                                               const float beta[2], float *C_out, int64_t ldC, int64_t row_begin,
                                               int64_t row_end, int with_mass);
+
+/* The dense stage alone, the device counterpart of the reference's private
+ * BoundaryOperatorKernel() (BoundaryOperatorKernel.hpp:5-28, kernel
+ * BoundaryOperatorKernel.cl:5-239; no public counterpart): on device
+ * triangle blocks (simplex_count x wave_count, leading dimension wave_count),
+ *   C_tri[i, :] = sum_{j != i} A_ij(kappa) B_tri[j, :],  i in [row_begin, row_end),
+ * with the loaded operators and the current apply mode: _c in the plain FP32
+ * or the tensor-core form, _z in the FP64 form (BAEMM_APPLY_FP64 required).
+ * Rows outside the range are left untouched.  No AvOp, diagonal or mass. */
+int baemm_boundary_operator_kernel_dev_c(baemm_ctx *ctx, const float *B_tri, float *C_tri, int64_t row_begin,
+                                         int64_t row_end);
+int baemm_boundary_operator_kernel_dev_z(baemm_ctx *ctx, const double *B_tri, double *C_tri, int64_t row_begin,
+                                         int64_t row_end);
 
 /* ApplyNearFieldOperators_PL (ApplyNearFieldOperators.hpp:56-122, kernel
  * NearFieldOperatorKernel.cl:5-194): the boundary potential of the vertex

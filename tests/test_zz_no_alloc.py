@@ -1,11 +1,13 @@
 """GPU test of the allocation-free boundary apply (collected last on purpose).
 
 baemm_apply_boundary_operators_noalloc_dev_c serves callers that cannot
-allocate device memory while they run (stream capture, latency-critical loops,
-hosts that own all device memory): its intermediate blocks live in a fixed
-32 MiB device array of the library.  Called through the C ABI, it must give
-the same result as the allocating device-pointer apply, on two calls in a row
-(the array keeps the previous call's contents), and it must reject problems
+allocate device memory while they run (a host framework that owns all device
+memory, a server that must not grow its footprint, a loop that cannot afford
+cudaMalloc's implicit synchronisation): its intermediate blocks live in a fixed
+32 MiB device array of the library.  Called through the C ABI on a fresh
+context, it must leave the free device memory unchanged from its second call
+on, give the same result as the allocating device-pointer apply on two calls in
+a row (the array keeps the previous call's contents), and reject problems
 larger than its array.
 """
 import ctypes as C
@@ -41,16 +43,22 @@ def test_noalloc_apply_matches_allocating_apply_twice():
         rng = np.random.default_rng(99)
         B = torch.from_numpy((rng.standard_normal((coords.shape[0], 32)) +
                               1j * rng.standard_normal((coords.shape[0], 32))).astype(np.complex64)).cuda()
+        # every torch block exists before the first no-alloc call, so torch allocates nothing in between
+        outs = [torch.full_like(B, complex(np.nan, np.nan)) for _ in range(2)]
         C_ref = torch.zeros_like(B)
+        torch.cuda.synchronize()
+        free = []
+        for C_na in outs:   # the first call on this context (array lookup, kernel loading), then a second
+            st = _call(L.baemm_apply_boundary_operators_noalloc_dev_c, H, B, C_na)
+            assert st == 0, L.baemm_last_error(H._h)
+            H.Synchronize()
+            free.append(torch.cuda.mem_get_info()[0])
+        assert free[1] == free[0], "the second no-alloc call changed the free device memory"
         assert _call(L.baemm_apply_boundary_operators_dev_c, H, B, C_ref) == 0
         H.Synchronize()
         ref = C_ref.cpu().numpy()
         assert np.isfinite(ref).all() and np.abs(ref).max() > 0
-        for _ in range(2):
-            C_na = torch.full_like(B, complex(np.nan, np.nan))
-            st = _call(L.baemm_apply_boundary_operators_noalloc_dev_c, H, B, C_na)
-            assert st == 0, L.baemm_last_error(H._h)
-            H.Synchronize()
+        for C_na in outs:
             assert relerr(C_na.cpu().numpy(), ref) < TOL
         H.UnloadBoundaryOperators_PL()
 
