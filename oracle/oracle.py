@@ -21,6 +21,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(HERE, "_build", "liboracle.so")
 REF_SO = os.path.join(HERE, "_ref", "libbaemm_refcl.so")
+REF_FAST_SO = os.path.join(HERE, "_ref", "libbaemm_refcl_fast.so")   # -ffast-math: the timed CPU baseline only
 
 _dp = C.POINTER(C.c_double)
 _fp = C.POINTER(C.c_float)
@@ -29,11 +30,25 @@ _i64p = C.POINTER(C.c_int64)
 
 
 def build(reference_root: str | None = None) -> None:
-    """Compile the restatement, and the reference kernels when the reference tree exists."""
+    """Compile the restatement, and the reference kernels when the reference
+    tree exists (build_ref.sh finds it from the argument, BAEMM_REFERENCE or
+    its own default, and skips cleanly without one)."""
     subprocess.check_call([os.path.join(HERE, "build_oracle.sh")])
-    ref = reference_root or os.environ.get("BAEMM_REFERENCE", "/root/reference")
-    if os.path.isdir(ref):
-        subprocess.check_call([os.path.join(HERE, "build_ref.sh"), ref])
+    ref = reference_root or os.environ.get("BAEMM_REFERENCE")
+    subprocess.check_call([os.path.join(HERE, "build_ref.sh")] + ([ref] if ref else []))
+
+
+def reference_root() -> str | None:
+    """The reference tree: BAEMM_REFERENCE, else the root build_ref.sh last
+    built from (oracle/_ref/REFERENCE_ROOT); None when neither exists."""
+    env = os.environ.get("BAEMM_REFERENCE")
+    if env:
+        return env if os.path.isdir(env) else None
+    rec = os.path.join(HERE, "_ref", "REFERENCE_ROOT")
+    if os.path.exists(rec):
+        root = open(rec).read().strip()
+        return root if os.path.isdir(root) else None
+    return None
 
 
 def _p(a, t=_dp):
@@ -87,6 +102,9 @@ def lib():
             "orc_dot_with_normals": [V, _dp, _dp, D],
             "orc_multiply_with_normals": [V, _dp, _dp, D, D],
             "orc_gmres_dense": [I64, I, _dp, _dp, _dp, I, I, D, C.POINTER(C.c_int)],
+            "orc_boundary_kernel_tri_rows": [V, _dp, _dp, I64, I64],
+            "orc_boundary_kernel_tri_index": [V, _dp, _dp, _i64p, I64],
+            "orc_set_geometry": [V, _dp, _dp],
         }
         for name, args in sig.items():
             getattr(L, name).argtypes = args
@@ -96,23 +114,29 @@ def lib():
     return _lib
 
 
-def ref_available() -> bool:
-    return os.path.exists(REF_SO)
+def ref_available(fast: bool = False) -> bool:
+    return os.path.exists(REF_FAST_SO if fast else REF_SO)
 
 
-def reflib():
+def reflib(fast: bool = False):
+    """The reference kernels compiled as C++: strict IEEE (the parity checker),
+    or fast=True, the -ffast-math build (the timed CPU baseline only)."""
     global _ref
     if _ref is None:
-        if not os.path.exists(REF_SO):
-            raise RuntimeError(f"reference kernel library missing: {REF_SO} (run oracle/build_ref.sh)")
-        _ref = C.CDLL(REF_SO)
-        _ref.refcl_max_threads.restype = C.c_int
+        _ref = {}
+    path = REF_FAST_SO if fast else REF_SO
+    if path not in _ref:
+        if not os.path.exists(path):
+            raise RuntimeError(f"reference kernel library missing: {path} (run oracle/build_ref.sh)")
+        L = C.CDLL(path)
+        L.refcl_max_threads.restype = C.c_int
         F, I = _fp, C.c_int
-        _ref.refcl_boundary.argtypes = [F, F, F, F, F, F, I, I, I, I, I, I]
-        _ref.refcl_farfield.argtypes = [F, F, F, F, F, F, F, I, I, I, I, I, I, I]
-        _ref.refcl_herglotz.argtypes = [F, F, F, F, F, F, F, I, I, I, I, I, I, I]
-        _ref.refcl_nearfield.argtypes = [F, F, F, F, F, F, F, I, I, I, I, I, I, I]
-    return _ref
+        L.refcl_boundary.argtypes = [F, F, F, F, F, F, I, I, I, I, I, I]
+        L.refcl_farfield.argtypes = [F, F, F, F, F, F, F, I, I, I, I, I, I, I]
+        L.refcl_herglotz.argtypes = [F, F, F, F, F, F, F, I, I, I, I, I, I, I]
+        L.refcl_nearfield.argtypes = [F, F, F, F, F, F, F, I, I, I, I, I, I, I]
+        _ref[path] = L
+    return _ref[path]
 
 
 def _c128(a):
@@ -210,6 +234,32 @@ class Oracle:
         Ct = np.zeros_like(Btri)
         lib().orc_boundary_kernel_tri(self._h, _p(Btri.view(np.float64)), _p(Ct.view(np.float64)))
         return Ct
+
+    def boundary_kernel_tri_rows(self, Btri, kappa, coeff, wave_count, wave_chunk_size, row_begin, row_end):
+        """boundary_kernel_tri for target rows [row_begin, row_end) only ((row_end - row_begin) x wc)."""
+        self.LoadParameters(kappa, coeff, wave_count, wave_chunk_size)
+        Btri = _c128(Btri)
+        Ct = np.zeros((row_end - row_begin, wave_count), np.complex128)
+        lib().orc_boundary_kernel_tri_rows(self._h, _p(Btri.view(np.float64)), _p(Ct.view(np.float64)),
+                                           int(row_begin), int(row_end))
+        return Ct
+
+    def boundary_kernel_tri_index(self, Btri, kappa, coeff, wave_count, wave_chunk_size, rows):
+        """boundary_kernel_tri for the target rows `rows` (any order): len(rows) x wc."""
+        self.LoadParameters(kappa, coeff, wave_count, wave_chunk_size)
+        Btri = _c128(Btri)
+        idx = np.ascontiguousarray(rows, np.int64)
+        Ct = np.zeros((idx.shape[0], wave_count), np.complex128)
+        lib().orc_boundary_kernel_tri_index(self._h, _p(Btri.view(np.float64)), _p(Ct.view(np.float64)),
+                                            _p(idx, _i64p), int(idx.shape[0]))
+        return Ct
+
+    def set_geometry(self, mid4, nrm4):
+        """Replace the midpoints and normals the kernels use (n x 4 each), e.g.
+        by another implementation's FP32 geometry, so that kernel arithmetic
+        compares on identical inputs."""
+        m, n = _f64(mid4).reshape(self.nt, 4), _f64(nrm4).reshape(self.nt, 4)
+        lib().orc_set_geometry(self._h, _p(m), _p(n))
 
     def farfield_kernel_tri(self, Btri, kappa, coeff, wave_count, wave_chunk_size):
         self.LoadParameters(kappa, coeff, wave_count, wave_chunk_size)
@@ -384,14 +434,15 @@ def scaled_coefficients(coeff, factor=1.0):
     return out.astype(np.complex64)
 
 
-def ref_boundary(mid4, nrm4, Btri, kappa, coeff_scaled, wave_chunk_size, row_begin=0, row_end=None, threads=0):
+def ref_boundary(mid4, nrm4, Btri, kappa, coeff_scaled, wave_chunk_size, row_begin=0, row_end=None, threads=0,
+                 fast=False):
     mid4 = np.ascontiguousarray(mid4, np.float32); nrm4 = np.ascontiguousarray(nrm4, np.float32)
     Btri = np.ascontiguousarray(Btri, np.complex64)
     n, wc = Btri.shape
     Cout = np.zeros_like(Btri)
     kap = np.ascontiguousarray(kappa, np.float32); co = np.ascontiguousarray(coeff_scaled, np.complex64)
     row_end = n if row_end is None else row_end
-    rc = reflib().refcl_boundary(_p(mid4, _fp), _p(nrm4, _fp), _p(Btri.view(np.float32), _fp),
+    rc = reflib(fast).refcl_boundary(_p(mid4, _fp), _p(nrm4, _fp), _p(Btri.view(np.float32), _fp),
                                  _p(Cout.view(np.float32), _fp), _p(kap, _fp), _p(co.view(np.float32), _fp),
                                  n, wc, int(wave_chunk_size), int(row_begin), int(row_end), int(threads))
     if rc != 0:
@@ -432,7 +483,7 @@ def ref_herglotz(mid4, nrm4, meas4, G, kappa, coeff_scaled, wave_chunk_size, thr
 
 
 def ref_nearfield(mid4, nrm4, Btri, points, kappa, coeff_scaled, wave_chunk_size, row_begin=0, row_end=None,
-                  threads=0):
+                  threads=0, fast=False):
     """The reference's NearFieldOperatorKernel.cl on triangle data: P (m x wc) at points (m x 3)."""
     mid4 = np.ascontiguousarray(mid4, np.float32); nrm4 = np.ascontiguousarray(nrm4, np.float32)
     Btri = np.ascontiguousarray(Btri, np.complex64)
@@ -444,7 +495,7 @@ def ref_nearfield(mid4, nrm4, Btri, points, kappa, coeff_scaled, wave_chunk_size
     Cout = np.zeros((m, wc), np.complex64)
     kap = np.ascontiguousarray(kappa, np.float32); co = np.ascontiguousarray(coeff_scaled, np.complex64)
     row_end = m if row_end is None else row_end
-    rc = reflib().refcl_nearfield(_p(mid4, _fp), _p(nrm4, _fp), _p(Btri.view(np.float32), _fp), _p(pts4, _fp),
+    rc = reflib(fast).refcl_nearfield(_p(mid4, _fp), _p(nrm4, _fp), _p(Btri.view(np.float32), _fp), _p(pts4, _fp),
                                   _p(Cout.view(np.float32), _fp), _p(kap, _fp), _p(co.view(np.float32), _fp),
                                   n, m, wc, int(wave_chunk_size), int(row_begin), int(row_end), int(threads))
     if rc != 0:
