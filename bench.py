@@ -75,16 +75,34 @@ def load_peaks():
     return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0, "source": "of fallback"}
 
 
+KERNEL_SOURCE = {"tc": "tc.cu", "fp32": "dense.cu", "fp64": "dense.cu"}
+
+
+def source_sha16(mode):
+    """Content hash of the source file of this mode's dense kernel."""
+    import hashlib
+    p = os.path.join(ROOT, "baemm_b200", "csrc", KERNEL_SOURCE[mode])
+    return hashlib.sha256(open(p, "rb").read()).hexdigest()[:16]
+
+
 def load_traffic(mode):
-    """Per-launch DRAM bytes (read + write) of the dense kernel on this workload,
-    from the committed ncu summary (profiles/traffic_torus.json), if any."""
+    """Per-launch DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of
+    the dense kernel on this workload, from the committed ncu summary
+    (profiles/traffic_torus.json), with the content hash of the kernel source
+    it was captured on: `stale` when the source has changed since."""
     p = os.path.join(ROOT, "profiles", "traffic_torus.json")
-    if os.path.exists(p):
-        try:
-            return json.load(open(p)).get(mode)
-        except Exception:
-            return None
-    return None
+    if not os.path.exists(p):
+        return None, None
+    try:
+        rec = json.load(open(p)).get(mode)
+    except Exception:
+        return None, None
+    if not isinstance(rec, dict) or "bytes" not in rec:
+        return None, None
+    now = source_sha16(mode)
+    src = {"from": "profiles/traffic_torus.json (ncu, one launch)", "captured_on_source_sha16": rec.get("source_sha16"),
+           "current_source_sha16": now, "stale": rec.get("source_sha16") != now}
+    return int(rec["bytes"]), src
 
 
 # ---------------------------------------------------------------------------
@@ -159,59 +177,102 @@ class ClockSampler:
 # ---------------------------------------------------------------------------
 # the reference's own kernel on the host (CPU baseline and --impl reference)
 # ---------------------------------------------------------------------------
+REF_FLAGS = ("g++ -O3 -march=x86-64-v3 -ffast-math -fopenmp (the counterpart of the reference's "
+             "-cl-fast-relaxed-math, Helmholtz_OpenCL.hpp:77)")
+
+
+class ReferenceRows:
+    """The reference BoundaryOperatorKernel.cl (compiled as C++ with fast math,
+    oracle/_ref/libbaemm_refcl_fast.so) on contiguous blocks of target rows
+    against all sources, OpenMP over rows on every host core.  Cost is
+    separable per target row, so a block's rows/s projects exactly to the full
+    apply; AvOp / AvOp^T (O(N wc)) are left out of the sample."""
+
+    def __init__(self, coords, tris, B_vertex, threads=0):
+        from oracle import oracle as O
+        self.O = O
+        orc = O.Oracle(coords, tris, np.eye(3), precision=32, threads=threads)
+        mid, nrm, area, _ = orc.geometry()
+        self.mid, self.nrm = mid, nrm
+        self.n = tris.shape[0]
+        # B_tri = AvOp B (PL -> PC), as the reference does before the kernel
+        self.Btri = ((area / 3.0)[:, None] * B_vertex[tris].sum(axis=1)).astype(np.complex64)
+        self.cs = O.scaled_coefficients(coefficients(KAPPA))
+        self.threads = threads
+        self.cores = int(threads or O.reflib(fast=True).refcl_max_threads())
+        self.next_row = 0
+
+    def run(self, rows):
+        """Time one block of `rows` target rows (the next block, wrapping around); seconds."""
+        r0 = self.next_row if self.next_row + rows <= self.n else 0
+        self.next_row = r0 + rows
+        t0 = time.perf_counter()
+        self.O.ref_boundary(self.mid, self.nrm, self.Btri, KAPPA, self.cs, WCS, r0, r0 + rows, self.threads,
+                            fast=True)
+        return time.perf_counter() - t0
+
+    def rows_for(self, seconds):
+        """Rows whose block takes about `seconds` (from a short calibration run)."""
+        rows = max(self.cores, 8)
+        dt = self.run(rows)
+        while dt < 0.25 * seconds and rows < self.n:   # short runs are dominated by start-up
+            rows = int(min(self.n, rows * 4))
+            dt = self.run(rows)
+        return int(min(self.n, max(self.cores, rows * seconds / max(dt, 1e-3))))
+
+    def rate(self, rows, dt):
+        return rows * self.n * WC / dt / 1e9
+
+    def sample_text(self, rows):
+        return (f"reference BoundaryOperatorKernel.cl (oracle/_ref, compiled as C++: {REF_FLAGS}) on {rows} "
+                f"contiguous target rows x all {self.n} sources x 64 RHS per step, OpenMP over rows; projected "
+                f"per interaction to the full apply (cost is separable per target row); AvOp/AvOp^T (O(N wc)) "
+                f"not in the sample")
+
+
 def reference_rows_rate(coords, tris, B_vertex, target_seconds=15.0, threads=0):
-    """GInteractions/s of the reference BoundaryOperatorKernel.cl (compiled as
-    C++, oracle/_ref) on a contiguous block of target rows against all sources.
-    Cost is separable per target row, so rows/s scales exactly to the full apply."""
+    """GInteractions/s of the reference kernel on one sample of about
+    `target_seconds` (the GPU line's cpu_baseline)."""
     from oracle import oracle as O
-    if not O.ref_available():
+    if not O.ref_available(fast=True):
         return None
-    orc = O.Oracle(coords, tris, np.eye(3), precision=32, threads=threads)
-    mid, nrm, area, _ = orc.geometry()
-    n = tris.shape[0]
-    # B_tri = AvOp B (PL -> PC), as the reference does before the kernel
-    a3 = (area / 3.0).astype(np.float64)
-    Btri = (a3[:, None] * B_vertex[tris].sum(axis=1)).astype(np.complex64)
-    cs = O.scaled_coefficients(coefficients(KAPPA))
-    nthreads = threads or O.reflib().refcl_max_threads()
-    rows = max(nthreads, 8)
-    t0 = time.perf_counter()
-    O.ref_boundary(mid, nrm, Btri, KAPPA, cs, WCS, 0, rows, threads)
-    dt = time.perf_counter() - t0
-    rows2 = int(min(n - rows, max(rows, rows * target_seconds / max(dt, 1e-3))))
-    t0 = time.perf_counter()
-    O.ref_boundary(mid, nrm, Btri, KAPPA, cs, WCS, rows, rows + rows2, threads)
-    dt = time.perf_counter() - t0
-    inter = rows2 * n * WC
-    return {"value": inter / dt / 1e9, "unit": UNIT, "cores": int(nthreads), "kind": "reference",
-            "seconds": dt, "rows": rows2,
-            "sample": f"reference BoundaryOperatorKernel.cl (oracle/_ref, compiled as C++) on {rows2} contiguous "
-                      f"target rows x all {n} sources x 64 RHS, OpenMP over rows; scaled per interaction "
-                      f"(cost is separable per target row); AvOp/AvOp^T (O(N wc)) not in the sample"}
+    R = ReferenceRows(coords, tris, B_vertex, threads)
+    rows = R.rows_for(target_seconds)
+    dt = R.run(rows)
+    return {"value": R.rate(rows, dt), "unit": UNIT, "cores": R.cores, "kind": "reference", "seconds": dt,
+            "rows": rows, "projected": True, "sample": R.sample_text(rows)}
 
 
 def run_reference_arm(args, rank, world):
+    """--impl reference: rank 0 alone times the reference kernel on the host
+    cores; `warmup` untimed and `steps` timed samples of the same size (about
+    BAEMM_REF_SECONDS, default 4 s, each), every step a different block of
+    target rows."""
     if rank != 0:
         return 0
-    coords, tris, B = build_workload()
-    cpu = reference_rows_rate(coords, tris, B, target_seconds=float(os.environ.get("BAEMM_REF_SECONDS", "12")))
-    if cpu is None:
-        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libbaemm_refcl.so not built"}))
+    from oracle import oracle as O
+    if not O.ref_available(fast=True):
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libbaemm_refcl_fast.so not built "
+                                                              "(oracle/build_ref.sh needs the reference tree)"}))
         return 0
-    vals = [cpu["value"]]
-    for _ in range(max(0, args.steps - 1)):
-        c2 = reference_rows_rate(coords, tris, B, target_seconds=float(os.environ.get("BAEMM_REF_SECONDS", "12")))
-        vals.append(c2["value"])
-    v = float(np.mean(vals))
+    coords, tris, B = build_workload(small=args.small)
+    R = ReferenceRows(coords, tris, B)
+    rows = R.rows_for(float(os.environ.get("BAEMM_REF_SECONDS", "4")))
+    for _ in range(args.warmup):
+        R.run(rows)
+    dts = [R.run(rows) for _ in range(args.steps)]
+    v = R.rate(rows * args.steps, float(np.sum(dts)))
     n = tris.shape[0]
     line = {
         "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": n * n * WC / (v * 1e9) * 1e3, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "fp32", "data": "synthetic",
-        "config": {"workload": WORKLOAD if not args.small else "SMALL torus 80x240 (profiling only)", "interactions_per_step": n * n * WC, "parallelism": "host cores",
-                   "l2": "n/a (CPU)"},
-        "cpu_baseline": {"value": v, "unit": UNIT, "cores": cpu["cores"], "kind": "reference",
-                         "sample": cpu["sample"]},
+        "projected": True, "rows_sampled_per_step": rows,
+        "sample_ms_per_step": float(np.mean(dts)) * 1e3,
+        "config": {"workload": WORKLOAD if not args.small else "SMALL torus 80x240 (profiling only)",
+                   "interactions_per_step": n * n * WC, "parallelism": "host cores", "l2": "n/a (CPU)"},
+        "cpu_baseline": {"value": v, "unit": UNIT, "cores": R.cores, "kind": "reference", "projected": True,
+                         "sample": R.sample_text(rows)},
         "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line))
@@ -241,27 +302,34 @@ def whole_job_rate(world: int, interactions_per_step: int, steps: int, total_ms:
 def roofline_model(n_targets, n_sources, n_k, inter, mode, peaks, clk_mhz, n_sm, kernel_ms):
     """Roofline model of one dense launch (algorithmic work per launch):
     W = 8 I contraction FLOPs, G = N_t N_s n_k kernel evaluations (2 MUFU sincos
-    + 20 FP32 FLOPs each) and N_t N_s rsqrt;
-    plain form T* = (W + 20 G) / P_fp32,
-    tensor-core form T* = max(W / P_tf32, (2 G + N_t N_s) / P_mufu, 20 G / P_fp32)."""
+    + 20 FLOPs each) and N_t N_s rsqrt;
+    plain FP32 form T* = (W + 20 G) / P_fp32, FP64 form T* = (W + 20 G) / P_fp64,
+    tensor-core form T* = max(W / P_tf32, (2 G + N_t N_s) / P_mufu, 20 G / P_fp32).
+    Each term comes with its work and rate, so achieved = work / t and
+    frac = achieved / rate = term / t."""
     G = float(n_targets) * n_sources * n_k
     f_hz = (clk_mhz or 1965.0) * 1e6
     p_fp32 = n_sm * 128 * 2 * f_hz               # FFMA: 128 lanes/SM/clk
+    p_fp64 = n_sm * 64 * 2 * f_hz                # DFMA: 64 lanes/SM/clk
     p_mufu = n_sm * 16 * f_hz                    # MUFU: 16 lanes/SM/clk
     p_tf32 = peaks["bf16_tflops"] * 1e12 / 2.0   # dense TF32 = half the measured dense BF16 rate
-    terms = {"tensor_tf32_ms": 8.0 * inter / p_tf32 * 1e3,
-             "mufu_ms": (2 * G + float(n_targets) * n_sources) / p_mufu * 1e3,
-             "fp32_ms": 20.0 * G / p_fp32 * 1e3}
-    if mode == "tc":
-        t_star = max(terms.values())
-        limiter = max(terms, key=terms.get)
-    else:
-        t_star = (8.0 * inter + 20.0 * G) / p_fp32 * 1e3
-        limiter = "fp32_ms"
+    W = 8.0 * inter
+    work = {"tensor_tf32": (W, p_tf32, "TFLOP/s"),
+            "mufu": (2 * G + float(n_targets) * n_sources, p_mufu, "Top/s (MUFU sin, cos, rsqrt)"),
+            "fp32": (20.0 * G, p_fp32, "TFLOP/s")}
+    if mode == "fp32":
+        work = {"fp32": (W + 20.0 * G, p_fp32, "TFLOP/s")}
+    elif mode == "fp64":
+        work = {"fp64": (W + 20.0 * G, p_fp64, "TFLOP/s")}
+    terms = {k + "_ms": w / r * 1e3 for k, (w, r, _) in work.items()}
+    limiter = max(terms, key=terms.get)
+    t_star = terms[limiter]
+    w, r, unit = work[limiter[:-3]]
     return {"T_star_ms": t_star, "limiter": limiter, "terms_ms": terms, "frac": t_star / kernel_ms,
+            "achieved": w / (kernel_ms * 1e-3) / 1e12, "peak": r / 1e12, "unit": unit,
             "clock_mhz": clk_mhz or 1965.0,
-            "peaks": "P_fp32 = SMs x 256 FLOP/clk, P_mufu = SMs x 16/clk at the sampled SM clock; "
-                     "P_tf32 = measured dense BF16 / 2"}
+            "peaks": "P_fp32 = SMs x 256 FLOP/clk, P_fp64 = SMs x 128 FLOP/clk, P_mufu = SMs x 16/clk at the "
+                     "sampled SM clock; P_tf32 = measured dense BF16 / 2"}
 
 
 # ---------------------------------------------------------------------------
@@ -398,7 +466,7 @@ def run_gpu_arm(args, rank, world, local_rank):
     dense_avg = float(np.mean(dense_ms))
     flops = 8.0 * inter_kernel
     achieved = flops / (dense_avg * 1e-3) / 1e12
-    traffic = load_traffic(args.mode)
+    traffic, traffic_src = load_traffic(args.mode)
     kernel_name = {"tc": "boundary_tc_kernel", "fp32": "boundary_dense_kernel", "fp64": "boundary_dense_kernel<double>"}[args.mode]
     cpu = None
     if world == 1 and not args.no_cpu_baseline:
@@ -419,12 +487,15 @@ def run_gpu_arm(args, rank, world, local_rank):
                                    f"replicas x{world}" if world > 1 else "single GPU"),
                    "l2": "flushed (256 MiB write) before every timed step",
                    "phase_ms_last": list(H.LastApplyTimes()) if False else None},
-        "roofline": {"bound": "tensor", "kernel": kernel_name, "achieved": achieved,
-                     "peak": peaks["bf16_tflops"], "unit": "TFLOP/s", "frac": achieved / peaks["bf16_tflops"],
-                     "peak_source": peaks["source"] + " (dense bf16 burst)",
-                     "algorithmic": "8 * N_t * N_s * wave_count FLOPs per launch (complex MACs), counted once; "
+        "roofline": {"bound": model["limiter"][:-3], "kernel": kernel_name, "achieved": model["achieved"],
+                     "peak": model["peak"], "unit": model["unit"], "frac": model["frac"],
+                     "peak_source": ("nominal SM pipe rates at the sampled clock" if model["limiter"] != "tensor_tf32_ms"
+                                     else peaks["source"] + " (dense bf16 burst / 2)"),
+                     "algorithmic": "the limiting term of the dense kernel's model (below) per launch; "
                                     "N_t = this rank's target rows",
-                     "dense_kernel_ms": dense_avg, "traffic": traffic, "model": model},
+                     "dense_kernel_ms": dense_avg, "traffic": traffic, "traffic_source": traffic_src,
+                     "algorithmic_bytes": int(nt * WC * 8 * 2 + ((nt + 15) // 16) * 384),
+                     "model": model},
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(B.nbytes),
                 "d2h_bytes_per_step": int(B.nbytes), "ms_per_step": e2e_total / args.steps},
         "gpu_launches": int(launches),
@@ -444,11 +515,18 @@ def run_gpu_arm(args, rank, world, local_rank):
                    "frac_of_hbm_peak": nb / (ms * 1e-3) / 1e9 / peaks["hbm_gbs"],
                    "peak_source": peaks["source"] + " (copy bandwidth)"}
             for name, ms, nb in (("avop", ph[0], avop_bytes), ("avopT_epilogue", ph[2], epi_bytes))}
+    if args.mode == "tc":
+        # the tensor pipe beside the limiter: algorithmic contraction FLOPs (8 I, counted once) and the
+        # FLOPs the compensated products issue (Ahi [Bhi | Blo] + Alo Bhi: 3 x 8 I) against dense TF32
+        p_tf32 = peaks["bf16_tflops"] / 2.0
+        line["roofline"]["tensor_pipe"] = {
+            "algorithmic_TFLOP_s": achieved, "issued_TFLOP_s": 3.0 * achieved, "peak_tf32_TFLOP_s": p_tf32,
+            "frac_issued": 3.0 * achieved / p_tf32, "peak_source": peaks["source"] + " (dense bf16 burst / 2)"}
     if compare is not None:
         line["compare"] = compare
     if cpu is not None:
         line["cpu_baseline"] = {"value": cpu["value"], "unit": UNIT, "cores": cpu["cores"], "kind": cpu["kind"],
-                                "sample": cpu["sample"]}
+                                "projected": True, "sample": cpu["sample"]}
     print(json.dumps(line), flush=True)
     H.close()
     return 0
