@@ -25,6 +25,8 @@ TUNE_DENSE_VARIANT = 1
 TUNE_TC_SEGMENT = 2
 TUNE_TC_CTAS = 3
 TUNE_TC_STAGGER = 4
+TUNE_TC_GEN_WARPS = 5
+TUNE_TC_CHUNKS = 6
 
 dp = C.POINTER(C.c_double)
 fp = C.POINTER(C.c_float)
@@ -56,6 +58,10 @@ class TuneResult(C.Structure):
         ("candidates", C.c_int32),
         ("best_ms", C.c_double),
         ("before_ms", C.c_double),
+        ("tc_gen_warps", C.c_int32),
+        ("tc_chunks", C.c_int32),
+        ("cached", C.c_int32),
+        ("reserved", C.c_int32),
     ]
 
 
@@ -112,6 +118,8 @@ SIGNATURES = {
     "baemm_apply_far_field_operators_dev_z": (I, [vp, dp, vp, I64, dp, vp, I64]),
     "baemm_apply_boundary_operators_rows_dev_z": (I, [vp, dp, vp, I64, dp, vp, I64, I64, I64, I]),
     "baemm_apply_boundary_operators_rows_dev_c": (I, [vp, fp, vp, I64, fp, vp, I64, I64, I64, I]),
+    "baemm_boundary_operator_kernel_dev_c": (I, [vp, vp, vp, I64, I64]),
+    "baemm_boundary_operator_kernel_dev_z": (I, [vp, vp, vp, I64, I64]),
     "baemm_apply_near_field_operators_z": (I, [vp, dp, dp, I64, dp, dp, I64, dp, I64]),
     "baemm_apply_near_field_operators_c": (I, [vp, fp, fp, I64, fp, fp, I64, fp, I64]),
     "baemm_apply_near_field_operators_full_z": (I, [vp, dp, dp, I64, dp, dp, I64, dp, dp, I, I, dp, I64]),
@@ -136,6 +144,8 @@ SIGNATURES = {
     "baemm_gauss_newton_solve": (I, [vp, dp, I, dp, I, REAL_OP, vp, REAL_OP, vp, D, dp, I64, D, dp, I64,
                                      C.POINTER(dp), I, D, D, D, I, C.POINTER(C.c_int)]),
     "baemm_set_profiling": (I, [vp, I]),
+    "baemm_profile_krylov": (I, [vp, I, I, I, dp]),
+    "baemm_autotune_forget": (None, []),
     "baemm_last_apply_times": (I, [vp, fp]),
     "baemm_kernel_launch_count": (I64, []),
     "baemm_free": (None, [vp]),

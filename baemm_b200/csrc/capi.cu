@@ -456,15 +456,24 @@ int baemm_set_tuning(baemm_ctx *ctx, int key, int value)
                 break;
             case BAEMM_TUNE_TC_SEGMENT:
                 BAEMM_REQUIRE(value >= 1, BAEMM_ERR_ARG, "segment length must be >= 1");
-                c.tc_seg_tiles = value;
+                c.tc_tune.seg_tiles = value;
                 break;
             case BAEMM_TUNE_TC_STAGGER:
                 BAEMM_REQUIRE(value >= -1 && value <= 1 << 20, BAEMM_ERR_ARG, "stagger must be -1 or >= 0");
-                c.tc_stagger = value;
+                c.tc_tune.stagger = value;
                 break;
             case BAEMM_TUNE_TC_CTAS:
                 BAEMM_REQUIRE(value >= 0 && value <= 65535, BAEMM_ERR_ARG, "grid size must be in [0, 65535]");
-                c.tc_ctas = value;
+                c.tc_tune.ctas = value;
+                break;
+            case BAEMM_TUNE_TC_GEN_WARPS:
+                BAEMM_REQUIRE(value == 8 || value == 16, BAEMM_ERR_ARG, "generator warps must be 8 or 16");
+                c.tc_tune.gen_warps = value;
+                break;
+            case BAEMM_TUNE_TC_CHUNKS:
+                BAEMM_REQUIRE(value == 0 || value == 1 || value == 2 || value == 4, BAEMM_ERR_ARG,
+                              "chunks per unit must be 0, 1, 2 or 4");
+                c.tc_tune.chunks = value;
                 break;
             default: throw Error(BAEMM_ERR_ARG, "unknown tuning key");
         }
@@ -474,9 +483,11 @@ int baemm_get_tuning(const baemm_ctx *ctx, int key)
 {
     if (!ctx || !ctx->impl) return -1;
     if (key == BAEMM_TUNE_DENSE_VARIANT) return ctx->impl->dense_variant;
-    if (key == BAEMM_TUNE_TC_SEGMENT) return ctx->impl->tc_seg_tiles;
-    if (key == BAEMM_TUNE_TC_CTAS) return ctx->impl->tc_ctas;
-    if (key == BAEMM_TUNE_TC_STAGGER) return ctx->impl->tc_stagger;
+    if (key == BAEMM_TUNE_TC_SEGMENT) return ctx->impl->tc_tune.seg_tiles;
+    if (key == BAEMM_TUNE_TC_CTAS) return ctx->impl->tc_tune.ctas;
+    if (key == BAEMM_TUNE_TC_STAGGER) return ctx->impl->tc_tune.stagger;
+    if (key == BAEMM_TUNE_TC_GEN_WARPS) return ctx->impl->tc_tune.gen_warps;
+    if (key == BAEMM_TUNE_TC_CHUNKS) return ctx->impl->tc_tune.chunks;
     return -1;
 }
 int baemm_get_apply_mode(const baemm_ctx *ctx) { return (ctx && ctx->impl) ? ctx->impl->apply_mode : -1; }
@@ -609,6 +620,61 @@ int baemm_apply_boundary_operators_rows_dev_c(baemm_ctx *ctx, const float alpha[
         BAEMM_REQUIRE(B && C, BAEMM_ERR_ARG, "null block");
         c.apply_boundary_rows<float2>(c2(alpha), reinterpret_cast<const float2 *>(B), ldB, c2(beta),
                                       reinterpret_cast<float2 *>(C), ldC, row_begin, row_end, with_mass != 0);
+    });
+}
+
+int baemm_profile_krylov(baemm_ctx *ctx, int columns, int iterations, int basis, double out[10])
+{
+    return guarded(ctx, [&](Ctx &c) {
+        BAEMM_REQUIRE(out, BAEMM_ERR_ARG, "null output");
+        BAEMM_REQUIRE(columns >= 1 && 2 * columns <= baemm::kMaxKrylovColumns && iterations >= 1 && basis >= 1 &&
+                          basis <= baemm::kMaxRestart + 1,
+                      BAEMM_ERR_ARG, "profile_krylov: sizes out of range");
+        const bool v64 = c.mass_values_fp64();
+        const int rc = 2 * columns;   // complex columns as interleaved real columns (ApplyMassInverse.hpp:71-98)
+        double cg_ms[3], gs_ms[2];
+        baemm::CgSolver cg;
+        cg.profile(c.mesh, v64, rc, iterations, c.stream, cg_ms);
+        baemm::profile_gram_schmidt(c.mesh.nv, columns, basis, iterations, c.stream, gs_ms);
+        const double n = (double)c.mesh.nv, nnz = (double)c.mass_inner_h.size(), vs = v64 ? 8.0 : 4.0;
+        const double vec = n * rc * 8.0, cvec = n * columns * 16.0;
+        out[0] = cg_ms[0]; out[1] = cg_ms[1]; out[2] = cg_ms[2]; out[3] = gs_ms[0]; out[4] = gs_ms[1];
+        out[5] = (n + 1) * 4 + nnz * (4 + vs) + 2 * vec;   // CSR, p gathered once, q written
+        out[6] = n * vs + 7 * vec;                          // L; x, p, r, q read; x, r, z written
+        out[7] = 3 * vec;                                   // z, p read; p written
+        out[8] = (basis + 1) * cvec;                        // w and the basis vectors read
+        out[9] = (basis + 2) * cvec;                        // w and the basis read, w written
+    });
+}
+
+int baemm_boundary_operator_kernel_dev_c(baemm_ctx *ctx, const float *B_tri, float *C_tri, int64_t row_begin,
+                                         int64_t row_end)
+{
+    return guarded(ctx, [&](Ctx &c) {
+        c.require_loaded();
+        BAEMM_REQUIRE(B_tri && C_tri, BAEMM_ERR_ARG, "null block");
+        BAEMM_REQUIRE(c.apply_mode != BAEMM_APPLY_FP64, BAEMM_ERR_ARG,
+                      "the FP64 apply mode takes complex128 blocks (baemm_boundary_operator_kernel_dev_z)");
+        BAEMM_REQUIRE(row_begin >= 0 && row_begin <= row_end && row_end <= c.mesh.nt, BAEMM_ERR_ARG,
+                      "row range outside [0, simplex_count]");
+        if (row_end > row_begin && c.flags.any_layer())
+            c.boundary_kernel_rows<float>(reinterpret_cast<const float2 *>(B_tri), reinterpret_cast<float2 *>(C_tri), row_begin,
+                                 row_end);
+    });
+}
+int baemm_boundary_operator_kernel_dev_z(baemm_ctx *ctx, const double *B_tri, double *C_tri, int64_t row_begin,
+                                         int64_t row_end)
+{
+    return guarded(ctx, [&](Ctx &c) {
+        c.require_loaded();
+        BAEMM_REQUIRE(B_tri && C_tri, BAEMM_ERR_ARG, "null block");
+        BAEMM_REQUIRE(c.apply_mode == BAEMM_APPLY_FP64, BAEMM_ERR_ARG,
+                      "complex128 blocks need the FP64 apply mode (BAEMM_APPLY_FP64)");
+        BAEMM_REQUIRE(row_begin >= 0 && row_begin <= row_end && row_end <= c.mesh.nt, BAEMM_ERR_ARG,
+                      "row range outside [0, simplex_count]");
+        if (row_end > row_begin && c.flags.any_layer())
+            c.boundary_kernel_rows<double>(reinterpret_cast<const double2 *>(B_tri), reinterpret_cast<double2 *>(C_tri),
+                                  row_begin, row_end);
     });
 }
 

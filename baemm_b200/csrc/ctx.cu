@@ -314,7 +314,10 @@ void Ctx::load_parameters(const double *kappa, const zc *coeff, int wc, int wcs,
         for (int gi = 0; gi < groups; ++gi) prm16_f_h[gi] = prm_f_h[gi / rep];
         BAEMM_CUDA(cudaMemcpyAsync(prm16_f.reserve(groups), prm16_f_h.data(), groups * sizeof(ChunkParamsF),
                                    cudaMemcpyHostToDevice, stream));
+        tc_form = tc_coeff_form(prm16_f_h.data(), groups);
     }
+    else
+        tc_form = TcCoeffForm();
 }
 
 void Ctx::require_loaded() const
@@ -336,9 +339,9 @@ void Ctx::dense_apply(const cplx<R> *Btri, cplx<R> *Ctri, int64_t r0, int64_t r1
             launch_tc_tile_geometry(mesh, mesh.tgeo_f.reserve(tc_tile_geometry_floats(mesh.nt)), stream);
             tc_geo_ready = true;
         }
-        const size_t ws_elems = tc_workspace_elems(tc_ctas);
-        launch_boundary_tc(mesh, flags, prm16_f.p, wave_count, wave_chunk_size, mesh.tgeo_f.p, Btri, Ctri,
-                           tc_ws.reserve(ws_elems), ws_elems, tc_err.p, stream, tc_seg_tiles, tc_ctas, tc_stagger, r0,
+        const size_t ws_elems = tc_workspace_elems(tc_tune.ctas);
+        launch_boundary_tc(mesh, flags, prm16_f.p, tc_form, wave_count, wave_chunk_size, mesh.tgeo_f.p, Btri, Ctri,
+                           tc_ws.reserve(ws_elems), ws_elems, tc_err.p, stream, tc_tune, r0,
                            r1);
         tc_pending = true;
     }
@@ -458,9 +461,9 @@ void Ctx::apply_nearfield(Text alpha, const Text *B, int64_t ldB, Text beta, Tex
                 launch_tc_tile_geometry(mesh, mesh.tgeo_f.reserve(tc_tile_geometry_floats(mesh.nt)), stream);
                 tc_geo_ready = true;
             }
-            const size_t ws_elems = tc_workspace_elems(tc_ctas);
-            launch_nearfield_tc(mesh, nf, prm16_f.p, wave_count, wave_chunk_size, mesh.tgeo_f.p, p4, npts, Bt, Cp,
-                                tc_ws.reserve(ws_elems), ws_elems, tc_err.p, stream, tc_seg_tiles, tc_ctas, tc_stagger);
+            const size_t ws_elems = tc_workspace_elems(tc_tune.ctas);
+            launch_nearfield_tc(mesh, nf, prm16_f.p, tc_form, wave_count, wave_chunk_size, mesh.tgeo_f.p, p4, npts, Bt, Cp,
+                                tc_ws.reserve(ws_elems), ws_elems, tc_err.p, stream, tc_tune);
             tc_pending = true;
         }
         else
@@ -478,6 +481,7 @@ template void Ctx::apply_nearfield<double2>(double2, const double2 *, int64_t, d
 template void Ctx::apply_nearfield<float2>(float2, const float2 *, int64_t, float2, float2 *, int64_t, const double *,
                                            int64_t);
 template void Ctx::dense_apply<float>(const float2 *, float2 *, int64_t, int64_t);
+template void Ctx::dense_apply<double>(const double2 *, double2 *, int64_t, int64_t);
 template void Ctx::apply_boundary_rows<double2>(double2, const double2 *, int64_t, double2, double2 *, int64_t,
                                                 int64_t, int64_t, bool);
 template void Ctx::apply_boundary_rows<float2>(float2, const float2 *, int64_t, float2, float2 *, int64_t, int64_t,

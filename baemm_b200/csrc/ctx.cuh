@@ -43,6 +43,7 @@ public:
     DevBuf<ChunkParamsF> prm_f;
     std::vector<ChunkParamsF> prm16_f_h;   // per 16-column group (tensor-core form)
     DevBuf<ChunkParamsF> prm16_f;
+    TcCoeffForm tc_form;                    // coefficient structure the tensor-core form specialises on
     DevBuf<ChunkParamsD> prm_d;
     bool operators_loaded = false;
 
@@ -51,9 +52,7 @@ public:
     int gmres_max_iter = 30, gmres_max_restarts = 3;
     int apply_mode = BAEMM_APPLY_FP32;
     int dense_variant = 0;            // plain FP32 dense kernel variant (launch_boundary_dense)
-    int tc_seg_tiles = 16;            // tensor-core form: tiles per TMEM partial sum
-    int tc_ctas = 0;                  // tensor-core form: persistent grid size (0 = one CTA per SM)
-    int tc_stagger = 0;               // tensor-core form: sweep offset between CTAs (tiles; -1 = spread)
+    TcTuning tc_tune;                 // tensor-core form settings (TcTuning in ops.cuh)
     DevBuf<float2> tc_ws;             // tensor-core form: partial sums of target blocks split between CTAs
     bool tc_geo_ready = false;        // mesh.tgeo_f built
     int ir_max_steps = 0;
@@ -101,6 +100,14 @@ public:
     template <class Text>
     void apply_boundary_rows(Text alpha, const Text *B, int64_t ldB, Text beta, Text *C, int64_t ldC, int64_t r0,
                              int64_t r1, bool with_mass);
+    // The dense stage alone on device triangle blocks (BoundaryOperatorKernel.hpp:5-28):
+    // Ctri rows [r0, r1) = K[r0, r1) Btri in the current arithmetic (R = float: plain or
+    // tensor-core form; R = double: FP64).
+    template <class R>
+    void boundary_kernel_rows(const cplx<R> *Btri, cplx<R> *Ctri, int64_t r0, int64_t r1)
+    {
+        dense_apply<R>(Btri, Ctri, r0, r1);
+    }
     // Far field: C (nm x wc) = alpha FF B + beta C   (ApplyFarFieldOperators.hpp:356-412)
     void apply_farfield(zc alpha, const double2 *B, int64_t ldB, zc beta, double2 *C, int64_t ldC);
     // ApplyNearFieldOperators.hpp:56-122 on device blocks: C (npts x wc) =

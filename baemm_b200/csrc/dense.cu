@@ -109,7 +109,11 @@ boundary_dense_kernel(DenseTargets<R> tg, const R *__restrict__ mid4, const R *_
             n0 = nrm4[4 * gi]; n1 = nrm4[4 * gi + 1]; n2 = nrm4[4 * gi + 2];
         }
     }
-    cplx<R> acc[COLS];
+    // FP32: two-level sum -- each 64-source tile into fresh accumulators, then
+    // into the running total (the error of one long FP32 chain over ~1e5
+    // sources would be ~5x larger); FP64: one accumulator.
+    constexpr bool kTwoLevel = std::is_same<R, float>::value;
+    cplx<R> acc[COLS], tacc[COLS];
     #pragma unroll
     for (int k = 0; k < COLS; ++k) { acc[k].x = R(0); acc[k].y = R(0); }
 
@@ -119,6 +123,13 @@ boundary_dense_kernel(DenseTargets<R> tg, const R *__restrict__ mid4, const R *_
         stage_tile<R, COLS, DL, false>(tile, mid4, nrm4, B, wc, col0, j0, n);
         __syncthreads();
         const int smax = min(kTile, n - j0);
+        #pragma unroll
+        for (int k = 0; k < COLS; ++k)
+        {
+            tacc[k].x = R(0);
+            tacc[k].y = R(0);
+        }
+        cplx<R>(&sum)[COLS] = kTwoLevel ? tacc : acc;
         #pragma unroll 2
         for (int s = 0; s < smax; ++s)
         {
@@ -160,7 +171,16 @@ boundary_dense_kernel(DenseTargets<R> tg, const R *__restrict__ mid4, const R *_
                 A.y += fx * g1 + fy * g0;
             }
             #pragma unroll
-            for (int k = 0; k < COLS; ++k) cfma(acc[k], A, tile.B[s][k]);
+            for (int k = 0; k < COLS; ++k) cfma(sum[k], A, tile.B[s][k]);
+        }
+        if (kTwoLevel)
+        {
+            #pragma unroll
+            for (int k = 0; k < COLS; ++k)
+            {
+                acc[k].x += tacc[k].x;
+                acc[k].y += tacc[k].y;
+            }
         }
     }
     if (i < tg.m)
@@ -220,7 +240,7 @@ boundary_packed_kernel(DenseTargets<float> tg, const float *__restrict__ mid4, c
             }
         }
     }
-    float2 acc[TT][kPackedCols];
+    float2 acc[TT][kPackedCols], tacc[TT][kPackedCols];   // running total, this tile's sum (two-level sum)
     #pragma unroll
     for (int t = 0; t < TT; ++t)
         #pragma unroll
@@ -251,6 +271,10 @@ boundary_packed_kernel(DenseTargets<float> tg, const float *__restrict__ mid4, c
         }
         __syncthreads();
         const int smax = min(kTile, n - j0);
+        #pragma unroll
+        for (int t = 0; t < TT; ++t)
+            #pragma unroll
+            for (int k = 0; k < kPackedCols; ++k) tacc[t][k] = make_float2(0.f, 0.f);
         for (int s = 0; s < smax; ++s)
         {
             const float4 yv = tile.y[s];
@@ -305,11 +329,15 @@ boundary_packed_kernel(DenseTargets<float> tg, const float *__restrict__ mid4, c
                 #pragma unroll
                 for (int t = 0; t < TT; ++t)
                 {
-                    acc[t][k] = __ffma2_rn(Ar[t], b, acc[t][k]);
-                    acc[t][k] = __ffma2_rn(Ai[t], bw, acc[t][k]);
+                    tacc[t][k] = __ffma2_rn(Ar[t], b, tacc[t][k]);
+                    tacc[t][k] = __ffma2_rn(Ai[t], bw, tacc[t][k]);
                 }
             }
         }
+        #pragma unroll
+        for (int t = 0; t < TT; ++t)
+            #pragma unroll
+            for (int k = 0; k < kPackedCols; ++k) acc[t][k] = __fadd2_rn(acc[t][k], tacc[t][k]);
     }
     #pragma unroll
     for (int t = 0; t < TT; ++t)

@@ -7,6 +7,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <vector>
 
 namespace baemm
 {
@@ -81,10 +82,120 @@ __device__ __forceinline__ void block_reduce_store(double v, double *sm, int tr,
 // ============================== CG =============================================
 // col_ layout: [0,c) rz  [c,2c) bn  [2c,3c) alpha  [3c,4c) beta ; flags_: [0] done [1] iters [2..) conv
 
+
+
+// Sum of one column of the per-block partial sums, partial[q * ld + off] over
+// q < nblk, by one warp: lane l takes q = l, l + 32, ..., a shuffle tree adds
+// the lanes in a fixed order and every lane returns lane 0's total (so the
+// result does not depend on timing).  The finalize kernels below give each
+// column its own warp, instead of one thread summing all nblk values in turn.
+__device__ __forceinline__ double warp_sum_partials(const double *__restrict__ partial, int64_t ld, int64_t off,
+                                                    int nblk)
+{
+    const int lane = threadIdx.x & 31;
+    double s = 0.0;
+    for (int q = lane; q < nblk; q += 32) s += partial[(int64_t)q * ld + off];
+    #pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+    return __shfl_sync(0xffffffffu, s, 0);
+}
+
+// The same over partial sums written by other blocks of the running kernel:
+// loads that bypass L1 (the lines may be stale there).
+__device__ __forceinline__ double warp_sum_partials_cg(const double *partial, int64_t ld, int64_t off, int nblk)
+{
+    const int lane = threadIdx.x & 31;
+    double s = 0.0;
+    for (int q = lane; q < nblk; q += 32) s += __ldcg(partial + (int64_t)q * ld + off);
+    #pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+    return __shfl_sync(0xffffffffu, s, 0);
+}
+
+// Called by every thread of every block after the block has written its
+// partial sums: true (in all threads) in the one block that finished last,
+// which then sees every block's partials.  The counter is back at zero when
+// the kernel ends.  (The "last block" reduction: the finalize step runs in
+// the producing kernel instead of a launch of its own.)
+__device__ __forceinline__ bool last_block(unsigned int *counter)
+{
+    __shared__ bool last;
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0)
+    {
+        const unsigned int nb = gridDim.x * gridDim.y;
+        last = atomicAdd(counter, 1u) == nb - 1;
+        if (last) *counter = 0u;
+    }
+    __syncthreads();
+    if (last) __threadfence();
+    return last;
+}
+
+// Column sums of the CG phases, one warp per column (ApplyMassInverse.hpp:67-147):
+//   init:  rz = <r, z>, bn = ||b||, convergence of zero columns
+//   alpha: alpha = rz / <p, q>
+//   beta:  beta = rz_new / rz, rz = rz_new, convergence ||r|| <= tol ||b||
+// col layout: [0,c) rz  [c,2c) bn  [2c,3c) alpha  [3c,4c) beta ; flags: [0] done [1] iters [2..) conv
+__device__ void cg_fin_init(int c, int nblk, const double *partial, double *col, int *flags, double tol)
+{
+    int all = 1;
+    const int warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5, lane = threadIdx.x & 31;
+    for (int k = warp; k < c; k += nwarps)
+    {
+        const double rz = warp_sum_partials_cg(partial, 2 * c, k, nblk);
+        const double bb = warp_sum_partials_cg(partial, 2 * c, c + k, nblk);
+        if (lane != 0) continue;
+        const double bn = sqrt(bb);
+        col[k] = rz;
+        col[c + k] = bn;
+        col[2 * c + k] = 0.0;
+        col[3 * c + k] = 0.0;
+        const int cv = (bn <= tol * bn) ? 1 : 0;
+        flags[2 + k] = cv;
+        all &= cv;
+    }
+    all = __syncthreads_and(all);
+    if (threadIdx.x == 0) { flags[0] = all; flags[1] = 0; }
+}
+
+__device__ void cg_fin_alpha(int c, int nblk, const double *partial, double *col, const int *flags)
+{
+    const int warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5, lane = threadIdx.x & 31;
+    for (int k = warp; k < c; k += nwarps)
+    {
+        const double pq = warp_sum_partials_cg(partial, c, k, nblk);
+        if (lane == 0) col[2 * c + k] = (flags[2 + k] || pq == 0.0) ? 0.0 : col[k] / pq;
+    }
+}
+
+__device__ void cg_fin_beta(int c, int nblk, const double *partial, double *col, int *flags, double tol)
+{
+    int all = 1;
+    const int warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5, lane = threadIdx.x & 31;
+    for (int k = warp; k < c; k += nwarps)
+    {
+        const double rzn = warp_sum_partials_cg(partial, 2 * c, k, nblk);
+        const double rr = warp_sum_partials_cg(partial, 2 * c, c + k, nblk);
+        if (lane != 0) continue;
+        const int was = flags[2 + k];
+        col[3 * c + k] = (was || col[k] == 0.0) ? 0.0 : rzn / col[k];
+        col[k] = rzn;
+        const int cv = was || (sqrt(rr) <= tol * col[c + k]);
+        flags[2 + k] = cv;
+        all &= cv;
+    }
+    all = __syncthreads_and(all);
+    if (threadIdx.x == 0) { flags[0] = all; flags[1] += 1; }
+}
+
+
 template <class RV>
 __global__ void cg_init_kernel(int64_t n, int c, int cp, int rp, int64_t rpb, const double *__restrict__ b,
                                int64_t ldb, const RV *__restrict__ L, double *__restrict__ x, double *__restrict__ r,
-                               double *__restrict__ z, double *__restrict__ p, double *__restrict__ partial)
+                               double *__restrict__ z, double *__restrict__ p, double *partial,
+                               unsigned int *counter, double *col, int *flags, double tol)
 {
     __shared__ double sm[RT];
     const int tr = threadIdx.x / cp, tc = threadIdx.x % cp;
@@ -107,52 +218,14 @@ __global__ void cg_init_kernel(int64_t n, int c, int cp, int rp, int64_t rpb, co
     double *out = partial + (int64_t)blockIdx.x * 2 * c;
     block_reduce_store(rz, sm, tr, tc, cp, rp, active, out + k);
     block_reduce_store(bb, sm, tr, tc, cp, rp, active, out + c + k);
-}
-
-
-// Sum of one column of the per-block partial sums, partial[q * ld + off] over
-// q < nblk, by one warp: lane l takes q = l, l + 32, ..., a shuffle tree adds
-// the lanes in a fixed order and every lane returns lane 0's total (so the
-// result does not depend on timing).  The finalize kernels below give each
-// column its own warp, instead of one thread summing all nblk values in turn.
-__device__ __forceinline__ double warp_sum_partials(const double *__restrict__ partial, int64_t ld, int64_t off,
-                                                    int nblk)
-{
-    const int lane = threadIdx.x & 31;
-    double s = 0.0;
-    for (int q = lane; q < nblk; q += 32) s += partial[(int64_t)q * ld + off];
-    #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
-    return __shfl_sync(0xffffffffu, s, 0);
-}
-
-__global__ void cg_finalize_init_kernel(int c, int nblk, const double *__restrict__ partial, double *__restrict__ col,
-                                        int *__restrict__ flags, double tol)
-{
-    int all = 1;
-    const int warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5, lane = threadIdx.x & 31;
-    for (int k = warp; k < c; k += nwarps)
-    {
-        const double rz = warp_sum_partials(partial, 2 * c, k, nblk);
-        const double bb = warp_sum_partials(partial, 2 * c, c + k, nblk);
-        if (lane != 0) continue;
-        const double bn = sqrt(bb);
-        col[k] = rz;
-        col[c + k] = bn;
-        col[2 * c + k] = 0.0;
-        col[3 * c + k] = 0.0;
-        const int cv = (bn <= tol * bn) ? 1 : 0;
-        flags[2 + k] = cv;
-        all &= cv;
-    }
-    all = __syncthreads_and(all);
-    if (threadIdx.x == 0) { flags[0] = all; flags[1] = 0; }
+    if (last_block(counter)) cg_fin_init(c, gridDim.x, partial, col, flags, tol);
 }
 
 template <class RV>
 __global__ void cg_matvec_kernel(int64_t n, int c, int cp, int rp, int64_t rpb, const int32_t *__restrict__ mo,
                                  const int32_t *__restrict__ mi, const RV *__restrict__ mv, const double *__restrict__ p,
-                                 double *__restrict__ q, double *__restrict__ partial, const int *__restrict__ flags)
+                                 double *__restrict__ q, double *partial, unsigned int *counter, double *col,
+                                 const int *flags)
 {
     if (flags[0]) return;
     __shared__ double sm[RT];
@@ -172,25 +245,15 @@ __global__ void cg_matvec_kernel(int64_t n, int c, int cp, int rp, int64_t rpb, 
         }
     }
     block_reduce_store(pq, sm, tr, tc, cp, rp, active, partial + (int64_t)blockIdx.x * c + k);
+    if (last_block(counter)) cg_fin_alpha(c, gridDim.x, partial, col, flags);
 }
 
-__global__ void cg_finalize_alpha_kernel(int c, int nblk, const double *__restrict__ partial, double *__restrict__ col,
-                                         const int *__restrict__ flags)
-{
-    if (flags[0]) return;
-    const int warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5, lane = threadIdx.x & 31;
-    for (int k = warp; k < c; k += nwarps)
-    {
-        const double pq = warp_sum_partials(partial, c, k, nblk);
-        if (lane == 0) col[2 * c + k] = (flags[2 + k] || pq == 0.0) ? 0.0 : col[k] / pq;
-    }
-}
 
 template <class RV>
 __global__ void cg_update_kernel(int64_t n, int c, int cp, int rp, int64_t rpb, const RV *__restrict__ L,
-                                 const double *__restrict__ col, double *__restrict__ x, double *__restrict__ r,
+                                 double *col, double *__restrict__ x, double *__restrict__ r,
                                  double *__restrict__ z, const double *__restrict__ p, const double *__restrict__ q,
-                                 double *__restrict__ partial, const int *__restrict__ flags)
+                                 double *partial, unsigned int *counter, int *flags, double tol)
 {
     if (flags[0]) return;
     __shared__ double sm[RT];
@@ -217,29 +280,9 @@ __global__ void cg_update_kernel(int64_t n, int c, int cp, int rp, int64_t rpb, 
     double *out = partial + (int64_t)blockIdx.x * 2 * c;
     block_reduce_store(rz, sm, tr, tc, cp, rp, active, out + k);
     block_reduce_store(rr, sm, tr, tc, cp, rp, active, out + c + k);
+    if (last_block(counter)) cg_fin_beta(c, gridDim.x, partial, col, flags, tol);
 }
 
-__global__ void cg_finalize_beta_kernel(int c, int nblk, const double *__restrict__ partial, double *__restrict__ col,
-                                        int *__restrict__ flags, double tol)
-{
-    if (flags[0]) return;
-    int all = 1;
-    const int warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5, lane = threadIdx.x & 31;
-    for (int k = warp; k < c; k += nwarps)
-    {
-        const double rzn = warp_sum_partials(partial, 2 * c, k, nblk);
-        const double rr = warp_sum_partials(partial, 2 * c, c + k, nblk);
-        if (lane != 0) continue;
-        const int was = flags[2 + k];
-        col[3 * c + k] = (was || col[k] == 0.0) ? 0.0 : rzn / col[k];
-        col[k] = rzn;
-        const int cv = was || (sqrt(rr) <= tol * col[c + k]);
-        flags[2 + k] = cv;
-        all &= cv;
-    }
-    all = __syncthreads_and(all);
-    if (threadIdx.x == 0) { flags[0] = all; flags[1] += 1; }
-}
 
 __global__ void cg_pupdate_kernel(int64_t total, int c, const double *__restrict__ col, const double *__restrict__ z,
                                   double *__restrict__ p, const int *__restrict__ flags)
@@ -551,21 +594,24 @@ void CgSolver::enqueue_mass(const MeshDev &m, bool fp64_values, const double *b,
     flags_.reserve(2 + (size_t)c);
     const Layout L = make_layout(n, c);
     partial_.reserve((size_t)L.nblk * 2 * c);
+    if (!counter_.p)
+    {
+        counter_.reserve(1);
+        BAEMM_CUDA(cudaMemsetAsync(counter_.p, 0, sizeof(unsigned int), st));
+    }
     if (!host_flags_) BAEMM_CUDA(cudaMallocHost(&host_flags_, 2 * sizeof(int)));
     dim3 grid(L.nblk, L.nchunk);
-    const int fin = std::min(1024, 32 * c);   // finalize kernels: one warp per column
     auto run = [&](auto Lv, auto Mv) {
+        // three launches per iteration: each column-sum step runs in the last
+        // block of the kernel that produced the partial sums
         cg_init_kernel<<<grid, RT, 0, st>>>(n, c, L.cp, L.rp, L.rows_per_block, b, ldb, Lv, x_.p, r_.p, z_.p, p_.p,
-                                            partial_.p);
-        cg_finalize_init_kernel<<<1, fin, 0, st>>>(c, L.nblk, partial_.p, col_.p, flags_.p, tol);
+                                            partial_.p, counter_.p, col_.p, flags_.p, tol);
         for (int it = 0; it < max_iter; ++it)
         {
             cg_matvec_kernel<<<grid, RT, 0, st>>>(n, c, L.cp, L.rp, L.rows_per_block, m.mass_outer, m.mass_inner, Mv,
-                                                  p_.p, q_.p, partial_.p, flags_.p);
-            cg_finalize_alpha_kernel<<<1, fin, 0, st>>>(c, L.nblk, partial_.p, col_.p, flags_.p);
+                                                  p_.p, q_.p, partial_.p, counter_.p, col_.p, flags_.p);
             cg_update_kernel<<<grid, RT, 0, st>>>(n, c, L.cp, L.rp, L.rows_per_block, Lv, col_.p, x_.p, r_.p, z_.p,
-                                                  p_.p, q_.p, partial_.p, flags_.p);
-            cg_finalize_beta_kernel<<<1, fin, 0, st>>>(c, L.nblk, partial_.p, col_.p, flags_.p, tol);
+                                                  p_.p, q_.p, partial_.p, counter_.p, flags_.p, tol);
             cg_pupdate_kernel<<<eg(N), 256, 0, st>>>(N, c, col_.p, z_.p, p_.p, flags_.p);
         }
     };
@@ -575,6 +621,120 @@ void CgSolver::enqueue_mass(const MeshDev &m, bool fp64_values, const double *b,
     cg_output_kernel<<<eg(N), 256, 0, st>>>(n, c, x_.p, y, ldy);
     BAEMM_LAUNCH_CHECK();
     BAEMM_CUDA(cudaMemcpyAsync(host_flags_, flags_.p, 2 * sizeof(int), cudaMemcpyDeviceToHost, st));
+}
+
+void CgSolver::profile(const MeshDev &m, bool fp64_values, int c, int iterations, cudaStream_t st, double ms_out[3])
+{
+    const int64_t n = m.nv;
+    BAEMM_REQUIRE(c >= 1 && c <= kMaxKrylovColumns, BAEMM_ERR_SIZE, "CG column count out of range");
+    BAEMM_REQUIRE(iterations >= 1, BAEMM_ERR_ARG, "at least one iteration");
+    const int64_t N = n * c;
+    DevBuf<double> b;
+    b.reserve(N);
+    std::vector<double> ones((size_t)N, 1.0);
+    BAEMM_CUDA(cudaMemcpyAsync(b.p, ones.data(), N * sizeof(double), cudaMemcpyHostToDevice, st));
+    x_.reserve(N); r_.reserve(N); z_.reserve(N); p_.reserve(N); q_.reserve(N);
+    col_.reserve(4 * (size_t)c);
+    flags_.reserve(2 + (size_t)c);
+    const Layout L = make_layout(n, c);
+    partial_.reserve((size_t)L.nblk * 2 * c);
+    if (!counter_.p)
+    {
+        counter_.reserve(1);
+        BAEMM_CUDA(cudaMemsetAsync(counter_.p, 0, sizeof(unsigned int), st));
+    }
+    dim3 grid(L.nblk, L.nchunk);
+    cudaEvent_t ev[4];
+    for (auto &e : ev) BAEMM_CUDA(cudaEventCreate(&e));
+    double acc[3] = {0.0, 0.0, 0.0};
+    auto run = [&](auto Lv, auto Mv) {
+        // tol < 0: no column converges, every launch does its work
+        cg_init_kernel<<<grid, RT, 0, st>>>(n, c, L.cp, L.rp, L.rows_per_block, b.p, c, Lv, x_.p, r_.p, z_.p, p_.p,
+                                            partial_.p, counter_.p, col_.p, flags_.p, -1.0);
+        for (int it = 0; it < iterations; ++it)
+        {
+            BAEMM_CUDA(cudaEventRecord(ev[0], st));
+            cg_matvec_kernel<<<grid, RT, 0, st>>>(n, c, L.cp, L.rp, L.rows_per_block, m.mass_outer, m.mass_inner, Mv,
+                                                  p_.p, q_.p, partial_.p, counter_.p, col_.p, flags_.p);
+            BAEMM_CUDA(cudaEventRecord(ev[1], st));
+            cg_update_kernel<<<grid, RT, 0, st>>>(n, c, L.cp, L.rp, L.rows_per_block, Lv, col_.p, x_.p, r_.p, z_.p,
+                                                  p_.p, q_.p, partial_.p, counter_.p, flags_.p, -1.0);
+            BAEMM_CUDA(cudaEventRecord(ev[2], st));
+            cg_pupdate_kernel<<<eg(N), 256, 0, st>>>(N, c, col_.p, z_.p, p_.p, flags_.p);
+            BAEMM_CUDA(cudaEventRecord(ev[3], st));
+            BAEMM_CUDA(cudaEventSynchronize(ev[3]));
+            for (int q = 0; q < 3; ++q)
+            {
+                float ms = 0.f;
+                BAEMM_CUDA(cudaEventElapsedTime(&ms, ev[q], ev[q + 1]));
+                acc[q] += ms;
+            }
+        }
+    };
+    try
+    {
+        if (fp64_values) run(m.lumped_d.p, m.mass_d.p);
+        else run(m.lumped_f.p, m.mass_f.p);
+        BAEMM_LAUNCH_CHECK();
+    }
+    catch (...)
+    {
+        for (auto &e : ev) cudaEventDestroy(e);
+        throw;
+    }
+    for (auto &e : ev) BAEMM_CUDA(cudaEventDestroy(e));
+    for (int q = 0; q < 3; ++q) ms_out[q] = acc[q] / iterations;
+}
+
+void profile_gram_schmidt(int64_t n, int c, int nvec, int reps, cudaStream_t st, double ms_out[2])
+{
+    BAEMM_REQUIRE(c >= 1 && c <= kMaxKrylovColumns && nvec >= 1 && nvec <= kMaxRestart + 1 && reps >= 1,
+                  BAEMM_ERR_ARG, "Gram-Schmidt profile: sizes out of range");
+    const int64_t N = n * c;
+    DevBuf<double2> V, w, h;
+    V.reserve((size_t)nvec * N);
+    w.reserve(N);
+    h.reserve((size_t)nvec * c);
+    const Layout L = make_layout(n, c);
+    DevBuf<double> partial;
+    partial.reserve((size_t)L.nblk * nvec * c * 2);
+    // constant blocks (the timing does not depend on the values); h small so w stays finite
+    BAEMM_CUDA(cudaMemsetAsync(V.p, 0, (size_t)nvec * N * sizeof(double2), st));
+    BAEMM_CUDA(cudaMemsetAsync(w.p, 0, N * sizeof(double2), st));
+    BAEMM_CUDA(cudaMemsetAsync(h.p, 0, (size_t)nvec * c * sizeof(double2), st));
+    dim3 grid(L.nblk, L.nchunk);
+    cudaEvent_t ev[3];
+    for (auto &e : ev) BAEMM_CUDA(cudaEventCreate(&e));
+    double acc[2] = {0.0, 0.0};
+    try
+    {
+        for (int r = 0; r <= reps; ++r)   // the first round is a warm-up
+        {
+            BAEMM_CUDA(cudaEventRecord(ev[0], st));
+            gs_dot_kernel<double2><<<grid, RT, 0, st>>>(n, c, L.cp, L.rp, L.rows_per_block, V.p, nvec, w.p,
+                                                        partial.p);
+            BAEMM_CUDA(cudaEventRecord(ev[1], st));
+            gs_update_kernel<double2><<<eg(N), 256, 0, st>>>(n, c, V.p, nvec, h.p, w.p);
+            BAEMM_CUDA(cudaEventRecord(ev[2], st));
+            BAEMM_CUDA(cudaEventSynchronize(ev[2]));
+            BAEMM_LAUNCH_CHECK();
+            if (r == 0) continue;
+            for (int q = 0; q < 2; ++q)
+            {
+                float ms = 0.f;
+                BAEMM_CUDA(cudaEventElapsedTime(&ms, ev[q], ev[q + 1]));
+                acc[q] += ms;
+            }
+        }
+    }
+    catch (...)
+    {
+        for (auto &e : ev) cudaEventDestroy(e);
+        throw;
+    }
+    for (auto &e : ev) BAEMM_CUDA(cudaEventDestroy(e));
+    ms_out[0] = acc[0] / reps;
+    ms_out[1] = acc[1] / reps;
 }
 
 // =================================== GMRES host ===================================

@@ -39,12 +39,24 @@ public:
     void enqueue_mass(const MeshDev &m, bool fp64_values, const double *b, int64_t ldb, double *y, int64_t ldy, int c,
                       double tol, int max_iter, cudaStream_t st);
     bool finish(cudaStream_t st, int *iterations);
+    // Device time of the CG iteration's kernels on the mesh's mass matrix:
+    // `iterations` iterations on c real columns (right-hand side all ones,
+    // no column allowed to converge), each launch bracketed by CUDA events.
+    // ms_out: mean ms per launch of {matvec, update, p update}.
+    void profile(const MeshDev &m, bool fp64_values, int c, int iterations, cudaStream_t st, double ms_out[3]);
 
 private:
     DevBuf<double> x_, r_, z_, p_, q_, col_, partial_;
     DevBuf<int> flags_;
+    DevBuf<unsigned int> counter_;   // last-block detection of the column sums (zero between kernels)
     int *host_flags_ = nullptr;
 };
+
+// Device time of one classical Gram-Schmidt pass of a GMRES iteration on an
+// n x c complex block against nvec basis vectors (the kernels of the batched
+// GMRES below, on scratch blocks of constant values): mean ms per launch of
+// {dot products, update}, over `reps` launches each.
+void profile_gram_schmidt(int64_t n, int c, int nvec, int reps, cudaStream_t st, double ms_out[2]);
 
 template <class S>   // S = double (real) or double2 (complex)
 class GmresSolver

@@ -130,18 +130,41 @@ void launch_pack_points(int64_t m, const double *pts3, R *pts4, cudaStream_t st)
 // tcgen05 MMAs per K step, FP32 accumulation in TMEM.  wave_chunk_size 16.
 // `err` (device int) receives a non-zero code when a bounded wait gave up.
 bool tc_supported(int wc, int wcs);
-// seg_tiles: 16-source tiles accumulated in TMEM before the partial sum is
-// added to FP32 registers (bounds the tensor-core accumulation chain).
-void launch_boundary_tc(const MeshDev &m, const OpFlags &f, const void *chunk_params, int wc, int wcs,
-                        const float *tgeo, const float2 *Btri, float2 *Ctri, float2 *ws, size_t ws_elems, int *err,
-                        cudaStream_t st, int seg_tiles = 16, int ctas = 0, int stagger = 0, int64_t row_begin = 0,
-                        int64_t row_end = -1);
+// The coefficient structure of the loaded chunks the tensor-core form
+// specialises on (host side, once per LoadParameters): ki = every chunk has
+// c1 = i s kappa with one common s, and c2, c3 real and common to all chunks
+// (the mixed BIE and DtN tuples of FarField.hpp).
+struct TcCoeffForm
+{
+    bool ki = false;
+    float s = 0.f;
+};
+TcCoeffForm tc_coeff_form(const ChunkParamsF *host_params, int groups);
+// Settings of the tensor-core form (the autotuner's search space):
+//   seg_tiles  16-source tiles accumulated in TMEM before the partial sum is
+//              added to FP32 registers (bounds the tensor-core accumulation chain);
+//   ctas       persistent grid size (0: one CTA per SM);
+//   stagger    sweep offset between CTAs (tiles; -1: spread evenly);
+//   gen_warps  generator warps, 8 or 16;
+//   chunks     16-column groups per work unit, 1, 2 or 4 (0: the most the wave shape allows).
+struct TcTuning
+{
+    int seg_tiles = 16;
+    int ctas = 0;
+    int stagger = 0;
+    int gen_warps = 16;
+    int chunks = 0;
+};
+// The chunk groups per work unit a launch uses for wave_count wc and the setting `chunks`.
+int tc_chunks_per_unit(int wc, int chunks);
+void launch_boundary_tc(const MeshDev &m, const OpFlags &f, const void *chunk_params, const TcCoeffForm &form, int wc,
+                        int wcs, const float *tgeo, const float2 *Btri, float2 *Ctri, float2 *ws, size_t ws_elems,
+                        int *err, cudaStream_t st, const TcTuning &tune, int64_t row_begin = 0, int64_t row_end = -1);
 // The tensor-core form of the near field: targets pts4 (npts x 4 floats), no
 // pair excluded, flags without the adjoint double layer.
-void launch_nearfield_tc(const MeshDev &m, const OpFlags &f, const void *chunk_params, int wc, int wcs,
-                         const float *tgeo, const float *pts4, int64_t npts, const float2 *Btri, float2 *Cpts,
-                         float2 *ws, size_t ws_elems, int *err, cudaStream_t st, int seg_tiles = 16, int ctas = 0,
-                         int stagger = 0);
+void launch_nearfield_tc(const MeshDev &m, const OpFlags &f, const void *chunk_params, const TcCoeffForm &form,
+                         int wc, int wcs, const float *tgeo, const float *pts4, int64_t npts, const float2 *Btri,
+                         float2 *Cpts, float2 *ws, size_t ws_elems, int *err, cudaStream_t st, const TcTuning &tune);
 // Source geometry of the tensor-core form, per 16-source tile (built once per mesh).
 size_t tc_tile_geometry_floats(int64_t nt);
 void launch_tc_tile_geometry(const MeshDev &m, float *tgeo, cudaStream_t st);

@@ -48,6 +48,7 @@
 #include "ops.cuh"
 
 #include <algorithm>
+#include <cmath>
 #include <cstddef>
 #include <mutex>
 
@@ -61,23 +62,22 @@ constexpr int TC_SRC = 16;         // sources per K tile
 constexpr int TC_N = 32;           // MMA N: 16 columns as (re | im)
 constexpr int TC_CHMAX = 4;        // chunks per work unit
 constexpr int TC_MAXCHUNKS = 32;   // wave_count <= 512 with wave_chunk_size 16
-// Generator warps: 16 (4 per SM sub-partition, 4 sources per thread and tile,
-// <= 96 registers at 640 threads) hide the latency of the entry evaluation
-// better than 8 (8 sources per thread): 146 vs 159 ms on the 153,600-triangle
-// torus with 64 right-hand sides.
-#ifndef BAEMM_TC_GEN_WARPS
-#define BAEMM_TC_GEN_WARPS 16
-#endif
-constexpr int TC_GEN_WARPS = BAEMM_TC_GEN_WARPS;   // 8 or 16
-constexpr int TC_GEN_THREADS = 32 * TC_GEN_WARPS;
-constexpr int TC_GROUPS = TC_GEN_WARPS / 4;        // source groups of a tile (4 warps cover the 128 rows)
-constexpr int TC_SPT = 16 / TC_GROUPS;             // sources per generator thread and tile
-constexpr int TC_PPT = TC_SPT / 2;                 // their pairs
-constexpr int TC_KPT = 2 * TC_SPT;                 // their K columns of an A stage
-constexpr int TC_CPG = 16 / TC_GROUPS;             // right-hand sides per thread in the drain
-static_assert(TC_GEN_WARPS == 8 || TC_GEN_WARPS == 16, "8 or 16 generator warps");
+// Generator warps GW = 16 (4 per SM sub-partition, 4 sources per thread and
+// tile) or 8 (8 sources per thread); the autotuner picks one per problem
+// shape.  16 hide the latency of the entry evaluation better on large blocks.
 constexpr int TC_EXP_THREADS = 64;
-constexpr int TC_THREADS = TC_GEN_THREADS + TC_EXP_THREADS + 64;   // + TMA producer warp + MMA warp
+template <int GW>
+struct TcShape
+{
+    static_assert(GW == 8 || GW == 16, "8 or 16 generator warps");
+    static constexpr int GEN_THREADS = 32 * GW;
+    static constexpr int GROUPS = GW / 4;        // source groups of a tile (4 warps cover the 128 rows)
+    static constexpr int SPT = 16 / GROUPS;      // sources per generator thread and tile
+    static constexpr int PPT = SPT / 2;          // their pairs
+    static constexpr int KPT = 2 * SPT;          // their K columns of an A stage
+    static constexpr int CPG = 16 / GROUPS;      // right-hand sides per thread in the drain
+    static constexpr int THREADS = GEN_THREADS + TC_EXP_THREADS + 64;   // + bulk-copy warp + MMA warp
+};
 constexpr int TC_ASTAGES = 4;      // A stages in TMEM (one chunk of one tile each)
 constexpr int TC_BSTAGES = 3;      // expanded B image stages in shared memory
 constexpr int TC_RSTAGES = 6;      // raw tile stages filled by bulk copies
@@ -183,17 +183,22 @@ __device__ __forceinline__ bool wait_bar(uint64_t *bar, uint32_t parity, volatil
     return false;
 }
 
-// Non-blocking test of the phase (no suspension).
-__device__ __forceinline__ bool mbar_test_wait(uint64_t *bar, uint32_t parity)
+// The slow path of a wait, out of line so that the hot loops stay small: the
+// fast path is one suspending try_wait.
+__device__ __noinline__ bool wait_bar_slow(uint64_t *bar, uint32_t parity, volatile int *abort_flag, int *err,
+                                           int code)
 {
-    uint32_t ok;
-    asm volatile("{\n\t.reg .pred p;\n\t"
-                 "mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-                 "selp.u32 %0, 1, 0, p;\n\t}"
-                 : "=r"(ok)
-                 : "r"(smem_u32(bar)), "r"(parity)
-                 : "memory");
-    return ok != 0;
+    return wait_bar(bar, parity, abort_flag, err, code);
+}
+
+// Warp-uniform bounded wait: true on every lane when the phase completed for
+// the whole warp (the warp-collective tcgen05 instructions that follow need
+// the warp to agree).
+__device__ __forceinline__ bool warp_wait(uint64_t *bar, uint32_t parity, volatile int *abort_flag, int *err, int code)
+{
+    bool got = mbar_try_wait(bar, parity);
+    if (!got) got = wait_bar_slow(bar, parity, abort_flag, err, code);
+    return __all_sync(0xffffffffu, got);
 }
 
 // One lane of a converged warp (the lowest), for the single-thread
@@ -347,6 +352,7 @@ struct TcPlan
     int tail_blocks;   // ncg * nblk - full_waves * ctas
     int64_t tail_units;   // tail_blocks * ntiles
     int stagger;       // whole-block sweeps of CTA k start at tile (k % 8) * stagger; -1: k * ntiles / ctas
+    float ki_s;        // KI form: the common ratio s = c1.y / kappa (scaled coefficients)
 };
 
 __host__ __device__ __forceinline__ int64_t tc_tail_start(const TcPlan &p, int k)
@@ -398,15 +404,141 @@ struct PieceIter
     }
 };
 
+// The kernel entries of one wave chunk for this thread's PPT source pairs,
+// in the A operand's K order (Re A_s0, Re A_s1, Im A_s0, Im A_s1) per pair,
+// split into hi (the FP32 bits; the tensor core reads their top 19 as TF32)
+// and lo = x - trunc_tf32(x).  P: the chunk's broadcast pairs kappa, -kappa,
+// c1.x, c1.y, -c2.x, -c2.y, c3.x, c3.y.  Per pair: rinv = 1/r, r, dmu =
+// (z.mu_j)/r^3, dnu = (z.nu_i)/r^3 (zero rinv masks a pair).
+//   A = e^{i k r} h,  h = c1 / r + u + i k r (-u),  u = -(c2 dmu - c3 dnu):
+//   hx = c1x / r + ux + k r uy,   hy = c1y / r + uy - k r ux.
 // RI: every chunk's single-layer coefficient is imaginary and its double- and
 // adjoint-double-layer coefficients are real (the mixed BIE and DtN tuples of
-// FarField.hpp), so the double-layer factor u below is real.
-template <int CH, bool SL, bool DL, bool ADL, bool RI>
-__global__ void __launch_bounds__(TC_THREADS, 1)
+// FarField.hpp), so u is real: hx = ux, hy = c1y / r - k r ux.  The sincos is
+// taken of -k r there, which gives -sin(k r) and saves the negation of the
+// rotation's real part.
+template <int PPT, bool SL, bool DL, bool ADL, bool RI>
+__device__ __forceinline__ void tc_entries(const float2 *__restrict__ P, const float2 (&rinv)[PPT],
+                                           const float2 (&r)[PPT], const float2 (&dmu)[PPT],
+                                           const float2 (&dnu)[PPT], uint32_t (&hi)[4 * PPT],
+                                           uint32_t (&lo)[4 * PPT])
+{
+    const float2 m1 = make_float2(-1.f, -1.f);
+    #pragma unroll
+    for (int p = 0; p < PPT; ++p)
+    {
+        float2 ax, ay;
+        if (RI)
+        {
+            const float2 nkr = __fmul2_rn(P[1], r[p]);   // -k r
+            float sn0, cs0, sn1, cs1;
+            __sincosf(nkr.x, &sn0, &cs0);
+            __sincosf(nkr.y, &sn1, &cs1);
+            const float2 cs = make_float2(cs0, cs1), nsn = make_float2(sn0, sn1);   // cos(k r), -sin(k r)
+            float2 ux = make_float2(0.f, 0.f);
+            if (DL) ux = __fmul2_rn(P[4], dmu[p]);
+            if (ADL) ux = DL ? __ffma2_rn(P[6], dnu[p], ux) : __fmul2_rn(P[6], dnu[p]);
+            float2 hy;
+            if (DL || ADL) hy = SL ? __ffma2_rn(nkr, ux, __fmul2_rn(P[3], rinv[p])) : __fmul2_rn(nkr, ux);
+            else hy = __fmul2_rn(P[3], rinv[p]);
+            // (ax, ay) = (ux cs - hy sn, ux sn + hy cs)
+            ax = __ffma2_rn(hy, nsn, __fmul2_rn(ux, cs));
+            ay = __ffma2_rn(hy, cs, __fmul2_rn(ux, __fmul2_rn(m1, nsn)));
+            if (!(DL || ADL)) ax = __fmul2_rn(hy, nsn);
+        }
+        else
+        {
+            const float2 kr = __fmul2_rn(P[0], r[p]);
+            float sn0, cs0, sn1, cs1;
+            __sincosf(kr.x, &sn0, &cs0);
+            __sincosf(kr.y, &sn1, &cs1);
+            const float2 cs = make_float2(cs0, cs1), sn = make_float2(sn0, sn1);
+            float2 hx = make_float2(0.f, 0.f), hy = make_float2(0.f, 0.f);
+            if (SL)
+            {
+                hx = __fmul2_rn(P[2], rinv[p]);
+                hy = __fmul2_rn(P[3], rinv[p]);
+            }
+            if (DL || ADL)
+            {
+                float2 ux = make_float2(0.f, 0.f), uy = make_float2(0.f, 0.f);
+                if (DL) { ux = __fmul2_rn(P[4], dmu[p]); uy = __fmul2_rn(P[5], dmu[p]); }
+                if (ADL) { ux = __ffma2_rn(P[6], dnu[p], ux); uy = __ffma2_rn(P[7], dnu[p], uy); }
+                const float2 nkr = __fmul2_rn(P[1], r[p]);
+                hx = __ffma2_rn(kr, uy, __fadd2_rn(hx, ux));
+                hy = __ffma2_rn(nkr, ux, __fadd2_rn(hy, uy));
+            }
+            // (ax, ay) = (hx cs - hy sn, hx sn + hy cs)
+            ax = __ffma2_rn(hy, __fmul2_rn(m1, sn), __fmul2_rn(hx, cs));
+            ay = __ffma2_rn(hy, cs, __fmul2_rn(hx, sn));
+        }
+        const float2 tx = make_float2(__uint_as_float(__float_as_uint(ax.x) & 0xffffe000u),
+                                      __uint_as_float(__float_as_uint(ax.y) & 0xffffe000u));
+        const float2 ty = make_float2(__uint_as_float(__float_as_uint(ay.x) & 0xffffe000u),
+                                      __uint_as_float(__float_as_uint(ay.y) & 0xffffe000u));
+        const float2 lx = __ffma2_rn(tx, m1, ax), ly = __ffma2_rn(ty, m1, ay);
+        hi[4 * p + 0] = __float_as_uint(ax.x);
+        hi[4 * p + 1] = __float_as_uint(ax.y);
+        hi[4 * p + 2] = __float_as_uint(ay.x);
+        hi[4 * p + 3] = __float_as_uint(ay.y);
+        lo[4 * p + 0] = __float_as_uint(lx.x);
+        lo[4 * p + 1] = __float_as_uint(lx.y);
+        lo[4 * p + 2] = __float_as_uint(ly.x);
+        lo[4 * p + 3] = __float_as_uint(ly.y);
+    }
+}
+
+// KI: RI with the structure of the BIE and DtN tuples over all chunks:
+// c1 = i s kappa with s common, c2 and c3 real and common.  Then
+//   hy = c1y / r - k r ux = kappa v,   v = s / r - r ux,
+// and ux, -ux and v are per source pair, shared by every chunk (computed with
+// the pair geometry): a chunk costs the phase, its sincos, hy, the rotation
+// and the split.
+template <int PPT>
+__device__ __forceinline__ void tc_entries_ki(const float2 *__restrict__ P, const float2 (&r)[PPT],
+                                              const float2 (&ux)[PPT], const float2 (&nux)[PPT],
+                                              const float2 (&v)[PPT], uint32_t (&hi)[4 * PPT],
+                                              uint32_t (&lo)[4 * PPT])
+{
+    const float2 m1 = make_float2(-1.f, -1.f);
+    #pragma unroll
+    for (int p = 0; p < PPT; ++p)
+    {
+        const float2 nkr = __fmul2_rn(P[1], r[p]);   // -k r
+        float sn0, cs0, sn1, cs1;
+        __sincosf(nkr.x, &sn0, &cs0);
+        __sincosf(nkr.y, &sn1, &cs1);
+        const float2 cs = make_float2(cs0, cs1), nsn = make_float2(sn0, sn1);   // cos(k r), -sin(k r)
+        const float2 hy = __fmul2_rn(P[0], v[p]);
+        // (ax, ay) = (ux cs - hy sn, ux sn + hy cs)
+        const float2 ax = __ffma2_rn(hy, nsn, __fmul2_rn(ux[p], cs));
+        const float2 ay = __ffma2_rn(hy, cs, __fmul2_rn(nux[p], nsn));
+        const float2 tx = make_float2(__uint_as_float(__float_as_uint(ax.x) & 0xffffe000u),
+                                      __uint_as_float(__float_as_uint(ax.y) & 0xffffe000u));
+        const float2 ty = make_float2(__uint_as_float(__float_as_uint(ay.x) & 0xffffe000u),
+                                      __uint_as_float(__float_as_uint(ay.y) & 0xffffe000u));
+        const float2 lx = __ffma2_rn(tx, m1, ax), ly = __ffma2_rn(ty, m1, ay);
+        hi[4 * p + 0] = __float_as_uint(ax.x);
+        hi[4 * p + 1] = __float_as_uint(ax.y);
+        hi[4 * p + 2] = __float_as_uint(ay.x);
+        hi[4 * p + 3] = __float_as_uint(ay.y);
+        lo[4 * p + 0] = __float_as_uint(lx.x);
+        lo[4 * p + 1] = __float_as_uint(lx.y);
+        lo[4 * p + 2] = __float_as_uint(ly.x);
+        lo[4 * p + 3] = __float_as_uint(ly.y);
+    }
+}
+
+// RI, KI: see tc_entries and tc_entries_ki.  GW: generator warps (TcShape).
+template <int GW, int CH, bool SL, bool DL, bool ADL, bool RI, bool KI>
+__global__ void __launch_bounds__(TcShape<GW>::THREADS, 1)
 boundary_tc_kernel(const float *__restrict__ mid4, const float *__restrict__ nrm4, const TcTileGeo *__restrict__ tgeo,
                    const float2 *__restrict__ Btri, float2 *__restrict__ Ctri, float2 *__restrict__ ws,
                    const ChunkParamsF *__restrict__ prm, const TcPlan plan, int *err)
 {
+    constexpr int TC_GEN_THREADS = TcShape<GW>::GEN_THREADS;
+    constexpr int TC_SPT = TcShape<GW>::SPT, TC_PPT = TcShape<GW>::PPT, TC_KPT = TcShape<GW>::KPT;
+    constexpr int TC_CPG = TcShape<GW>::CPG;
     extern __shared__ __align__(1024) uint8_t smem_raw[];
     // Align inside the shared window by pointer arithmetic on the shared array,
     // so every access below compiles to a shared-memory instruction.
@@ -460,32 +592,33 @@ boundary_tc_kernel(const float *__restrict__ mid4, const float *__restrict__ nrm
     if (tid < TC_GEN_THREADS)
     {
         // ------------------------------ generators ------------------------------
-        constexpr int CC = 1;                 // A stages published together
-        uint32_t hiA[TC_KPT], loA[TC_KPT], hiB[TC_KPT], loB[TC_KPT];   // alternating register buffers of consecutive chunks
+        // Per tile: the pair geometry (shared by every chunk), then per chunk
+        // (unrolled): its entries, publication of the previous chunk's A stage,
+        // the wait for this chunk's stage, two TMEM stores.  The ring index of
+        // chunk c of tile T is (T CH + c) mod TC_ASTAGES, a compile-time
+        // column offset when CH == TC_ASTAGES.
         const int q = warp & 3, g = warp >> 2;
         const int row = q * 32 + lane;
         const uint32_t lane_addr = tbase + ((uint32_t)(q * 32) << 16);
+        const uint32_t a_addr = lane_addr + (uint32_t)(TC_ACOL + g * TC_KPT);
         float2 *acc_row = &sm.acc[row][g * TC_CPG];
         bool ok = true;
-        int pending[CC];    // A stages written but not yet published
-        int npending = 0;
-        int T = 0, SG = 0;  // tiles and TMEM segments handled so far by this CTA
+        bool pend = false;          // an A stage is written and not yet published
+        uint32_t pend_stage = 0;
+        int T = 0, SG = 0;          // tiles and TMEM segments handled so far by this CTA
         auto publish = [&]() {
-            if (npending > 0)
+            if (pend)
             {
                 asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
                 tc_fence_before();
-                #pragma unroll
-                for (int k = 0; k < CC; ++k)
-                    if (k < npending) mbar_arrive(&sm.a_full[pending[k]]);
-                npending = 0;
+                mbar_arrive(&sm.a_full[pend_stage]);
+                pend = false;
             }
         };
         // add (or, first in a piece, store) the finished TMEM partial sum of
         // segment `sg` (main + correction) into this thread's accumulator row
         auto drain = [&](int sg, bool first) {
-            const bool got = wait_bar(&sm.seg_full, (uint32_t)sg & 1u, abort_flag, err, 2);
-            if (!__all_sync(0xffffffffu, got)) return false;
+            if (!warp_wait(&sm.seg_full, (uint32_t)sg & 1u, abort_flag, err, 2)) return false;
             tc_fence_after();
             #pragma unroll
             for (int c = 0; c < CH; ++c)
@@ -515,7 +648,6 @@ boundary_tc_kernel(const float *__restrict__ mid4, const float *__restrict__ nrm
         };
         PieceIter it(plan, k_cta);
         int cg, blk, tb, te, slot, rot;
-        const float2 m1 = make_float2(-1.f, -1.f);
         while (ok && it.next(plan, cg, blk, tb, te, slot, rot))
         {
             const int i = blk * TC_M + row;
@@ -532,30 +664,34 @@ boundary_tc_kernel(const float *__restrict__ mid4, const float *__restrict__ nrm
                     tn0 = make_float2(v.x, v.x); tn1 = make_float2(v.y, v.y); tn2 = make_float2(v.z, v.z);
                 }
             }
+            const float2 *Pg = sm.prm[cg * CH];
+            // the source tiles that hold the target block's own triangles (masked)
+            const int self_lo = plan.self ? (plan.off + blk * TC_M) / TC_SRC : ntiles;
+            const int self_hi = plan.self ? (plan.off + blk * TC_M + TC_M - 1) / TC_SRC : -1;
             bool first_drain = true;
             // A finished segment is drained right after the next segment's first
-            // step is queued, so the tensor core has work waiting when it resumes.
+            // chunk is stored, so the tensor core has work waiting when it resumes.
             int drain_due = -1;
             for (int t = tb; t < te; ++t, ++T)
             {
                 const int rs = T % TC_RSTAGES;
                 const int ts = t + rot < ntiles ? t + rot : t + rot - ntiles;   // source tile (rot < ntiles)
+                if (!warp_wait(&sm.r_full[rs], (uint32_t)(T / TC_RSTAGES) & 1u, abort_flag, err, 1))
                 {
-                    const bool got = wait_bar(&sm.r_full[rs], (uint32_t)(T / TC_RSTAGES) & 1u, abort_flag, err, 1);
-                    if (!__all_sync(0xffffffffu, got)) { ok = false; break; }
+                    ok = false;
+                    break;
                 }
                 // per source pair: 1/r, r, (z.mu_j)/r^3, (z.nu_i)/r^3; shared by every chunk
                 float2 rinv[TC_PPT], r[TC_PPT], dmu[TC_PPT], dnu[TC_PPT];
                 {
                     const TcTileGeo &G = sm.raw[rs].geo;
+                    const int s0 = g * TC_SPT;
                     // tiles that hold the target itself or padding past the end need masks
-                    const bool special = (ts == ntiles - 1) ||
-                                         (plan.self && ts * TC_SRC < plan.off + blk * TC_M + TC_M &&
-                                          ts * TC_SRC + TC_SRC > plan.off + blk * TC_M);
+                    const bool special = (ts == ntiles - 1) || (ts >= self_lo && ts <= self_hi);
                     #pragma unroll
                     for (int p = 0; p < TC_PPT; ++p)
                     {
-                        const int sl = g * TC_SPT + 2 * p;
+                        const int sl = s0 + 2 * p;
                         const float2 zx = __fadd2_rn(*reinterpret_cast<const float2 *>(&G.x[sl]), nx0);
                         const float2 zy = __fadd2_rn(*reinterpret_cast<const float2 *>(&G.y[sl]), nx1);
                         const float2 zz = __fadd2_rn(*reinterpret_cast<const float2 *>(&G.z[sl]), nx2);
@@ -581,104 +717,50 @@ boundary_tc_kernel(const float *__restrict__ mid4, const float *__restrict__ nrm
                     }
                 }
                 mbar_arrive(&sm.r_empty[rs]);
-                // One chunk: evaluate its kernel entries into (hi, lo), publish the
-                // previous chunk's A stage, store this one.  Consecutive chunks use
-                // the two register buffers alternately, so the math of a chunk never
-                // writes registers the previous chunk's TMEM stores still read.
-                auto do_chunk = [&](int c, uint32_t (&hi)[TC_KPT], uint32_t (&lo)[TC_KPT]) -> bool {
-                    const int u = T * CH + c;
-                    const int stage = u % TC_ASTAGES;
-                    // test the A stage now; the answer arrives during the math
-                    bool ready = u < TC_ASTAGES ||
-                                 mbar_test_wait(&sm.a_empty[stage], (uint32_t)((u / TC_ASTAGES) - 1) & 1u);
-                    const float2 *P = sm.prm[cg * CH + c];
-                    const float2 kap = P[0], nkap = P[1], c1x = P[2], c1y = P[3];
-                    const float2 nc2x = P[4], nc2y = P[5], c3x = P[6], c3y = P[7];
+                // KI: ux = -(c2 dmu - c3 dnu), -ux and v = s / r - r ux per pair (every chunk's c2, c3 and s)
+                float2 kux[TC_PPT], knux[TC_PPT], kv[TC_PPT];
+                if (KI)
+                {
+                    const float2 s2 = make_float2(plan.ki_s, plan.ki_s);
                     #pragma unroll
                     for (int p = 0; p < TC_PPT; ++p)
                     {
-                        // A = e^{i k r} h,  h = c1 / r + w (i k r - 1) = c1 / r + u + i k r (-u),  u = -w
-                        //   hx = c1x / r + ux + k r uy,   hy = c1y / r + uy - k r ux
-                        const float2 kr = __fmul2_rn(kap, r[p]);
-                        float sn0, cs0, sn1, cs1;
-                        __sincosf(kr.x, &sn0, &cs0);
-                        __sincosf(kr.y, &sn1, &cs1);
-                        const float2 cs = make_float2(cs0, cs1), sn = make_float2(sn0, sn1);
-                        float2 hx = make_float2(0.f, 0.f), hy = make_float2(0.f, 0.f);
-                        if (RI)
-                        {
-                            // c1 = i c1y, c2 and c3 real: u = (ux, 0), hx = ux, hy = c1y / r - k r ux
-                            if (SL) hy = __fmul2_rn(c1y, rinv[p]);
-                            if (DL || ADL)
-                            {
-                                float2 ux = DL ? __fmul2_rn(nc2x, dmu[p]) : make_float2(0.f, 0.f);
-                                if (ADL) ux = DL ? __ffma2_rn(c3x, dnu[p], ux) : __fmul2_rn(c3x, dnu[p]);
-                                const float2 nkr = __fmul2_rn(nkap, r[p]);
-                                hx = ux;
-                                hy = SL ? __ffma2_rn(nkr, ux, hy) : __fmul2_rn(nkr, ux);
-                            }
-                        }
-                        else if (SL)
-                        {
-                            hx = __fmul2_rn(c1x, rinv[p]);
-                            hy = __fmul2_rn(c1y, rinv[p]);
-                        }
-                        if (!RI && (DL || ADL))
-                        {
-                            float2 ux = make_float2(0.f, 0.f), uy = make_float2(0.f, 0.f);
-                            if (DL) { ux = __fmul2_rn(nc2x, dmu[p]); uy = __fmul2_rn(nc2y, dmu[p]); }
-                            if (ADL) { ux = __ffma2_rn(c3x, dnu[p], ux); uy = __ffma2_rn(c3y, dnu[p], uy); }
-                            const float2 nkr = __fmul2_rn(nkap, r[p]);
-                            hx = __ffma2_rn(kr, uy, __fadd2_rn(hx, ux));
-                            hy = __ffma2_rn(nkr, ux, __fadd2_rn(hy, uy));
-                        }
-                        // (ax, ay) = (hx cs - hy sn, hx sn + hy cs)
-                        const float2 msn = __fmul2_rn(m1, sn);
-                        const float2 ax = __ffma2_rn(hy, msn, __fmul2_rn(hx, cs));
-                        const float2 ay = __ffma2_rn(hy, cs, __fmul2_rn(hx, sn));
-                        // hi = the FP32 bits (read as TF32 by the tensor core), lo = x - trunc_tf32(x)
-                        const float2 tx = make_float2(__uint_as_float(__float_as_uint(ax.x) & 0xffffe000u),
-                                                      __uint_as_float(__float_as_uint(ax.y) & 0xffffe000u));
-                        const float2 ty = make_float2(__uint_as_float(__float_as_uint(ay.x) & 0xffffe000u),
-                                                      __uint_as_float(__float_as_uint(ay.y) & 0xffffe000u));
-                        const float2 lx = __ffma2_rn(tx, m1, ax), ly = __ffma2_rn(ty, m1, ay);
-                        hi[4 * p + 0] = __float_as_uint(ax.x);
-                        hi[4 * p + 1] = __float_as_uint(ax.y);
-                        hi[4 * p + 2] = __float_as_uint(ay.x);
-                        hi[4 * p + 3] = __float_as_uint(ay.y);
-                        lo[4 * p + 0] = __float_as_uint(lx.x);
-                        lo[4 * p + 1] = __float_as_uint(lx.y);
-                        lo[4 * p + 2] = __float_as_uint(ly.x);
-                        lo[4 * p + 3] = __float_as_uint(ly.y);
+                        float2 ux = make_float2(0.f, 0.f);
+                        if (DL) ux = __fmul2_rn(Pg[4], dmu[p]);
+                        if (ADL) ux = DL ? __ffma2_rn(Pg[6], dnu[p], ux) : __fmul2_rn(Pg[6], dnu[p]);
+                        kux[p] = ux;
+                        knux[p] = make_float2(-ux.x, -ux.y);
+                        kv[p] = __ffma2_rn(r[p], knux[p], __fmul2_rn(s2, rinv[p]));
                     }
+                }
+                #pragma unroll
+                for (int c = 0; c < CH; ++c)
+                {
+                    uint32_t hi[TC_KPT], lo[TC_KPT];
+                    if (KI) tc_entries_ki<TC_PPT>(Pg + 8 * c, r, kux, knux, kv, hi, lo);
+                    else tc_entries<TC_PPT, SL, DL, ADL, RI>(Pg + 8 * c, rinv, r, dmu, dnu, hi, lo);
+                    const uint32_t u = (uint32_t)T * CH + c;
+                    const uint32_t stage = u % TC_ASTAGES;
                     // publish the previous chunk's stage now that its stores had this math to land
                     publish();
-                    if (!ready)
-                        ready = wait_bar(&sm.a_empty[stage], (uint32_t)((u / TC_ASTAGES) - 1) & 1u, abort_flag, err, 3);
-                    // the tcgen05 stores below are warp-collective: the warp agrees on the outcome
-                    if (!__all_sync(0xffffffffu, ready)) return false;
+                    // the stage is free once the MMAs that read it four chunks ago completed
+                    if (!warp_wait(&sm.a_empty[stage], ((u / TC_ASTAGES) & 1u) ^ 1u, abort_flag, err, 3))
+                    {
+                        ok = false;
+                        break;
+                    }
                     tc_fence_after();
-                    const uint32_t acol = TC_ACOL + (uint32_t)stage * 64u + (uint32_t)(g * TC_KPT);
-                    tmem_st<TC_KPT>(lane_addr + acol, hi);
-                    tmem_st<TC_KPT>(lane_addr + acol + 32u, lo);
-                    pending[0] = stage;
-                    npending = 1;
-                    if (drain_due >= 0)
+                    tmem_st<TC_KPT>(a_addr + stage * 64u, hi);
+                    tmem_st<TC_KPT>(a_addr + stage * 64u + 32u, lo);
+                    pend = true;
+                    pend_stage = stage;
+                    if (c == 0 && drain_due >= 0)
                     {
                         publish();
-                        if (!drain(drain_due, first_drain)) return false;
+                        if (!drain(drain_due, first_drain)) { ok = false; break; }
                         first_drain = false;
                         drain_due = -1;
                     }
-                    return true;
-                };
-                // pairs of chunks: two copies of the chunk body (more would overflow the
-                // instruction cache)
-                #pragma unroll 1
-                for (int c0 = 0; c0 < CH; c0 += 2)
-                {
-                    if (!do_chunk(c0, hiA, loA)) { ok = false; break; }
-                    if (c0 + 1 < CH && !do_chunk(c0 + 1, hiB, loB)) { ok = false; break; }
                 }
                 if (!ok) break;
                 const int lt = t - tb;
@@ -723,11 +805,20 @@ boundary_tc_kernel(const float *__restrict__ mid4, const float *__restrict__ nrm
     else if (tid < TC_GEN_THREADS + TC_EXP_THREADS)
     {
         // ------------------------------ expanders ------------------------------
-        // item = (16-byte group of sources sp, chunk c, row pair qq / qq + 16);
+        // Thread (image row qq, source pairs sp = spb, spb + 4) of every chunk:
         // 8 lanes of a quarter-warp write 8 different rows' swizzled 16-byte
-        // groups, which cover all 32 banks.
+        // groups, which cover all 32 banks.  Rows of the raw tile past the last
+        // source were zero-filled by the producer.
         const int lt = tid - TC_GEN_THREADS;
-        constexpr int items = (TC_SRC / 2) * CH * 16;
+        const int qq = lt & 15, spb = lt >> 4;
+        static_assert(TC_EXP_THREADS == 64 && TC_SRC == 16, "expander layout: 16 rows x 4 pair slots");
+        uint32_t o_re[2], o_im[2];
+        #pragma unroll
+        for (int h = 0; h < 2; ++h)
+        {
+            o_re[h] = img_off16(qq, spb + 4 * h);
+            o_im[h] = img_off16(qq + 16, spb + 4 * h);
+        }
         PieceIter it(plan, k_cta);
         int cg, blk, tb, te, slot, rot, T = 0;
         bool ok = true;
@@ -737,34 +828,34 @@ boundary_tc_kernel(const float *__restrict__ mid4, const float *__restrict__ nrm
             {
                 const int rs = T % TC_RSTAGES, b = T % TC_BSTAGES;
                 if (!wait_bar(&sm.r_full[rs], (uint32_t)(T / TC_RSTAGES) & 1u, abort_flag, err, 4)) { ok = false; break; }
-                if (T >= TC_BSTAGES &&
-                    !wait_bar(&sm.b_empty[b], (uint32_t)((T / TC_BSTAGES) - 1) & 1u, abort_flag, err, 5))
+                if (!wait_bar(&sm.b_empty[b], ((uint32_t)(T / TC_BSTAGES) & 1u) ^ 1u, abort_flag, err, 5))
                 {
                     ok = false;
                     break;
                 }
-                const int ts = t + rot < ntiles ? t + rot : t + rot - ntiles;   // source tile (rot < ntiles)
-                const int nsrc = n - ts * TC_SRC;   // valid rows in this tile (may exceed 16)
-                #pragma unroll 2
-                for (int e = lt; e < items; e += TC_EXP_THREADS)
+                const TcRaw &R = sm.raw[rs];
+                constexpr uint32_t sgn = 0x80000000u;
+                #pragma unroll
+                for (int h = 0; h < 2; ++h)
                 {
-                    const int qq = e & 15, sp = (e >> 4) & 7, c = e >> 7;
-                    const int s0 = 2 * sp, s1 = s0 + 1;
-                    const float2 v0 = (s0 < nsrc) ? sm.raw[rs].b[s0][c * 16 + qq] : make_float2(0.f, 0.f);
-                    const float2 v1 = (s1 < nsrc) ? sm.raw[rs].b[s1][c * 16 + qq] : make_float2(0.f, 0.f);
-                    uint32_t hr0, lr0, hi0, li0, hr1, lr1, hi1, li1;
-                    split_tf32(v0.x, hr0, lr0);
-                    split_tf32(v0.y, hi0, li0);
-                    split_tf32(v1.x, hr1, lr1);
-                    split_tf32(v1.y, hi1, li1);
-                    constexpr uint32_t sgn = 0x80000000u;
-                    uint8_t *hi_img = sm.img[b][c][0];
-                    uint8_t *lo_img = sm.img[b][c][1];
-                    // row qq (real part of C): (Re b0, Re b1, -Im b0, -Im b1); row qq + 16: (Im b0, Im b1, Re b0, Re b1)
-                    *reinterpret_cast<uint4 *>(hi_img + img_off16(qq, sp)) = make_uint4(hr0, hr1, hi0 ^ sgn, hi1 ^ sgn);
-                    *reinterpret_cast<uint4 *>(lo_img + img_off16(qq, sp)) = make_uint4(lr0, lr1, li0 ^ sgn, li1 ^ sgn);
-                    *reinterpret_cast<uint4 *>(hi_img + img_off16(qq + 16, sp)) = make_uint4(hi0, hi1, hr0, hr1);
-                    *reinterpret_cast<uint4 *>(lo_img + img_off16(qq + 16, sp)) = make_uint4(li0, li1, lr0, lr1);
+                    const int s0 = 2 * (spb + 4 * h);
+                    #pragma unroll
+                    for (int c = 0; c < CH; ++c)
+                    {
+                        const float2 v0 = R.b[s0][c * 16 + qq], v1 = R.b[s0 + 1][c * 16 + qq];
+                        uint32_t hr0, lr0, hi0, li0, hr1, lr1, hi1, li1;
+                        split_tf32(v0.x, hr0, lr0);
+                        split_tf32(v0.y, hi0, li0);
+                        split_tf32(v1.x, hr1, lr1);
+                        split_tf32(v1.y, hi1, li1);
+                        uint8_t *hi_img = sm.img[b][c][0];
+                        uint8_t *lo_img = sm.img[b][c][1];
+                        // row qq (real part of C): (Re b0, Re b1, -Im b0, -Im b1); row qq + 16: (Im b0, Im b1, Re b0, Re b1)
+                        *reinterpret_cast<uint4 *>(hi_img + o_re[h]) = make_uint4(hr0, hr1, hi0 ^ sgn, hi1 ^ sgn);
+                        *reinterpret_cast<uint4 *>(lo_img + o_re[h]) = make_uint4(lr0, lr1, li0 ^ sgn, li1 ^ sgn);
+                        *reinterpret_cast<uint4 *>(hi_img + o_im[h]) = make_uint4(hi0, hi1, hr0, hr1);
+                        *reinterpret_cast<uint4 *>(lo_img + o_im[h]) = make_uint4(li0, li1, lr0, lr1);
+                    }
                 }
                 asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
                 mbar_arrive(&sm.r_empty[rs]);
@@ -785,17 +876,25 @@ boundary_tc_kernel(const float *__restrict__ mid4, const float *__restrict__ nrm
             for (int t = tb; t < te; ++t, ++T)
             {
                 const int rs = T % TC_RSTAGES;
-                if (T >= TC_RSTAGES)
+                if (!warp_wait(&sm.r_empty[rs], ((uint32_t)(T / TC_RSTAGES) & 1u) ^ 1u, abort_flag, err, 6))
                 {
-                    const bool got =
-                        wait_bar(&sm.r_empty[rs], (uint32_t)((T / TC_RSTAGES) - 1) & 1u, abort_flag, err, 6);
-                    if (!__all_sync(0xffffffffu, got)) { ok = false; break; }
+                    ok = false;
+                    break;
+                }
+                const int ts = t + rot < ntiles ? t + rot : t + rot - ntiles;   // source tile (rot < ntiles)
+                const int j0 = ts * TC_SRC;
+                const int rows = min(TC_SRC, n - j0);
+                if (rows < TC_SRC)
+                {
+                    // the last tile: zero rows past the end, which the expanders read
+                    // (their kernel entries are zero, so the values only need to be finite)
+                    float4 *z = reinterpret_cast<float4 *>(sm.raw[rs].b[rows]);
+                    const int nz = (TC_SRC - rows) * (TC_CHMAX * 16) / 2;
+                    for (int e = lane; e < nz; e += 32) z[e] = make_float4(0.f, 0.f, 0.f, 0.f);
+                    __syncwarp();
                 }
                 if (elect_one())
                 {
-                    const int ts = t + rot < ntiles ? t + rot : t + rot - ntiles;   // source tile (rot < ntiles)
-                    const int j0 = ts * TC_SRC;
-                    const int rows = min(TC_SRC, n - j0);
                     mbar_expect_tx(&sm.r_full[rs], (uint32_t)rows * row_bytes + (uint32_t)sizeof(TcTileGeo));
                     bulk_g2s(&sm.raw[rs].geo, tgeo + ts, (uint32_t)sizeof(TcTileGeo), &sm.r_full[rs]);
                     // one contiguous block when the tile's rows are whole B_tri rows of
@@ -937,7 +1036,7 @@ __global__ void tc_fixup_kernel(const float2 *__restrict__ ws, float2 *__restric
     }
 }
 
-template <int CH, bool SL, bool DL, bool ADL, bool RI>
+template <int GW, int CH, bool SL, bool DL, bool ADL, bool RI, bool KI>
 void tc_launch(cudaStream_t st, const float *mid, const float *nrm, const TcTileGeo *tg, const float2 *B, float2 *C,
                float2 *ws, const ChunkParamsF *p, const TcPlan &plan, int *err)
 {
@@ -954,28 +1053,44 @@ void tc_launch(cudaStream_t st, const float *mid, const float *nrm, const TcTile
         std::lock_guard<std::mutex> lock(mu);
         if (dev < 0 || dev >= 64 || !done[dev])
         {
-            BAEMM_CUDA(cudaFuncSetAttribute(boundary_tc_kernel<CH, SL, DL, ADL, RI>,
+            BAEMM_CUDA(cudaFuncSetAttribute(boundary_tc_kernel<GW, CH, SL, DL, ADL, RI, KI>,
                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
             if (dev >= 0 && dev < 64) done[dev] = true;
         }
     }
-    boundary_tc_kernel<CH, SL, DL, ADL, RI><<<plan.ctas, TC_THREADS, bytes, st>>>(mid, nrm, tg, B, C, ws, p, plan, err);
+    boundary_tc_kernel<GW, CH, SL, DL, ADL, RI, KI><<<plan.ctas, TcShape<GW>::THREADS, bytes, st>>>(
+        mid, nrm, tg, B, C, ws, p, plan, err);
 }
 
-template <int CH, bool RI>
+template <int GW, int CH, bool RI>
 void tc_flags(int code, cudaStream_t st, const float *mid, const float *nrm, const TcTileGeo *tg, const float2 *B,
               float2 *C, float2 *ws, const ChunkParamsF *p, const TcPlan &plan, int *err)
 {
     switch (code)
     {
-        case 1: tc_launch<CH, true, false, false, RI>(st, mid, nrm, tg, B, C, ws, p, plan, err); break;
-        case 2: tc_launch<CH, false, true, false, RI>(st, mid, nrm, tg, B, C, ws, p, plan, err); break;
-        case 3: tc_launch<CH, true, true, false, RI>(st, mid, nrm, tg, B, C, ws, p, plan, err); break;
-        case 4: tc_launch<CH, false, false, true, RI>(st, mid, nrm, tg, B, C, ws, p, plan, err); break;
-        case 5: tc_launch<CH, true, false, true, RI>(st, mid, nrm, tg, B, C, ws, p, plan, err); break;
-        case 6: tc_launch<CH, false, true, true, RI>(st, mid, nrm, tg, B, C, ws, p, plan, err); break;
-        case 7: tc_launch<CH, true, true, true, RI>(st, mid, nrm, tg, B, C, ws, p, plan, err); break;
+        case 1: tc_launch<GW, CH, true, false, false, RI, false>(st, mid, nrm, tg, B, C, ws, p, plan, err); break;
+        case 2: tc_launch<GW, CH, false, true, false, RI, false>(st, mid, nrm, tg, B, C, ws, p, plan, err); break;
+        case 3: tc_launch<GW, CH, true, true, false, RI, false>(st, mid, nrm, tg, B, C, ws, p, plan, err); break;
+        case 4: tc_launch<GW, CH, false, false, true, RI, false>(st, mid, nrm, tg, B, C, ws, p, plan, err); break;
+        case 5: tc_launch<GW, CH, true, false, true, RI, false>(st, mid, nrm, tg, B, C, ws, p, plan, err); break;
+        case 6: tc_launch<GW, CH, false, true, true, RI, false>(st, mid, nrm, tg, B, C, ws, p, plan, err); break;
+        case 7: tc_launch<GW, CH, true, true, true, RI, false>(st, mid, nrm, tg, B, C, ws, p, plan, err); break;
         default: break;
+    }
+}
+
+// The KI form for the operator combinations of the solves: the mixed BIE
+// (SL + DL), the DtN operator (SL + ADL) and all three layers.
+template <int GW, int CH>
+bool tc_flags_ki(int code, cudaStream_t st, const float *mid, const float *nrm, const TcTileGeo *tg, const float2 *B,
+                 float2 *C, float2 *ws, const ChunkParamsF *p, const TcPlan &plan, int *err)
+{
+    switch (code)
+    {
+        case 3: tc_launch<GW, CH, true, true, false, true, true>(st, mid, nrm, tg, B, C, ws, p, plan, err); return true;
+        case 5: tc_launch<GW, CH, true, false, true, true, true>(st, mid, nrm, tg, B, C, ws, p, plan, err); return true;
+        case 7: tc_launch<GW, CH, true, true, true, true, true>(st, mid, nrm, tg, B, C, ws, p, plan, err); return true;
+        default: return false;
     }
 }
 
@@ -992,6 +1107,33 @@ int device_sm_count()
 }
 
 } // namespace
+
+TcCoeffForm tc_coeff_form(const ChunkParamsF *h, int groups)
+{
+    TcCoeffForm out;
+    if (groups < 1 || h[0].kappa == 0.f) return out;
+    const float s = h[0].c[1].y / h[0].kappa;
+    for (int i = 0; i < groups; ++i)
+    {
+        const ChunkParamsF &q = h[i];
+        if (q.kappa == 0.f || q.c[1].x != 0.f || q.c[2].y != 0.f || q.c[3].y != 0.f) return out;
+        if (q.c[2].x != h[0].c[2].x || q.c[3].x != h[0].c[3].x) return out;
+        // c1.y = s kappa up to the rounding of the scaled coefficients (a few ulps)
+        if (std::fabs(q.c[1].y - s * q.kappa) > 1e-6f * std::fabs(q.c[1].y)) return out;
+    }
+    out.ki = true;
+    out.s = s;
+    return out;
+}
+
+int tc_chunks_per_unit(int wc, int chunks)
+{
+    const int groups = wc / 16;
+    int ch = (groups % 4 == 0) ? 4 : (groups % 2 == 0) ? 2 : 1;   // the most the wave shape allows
+    if (chunks == 1 || chunks == 2 || chunks == 4)
+        while (ch > chunks) ch /= 2;
+    return ch;
+}
 
 // Groups of 16 columns share a wavenumber: wave_chunk_size a multiple of 16.
 bool tc_supported(int wc, int wcs) { return wcs % 16 == 0 && wcs > 0 && wc % wcs == 0 && wc <= 16 * TC_MAXCHUNKS; }
@@ -1015,16 +1157,44 @@ void launch_tc_tile_geometry(const MeshDev &m, float *tgeo, cudaStream_t st)
 
 namespace
 {
+template <int GW>
+void tc_dispatch(int CH, bool ri, bool ki, int code, cudaStream_t st, const float *pts4, const float *nrm,
+                 const TcTileGeo *tg, const float2 *Btri, float2 *Ctri, float2 *ws, const ChunkParamsF *p,
+                 const TcPlan &plan, int *err)
+{
+    bool done = false;
+    if (ri && ki)
+    {
+        if (CH == 4) done = tc_flags_ki<GW, 4>(code, st, pts4, nrm, tg, Btri, Ctri, ws, p, plan, err);
+        else if (CH == 2) done = tc_flags_ki<GW, 2>(code, st, pts4, nrm, tg, Btri, Ctri, ws, p, plan, err);
+        else done = tc_flags_ki<GW, 1>(code, st, pts4, nrm, tg, Btri, Ctri, ws, p, plan, err);
+    }
+    if (done) return;
+    if (ri)
+    {
+        if (CH == 4) tc_flags<GW, 4, true>(code, st, pts4, nrm, tg, Btri, Ctri, ws, p, plan, err);
+        else if (CH == 2) tc_flags<GW, 2, true>(code, st, pts4, nrm, tg, Btri, Ctri, ws, p, plan, err);
+        else tc_flags<GW, 1, true>(code, st, pts4, nrm, tg, Btri, Ctri, ws, p, plan, err);
+    }
+    else
+    {
+        if (CH == 4) tc_flags<GW, 4, false>(code, st, pts4, nrm, tg, Btri, Ctri, ws, p, plan, err);
+        else if (CH == 2) tc_flags<GW, 2, false>(code, st, pts4, nrm, tg, Btri, Ctri, ws, p, plan, err);
+        else tc_flags<GW, 1, false>(code, st, pts4, nrm, tg, Btri, Ctri, ws, p, plan, err);
+    }
+}
+
 // One launch of the tensor-core form over the targets (pts4, m_targets) and all
 // nt sources of the mesh; self = 1: the targets are the midpoints of triangles
 // off .. off + m_targets - 1 and the pair i == j is excluded.
-void tc_run(const MeshDev &m, const OpFlags &f, const void *chunk_params, int wc, int wcs, const float *tgeo,
-            const float *pts4, int64_t m_targets, int self, int64_t off, const float2 *Btri, float2 *Ctri, float2 *ws,
-            size_t ws_elems, int *err, cudaStream_t st, int seg_tiles, int ctas, int stagger)
+void tc_run(const MeshDev &m, const OpFlags &f, const void *chunk_params, const TcCoeffForm &form, int wc, int wcs,
+            const float *tgeo, const float *pts4, int64_t m_targets, int self, int64_t off, const float2 *Btri,
+            float2 *Ctri, float2 *ws, size_t ws_elems, int *err, cudaStream_t st, const TcTuning &tune)
 {
     BAEMM_REQUIRE(tc_supported(wc, wcs), BAEMM_ERR_SIZE,
                   "tensor-core apply needs wave_chunk_size a multiple of 16 and wave_count <= 512");
     BAEMM_REQUIRE(m_targets <= INT32_MAX - TC_M, BAEMM_ERR_SIZE, "too many targets");
+    BAEMM_REQUIRE(tune.gen_warps == 8 || tune.gen_warps == 16, BAEMM_ERR_ARG, "generator warps: 8 or 16");
     if (!f.any_layer() || m.nt == 0 || m_targets == 0) return;
     TcPlan plan;
     plan.n = (int)m.nt;
@@ -1032,18 +1202,19 @@ void tc_run(const MeshDev &m, const OpFlags &f, const void *chunk_params, int wc
     plan.self = self;
     plan.off = (int)off;
     plan.wc = wc;
-    const int CH = (wc % 64 == 0) ? 4 : (wc % 32 == 0) ? 2 : 1;
+    const int CH = tc_chunks_per_unit(wc, tune.chunks);
     plan.ncg = wc / (16 * CH);
     plan.nblk = ceil_div(plan.m, TC_M);
     plan.ntiles = ceil_div(plan.n, TC_SRC);
-    plan.seg_tiles = std::max(1, seg_tiles);
+    plan.seg_tiles = std::max(1, tune.seg_tiles);
     const int blocks = plan.ncg * plan.nblk;
-    if (ctas <= 0) ctas = device_sm_count();
+    const int ctas = tune.ctas > 0 ? tune.ctas : device_sm_count();
     plan.ctas = (int)std::min<int64_t>(ctas, (int64_t)blocks * plan.ntiles);
     plan.full_waves = blocks / plan.ctas;
     plan.tail_blocks = blocks - plan.full_waves * plan.ctas;
     plan.tail_units = (int64_t)plan.tail_blocks * plan.ntiles;
-    plan.stagger = stagger;
+    plan.stagger = tune.stagger;
+    plan.ki_s = form.s;
     BAEMM_REQUIRE(ws && ws_elems >= tc_workspace_elems(plan.ctas), BAEMM_ERR_ARG, "tensor-core workspace too small");
     const int code = (f.sl() ? 1 : 0) | (f.dl() ? 2 : 0) | (f.adl() ? 4 : 0);
     const auto *p = static_cast<const ChunkParamsF *>(chunk_params);
@@ -1052,18 +1223,8 @@ void tc_run(const MeshDev &m, const OpFlags &f, const void *chunk_params, int wc
     BAEMM_REQUIRE(tg, BAEMM_ERR_ARG, "tensor-core tile geometry missing");
     // the real / imaginary coefficient structure of the BIE solves (see boundary_tc_kernel)
     const bool ri = !f.re_sl && !f.im_dl && !f.im_adl && (f.dl() || f.adl());
-    if (ri)
-    {
-        if (CH == 4) tc_flags<4, true>(code, st, pts4, nrm, tg, Btri, Ctri, ws, p, plan, err);
-        else if (CH == 2) tc_flags<2, true>(code, st, pts4, nrm, tg, Btri, Ctri, ws, p, plan, err);
-        else tc_flags<1, true>(code, st, pts4, nrm, tg, Btri, Ctri, ws, p, plan, err);
-    }
-    else
-    {
-        if (CH == 4) tc_flags<4, false>(code, st, pts4, nrm, tg, Btri, Ctri, ws, p, plan, err);
-        else if (CH == 2) tc_flags<2, false>(code, st, pts4, nrm, tg, Btri, Ctri, ws, p, plan, err);
-        else tc_flags<1, false>(code, st, pts4, nrm, tg, Btri, Ctri, ws, p, plan, err);
-    }
+    if (tune.gen_warps == 8) tc_dispatch<8>(CH, ri, form.ki, code, st, pts4, nrm, tg, Btri, Ctri, ws, p, plan, err);
+    else tc_dispatch<16>(CH, ri, form.ki, code, st, pts4, nrm, tg, Btri, Ctri, ws, p, plan, err);
     BAEMM_LAUNCH_CHECK();
     if (plan.tail_blocks > 0)
     {
@@ -1073,23 +1234,22 @@ void tc_run(const MeshDev &m, const OpFlags &f, const void *chunk_params, int wc
 }
 } // namespace
 
-void launch_boundary_tc(const MeshDev &m, const OpFlags &f, const void *chunk_params, int wc, int wcs,
-                        const float *tgeo, const float2 *Btri, float2 *Ctri, float2 *ws, size_t ws_elems, int *err,
-                        cudaStream_t st, int seg_tiles, int ctas, int stagger, int64_t row_begin, int64_t row_end)
+void launch_boundary_tc(const MeshDev &m, const OpFlags &f, const void *chunk_params, const TcCoeffForm &form, int wc,
+                        int wcs, const float *tgeo, const float2 *Btri, float2 *Ctri, float2 *ws, size_t ws_elems,
+                        int *err, cudaStream_t st, const TcTuning &tune, int64_t row_begin, int64_t row_end)
 {
     const int64_t r0 = std::max<int64_t>(0, row_begin), r1 = row_end < 0 ? m.nt : std::min<int64_t>(row_end, m.nt);
     if (r1 <= r0) return;
-    tc_run(m, f, chunk_params, wc, wcs, tgeo, m.mid_f + 4 * r0, r1 - r0, 1, r0, Btri, Ctri + r0 * wc, ws, ws_elems,
-           err, st, seg_tiles, ctas, stagger);
+    tc_run(m, f, chunk_params, form, wc, wcs, tgeo, m.mid_f + 4 * r0, r1 - r0, 1, r0, Btri, Ctri + r0 * wc, ws, ws_elems,
+           err, st, tune);
 }
 
-void launch_nearfield_tc(const MeshDev &m, const OpFlags &f, const void *chunk_params, int wc, int wcs,
-                         const float *tgeo, const float *pts4, int64_t npts, const float2 *Btri, float2 *Cpts,
-                         float2 *ws, size_t ws_elems, int *err, cudaStream_t st, int seg_tiles, int ctas, int stagger)
+void launch_nearfield_tc(const MeshDev &m, const OpFlags &f, const void *chunk_params, const TcCoeffForm &form,
+                         int wc, int wcs, const float *tgeo, const float *pts4, int64_t npts, const float2 *Btri,
+                         float2 *Cpts, float2 *ws, size_t ws_elems, int *err, cudaStream_t st, const TcTuning &tune)
 {
     BAEMM_REQUIRE(!f.adl() && !f.mass(), BAEMM_ERR_ARG, "near field: single and double layer only");
-    tc_run(m, f, chunk_params, wc, wcs, tgeo, pts4, npts, 0, 0, Btri, Cpts, ws, ws_elems, err, st, seg_tiles, ctas,
-           stagger);
+    tc_run(m, f, chunk_params, form, wc, wcs, tgeo, pts4, npts, 0, 0, Btri, Cpts, ws, ws_elems, err, st, tune);
 }
 
 } // namespace baemm

@@ -2,19 +2,48 @@
 //
 // The kernel shapes that matter depend on the mesh size and the wave block:
 // the plain FP32 form has three variants (scalar FMA with 16 columns per
-// thread, packed FP32x2 with one or two targets per thread), the tensor-core
-// form the length of its TMEM accumulation segment.  The tuner runs each
-// candidate on the loaded operators with the context's mesh and wave counts
-// (a constant right-hand-side block; the kernels' cost does not depend on the
-// values), times it with CUDA events on the context's stream, keeps the
-// fastest and reports it.
+// thread, packed FP32x2 with one or two targets per thread); the tensor-core
+// form has its generator-warp count (8 or 16), the 16-column groups per work
+// unit (1, 2 or 4: fewer give small meshes more units to spread over the SMs
+// at the cost of re-evaluating the pair geometry per group) and the length of
+// its TMEM accumulation segment.  The tuner runs each candidate on the loaded
+// operators with the context's mesh and wave counts (a constant
+// right-hand-side block; the kernels' cost does not depend on the values),
+// times it with CUDA events on the context's stream and keeps the fastest.
+// The tensor-core search is two-staged: warps x chunks at the default
+// segment, then the segment lengths around the winner.
+//
+// Choices are cached for the process per (device, mesh size, wave shape,
+// arithmetic form, operator structure): a second context with the same key,
+// or the same context after a re-mesh of equal size, takes the cached choice
+// without timing anything.
 #include <algorithm>
+#include <map>
+#include <mutex>
+#include <tuple>
 #include <vector>
 
 #include "ctx.cuh"
 
 namespace baemm
 {
+namespace
+{
+
+using TuneKey = std::tuple<int, int64_t, int64_t, int, int, int, int, int>;
+
+struct TuneChoice
+{
+    int dense_variant = 0;
+    TcTuning tc;
+    double best_ms = 0.0;
+    int candidates = 0;
+};
+
+std::mutex g_tune_mutex;
+std::map<TuneKey, TuneChoice> g_tune_cache;
+
+} // namespace
 
 void Ctx::autotune(int mode, int repeats, baemm_tune_result *out)
 {
@@ -26,6 +55,37 @@ void Ctx::autotune(int mode, int repeats, baemm_tune_result *out)
     repeats = std::max(1, repeats);
     BAEMM_CUDA(cudaSetDevice(device));
     if (mode == BAEMM_APPLY_TC && !tc_supported(wave_count, wave_chunk_size)) mode = BAEMM_APPLY_FP32;
+    *out = baemm_tune_result{};
+    out->apply_mode = mode;
+
+    const int code = (flags.sl() ? 1 : 0) | (flags.dl() ? 2 : 0) | (flags.adl() ? 4 : 0);
+    const bool ri = !flags.re_sl && !flags.im_dl && !flags.im_adl && (flags.dl() || flags.adl());
+    const int form = (ri ? 1 : 0) | (tc_form.ki ? 2 : 0);
+    const TuneKey key{device, mesh.nt, mesh.nv, wave_count, wave_chunk_size, mode, code, form};
+    auto report = [&](const TuneChoice &ch, double before, int cached) {
+        out->dense_variant = dense_variant;
+        out->tc_segment = tc_tune.seg_tiles;
+        out->tc_ctas = tc_tune.ctas;
+        out->tc_stagger = tc_tune.stagger;
+        out->candidates = ch.candidates;
+        out->best_ms = ch.best_ms;
+        out->before_ms = before;
+        out->tc_gen_warps = tc_tune.gen_warps;
+        out->tc_chunks = tc_chunks_per_unit(wave_count, tc_tune.chunks);
+        out->cached = cached;
+    };
+    {
+        std::lock_guard<std::mutex> lock(g_tune_mutex);
+        auto it = g_tune_cache.find(key);
+        if (it != g_tune_cache.end())
+        {
+            ++graph_state;
+            if (mode == BAEMM_APPLY_TC) tc_tune = it->second.tc;
+            else dense_variant = it->second.dense_variant;
+            report(it->second, -1.0, 1);
+            return;
+        }
+    }
 
     const size_t elems = (size_t)mesh.nt * (size_t)wave_count;
     float2 *Bt = Btri_f.reserve(elems), *Ct = Ctri_f.reserve(elems);
@@ -34,7 +94,8 @@ void Ctx::autotune(int mode, int repeats, baemm_tune_result *out)
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     BAEMM_CUDA(cudaEventCreate(&e0));
     BAEMM_CUDA(cudaEventCreate(&e1));
-    const int saved_mode = apply_mode, saved_variant = dense_variant, saved_seg = tc_seg_tiles;
+    const int saved_mode = apply_mode, saved_variant = dense_variant;
+    const TcTuning saved_tc = tc_tune;
     auto time_current = [&]() {
         dense_apply<float>(Bt, Ct);   // warm-up (and first-use set-up)
         float best = 1e30f;
@@ -51,59 +112,78 @@ void Ctx::autotune(int mode, int repeats, baemm_tune_result *out)
         if (tc_pending) check_tc_error();
         return (double)best;
     };
+    TuneChoice choice;
     try
     {
         apply_mode = mode;
         const double before = time_current();
-        std::vector<int> cands;
-        if (mode == BAEMM_APPLY_TC)
-            cands = {4, 8, 16, 32};
-        else
-            for (int v = 0; v < kDenseVariants; ++v) cands.push_back(v);
-        double best = 1e300;
-        int best_c = mode == BAEMM_APPLY_TC ? saved_seg : saved_variant;
-        for (int c : cands)
-        {
-            if (mode == BAEMM_APPLY_TC) tc_seg_tiles = c;
-            else dense_variant = c;
-            const double ms = time_current();
-            if (ms < best)
+        choice.best_ms = 1e300;
+        auto consider = [&](double ms) {
+            ++choice.candidates;
+            if (ms < choice.best_ms)
             {
-                best = ms;
-                best_c = c;
+                choice.best_ms = ms;
+                choice.tc = tc_tune;
+                choice.dense_variant = dense_variant;
             }
-        }
+        };
         if (mode == BAEMM_APPLY_TC)
         {
-            tc_seg_tiles = best_c;
+            const int most = tc_chunks_per_unit(wave_count, 0);
+            std::vector<int> chunk_opts;
+            for (int ch = most; ch >= 1; ch /= 2) chunk_opts.push_back(ch);
+            for (int gw : {16, 8})
+                for (int ch : chunk_opts)
+                {
+                    tc_tune = saved_tc;
+                    tc_tune.gen_warps = gw;
+                    tc_tune.chunks = ch;
+                    tc_tune.seg_tiles = 16;
+                    consider(time_current());
+                }
+            const TcTuning stage1 = choice.tc;
+            for (int seg : {8, 32})
+            {
+                tc_tune = stage1;
+                tc_tune.seg_tiles = seg;
+                consider(time_current());
+            }
+            tc_tune = choice.tc;
             dense_variant = saved_variant;
         }
         else
         {
-            dense_variant = best_c;
-            tc_seg_tiles = saved_seg;
+            for (int v = 0; v < kDenseVariants; ++v)
+            {
+                dense_variant = v;
+                consider(time_current());
+            }
+            dense_variant = choice.dense_variant;
+            tc_tune = saved_tc;
         }
         apply_mode = saved_mode;
-        out->apply_mode = mode;
-        out->dense_variant = dense_variant;
-        out->tc_segment = tc_seg_tiles;
-        out->tc_ctas = tc_ctas;
-        out->tc_stagger = tc_stagger;
-        out->candidates = (int32_t)cands.size();
-        out->best_ms = best;
-        out->before_ms = before;
+        ++graph_state;
+        report(choice, before, 0);
     }
     catch (...)
     {
         apply_mode = saved_mode;
         dense_variant = saved_variant;
-        tc_seg_tiles = saved_seg;
+        tc_tune = saved_tc;
         cudaEventDestroy(e0);
         cudaEventDestroy(e1);
         throw;
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
+    std::lock_guard<std::mutex> lock(g_tune_mutex);
+    g_tune_cache[key] = choice;
+}
+
+void autotune_forget()
+{
+    std::lock_guard<std::mutex> lock(g_tune_mutex);
+    g_tune_cache.clear();
 }
 
 } // namespace baemm
@@ -123,4 +203,16 @@ extern "C" int baemm_autotune(baemm_ctx *ctx, int mode, int repeats, baemm_tune_
         c.last_error = e.what();
         return e.code;
     }
+    catch (const std::bad_alloc &)
+    {
+        c.last_error = "host allocation failed";
+        return BAEMM_ERR_ALLOC;
+    }
+    catch (const std::exception &e)
+    {
+        c.last_error = e.what();
+        return BAEMM_ERR_ARG;
+    }
 }
+
+extern "C" void baemm_autotune_forget(void) { baemm::autotune_forget(); }

@@ -465,6 +465,45 @@ class Helmholtz_CUDA:
                         1 if with_mass else 0))
         return C_out
 
+    def ProfileKrylov(self, columns=32, iterations=20, basis=12):
+        """Device time of the Krylov-vector kernels on this mesh (no reference
+        counterpart): the CG mass inverse on 2 * columns real columns and one
+        Gram-Schmidt pass of a GMRES iteration on `columns` complex columns
+        against `basis` vectors.  Per kernel: ms per launch, algorithmic bytes
+        per launch and the rate (GB/s)."""
+        out = np.zeros(10)
+        self._ck(self._lib.baemm_profile_krylov(self._h, int(columns), int(iterations), int(basis), _dp(out)))
+        names = ("cg_matvec", "cg_update", "cg_pupdate", "gs_dot", "gs_update")
+        return {n: {"ms": float(out[q]), "algorithmic_bytes": float(out[5 + q]),
+                    "GB_s": float(out[5 + q] / (out[q] * 1e-3) / 1e9) if out[q] > 0 else None}
+                for q, n in enumerate(names)}
+
+    def BoundaryOperatorKernel(self, B_tri, C_tri, row_begin=0, row_end=None):
+        """The dense stage alone on torch CUDA triangle blocks (simplex_count x
+        wave_count): C_tri[i] = sum_{j != i} A_ij B_tri[j] for target triangles
+        i in [row_begin, row_end), with the loaded operators and the current
+        apply mode -- the reference's private BoundaryOperatorKernel()
+        (BoundaryOperatorKernel.hpp:5-28).  complex64 blocks run the plain FP32
+        or tensor-core form, complex128 blocks the FP64 form."""
+        import torch
+        if not (_is_torch_cuda(B_tri) and _is_torch_cuda(C_tri)):
+            raise TypeError("BoundaryOperatorKernel takes torch CUDA tensors")
+        if B_tri.dtype == torch.complex128:
+            fn = self._lib.baemm_boundary_operator_kernel_dev_z
+        elif B_tri.dtype == torch.complex64:
+            fn = self._lib.baemm_boundary_operator_kernel_dev_c
+        else:
+            raise TypeError("B_tri must be complex64 or complex128")
+        nt = self.SimplexCount()
+        wc = self.GetWaveCount()
+        for X in (B_tri, C_tri):
+            if X.dtype != B_tri.dtype or tuple(X.shape) != (nt, wc) or not X.is_contiguous():
+                raise ValueError(f"triangle blocks must be contiguous ({nt}, {wc}) tensors of one dtype")
+        row_end = nt if row_end is None else int(row_end)
+        with self._on_torch_stream(B_tri):
+            self._ck(fn(self._h, C.c_void_p(B_tri.data_ptr()), C.c_void_p(C_tri.data_ptr()), int(row_begin), row_end))
+        return C_tri
+
     def ApplyNearFieldOperators_PL(self, alpha, B_in, beta, C_out, *args):
         """C_out (points x wc) = alpha (c1 SL + c2 DL)(points) AvOp B_in + beta C_out
         (ApplyNearFieldOperators.hpp:27-122), the boundary potential at points

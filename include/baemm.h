@@ -144,11 +144,18 @@ int baemm_get_apply_mode(const baemm_ctx *ctx);
  *                             one CTA per SM)
  *   BAEMM_TUNE_TC_STAGGER     tensor-core form: CTA k starts its sweep of the
  *                             source tiles at tile (k % 8) * value (default 0:
- *                             all in step); -1 spreads the starts over all tiles */
+ *                             all in step); -1 spreads the starts over all tiles
+ *   BAEMM_TUNE_TC_GEN_WARPS   tensor-core form: warps evaluating the kernel
+ *                             entries, 8 or 16 (default 16)
+ *   BAEMM_TUNE_TC_CHUNKS      tensor-core form: 16-column groups per work unit,
+ *                             1, 2 or 4 (default 0: the most the wave shape
+ *                             allows; fewer give small meshes more work units) */
 #define BAEMM_TUNE_DENSE_VARIANT 1
 #define BAEMM_TUNE_TC_SEGMENT    2
 #define BAEMM_TUNE_TC_CTAS       3
 #define BAEMM_TUNE_TC_STAGGER    4
+#define BAEMM_TUNE_TC_GEN_WARPS  5
+#define BAEMM_TUNE_TC_CHUNKS     6
 int baemm_set_tuning(baemm_ctx *ctx, int key, int value);
 int baemm_get_tuning(const baemm_ctx *ctx, int key);
 /* CUDA graphs for the solvers' inner operators (no reference counterpart;
@@ -165,12 +172,17 @@ int baemm_get_tuning(const baemm_ctx *ctx, int key);
 int baemm_set_graphs(baemm_ctx *ctx, int on);
 int baemm_graph_stats(const baemm_ctx *ctx, int64_t *captures, int64_t *replays);
 /* Autotuner (no reference counterpart): times the dense-kernel settings of
- * `mode` (BAEMM_APPLY_FP32: the three plain variants; BAEMM_APPLY_TC: the
- * tensor-core segment lengths 4/8/16/32) on the loaded operators, with the
- * mesh and wave counts of the context, `repeats` timed runs each (>= 1),
- * keeps the fastest in the context and reports it.  A TC request whose wave
- * shape the tensor-core form does not support tunes the plain kernel.
- * Requires baemm_load_boundary_operators; synchronises the context. */
+ * `mode` on the loaded operators, with the mesh and wave counts of the
+ * context, `repeats` timed runs each (>= 1), keeps the fastest in the context
+ * and reports it.  BAEMM_APPLY_FP32: the three plain variants;
+ * BAEMM_APPLY_TC: generator warps {16, 8} x chunk groups per unit {4, 2, 1}
+ * (those the wave shape allows) at segment 16, then segments {8, 32} around
+ * the winner.  A TC request whose wave shape the tensor-core form does not
+ * support tunes the plain kernel.  The choice is cached for the process per
+ * (device, simplex and vertex count, wave_count, wave_chunk_size, form,
+ * operator structure): a later call with the same key applies it without
+ * timing (cached = 1, before_ms = -1).  Requires
+ * baemm_load_boundary_operators; synchronises the context. */
 typedef struct baemm_tune_result
 {
     int32_t apply_mode;      /* the form tuned (BAEMM_APPLY_*) */
@@ -180,9 +192,15 @@ typedef struct baemm_tune_result
     int32_t tc_stagger;      /* BAEMM_TUNE_TC_STAGGER in force */
     int32_t candidates;      /* settings timed */
     double  best_ms;         /* dense-kernel time of the chosen setting */
-    double  before_ms;       /* dense-kernel time of the setting in force before */
+    double  before_ms;       /* dense-kernel time of the setting in force before (-1: cached) */
+    int32_t tc_gen_warps;    /* chosen BAEMM_TUNE_TC_GEN_WARPS */
+    int32_t tc_chunks;       /* chunk groups per work unit in force */
+    int32_t cached;          /* 1: taken from the process cache, nothing timed */
+    int32_t reserved;
 } baemm_tune_result;
 int baemm_autotune(baemm_ctx *ctx, int mode, int repeats, baemm_tune_result *out);
+/* Empties the autotuner's process cache (the next baemm_autotune times again). */
+void baemm_autotune_forget(void);
 /* FP64 iterative refinement around the inner GMRES (0 = off, the reference's
  * behaviour).  When on, the solve's outer residual uses the FP64 apply and
  * the inner GMRES uses the context's apply mode. No reference counterpart. */
@@ -419,6 +437,18 @@ int baemm_gauss_newton_solve(baemm_ctx *ctx, const double *kappa, int wave_chunk
                              double gmres_tol_inner, double gmres_tol_outer, int solver, int *succeeded);
 
 /* ---- tracing (the reference's Tools profiler, ptic/ptoc) -------------------- */
+
+/* Device time of the Krylov-vector kernels on this context's mesh (no
+ * reference counterpart; a measurement hook for ApplyMassInverse.hpp:48-156
+ * and the GMRES of FarField.hpp:706-708 as implemented here):
+ *   the CG mass inverse (the GMRES preconditioner) on 2 * columns real
+ *   columns for `iterations` iterations, and one Gram-Schmidt pass of a GMRES
+ *   iteration on `columns` complex columns against `basis` vectors.
+ * out[0..4]: mean ms per launch of {cg_matvec, cg_update, cg_pupdate,
+ * gs_dot, gs_update}; out[5..9]: their algorithmic bytes per launch (every
+ * operand read or written once: the mass CSR, the lumped inverse and the
+ * n x c vectors the kernel touches). */
+int baemm_profile_krylov(baemm_ctx *ctx, int columns, int iterations, int basis, double out[10]);
 
 /* Per-phase CUDA-event timing of boundary applies on this context (0 = off). */
 int baemm_set_profiling(baemm_ctx *ctx, int on);
