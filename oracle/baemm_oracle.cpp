@@ -290,6 +290,9 @@ struct Base
     virtual void load_parameters(const double *kappa, const cd *coeff, int wc, int wcs, double factor) = 0;
     virtual void avop(const cd *B, int64_t ldB, int ncols) = 0;               // -> internal B_tri
     virtual void boundary_kernel() = 0;                                        // B_tri -> C_tri
+    virtual void boundary_kernel_rows(int64_t r0, int64_t r1) = 0;             // target rows [r0, r1) only
+    virtual void boundary_kernel_index(const int64_t *idx, int64_t m, double *out) = 0;   // rows idx -> out (m x wc)
+    virtual void set_geometry(const double *mid4, const double *nrm4) = 0;      // replace midpoints and normals
     virtual void sl_diagonal() = 0;                                            // C_tri += diag term
     virtual void avopT_out(cd alpha, cd beta, cd *C, int64_t ldC, int ncols) = 0; // C = alpha AvOpT C_tri + beta C
     virtual void farfield_kernel() = 0;                                        // B_tri -> F (nm x wc)
@@ -724,12 +727,13 @@ struct Ctx : Base
 
     // Sum over sources j of T(i,j) * X[j], sequential in j for FP32 (the
     // reference's order), blocked two-level for FP64.
+    // Rows [r0, rows) when r0 is given (the rows below are left untouched).
     template <class Gen>
-    void dense_rows(int64_t rows, int64_t srcs, const C *X, C *Y, int chunk, Gen &&gen)
+    void dense_rows(int64_t rows, int64_t srcs, const C *X, C *Y, int chunk, Gen &&gen, int64_t r0 = 0)
     {
         const int wcs = wave_chunk_size, ld = wave_count;
         #pragma omp parallel for schedule(dynamic, 8) num_threads(threads)
-        for (int64_t i = 0; i < rows; ++i)
+        for (int64_t i = r0; i < rows; ++i)
         {
             std::vector<C> acc(wcs, C(0)), blk(wcs, C(0));
             const int64_t BLK = fp32 ? srcs : 256;
@@ -750,35 +754,91 @@ struct Ctx : Base
         }
     }
 
-    // BoundaryOperatorKernel.cl:100-224 (formula; the Re/Im flags only prune zero terms)
-    void boundary_kernel() override
+    // BoundaryOperatorKernel.cl:100-224 (formula; the Re/Im flags only prune zero terms):
+    // the entry A_ij of wave chunk ch.
+    C boundary_entry(int64_t i, int64_t j, int ch, bool dl, bool adl) const
+    {
+        if (i == j) return C(0);
+        const Real kap = kappa[ch];
+        const C c1 = c[4 * ch + 1], c2 = c[4 * ch + 2], c3 = c[4 * ch + 3];
+        const Real zx = mid[4 * j] - mid[4 * i], zy = mid[4 * j + 1] - mid[4 * i + 1], zz = mid[4 * j + 2] - mid[4 * i + 2];
+        const Real r = std::sqrt(zx * zx + zy * zy + zz * zz);
+        const Real rinv = Real(1) / r;
+        const Real kr = kap * r;
+        const Real sn = std::sin(kr), cs = std::cos(kr);
+        C A = c1 * C(cs * rinv, sn * rinv);
+        if (dl || adl)
+        {
+            const Real r3 = rinv * rinv * rinv;
+            const C g(-(kr * sn + cs) * r3, (kr * cs - sn) * r3);
+            C f(0);
+            if (dl) f += c2 * (zx * nrm[4 * j] + zy * nrm[4 * j + 1] + zz * nrm[4 * j + 2]);
+            if (adl) f -= c3 * (zx * nrm[4 * i] + zy * nrm[4 * i + 1] + zz * nrm[4 * i + 2]);
+            A += f * g;
+        }
+        return A;
+    }
+
+    void boundary_kernel() override { boundary_kernel_rows(0, nt); }
+
+    // The same for target rows [r0, r1) against all sources (the other rows of C_tri are zero).
+    void boundary_kernel_rows(int64_t r0, int64_t r1) override
     {
         Ctri.assign(nt * wave_count, C(0));
         const int kcc = wave_count / wave_chunk_size;   // truncating, BoundaryOperatorKernel.cl:17
         const bool dl = Re_dl || Im_dl, adl = Re_adl || Im_adl;
         for (int ch = 0; ch < kcc; ++ch)
+            dense_rows(r1, nt, Btri.data(), Ctri.data(), ch,
+                       [&](int64_t i, int64_t j) -> C { return boundary_entry(i, j, ch, dl, adl); }, r0);
+    }
+
+    // Target rows idx[0 .. m) (any order, repeats allowed) against all sources,
+    // into out (m x wave_count interleaved complex), the same arithmetic.
+    void boundary_kernel_index(const int64_t *idx, int64_t m, double *out) override
+    {
+        const int kcc = wave_count / wave_chunk_size;
+        const int wcs = wave_chunk_size, ld = wave_count;
+        const bool dl = Re_dl || Im_dl, adl = Re_adl || Im_adl;
+        #pragma omp parallel for schedule(dynamic, 4) num_threads(threads)
+        for (int64_t r = 0; r < m; ++r)
         {
-            const Real kap = kappa[ch];
-            const C c1 = c[4 * ch + 1], c2 = c[4 * ch + 2], c3 = c[4 * ch + 3];
-            dense_rows(nt, nt, Btri.data(), Ctri.data(), ch, [&](int64_t i, int64_t j) -> C {
-                if (i == j) return C(0);
-                const Real zx = mid[4 * j] - mid[4 * i], zy = mid[4 * j + 1] - mid[4 * i + 1], zz = mid[4 * j + 2] - mid[4 * i + 2];
-                const Real r = std::sqrt(zx * zx + zy * zy + zz * zz);
-                const Real rinv = Real(1) / r;
-                const Real kr = kap * r;
-                const Real sn = std::sin(kr), cs = std::cos(kr);
-                C A = c1 * C(cs * rinv, sn * rinv);
-                if (dl || adl)
+            const int64_t i = idx[r];
+            std::vector<C> acc(wcs), blk(wcs);
+            for (int ch = 0; ch < kcc; ++ch)
+            {
+                std::fill(acc.begin(), acc.end(), C(0));
+                const int64_t BLK = fp32 ? nt : 256;
+                for (int64_t j0 = 0; j0 < nt; j0 += BLK)
                 {
-                    const Real r3 = rinv * rinv * rinv;
-                    const C g(-(kr * sn + cs) * r3, (kr * cs - sn) * r3);
-                    C f(0);
-                    if (dl) f += c2 * (zx * nrm[4 * j] + zy * nrm[4 * j + 1] + zz * nrm[4 * j + 2]);
-                    if (adl) f -= c3 * (zx * nrm[4 * i] + zy * nrm[4 * i + 1] + zz * nrm[4 * i + 2]);
-                    A += f * g;
+                    std::fill(blk.begin(), blk.end(), C(0));
+                    const int64_t j1 = std::min(nt, j0 + BLK);
+                    for (int64_t j = j0; j < j1; ++j)
+                    {
+                        const C A = boundary_entry(i, j, ch, dl, adl);
+                        if (A == C(0)) continue;
+                        const C *x = &Btri[j * ld + ch * wcs];
+                        for (int k = 0; k < wcs; ++k) blk[k] += A * x[k];
+                    }
+                    for (int k = 0; k < wcs; ++k) acc[k] += blk[k];
                 }
-                return A;
-            });
+                for (int k = 0; k < wcs; ++k)
+                {
+                    out[2 * (r * ld + ch * wcs + k)] = (double)acc[k].real();
+                    out[2 * (r * ld + ch * wcs + k) + 1] = (double)acc[k].imag();
+                }
+            }
+        }
+    }
+
+    // Replace the midpoints and normals (4 per triangle) used by the kernels,
+    // e.g. by the FP32 geometry of another implementation: the kernels'
+    // arithmetic then compares on identical inputs.
+    void set_geometry(const double *mid4, const double *nrm4) override
+    {
+        for (int64_t e = 0; e < 4 * nt; ++e)
+        {
+            mid[e] = (Real)mid4[e];
+            nrm[e] = (Real)nrm4[e];
         }
     }
 
@@ -1149,6 +1209,45 @@ void orc_boundary_kernel_tri(void *h, const double *Btri, double *Ctri)
         d->boundary_kernel();
         for (int64_t e = 0; e < N; ++e) { Ctri[2 * e] = d->Ctri[e].real(); Ctri[2 * e + 1] = d->Ctri[e].imag(); }
     }
+}
+// The same for target rows [r0, r1): Ctri holds (r1 - r0) x wave_count (parity
+// of sampled rows of meshes too large for the full O(N^2) oracle).
+void orc_boundary_kernel_tri_rows(void *h, const double *Btri, double *Ctri, int64_t r0, int64_t r1)
+{
+    auto run = [&](auto *c) {
+        using Cx = typename std::remove_reference<decltype(c->Btri[0])>::type;
+        const int64_t N = c->nt * c->wave_count;
+        c->Btri.resize(N);
+        for (int64_t e = 0; e < N; ++e) c->Btri[e] = Cx(Btri[2 * e], Btri[2 * e + 1]);
+        c->boundary_kernel_rows(r0, r1);
+        const int64_t off = r0 * c->wave_count, M = (r1 - r0) * c->wave_count;
+        for (int64_t e = 0; e < M; ++e)
+        {
+            Ctri[2 * e] = c->Ctri[off + e].real();
+            Ctri[2 * e + 1] = c->Ctri[off + e].imag();
+        }
+    };
+    auto *b = static_cast<Base *>(h);
+    if (auto *c = dynamic_cast<Ctx<float> *>(b)) run(c);
+    else run(static_cast<Ctx<double> *>(b));
+}
+// Target rows idx[0 .. m) of the raw dense boundary kernel: Ctri holds m x wave_count.
+void orc_boundary_kernel_tri_index(void *h, const double *Btri, double *Ctri, const int64_t *idx, int64_t m)
+{
+    auto run = [&](auto *c) {
+        using Cx = typename std::remove_reference<decltype(c->Btri[0])>::type;
+        const int64_t N = c->nt * c->wave_count;
+        c->Btri.resize(N);
+        for (int64_t e = 0; e < N; ++e) c->Btri[e] = Cx(Btri[2 * e], Btri[2 * e + 1]);
+        c->boundary_kernel_index(idx, m, Ctri);
+    };
+    auto *b = static_cast<Base *>(h);
+    if (auto *c = dynamic_cast<Ctx<float> *>(b)) run(c);
+    else run(static_cast<Ctx<double> *>(b));
+}
+void orc_set_geometry(void *h, const double *mid4, const double *nrm4)
+{
+    static_cast<Base *>(h)->set_geometry(mid4, nrm4);
 }
 // Raw far-field kernel on triangle data (B_tri -> F, nm x wc), no AvOp / combine.
 void orc_farfield_kernel_tri(void *h, const double *Btri, double *F)

@@ -22,3 +22,31 @@ def tiny_meshes():
     strip_v = np.concatenate([np.stack([xs, 0 * xs, 0 * xs], 1), np.stack([xs[:9], 1 + 0 * xs[:9], 0.1 * xs[:9]], 1)])
     strip_t = [[i, i + 1, 10 + i] for i in range(9)] + [[i + 1, 11 + i, 10 + i] for i in range(8)]
     return {"tri1": tri1, "quad2": quad2, "tetra": tetra, "strip17": (strip_v, np.array(strip_t))}
+
+
+def oracle_apply_at_vertices(orc, tris, B, kappa, coeff, wave_count, wave_chunk_size, verts):
+    """The oracle's ApplyBoundaryOperators_PL (alpha 1, beta 0, no mass term) at
+    the vertices `verts` only, for meshes too large for the full O(N^2) oracle:
+    B_tri = AvOp B, the dense kernel on the triangles incident to `verts`
+    (orc.boundary_kernel_tri_index), the single-layer diagonal
+    c1 (diag_i + i kappa) B_tri[i] (ApplySingleLayerDiagonal.hpp:29-61) and
+    AvOp^T restricted to `verts`, in the oracle's precision and geometry."""
+    tris = np.asarray(tris)
+    _, _, area, diag = orc.geometry()
+    a3 = area / 3.0
+    Btri = a3[:, None] * np.asarray(B, np.complex128)[tris].sum(axis=1)
+    inc = [np.nonzero((tris == v).any(axis=1))[0] for v in verts]
+    rows = np.unique(np.concatenate(inc))
+    Ct = orc.boundary_kernel_tri_index(Btri, kappa, coeff, wave_count, wave_chunk_size, rows)
+    pos = {int(r): k for k, r in enumerate(rows)}
+    scale = 1.0 / (4.0 * np.pi)
+    c1 = np.asarray(coeff, np.complex128).reshape(-1, 4)[:, 1] * scale
+    kap = np.asarray(kappa, np.float64)
+    nch = wave_count // wave_chunk_size
+    fac = np.repeat(c1[None, :nch] * (diag[rows][:, None] + 1j * kap[None, :nch]), wave_chunk_size, axis=1)
+    Ct = Ct + fac * Btri[rows]
+    out = np.zeros((len(verts), wave_count), np.complex128)
+    for q, tri_list in enumerate(inc):
+        for i in tri_list:
+            out[q] += a3[i] * Ct[pos[int(i)]]
+    return out

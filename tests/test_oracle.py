@@ -275,3 +275,22 @@ def test_oracle_curl_operator_known_answer(sphere2, precision, tol):
     rows = np.add.reduceat(val * f[inner], outer[:-1])
     want = area[:, None] * np.cross(nrm[:, :3], g)
     assert np.max(np.abs(rows.reshape(nt, 3) - want)) < tol * np.max(np.abs(want))
+
+
+def test_apply_at_vertices_composition_matches_full_oracle_apply():
+    """The sampled-vertex composition used by the full-size torus GPU test
+    (tests/helpers.oracle_apply_at_vertices) equals the oracle's own full apply."""
+    from baemm_b200 import meshes
+    from tests.helpers import oracle_apply_at_vertices
+    coords, tris = meshes.icosphere(2)
+    kap = np.array([2.0, 5.0])
+    coeff = np.array([[0.0, -1j * k, 1.0, 0.0] for k in kap])
+    rng = np.random.default_rng(4)
+    B = rng.standard_normal((coords.shape[0], 32)) + 1j * rng.standard_normal((coords.shape[0], 32))
+    verts = np.array([0, 7, 33, 161])
+    for prec in (64, 32):
+        orc = O.Oracle(coords, tris, np.eye(3), precision=prec)
+        full = np.zeros_like(B)
+        orc.ApplyBoundaryOperators_PL(1.0, B, 0.0, full, kap, coeff, 32, 16)
+        part = oracle_apply_at_vertices(orc, tris, B, kap, coeff, 32, 16, verts)
+        assert np.linalg.norm(part - full[verts]) <= (1e-12 if prec == 64 else 1e-6) * np.linalg.norm(full[verts])
