@@ -3,7 +3,7 @@ the oracle, through the C ABI.  The oracle's near-field kernel is pinned to the
 reference's own NearFieldOperatorKernel.cl (tests/test_oracle.py).
 
 Tolerances (relative, Frobenius): the FP32 path within 1e-5 of the FP32 oracle;
-FP32 and tensor-core paths within 3e-5 of the FP64 oracle (their own rounding);
+FP32 and tensor-core paths within 1e-5 of the FP64 oracle;
 the FP64 path within 1e-11 of the FP64 oracle.
 """
 import numpy as np
@@ -16,7 +16,7 @@ from tests.helpers import crandn, relerr
 pytestmark = pytest.mark.gpu
 
 FP32_TOL = 1e-5
-FP32_VS64_TOL = 3e-5
+FP32_VS64_TOL = 1e-5
 FP64_TOL = 1e-11
 
 COEFFS = {
@@ -270,7 +270,7 @@ def test_nearfield_complex64_and_device_paths(env):
 def test_nearfield_full_size_torus():
     """The bench's near-field workload at a quarter of its points (torus
     153600 T, 64 RHS, 38400 points at least 0.05 from the surface): the
-    tensor-core and FP32 forms within 3e-5 of the FP64 path, which matches the
+    tensor-core and FP32 forms within 1e-5 of the FP64 path, which matches the
     FP64 oracle to 1e-11 on the small cases."""
     import torch
     coords, tris = meshes.torus(1.0, 0.4, 160, 480)

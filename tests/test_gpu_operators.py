@@ -1,8 +1,9 @@
 """GPU parity of the operator applies against the oracle (through the C ABI).
 
-Tolerances: FP32 path within 1e-5 relative (Frobenius) of the FP32 oracle and
-within 3e-5 of the FP64 oracle (the FP32 path's own rounding); FP64 path
-within 1e-11 of the FP64 oracle.
+Tolerances: the plain FP32 and the compensated tensor-core forms within 1e-5
+relative (Frobenius) of the FP32 oracle and of the FP64 oracle; FP64 path
+within 1e-11 of the FP64 oracle.  (Measured on the icosphere of level 3: at
+most 1.6e-6 against the FP64 oracle for every operator combination.)
 """
 import numpy as np
 import pytest
@@ -14,7 +15,7 @@ from tests.helpers import crandn, relerr, tiny_meshes
 pytestmark = pytest.mark.gpu
 
 FP32_TOL = 1e-5
-FP32_VS64_TOL = 3e-5
+FP32_VS64_TOL = 1e-5
 FP64_TOL = 1e-11
 
 COEFFS = {
@@ -209,8 +210,11 @@ def test_tensor_core_sweep_stagger(env, stagger):
 
 @pytest.mark.parametrize("mode", [APPLY_TC, APPLY_FP32])
 def test_autotune_keeps_results(env, mode):
-    """The autotuner picks one of its candidates, keeps it in the context, and
-    the apply with the chosen setting meets the same bar against FP64."""
+    """The autotuner times its candidates (tensor-core form: generator warps x
+    chunk groups per unit, then segment lengths), keeps the fastest in the
+    context -- no slower than the setting in force before, up to timing noise
+    -- and the apply with the chosen setting meets the same bar against FP64.
+    A second call with the same problem key takes the cached choice."""
     coords, tris, meas, H, o32, o64 = env
     kap = [2.0, 4.0, 8.0, 16.0]
     coeff = _coeff("bie", kap)
@@ -218,23 +222,58 @@ def test_autotune_keeps_results(env, mode):
     C64 = np.zeros_like(B)
     o64.ApplyBoundaryOperators_PL(1.0, B, 0.0, C64, kap, coeff, 64, 16)
     H.LoadBoundaryOperators_PL(kap, coeff, 64, 16)
-    seg0, var0 = H.GetTuning(_capi.TUNE_TC_SEGMENT), H.GetTuning(_capi.TUNE_DENSE_VARIANT)
+    keys = (_capi.TUNE_TC_SEGMENT, _capi.TUNE_DENSE_VARIANT, _capi.TUNE_TC_GEN_WARPS, _capi.TUNE_TC_CHUNKS)
+    saved = {k: H.GetTuning(k) for k in keys}
+    H._lib.baemm_autotune_forget()
     try:
-        r = H.Autotune(mode, repeats=1)
-        assert r["apply_mode"] == mode and r["best_ms"] > 0 and r["best_ms"] <= r["before_ms"] * 1.5
+        r = H.Autotune(mode, repeats=2)
+        assert r["apply_mode"] == mode and r["cached"] == 0
+        assert 0 < r["best_ms"] <= r["before_ms"] * 1.05
         if mode == APPLY_TC:
-            assert r["candidates"] == 4 and r["tc_segment"] in (4, 8, 16, 32)
+            # 16 and 8 generator warps x 4, 2 and 1 chunk groups, then segments 8 and 32
+            assert r["candidates"] == 8 and r["tc_segment"] in (8, 16, 32)
+            assert r["tc_gen_warps"] in (8, 16) and r["tc_chunks"] in (1, 2, 4)
             assert H.GetTuning(_capi.TUNE_TC_SEGMENT) == r["tc_segment"]
+            assert H.GetTuning(_capi.TUNE_TC_GEN_WARPS) == r["tc_gen_warps"]
         else:
             assert r["candidates"] == 3 and H.GetTuning(_capi.TUNE_DENSE_VARIANT) == r["dense_variant"]
+        again = H.Autotune(mode, repeats=2)
+        assert again["cached"] == 1 and again["best_ms"] == r["best_ms"]
         H.SetApplyMode(mode)
         C = np.zeros_like(B)
         H.ApplyBoundaryOperators_PL(1.0, B, 0.0, C)
     finally:
         H.SetApplyMode(APPLY_FP32)
-        H.SetTuning(_capi.TUNE_TC_SEGMENT, seg0)
-        H.SetTuning(_capi.TUNE_DENSE_VARIANT, var0)
+        for k, v in saved.items():
+            H.SetTuning(k, v)
         H.UnloadBoundaryOperators_PL()
+        H._lib.baemm_autotune_forget()
+    assert relerr(C, C64) < FP32_VS64_TOL
+
+
+@pytest.mark.parametrize("gw", [8, 16])
+@pytest.mark.parametrize("chunks", [1, 2, 4])
+@pytest.mark.parametrize("cname", ["bie", "dtn", "all"])
+def test_tensor_core_shapes_same_results(env, gw, chunks, cname):
+    """Every generator-warp count and chunk grouping the tuner may pick gives
+    the apply within the bar of the FP64 oracle (and the same result up to
+    FP32 rounding)."""
+    coords, tris, meas, H, o32, o64 = env
+    kap = [2.0, 3.0, 5.0, 7.5]
+    coeff = _coeff(cname, kap)
+    B = crandn(np.random.default_rng(5), coords.shape[0], 64)
+    C64 = np.zeros_like(B)
+    o64.ApplyBoundaryOperators_PL(1.0, B, 0.0, C64, kap, coeff, 64, 16)
+    H.SetApplyMode(APPLY_TC)
+    H.SetTuning(_capi.TUNE_TC_GEN_WARPS, gw)
+    H.SetTuning(_capi.TUNE_TC_CHUNKS, chunks)
+    try:
+        C = np.zeros_like(B)
+        H.ApplyBoundaryOperators_PL(1.0, B, 0.0, C, kap, coeff, 64, 16)
+    finally:
+        H.SetTuning(_capi.TUNE_TC_GEN_WARPS, 16)
+        H.SetTuning(_capi.TUNE_TC_CHUNKS, 0)
+        H.SetApplyMode(APPLY_FP32)
     assert relerr(C, C64) < FP32_VS64_TOL
 
 
@@ -563,7 +602,7 @@ def test_apply_at_the_maximum_wave_count(mode):
     o = O.Oracle(coords, tris, np.eye(3), precision=64)
     Co = C0.copy()
     o.ApplyBoundaryOperators_PL(0.5 - 1j, B, 0.25, Co, kap, coeff, 512, 64)
-    assert relerr(Cg, Co) < (1e-11 if mode == APPLY_FP64 else 3e-5)
+    assert relerr(Cg, Co) < (1e-11 if mode == APPLY_FP64 else FP32_VS64_TOL)
 
 
 @pytest.mark.parametrize("mode", [APPLY_FP32, APPLY_TC, APPLY_FP64])
@@ -588,7 +627,7 @@ def test_apply_on_tiny_meshes(mode, name):
     Co = C0.copy()
     o.ApplyBoundaryOperators_PL(0.5 - 1j, B, 0.25, Co, [3.0], coeff, 16, 16)
     assert np.isfinite(Cg).all()
-    assert relerr(Cg, Co) < (1e-11 if mode == APPLY_FP64 else 3e-5)
+    assert relerr(Cg, Co) < (1e-11 if mode == APPLY_FP64 else FP32_VS64_TOL)
 
 
 def test_error_statuses(env):

@@ -159,12 +159,12 @@ def test_derivative_and_adjoint_match_oracle(env):
     assert relerr(du_dn, du_o) < 1e-5
     DFo = np.zeros_like(DFg)
     o32.Derivative_FF(kap, inc, h, DFo, du_o, False, WaveType.Plane, 1e-10, 1e-10)
-    assert relerr(DFg, DFo) < 1e-4
+    assert relerr(DFg, DFo) < 1e-5
     g = crandn(rng, nm, wc)
     Yg, Yo = np.zeros((nv, 3)), np.zeros((nv, 3))
     H.AdjointDerivative_FF(kap, inc, g, Yg, du_dn, WaveType.Plane, 1e-10, 1e-10)
     o32.AdjointDerivative_FF(kap, inc, g, Yo, du_o, False, WaveType.Plane, 1e-10, 1e-10)
-    assert relerr(Yg, Yo) < 1e-4
+    assert relerr(Yg, Yo) < 1e-5
 
 
 def test_gauss_newton_matches_oracle():
@@ -197,5 +197,16 @@ def test_gauss_newton_matches_oracle():
         ok_c = H.GaussNewtonSolve(kap, inc, Mop, Pop, 1.0, B, 0.0, Xc, du_o.copy(), WaveType.Plane, 1e-10, 1e-8,
                                   1e-6, solver=1)
     assert ok_o and ok_g and ok_c
-    assert relerr(Xg, Xo) < 1e-4
-    assert relerr(Xc, Xo) < 1e-4
+    assert relerr(Xg, Xo) < 1e-5
+    assert relerr(Xc, Xo) < 1e-5
+
+
+def test_profile_krylov_reports_positive_rates(env):
+    """The Krylov-vector measurement hook: every kernel timed, bytes as stated."""
+    coords, tris, meas, inc, H, o32, o64 = env
+    prof = H.ProfileKrylov(columns=16, iterations=3, basis=4)
+    n = coords.shape[0]
+    for name, v in prof.items():
+        assert v["ms"] > 0 and v["algorithmic_bytes"] > 0 and v["GB_s"] > 0, name
+    assert prof["cg_pupdate"]["algorithmic_bytes"] == 3 * n * 32 * 8
+    assert prof["gs_update"]["algorithmic_bytes"] == (4 + 2) * n * 16 * 16
