@@ -169,12 +169,13 @@ class SolveServer:
     slots: concurrent solves; budget_bytes: device-memory admission budget
     (default: half the free device memory at start-up).
     apply_mode: APPLY_TC (default) or APPLY_FP32; graphs: replay the solver's
-    inner operators as CUDA graphs; autotune: tune the dense kernel once per
-    slot on its first request's shape.
+    inner operators as CUDA graphs; autotune (default on): tune the dense
+    kernel per problem shape (mesh size, right-hand-side count); the library
+    caches the choice per shape for the process, so each shape is timed once.
     """
 
     def __init__(self, meas_directions, slots: int = 6, budget_bytes: Optional[int] = None, apply_mode=None,
-                 graphs: bool = True, autotune: bool = False, device: int = 0,
+                 graphs: bool = True, autotune: bool = True, device: int = 0,
                  executor: Optional[Callable] = None):
         from ._capi import APPLY_TC
         self.meas = np.ascontiguousarray(np.asarray(meas_directions, dtype=np.float64).reshape(-1, 3))
@@ -189,7 +190,7 @@ class SolveServer:
         self._executor = executor or self._solve_on_slot
         self._contexts: dict = {}
         self._slot_mesh: dict = {}
-        self._tuned: set = set()
+        self._tuned: dict = {}          # slot -> problem shape whose tuned settings the context holds
         self.results: dict = {}
         self._lock = threading.Lock()
         self._t0 = 0.0
@@ -228,12 +229,16 @@ class SolveServer:
         dirs[: req.nrhs] = req.directions
         dirs[req.nrhs:] = req.directions[0]          # padding columns, discarded
         kap = np.array([req.kappa], dtype=np.float64)
-        if self.autotune and (slot, wcs) not in self._tuned:
+        shape = (req.triangles.shape[0], req.coords.shape[0], wcs)
+        if self.autotune and self._tuned.get(slot) != shape:
+            # the solve's operator structure (mixed BIE).  The library caches the choice per shape for the
+            # process, so only a shape's first request times anything; later ones apply the cached choice
+            # (a slot that served another shape in between must not keep that shape's settings).
             coeff = np.array([[0.5, -1j * req.kappa, 1.0, 0.0]])
             H.LoadBoundaryOperators_PL(kap, coeff, wcs, wcs)
             H.Autotune(self.apply_mode, repeats=1)
             H.UnloadBoundaryOperators_PL()
-            self._tuned.add((slot, wcs))
+            self._tuned[slot] = shape
         F = np.zeros((self.meas.shape[0], wcs), complex)
         H.FarField(kap, dirs, F, WaveType.Plane, req.cg_tol, req.gmres_tol)
         st = H.LastSolveStats()

@@ -527,8 +527,22 @@ def run_gpu_arm(args, rank, world, local_rank):
     if cpu is not None:
         line["cpu_baseline"] = {"value": cpu["value"], "unit": UNIT, "cores": cpu["cores"], "kind": cpu["kind"],
                                 "projected": True, "sample": cpu["sample"]}
-    print(json.dumps(line), flush=True)
     H.close()
+    if world == 1 and S is None and args.extras and not args.small:
+        # the other configurations, compact (not part of value): the scattering solve and a serving sample
+        res, apply, ntri = solve_runs(6, ("fp64", "fp32", "tc", "tc_ir"), with_apply_ms=False)
+        kry = res.pop("krylov_steps")
+        line["solve_icosphere6"] = {
+            "workload": SOLVE_WORKLOAD, "triangles": ntri,
+            "runs": {k: {q: v[q] for q in ("seconds", "gmres_iterations", "refinement_steps",
+                                           "far_field_rel_err_vs_fp64", "phi_rel_err_vs_fp64")}
+                     for k, v in res.items()},
+            "krylov_steps": kry}
+        line["serving_sample"] = dict(serve_runs(args.serve_sample, slots=6, seed=0), requests=args.serve_sample,
+                                      workload="perturbed-icosphere scattering solves, levels 4-6, kappa U[1,10], "
+                                               "1-64 plane waves, GMRES 1e-6, far field at 128 directions; "
+                                               "Poisson arrivals at 80 % of capacity for the latencies")
+    print(json.dumps(line), flush=True)
     return 0
 
 
@@ -677,16 +691,19 @@ SOLVE_WORKLOAD = ("unit icosphere level 6 (40962 V, 81920 T), kappa {4, 8} x 16 
                   "directions), far field at 256 Fibonacci directions, mixed indirect BIE, GMRES(30) + CG M^-1")
 
 
-def run_solve_workload(args):
-    """FarField (FarField.hpp:28-144) on the scattering-solve configuration:
-    plain FP32 apply, compensated tensor-core apply, the tensor-core apply
-    inside FP64 iterative refinement, and the FP64 path; errors of the far
-    field and of the boundary density phi against the FP64 solve at residual
-    1e-10 (the FP64 device path is held to 1e-11 of the FP64 oracle by the
-    tests at smaller sizes)."""
+def solve_runs(level=6, modes=("fp64", "fp32", "tc", "tc_ir"), with_apply_ms=True):
+    """FarField (FarField.hpp:28-144) on the scattering-solve configuration
+    (icosphere `level`, kappa {4, 8} x 16 Fibonacci plane waves, far field at
+    256 Fibonacci directions) in the given arithmetic forms: plain FP32 apply
+    to residual 1e-6, compensated tensor-core apply to 1e-6, the tensor-core
+    apply inside FP64 iterative refinement to 1e-10, and the FP64 path to
+    1e-10; wall time of one warm solve each, GMRES iterations, and the errors
+    of the far field and of the boundary density phi against the FP64 solve
+    (the FP64 device path is held to 1e-11 of the FP64 oracle by the tests at
+    smaller sizes).  Returns (runs, apply_ms, triangles)."""
     import torch
     from baemm_b200 import APPLY_FP32, APPLY_FP64, APPLY_TC, Helmholtz_CUDA, WaveType, meshes
-    coords, tris = meshes.icosphere(args.solve_level)
+    coords, tris = meshes.icosphere(level)
     meas = meshes.fibonacci_sphere(256)
     inc = meshes.fibonacci_sphere(16)
     kap = np.array([4.0, 8.0])
@@ -738,7 +755,6 @@ def run_solve_workload(args):
             H.UnloadBoundaryOperators_PL()
         return min(ts[1:])
 
-    modes = [m.strip() for m in args.solve_modes.split(",") if m.strip()]
     known = {"fp64": ("fp64_tol1e-10", APPLY_FP64, 1e-10, 0), "fp32": ("fp32_tol1e-6", APPLY_FP32, 1e-6, 0),
              "tc": ("tc_tol1e-6", APPLY_TC, 1e-6, 0), "tc_ir": ("tc_fp64ir_tol1e-10", APPLY_TC, 1e-10, 8)}
     bad = [m for m in modes if m not in known]
@@ -759,83 +775,128 @@ def run_solve_workload(args):
                      "refinement_steps": st["refinement_steps"],
                      "gmres_relative_residual": st["gmres_relative_residual"],
                      "far_field_rel_err_vs_fp64": rel(F, F64), "phi_rel_err_vs_fp64": rel(phi, phi64)}
-    apply = {name.split("_")[0]: apply_ms(mode) for m in ("tc", "fp32", "fp64") if m in modes
-             for name, mode, _, _ in [known[m]]}
+    apply = ({name.split("_")[0]: apply_ms(mode) for m in ("tc", "fp32", "fp64") if m in modes
+              for name, mode, _, _ in [known[m]]} if with_apply_ms else {})
+    # the Krylov-vector kernels of these solves (32 complex columns, basis of 12 = the iterations the
+    # tensor-core solve takes), against the measured copy bandwidth
+    peaks = load_peaks()
+    kry = H.ProfileKrylov(32, 20, 12)
+    for v in kry.values():
+        v["frac_of_hbm_peak"] = v["GB_s"] / peaks["hbm_gbs"] if v["GB_s"] else None
+    kry["note"] = ("algorithmic bytes per launch / CUDA-event time per launch; the 21 MB vectors stay in the 126 MB L2 "
+                   "between kernels, so rates above the HBM peak are possible; peak " + peaks["source"] +
+                   " copy bandwidth")
+    res["krylov_steps"] = kry
+    H.close()
+    return res, apply, int(tris.shape[0])
+
+
+def run_solve_workload(args):
+    modes = [m.strip() for m in args.solve_modes.split(",") if m.strip()]
+    res, apply, nt = solve_runs(args.solve_level, modes)
+    kry = res.pop("krylov_steps")
     head = "tc_fp64ir_tol1e-10" if "tc_fp64ir_tol1e-10" in res else next(iter(res))
     line = {"metric": "scattering solves/s (FarField)", "value": res[head]["solves_per_s"],
             "unit": "solves/s", "n_gpus": 1, "higher_is_better": True, "data": "synthetic",
             "config": {"workload": SOLVE_WORKLOAD if args.solve_level == 6 else f"icosphere level {args.solve_level}",
-                       "triangles": int(tris.shape[0]), "wave_count": 32, "meas_count": 256, "value_run": head},
-            "runs": res, "apply_ms": apply}
+                       "triangles": nt, "wave_count": 32, "meas_count": 256, "value_run": head},
+            "runs": res, "apply_ms": apply, "krylov_steps": kry}
     print(json.dumps(line), flush=True)
-    H.close()
     return 0
 
 
 # ---------------------------------------------------------------------------
 # the serving workload (--workload serve): not the headline line
 # ---------------------------------------------------------------------------
-def run_serve_workload(args):
+def serve_runs(n_requests, slots=6, seed=0, seq_sample=0, seq_tc=True, latency=True):
     """Stream of scattering-solve requests (icosphere levels 4-6 radially
     perturbed by a random degree-8 spherical-harmonic field of amplitude 0.1,
     kappa ~ U[1, 10], 1-64 plane waves, GMRES to 1e-6, far field at 128
-    directions).  Three runs over the same requests:
-      sequential  the plain FP32 apply, one request at a time (the baseline);
-      capacity    the serving loop (slots of resident contexts, memory-budget
-                  admission, tensor-core apply, CUDA-graph replay) with every
-                  request queued at once: solves/s is its throughput;
-      latency     the serving loop with Poisson arrivals at 80 % of that
-                  capacity: p50 / p99 of finish - arrival.
+    directions).  Runs over the same requests:
+      sequential_plain_fp32  the plain FP32 apply, one request at a time (the baseline);
+      sequential_tc          the tensor-core apply with graph replay, one request at a
+                             time (the same arithmetic as the server: the server's own
+                             gain over it is the batching);
+      capacity               the serving loop (slots of resident contexts, memory-budget
+                             admission, tensor-core apply, CUDA-graph replay) with every
+                             request queued at once: solves/s is its throughput;
+      latency                the serving loop with Poisson arrivals at 80 % of that
+                             capacity: p50 / p99 of finish - arrival.
     The far fields of the served runs are compared with the sequential ones."""
     from baemm_b200 import APPLY_FP32, APPLY_TC, meshes
     from baemm_b200.serving import SolveServer, make_stream, summarize
+    from baemm_b200.serving import SolveRequest
     meas = meshes.fibonacci_sphere(128)
-    reqs = make_stream(args.requests, rate=0.0, seed=args.serve_seed)
-    warm = make_stream(2, rate=0.0, levels=(4,), seed=12345)
+    reqs = make_stream(n_requests, rate=0.0, seed=seed)
+    # warm-up: one request per problem shape (mesh level x padded right-hand sides), so the
+    # autotuner's choices and the device buffers exist before any timing
+    warm = []
+    for level in (4, 5, 6):
+        coords_w, tris_w = meshes.icosphere(level)
+        for nrhs in (16, 32, 64):
+            d = meshes.fibonacci_sphere(nrhs)
+            warm.append(SolveRequest(len(warm) + 1000000, coords_w, tris_w, 3.0, d, mesh_key=("warm", level)))
 
     def at_once():
         for r in reqs:
             r.arrival = 0.0
         return reqs
 
-    n_seq = len(reqs) if args.seq_sample <= 0 else min(args.seq_sample, len(reqs))
-    with SolveServer(meas, slots=1, apply_mode=APPLY_FP32, graphs=False) as seq:
-        seq.run(warm, realtime=False)
-        t0 = time.perf_counter()
-        base = seq.run(at_once()[:n_seq], realtime=False)
-        t_seq = time.perf_counter() - t0
-    thr_plain = n_seq / t_seq
-    with SolveServer(meas, slots=args.slots, apply_mode=APPLY_TC, graphs=True) as srv:
+    n_seq = len(reqs) if seq_sample <= 0 else min(seq_sample, len(reqs))
+
+    def sequential(mode, graphs):
+        with SolveServer(meas, slots=1, apply_mode=mode, graphs=graphs) as seq:
+            seq.run(warm, realtime=False)
+            t0 = time.perf_counter()
+            out = seq.run(at_once()[:n_seq], realtime=False)
+            return out, time.perf_counter() - t0
+
+    base, t_seq = sequential(APPLY_FP32, False)
+    res = {"sequential_plain_fp32": {"solves_per_s": n_seq / t_seq, "seconds": t_seq, "requests": n_seq,
+                                     "note": "the first requests of the same stream" if n_seq < len(reqs) else "all"}}
+    if seq_tc:
+        _, t_tc = sequential(APPLY_TC, True)
+        res["sequential_tc"] = {"solves_per_s": n_seq / t_tc, "seconds": t_tc, "requests": n_seq}
+    with SolveServer(meas, slots=slots, apply_mode=APPLY_TC, graphs=True) as srv:
         srv.run(warm, realtime=False)
         t0 = time.perf_counter()
         cap = srv.run(at_once(), realtime=False)
         t_cap = time.perf_counter() - t0
-        peak = srv.scheduler.peak_running
         thr_served = len(reqs) / t_cap
-        rate = 0.8 * thr_served
-        rng = np.random.default_rng(args.serve_seed + 1)
-        t = 0.0
-        for r in reqs:
-            t += rng.exponential(1.0 / rate)
-            r.arrival = t
-        lat = srv.run(reqs, realtime=True)
-    s_lat = summarize(lat)
-    diff = max(max(float(np.linalg.norm(run[k].far_field - base[k].far_field) /
-                         max(np.linalg.norm(base[k].far_field), 1e-300)) for k in base) for run in (cap, lat))
-    line = {"metric": "served solves/s (scattering, FarField)", "value": thr_served, "unit": "solves/s",
-            "n_gpus": 1, "higher_is_better": True, "data": "synthetic",
+        res["capacity"] = {"solves_per_s": thr_served, "seconds": t_cap,
+                           "peak_concurrent": srv.scheduler.peak_running,
+                           "converged": int(sum(r.converged for r in cap.values())), "requests": len(reqs)}
+        served = [cap]
+        if latency:
+            rate = 0.8 * thr_served
+            rng = np.random.default_rng(seed + 1)
+            t = 0.0
+            for r in reqs:
+                t += rng.exponential(1.0 / rate)
+                r.arrival = t
+            lat = srv.run(reqs, realtime=True)
+            s_lat = summarize(lat)
+            res["latency_at_80pct_load"] = {"arrival_rate_per_s": rate, "p50_s": s_lat["p50_latency_s"],
+                                            "p99_s": s_lat["p99_latency_s"], "mean_s": s_lat["mean_latency_s"],
+                                            "solves_per_s": s_lat["solves_per_s"]}
+            served.append(lat)
+    res["speedup_vs_sequential_plain"] = thr_served / res["sequential_plain_fp32"]["solves_per_s"]
+    if seq_tc:
+        res["speedup_vs_sequential_tc"] = thr_served / res["sequential_tc"]["solves_per_s"]
+    res["max_far_field_rel_diff_served_vs_sequential"] = max(
+        max(float(np.linalg.norm(run[k].far_field - base[k].far_field) /
+                  max(np.linalg.norm(base[k].far_field), 1e-300)) for k in base) for run in served)
+    return res
+
+
+def run_serve_workload(args):
+    res = serve_runs(args.requests, args.slots, args.serve_seed, args.seq_sample)
+    line = {"metric": "served solves/s (scattering, FarField)", "value": res["capacity"]["solves_per_s"],
+            "unit": "solves/s", "n_gpus": 1, "higher_is_better": True, "data": "synthetic",
             "config": {"workload": "perturbed-icosphere scattering solves, levels 4-6, kappa U[1,10], 1-64 plane "
                                    "waves, GMRES 1e-6, far field at 128 directions",
-                       "requests": len(reqs), "slots": args.slots, "seed": args.serve_seed},
-            "capacity": {"solves_per_s": thr_served, "seconds": t_cap, "peak_concurrent": peak,
-                         "converged": int(sum(r.converged for r in cap.values()))},
-            "latency_at_80pct_load": {"arrival_rate_per_s": rate, "p50_s": s_lat["p50_latency_s"],
-                                      "p99_s": s_lat["p99_latency_s"], "mean_s": s_lat["mean_latency_s"],
-                                      "solves_per_s": s_lat["solves_per_s"]},
-            "sequential_plain_fp32": {"solves_per_s": thr_plain, "seconds": t_seq, "requests": n_seq,
-                                      "note": "the first requests of the same stream" if n_seq < len(reqs) else "all"},
-            "speedup_vs_sequential_plain": thr_served / thr_plain,
-            "max_far_field_rel_diff_served_vs_sequential": diff}
+                       "requests": args.requests, "slots": args.slots, "seed": args.serve_seed}}
+    line.update(res)
     print(json.dumps(line), flush=True)
     return 0
 
@@ -930,6 +991,9 @@ def main(argv=None):
                     help="apply: the headline operator-apply line; solve: the scattering-solve configuration; "
                          "serve: the request stream through the serving loop")
     ap.add_argument("--requests", type=int, default=100, help="requests of --workload serve")
+    ap.add_argument("--no-extras", dest="extras", action="store_false",
+                    help="default apply line without the solve and serving keys")
+    ap.add_argument("--serve-sample", type=int, default=48, help="requests of the default line's serving sample")
     ap.add_argument("--slots", type=int, default=6, help="serving slots of --workload serve")
     ap.add_argument("--serve-seed", type=int, default=0)
     ap.add_argument("--seq-sample", type=int, default=0,
