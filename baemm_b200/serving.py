@@ -169,14 +169,17 @@ class SolveServer:
     slots: concurrent solves; budget_bytes: device-memory admission budget
     (default: half the free device memory at start-up).
     apply_mode: APPLY_TC (default) or APPLY_FP32; graphs: replay the solver's
-    inner operators as CUDA graphs; autotune (default on): tune the dense
+    inner operators as CUDA graphs; pack (default on, tensor-core form): the
+    slots' operator applies of small problems share one persistent launch
+    (helmholtz.Packer, waiting at most pack_wait_us for the other solves in
+    progress); autotune (default on): tune the dense
     kernel per problem shape (mesh size, right-hand-side count); the library
     caches the choice per shape for the process, so each shape is timed once.
     """
 
     def __init__(self, meas_directions, slots: int = 6, budget_bytes: Optional[int] = None, apply_mode=None,
                  graphs: bool = True, autotune: bool = True, device: int = 0,
-                 executor: Optional[Callable] = None):
+                 executor: Optional[Callable] = None, pack: bool = True, pack_wait_us: int = 2000):
         from ._capi import APPLY_TC
         self.meas = np.ascontiguousarray(np.asarray(meas_directions, dtype=np.float64).reshape(-1, 3))
         self.slots = slots
@@ -189,6 +192,10 @@ class SolveServer:
         self.scheduler = Scheduler(slots, budget_bytes)
         self._executor = executor or self._solve_on_slot
         self._contexts: dict = {}
+        self.packer = None
+        if pack and self.apply_mode == APPLY_TC and executor is None:
+            from .helmholtz import Packer
+            self.packer = Packer(device, pack_wait_us)
         self._slot_mesh: dict = {}
         self._tuned: dict = {}          # slot -> problem shape whose tuned settings the context holds
         self.results: dict = {}
@@ -212,6 +219,8 @@ class SolveServer:
             H = Helmholtz_CUDA(req.coords, req.triangles, self.meas, device=self.device)
             H.SetApplyMode(self.apply_mode)
             H.SetGraphs(self.graphs)
+            if self.packer is not None:
+                H.SetPacker(self.packer)
             self._contexts[slot] = H
             self._slot_mesh[slot] = id(req) if req.mesh_key is None else req.mesh_key
             return H
@@ -298,10 +307,19 @@ class SolveServer:
             raise errors[0]
         return dict(self.results)
 
+    def pack_stats(self) -> dict:
+        """Packed launches and the problems they carried (zeros without packing)."""
+        return self.packer.stats() if self.packer is not None else {"launches": 0, "problems": 0}
+
     def close(self):
         for H in self._contexts.values():
+            if self.packer is not None:
+                H.SetPacker(None)
             H.close()
         self._contexts.clear()
+        if self.packer is not None:
+            self.packer.close()
+            self.packer = None
 
     def __enter__(self):
         return self
