@@ -146,6 +146,10 @@ SIGNATURES = {
     "baemm_set_profiling": (I, [vp, I]),
     "baemm_profile_krylov": (I, [vp, I, I, I, dp]),
     "baemm_autotune_forget": (None, []),
+    "baemm_packer_create": (vp, [I, I]),
+    "baemm_packer_destroy": (None, [vp]),
+    "baemm_set_packer": (I, [vp, vp]),
+    "baemm_packer_stats": (I, [vp, i64p, i64p]),
     "baemm_last_apply_times": (I, [vp, fp]),
     "baemm_kernel_launch_count": (I64, []),
     "baemm_free": (None, [vp]),

@@ -623,6 +623,62 @@ int baemm_apply_boundary_operators_rows_dev_c(baemm_ctx *ctx, const float alpha[
     });
 }
 
+struct baemm_packer
+{
+    baemm::Packer *impl = nullptr;
+};
+
+baemm_packer *baemm_packer_create(int device, int max_wait_us)
+{
+    try
+    {
+        int n = 0;
+        BAEMM_CUDA(cudaGetDeviceCount(&n));
+        BAEMM_REQUIRE(device >= 0 && device < n, BAEMM_ERR_ARG, "no such device");
+        auto *p = new baemm_packer;
+        try
+        {
+            p->impl = new baemm::Packer(device, max_wait_us);
+        }
+        catch (...)
+        {
+            delete p;
+            throw;
+        }
+        g_create_error.clear();
+        return p;
+    }
+    catch (const std::exception &e)
+    {
+        g_create_error = e.what();
+        return nullptr;
+    }
+}
+
+void baemm_packer_destroy(baemm_packer *p)
+{
+    if (!p) return;
+    delete p->impl;
+    delete p;
+}
+
+int baemm_set_packer(baemm_ctx *ctx, baemm_packer *p)
+{
+    return guarded(ctx, [&](Ctx &c) {
+        BAEMM_REQUIRE(!p || (p->impl && p->impl->device() == c.device), BAEMM_ERR_ARG,
+                      "the packer belongs to another device");
+        c.packer = p ? p->impl : nullptr;
+    });
+}
+
+int baemm_packer_stats(const baemm_packer *p, int64_t *launches, int64_t *problems)
+{
+    if (!p || !p->impl) return BAEMM_ERR_ARG;
+    if (launches) *launches = p->impl->launches();
+    if (problems) *problems = p->impl->problems();
+    return BAEMM_OK;
+}
+
 int baemm_profile_krylov(baemm_ctx *ctx, int columns, int iterations, int basis, double out[10])
 {
     return guarded(ctx, [&](Ctx &c) {

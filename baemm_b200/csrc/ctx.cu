@@ -315,6 +315,9 @@ void Ctx::load_parameters(const double *kappa, const zc *coeff, int wc, int wcs,
         BAEMM_CUDA(cudaMemcpyAsync(prm16_f.reserve(groups), prm16_f_h.data(), groups * sizeof(ChunkParamsF),
                                    cudaMemcpyHostToDevice, stream));
         tc_form = tc_coeff_form(prm16_f_h.data(), groups);
+        tc_broadcast_params(prm16_f_h.data(), groups, prm_bc_h);
+        BAEMM_CUDA(cudaMemcpyAsync(prm_bc.reserve(prm_bc_h.size()), prm_bc_h.data(), prm_bc_h.size() * sizeof(float2),
+                                   cudaMemcpyHostToDevice, stream));
     }
     else
         tc_form = TcCoeffForm();
@@ -339,9 +342,24 @@ void Ctx::dense_apply(const cplx<R> *Btri, cplx<R> *Ctri, int64_t r0, int64_t r1
             launch_tc_tile_geometry(mesh, mesh.tgeo_f.reserve(tc_tile_geometry_floats(mesh.nt)), stream);
             tc_geo_ready = true;
         }
+        // Only problems whose own launch cannot fill the GPU (at most two target blocks per SM) are packed;
+        // a large one would hold its packed partners back until its own sweep ends.
+        const int64_t blocks = (int64_t)(wave_count / (16 * tc_chunks_per_unit(wave_count, tc_tune.chunks))) *
+                               ceil_div(mesh.nt, 128);
+        if (packer && r0 == 0 && (r1 < 0 || r1 == mesh.nt) && blocks <= 2 * (int64_t)tc_sm_count() &&
+            tc_packable(flags, tc_form, wave_count, wave_chunk_size))
+        {
+            // one problem of the packer's next launch (the stream waits for that launch)
+            const uint8_t *img = launch_tc_expand(Btri, mesh.nt, wave_count, tc_img, stream);
+            const TcPackItem item{mesh.mid_f, mesh.nrm_f, mesh.tgeo_f.p, img, Ctri, prm_bc.p, tc_err.p, mesh.nt,
+                                  wave_count, tc_form.s};
+            packer->apply(item, flags, tc_tune, stream);
+            tc_pending = true;
+            return;
+        }
         const size_t ws_elems = tc_workspace_elems(tc_tune.ctas);
         launch_boundary_tc(mesh, flags, prm16_f.p, tc_form, wave_count, wave_chunk_size, mesh.tgeo_f.p, Btri, Ctri,
-                           tc_ws.reserve(ws_elems), ws_elems, tc_err.p, stream, tc_tune, r0,
+                           tc_ws.reserve(ws_elems), ws_elems, tc_img, tc_err.p, stream, tc_tune, r0,
                            r1);
         tc_pending = true;
     }
@@ -463,7 +481,7 @@ void Ctx::apply_nearfield(Text alpha, const Text *B, int64_t ldB, Text beta, Tex
             }
             const size_t ws_elems = tc_workspace_elems(tc_tune.ctas);
             launch_nearfield_tc(mesh, nf, prm16_f.p, tc_form, wave_count, wave_chunk_size, mesh.tgeo_f.p, p4, npts, Bt, Cp,
-                                tc_ws.reserve(ws_elems), ws_elems, tc_err.p, stream, tc_tune);
+                                tc_ws.reserve(ws_elems), ws_elems, tc_img, tc_err.p, stream, tc_tune);
             tc_pending = true;
         }
         else

@@ -11,6 +11,7 @@
 
 #include "krylov.cuh"
 #include "ops.cuh"
+#include "pack.cuh"
 
 namespace baemm
 {
@@ -42,8 +43,12 @@ public:
     std::vector<ChunkParamsD> prm_d_h;
     DevBuf<ChunkParamsF> prm_f;
     std::vector<ChunkParamsF> prm16_f_h;   // per 16-column group (tensor-core form)
+    std::vector<float2> prm_bc_h;
     DevBuf<ChunkParamsF> prm16_f;
     TcCoeffForm tc_form;                    // coefficient structure the tensor-core form specialises on
+    DevBuf<float2> prm_bc;                  // broadcast parameter pairs of the 16-column groups (packed launches)
+    DevBuf<uint8_t> tc_img;                 // the tensor-core form's expanded B operand (launch_tc_expand)
+    Packer *packer = nullptr;               // shared packer of concurrent solves' applies (not owned)
     DevBuf<ChunkParamsD> prm_d;
     bool operators_loaded = false;
 

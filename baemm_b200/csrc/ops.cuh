@@ -8,6 +8,7 @@
 //   AvOp^T           CSR over vertices: avt_outer (nv+1), avt_inner (3 nt) = triangle ids ascending
 //   Mass             CSR over vertices: mass_outer, mass_inner (sorted), values float and double
 #pragma once
+#include <vector>
 #include "common.cuh"
 
 namespace baemm
@@ -159,12 +160,62 @@ struct TcTuning
 int tc_chunks_per_unit(int wc, int chunks);
 void launch_boundary_tc(const MeshDev &m, const OpFlags &f, const void *chunk_params, const TcCoeffForm &form, int wc,
                         int wcs, const float *tgeo, const float2 *Btri, float2 *Ctri, float2 *ws, size_t ws_elems,
-                        int *err, cudaStream_t st, const TcTuning &tune, int64_t row_begin = 0, int64_t row_end = -1);
+                        DevBuf<uint8_t> &img, int *err, cudaStream_t st, const TcTuning &tune,
+                        int64_t row_begin = 0, int64_t row_end = -1);
 // The tensor-core form of the near field: targets pts4 (npts x 4 floats), no
 // pair excluded, flags without the adjoint double layer.
 void launch_nearfield_tc(const MeshDev &m, const OpFlags &f, const void *chunk_params, const TcCoeffForm &form,
                          int wc, int wcs, const float *tgeo, const float *pts4, int64_t npts, const float2 *Btri,
-                         float2 *Cpts, float2 *ws, size_t ws_elems, int *err, cudaStream_t st, const TcTuning &tune);
+                         float2 *Cpts, float2 *ws, size_t ws_elems, DevBuf<uint8_t> &img, int *err, cudaStream_t st,
+                         const TcTuning &tune);
+// The tensor-core form's B operand: every 16-source tile's hi / lo images of
+// B_tri (n x wc) per 16-column group, as the kernel's B stages hold them
+// (8 KB each); returns img's device block (grown as needed).
+const uint8_t *launch_tc_expand(const float2 *Btri, int64_t n, int wc, DevBuf<uint8_t> &img, cudaStream_t st);
+// ---- packed tensor-core launches (several problems in one persistent launch) ----
+// One problem as the host describes it: the boundary operator of one mesh
+// (targets = sources = its nt triangles) on its device blocks.
+struct TcPackItem
+{
+    const float *mid4, *nrm4;       // triangle midpoints and normals (float4)
+    const float *tgeo;              // tile geometry (launch_tc_tile_geometry)
+    const uint8_t *img;             // the expanded B operand (launch_tc_expand)
+    float2 *Ctri;
+    const float2 *prm_bcast;        // tc_broadcast_params on the device
+    int *err;                       // the problem's error word (a time-out lands here)
+    int64_t nt;
+    int wc;
+    float ki_s;
+};
+// Tables of packed launches: a grow-only device block and a pinned host copy
+// it is uploaded from (on the launch's stream; reused once the last upload
+// has completed).
+struct TcPackScratch
+{
+    DevBuf<uint8_t> dev;
+    uint8_t *host = nullptr;
+    size_t host_cap = 0;
+    cudaEvent_t uploaded = nullptr;
+    TcPackScratch() = default;
+    TcPackScratch(const TcPackScratch &) = delete;
+    TcPackScratch &operator=(const TcPackScratch &) = delete;
+    ~TcPackScratch();
+    void reserve(size_t bytes);
+    uint8_t *stage(const void *src, size_t bytes, cudaStream_t st);
+};
+// 8 broadcast pairs per 16-column group (kappa, -kappa, c1.x, c1.y, -c2.x, -c2.y, c3.x, c3.y).
+void tc_broadcast_params(const ChunkParamsF *host_params, int groups, std::vector<float2> &out);
+// SMs of the current device (cached).
+int tc_sm_count();
+// Whether the loaded operators can join a packed launch (the KI-form solve operators).
+bool tc_packable(const OpFlags &f, const TcCoeffForm &form, int wc, int wcs);
+// Problems with equal classes can share a packed launch (operator structure, chunk groups, warps, segment).
+int tc_pack_class(const OpFlags &f, int wc, const TcTuning &tune);
+// One launch over `count` problems of one class: whole target blocks, assigned
+// longest first to the least loaded CTA, so each problem's result is the same
+// whatever it is packed with.
+void launch_boundary_tc_packed(const TcPackItem *items, int count, const OpFlags &f, const TcTuning &tune,
+                               TcPackScratch &scratch, int *err, cudaStream_t st);
 // Source geometry of the tensor-core form, per 16-source tile (built once per mesh).
 size_t tc_tile_geometry_floats(int64_t nt);
 void launch_tc_tile_geometry(const MeshDev &m, float *tgeo, cudaStream_t st);

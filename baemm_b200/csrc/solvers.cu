@@ -27,9 +27,14 @@ void Ctx::bie_solve(const double *kappa, const zc *coeff4, const double2 *rhs, d
     operators_loaded = true;
     stats = baemm_solve_stats{};
     stats.cg_converged = 1;
+    // With a packer the dense stage joins the packer's launches, which cannot
+    // be captured in this context's graph: the apply then runs ungraphed.
+    PackerSession session(packer);
     GmresSolver<double2>::Op A = [&](const double2 *x, double2 *y) {
-        run_graphed(GraphKey{1, x, y, wc, wc, apply_mode, wave_count},
-                    [&] { apply_boundary<double2>(kOne, x, wc, kZero, y, wc); });
+        if (packer) apply_boundary<double2>(kOne, x, wc, kZero, y, wc);
+        else
+            run_graphed(GraphKey{1, x, y, wc, wc, apply_mode, wave_count},
+                        [&] { apply_boundary<double2>(kOne, x, wc, kZero, y, wc); });
     };
     GmresSolver<double2>::Op P = [&](const double2 *x, double2 *y) {
         mass_inverse_complex(x, wc, y, wc, wc, cg_tol);

@@ -49,6 +49,9 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstring>
+#include <utility>
+#include <vector>
 #include <cstddef>
 #include <mutex>
 
@@ -65,7 +68,6 @@ constexpr int TC_MAXCHUNKS = 32;   // wave_count <= 512 with wave_chunk_size 16
 // Generator warps GW = 16 (4 per SM sub-partition, 4 sources per thread and
 // tile) or 8 (8 sources per thread); the autotuner picks one per problem
 // shape.  16 hide the latency of the entry evaluation better on large blocks.
-constexpr int TC_EXP_THREADS = 64;
 template <int GW>
 struct TcShape
 {
@@ -76,11 +78,11 @@ struct TcShape
     static constexpr int PPT = SPT / 2;          // their pairs
     static constexpr int KPT = 2 * SPT;          // their K columns of an A stage
     static constexpr int CPG = 16 / GROUPS;      // right-hand sides per thread in the drain
-    static constexpr int THREADS = GEN_THREADS + TC_EXP_THREADS + 64;   // + bulk-copy warp + MMA warp
+    static constexpr int THREADS = GEN_THREADS + 64;   // + bulk-copy warp + MMA warp
 };
 constexpr int TC_ASTAGES = 4;      // A stages in TMEM (one chunk of one tile each)
-constexpr int TC_BSTAGES = 3;      // expanded B image stages in shared memory
-constexpr int TC_RSTAGES = 6;      // raw tile stages filled by bulk copies
+constexpr int TC_BSTAGES = 4;      // B image stages in shared memory (bulk copies of the expanded images)
+constexpr int TC_RSTAGES = 6;      // tile geometry stages (bulk copies)
 constexpr uint32_t TC_TMEM_COLS = 512;
 constexpr uint32_t TC_DCOLS = 2 * TC_N;             // per chunk: main (Ahi Bhi) | correction (Ahi Blo + Alo Bhi)
 constexpr uint32_t TC_ACC_COLS = TC_CHMAX * TC_DCOLS;   // the TMEM accumulator (256 columns)
@@ -97,18 +99,16 @@ struct TcTileGeo
 };
 static_assert(sizeof(TcTileGeo) % 16 == 0, "bulk copies move multiples of 16 bytes");
 
-// Raw tile: the 16 source rows of B_tri (this CTA's columns) plus the tile's
-// geometry, filled by cp.async.bulk.
-struct TcRaw
-{
-    float2 b[TC_SRC][TC_CHMAX * 16];   // 8 KB
-    TcTileGeo geo;
-};
+// The right-hand sides of one 16-source tile and one 16-column group as the
+// MMA's B operand: the hi and the lo image (32 rows each, see
+// tc_expand_kernel), 8 KB, expanded once per apply into global memory and
+// bulk-copied into a B stage as they are.
+constexpr int TC_GROUP_BYTES = 2 * TC_IMG;
 
 struct __align__(1024) TcSmem
 {
     uint8_t img[TC_BSTAGES][TC_CHMAX][2][TC_IMG];   // [stage][chunk][hi, lo]
-    TcRaw raw[TC_RSTAGES];
+    TcTileGeo geo[TC_RSTAGES];
     uint64_t a_full[TC_ASTAGES], a_empty[TC_ASTAGES];
     uint64_t b_full[TC_BSTAGES], b_empty[TC_BSTAGES];
     uint64_t r_full[TC_RSTAGES], r_empty[TC_RSTAGES];
@@ -125,8 +125,8 @@ struct __align__(1024) TcSmem
 static_assert(sizeof(TcSmem) + 1024 <= 227 * 1024, "shared memory per CTA");
 static_assert(offsetof(TcSmem, acc) % 16 == 0 && (sizeof(float2) * (TC_CHMAX * 16 + 2)) % 16 == 0,
               "accumulator rows are read and written as float4");
-static_assert(offsetof(TcSmem, raw) % 16 == 0 && offsetof(TcRaw, geo) % 16 == 0 && sizeof(TcRaw) % 16 == 0,
-              "bulk-copy destinations are 16-byte aligned");
+static_assert(offsetof(TcSmem, geo) % 16 == 0 && offsetof(TcSmem, img) % 1024 == 0 && TC_GROUP_BYTES % 1024 == 0,
+              "bulk-copy destinations are 16-byte aligned; images keep the 1024-byte swizzle alignment");
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
@@ -341,6 +341,22 @@ __device__ __forceinline__ uint32_t img_off16(int row, int sp) { return (uint32_
 // read at any time stay few and cached.  The remaining blocks ("tail") are
 // split evenly by 16-source tiles ("stream-K"): CTA k takes the tail units
 // [tail_start(k), tail_start(k + 1)), where a unit is one tile of one block.
+// One problem of a packed launch (device memory; the fields of a single
+// launch's plan and arguments, per problem).  prm: the broadcast parameter
+// pairs of the problem's chunk groups, 8 per group (kappa, -kappa, c1.x, c1.y,
+// -c2.x, -c2.y, c3.x, c3.y, each as (v, v)); err: the problem's error word.
+struct TcProblem
+{
+    const float *mid4, *nrm4;
+    const TcTileGeo *tgeo;
+    const uint8_t *img;   // the expanded B images (tc_expand_kernel)
+    float2 *Ctri;
+    const float2 *prm;
+    int *err;
+    int n, m, wc, nblk, ntiles, self, off;
+    float ki_s;
+};
+
 struct TcPlan
 {
     int n, wc, nblk, ntiles, ncg, seg_tiles;
@@ -353,6 +369,11 @@ struct TcPlan
     int64_t tail_units;   // tail_blocks * ntiles
     int stagger;       // whole-block sweeps of CTA k start at tile (k % 8) * stagger; -1: k * ntiles / ctas
     float ki_s;        // KI form: the common ratio s = c1.y / kappa (scaled coefficients)
+    // packed launch: CTA k runs the whole blocks pieces[cta_begin[k] .. cta_begin[k + 1]),
+    // each (problem, block of that problem); the scalar fields above are unused
+    const TcProblem *probs;
+    const int *cta_begin;
+    const int2 *pieces;
 };
 
 __host__ __device__ __forceinline__ int64_t tc_tail_start(const TcPlan &p, int k)
@@ -401,6 +422,69 @@ struct PieceIter
         cg = b / p.nblk;
         blk = b - cg * p.nblk;
         return true;
+    }
+};
+
+// The pieces of a packed launch: whole blocks, every sweep from the first
+// tile, so a problem's sums do not depend on what it is packed with.
+struct PackIter
+{
+    int e, e1;
+    __device__ PackIter() : e(0), e1(0) {}
+    __device__ PackIter(const TcPlan &p, int k) : e(p.cta_begin[k]), e1(p.cta_begin[k + 1]) {}
+    __device__ bool next(const TcPlan &p, int &prob, int &cg, int &blk, int &tb, int &te, int &slot, int &rot)
+    {
+        if (e >= e1) return false;
+        const int2 q = p.pieces[e++];
+        prob = q.x;
+        const int nblk = p.probs[prob].nblk;
+        cg = q.y / nblk;
+        blk = q.y - cg * nblk;
+        tb = 0;
+        te = p.probs[prob].ntiles;
+        slot = 0;
+        rot = 0;
+        return true;
+    }
+};
+
+// The problem a piece belongs to, as the roles read it.
+struct TcView
+{
+    const float *mid4, *nrm4;
+    const TcTileGeo *tgeo;
+    const uint8_t *img;
+    float2 *Ctri;
+    const float2 *prm;   // chunk group 0's 8 broadcast pairs (shared memory in a single launch)
+    int n, m, wc, ntiles, self, off;
+    float ki_s;
+};
+
+__device__ __forceinline__ TcView view_of(const TcProblem &q)
+{
+    return TcView{q.mid4, q.nrm4, q.tgeo, q.img, q.Ctri, q.prm, q.n, q.m, q.wc, q.ntiles, q.self, q.off, q.ki_s};
+}
+
+// Both piece walks behind one interface for the roles.
+template <bool PACK>
+struct Pieces
+{
+    PieceIter solo;
+    PackIter pack;
+    TcView single;
+    __device__ Pieces(const TcPlan &p, int k, const TcView &v)
+        : solo(p, PACK ? 0 : k), pack(PACK ? PackIter(p, k) : PackIter()), single(v) {}
+    __device__ bool next(const TcPlan &p, TcView &v, int &cg, int &blk, int &tb, int &te, int &slot, int &rot)
+    {
+        if (PACK)
+        {
+            int prob;
+            if (!pack.next(p, prob, cg, blk, tb, te, slot, rot)) return false;
+            v = view_of(p.probs[prob]);
+            return true;
+        }
+        v = single;
+        return solo.next(p, cg, blk, tb, te, slot, rot);
     }
 };
 
@@ -530,10 +614,11 @@ __device__ __forceinline__ void tc_entries_ki(const float2 *__restrict__ P, cons
 }
 
 // RI, KI: see tc_entries and tc_entries_ki.  GW: generator warps (TcShape).
-template <int GW, int CH, bool SL, bool DL, bool ADL, bool RI, bool KI>
+// PACK: a packed launch over plan.probs (the pointer arguments are unused).
+template <int GW, int CH, bool SL, bool DL, bool ADL, bool RI, bool KI, bool PACK>
 __global__ void __launch_bounds__(TcShape<GW>::THREADS, 1)
 boundary_tc_kernel(const float *__restrict__ mid4, const float *__restrict__ nrm4, const TcTileGeo *__restrict__ tgeo,
-                   const float2 *__restrict__ Btri, float2 *__restrict__ Ctri, float2 *__restrict__ ws,
+                   const uint8_t *__restrict__ img, float2 *__restrict__ Ctri, float2 *__restrict__ ws,
                    const ChunkParamsF *__restrict__ prm, const TcPlan plan, int *err)
 {
     constexpr int TC_GEN_THREADS = TcShape<GW>::GEN_THREADS;
@@ -545,7 +630,6 @@ boundary_tc_kernel(const float *__restrict__ mid4, const float *__restrict__ nrm
     TcSmem &sm = *reinterpret_cast<TcSmem *>(smem_raw + ((1024u - (smem_u32(smem_raw) & 1023u)) & 1023u));
     const int tid = threadIdx.x;
     const int warp = tid >> 5, lane = tid & 31;
-    const int n = plan.n, mt = plan.m, wc = plan.wc, ntiles = plan.ntiles;
     const int S = plan.seg_tiles;   // tiles per TMEM partial sum
     const int k_cta = blockIdx.x;
     volatile int *abort_flag = &sm.abort_flag;
@@ -559,18 +643,19 @@ boundary_tc_kernel(const float *__restrict__ mid4, const float *__restrict__ nrm
     if (tid == 0)
     {
         for (int k = 0; k < TC_ASTAGES; ++k) { mbar_init(&sm.a_full[k], TC_GEN_THREADS); mbar_init(&sm.a_empty[k], 1); }
-        for (int k = 0; k < TC_BSTAGES; ++k) { mbar_init(&sm.b_full[k], TC_EXP_THREADS); mbar_init(&sm.b_empty[k], 1); }
+        for (int k = 0; k < TC_BSTAGES; ++k) { mbar_init(&sm.b_full[k], 1); mbar_init(&sm.b_empty[k], 1); }
         for (int k = 0; k < TC_RSTAGES; ++k)
         {
             mbar_init(&sm.r_full[k], 1);
-            mbar_init(&sm.r_empty[k], TC_GEN_THREADS + TC_EXP_THREADS);
+            mbar_init(&sm.r_empty[k], TC_GEN_THREADS);
         }
         mbar_init(&sm.seg_full, 1);
         mbar_init(&sm.seg_empty, TC_GEN_THREADS);
         sm.abort_flag = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
-    for (int c = tid; c < wc / 16; c += blockDim.x)
+    // the single problem's broadcast parameter pairs (a packed launch reads each problem's from global memory)
+    for (int c = tid; c < (PACK ? 0 : plan.wc / 16); c += blockDim.x)
     {
         const ChunkParamsF p = prm[c];
         const float v[8] = {p.kappa, -p.kappa, p.c[1].x, p.c[1].y, -p.c[2].x, -p.c[2].y, p.c[3].x, p.c[3].y};
@@ -588,6 +673,8 @@ boundary_tc_kernel(const float *__restrict__ mid4, const float *__restrict__ nrm
     __syncthreads();
     tc_fence_after();
     const uint32_t tbase = sm.tmem_base;
+    const TcView V0{mid4, nrm4, tgeo, img, Ctri, &sm.prm[0][0], plan.n, plan.m, plan.wc, plan.ntiles, plan.self,
+                    plan.off, plan.ki_s};
 
     if (tid < TC_GEN_THREADS)
     {
@@ -646,28 +733,30 @@ boundary_tc_kernel(const float *__restrict__ mid4, const float *__restrict__ nrm
             mbar_arrive(&sm.seg_empty);
             return true;
         };
-        PieceIter it(plan, k_cta);
+        Pieces<PACK> it(plan, k_cta, V0);
+        TcView V;
         int cg, blk, tb, te, slot, rot;
-        while (ok && it.next(plan, cg, blk, tb, te, slot, rot))
+        while (ok && it.next(plan, V, cg, blk, tb, te, slot, rot))
         {
+            const int n = V.n, mt = V.m, wc = V.wc, ntiles = V.ntiles;
             const int i = blk * TC_M + row;
-            const int iself = plan.self ? plan.off + i : -1;   // the source excluded for this target (none: -1)
+            const int iself = V.self ? V.off + i : -1;   // the source excluded for this target (none: -1)
             // -x_i and nu_i as broadcast pairs
             float2 nx0 = make_float2(0.f, 0.f), nx1 = nx0, nx2 = nx0, tn0 = nx0, tn1 = nx0, tn2 = nx0;
             if (i < mt)
             {
-                const float4 m = reinterpret_cast<const float4 *>(mid4)[i];
+                const float4 m = reinterpret_cast<const float4 *>(V.mid4)[i];
                 nx0 = make_float2(-m.x, -m.x); nx1 = make_float2(-m.y, -m.y); nx2 = make_float2(-m.z, -m.z);
                 if (ADL)
                 {
-                    const float4 v = reinterpret_cast<const float4 *>(nrm4)[i];
+                    const float4 v = reinterpret_cast<const float4 *>(V.nrm4)[i];
                     tn0 = make_float2(v.x, v.x); tn1 = make_float2(v.y, v.y); tn2 = make_float2(v.z, v.z);
                 }
             }
-            const float2 *Pg = sm.prm[cg * CH];
+            const float2 *Pg = V.prm + cg * CH * 8;
             // the source tiles that hold the target block's own triangles (masked)
-            const int self_lo = plan.self ? (plan.off + blk * TC_M) / TC_SRC : ntiles;
-            const int self_hi = plan.self ? (plan.off + blk * TC_M + TC_M - 1) / TC_SRC : -1;
+            const int self_lo = V.self ? (V.off + blk * TC_M) / TC_SRC : ntiles;
+            const int self_hi = V.self ? (V.off + blk * TC_M + TC_M - 1) / TC_SRC : -1;
             bool first_drain = true;
             // A finished segment is drained right after the next segment's first
             // chunk is stored, so the tensor core has work waiting when it resumes.
@@ -684,7 +773,7 @@ boundary_tc_kernel(const float *__restrict__ mid4, const float *__restrict__ nrm
                 // per source pair: 1/r, r, (z.mu_j)/r^3, (z.nu_i)/r^3; shared by every chunk
                 float2 rinv[TC_PPT], r[TC_PPT], dmu[TC_PPT], dnu[TC_PPT];
                 {
-                    const TcTileGeo &G = sm.raw[rs].geo;
+                    const TcTileGeo &G = sm.geo[rs];
                     const int s0 = g * TC_SPT;
                     // tiles that hold the target itself or padding past the end need masks
                     const bool special = (ts == ntiles - 1) || (ts >= self_lo && ts <= self_hi);
@@ -721,7 +810,7 @@ boundary_tc_kernel(const float *__restrict__ mid4, const float *__restrict__ nrm
                 float2 kux[TC_PPT], knux[TC_PPT], kv[TC_PPT];
                 if (KI)
                 {
-                    const float2 s2 = make_float2(plan.ki_s, plan.ki_s);
+                    const float2 s2 = make_float2(V.ki_s, V.ki_s);
                     #pragma unroll
                     for (int p = 0; p < TC_PPT; ++p)
                     {
@@ -784,7 +873,7 @@ boundary_tc_kernel(const float *__restrict__ mid4, const float *__restrict__ nrm
             float2 *dst = nullptr;
             if (tb == 0 && te == ntiles)
             {
-                if (i < mt) dst = &Ctri[(int64_t)i * wc + cg * cw];
+                if (i < mt) dst = &V.Ctri[(int64_t)i * wc + cg * cw];
             }
             else
                 dst = &ws[((int64_t)(k_cta * 2 + slot) * TC_M + row) * (TC_CHMAX * 16)];
@@ -802,109 +891,37 @@ boundary_tc_kernel(const float *__restrict__ mid4, const float *__restrict__ nrm
         }
         if (!ok) publish();
     }
-    else if (tid < TC_GEN_THREADS + TC_EXP_THREADS)
+    else if (warp == TC_GEN_THREADS / 32)
     {
-        // ------------------------------ expanders ------------------------------
-        // Thread (image row qq, source pairs sp = spb, spb + 4) of every chunk:
-        // 8 lanes of a quarter-warp write 8 different rows' swizzled 16-byte
-        // groups, which cover all 32 banks.  Rows of the raw tile past the last
-        // source were zero-filled by the producer.
-        const int lt = tid - TC_GEN_THREADS;
-        const int qq = lt & 15, spb = lt >> 4;
-        static_assert(TC_EXP_THREADS == 64 && TC_SRC == 16, "expander layout: 16 rows x 4 pair slots");
-        uint32_t o_re[2], o_im[2];
-        #pragma unroll
-        for (int h = 0; h < 2; ++h)
-        {
-            o_re[h] = img_off16(qq, spb + 4 * h);
-            o_im[h] = img_off16(qq + 16, spb + 4 * h);
-        }
-        PieceIter it(plan, k_cta);
+        // ------------------------------ bulk-copy producer ------------------------------
+        // Per tile: its geometry into a geometry stage (for the generators) and
+        // its expanded B images of this piece's chunk group into a B stage (for
+        // the MMAs), each stage reused once its consumers released it.
+        const uint32_t img_bytes = (uint32_t)(CH * TC_GROUP_BYTES);
+        Pieces<PACK> it(plan, k_cta, V0);
+        TcView V;
         int cg, blk, tb, te, slot, rot, T = 0;
         bool ok = true;
-        while (ok && it.next(plan, cg, blk, tb, te, slot, rot))
+        while (ok && it.next(plan, V, cg, blk, tb, te, slot, rot))
         {
+            const int ntiles = V.ntiles, groups = V.wc / 16;
             for (int t = tb; t < te; ++t, ++T)
             {
                 const int rs = T % TC_RSTAGES, b = T % TC_BSTAGES;
-                if (!wait_bar(&sm.r_full[rs], (uint32_t)(T / TC_RSTAGES) & 1u, abort_flag, err, 4)) { ok = false; break; }
-                if (!wait_bar(&sm.b_empty[b], ((uint32_t)(T / TC_BSTAGES) & 1u) ^ 1u, abort_flag, err, 5))
-                {
-                    ok = false;
-                    break;
-                }
-                const TcRaw &R = sm.raw[rs];
-                constexpr uint32_t sgn = 0x80000000u;
-                #pragma unroll
-                for (int h = 0; h < 2; ++h)
-                {
-                    const int s0 = 2 * (spb + 4 * h);
-                    #pragma unroll
-                    for (int c = 0; c < CH; ++c)
-                    {
-                        const float2 v0 = R.b[s0][c * 16 + qq], v1 = R.b[s0 + 1][c * 16 + qq];
-                        uint32_t hr0, lr0, hi0, li0, hr1, lr1, hi1, li1;
-                        split_tf32(v0.x, hr0, lr0);
-                        split_tf32(v0.y, hi0, li0);
-                        split_tf32(v1.x, hr1, lr1);
-                        split_tf32(v1.y, hi1, li1);
-                        uint8_t *hi_img = sm.img[b][c][0];
-                        uint8_t *lo_img = sm.img[b][c][1];
-                        // row qq (real part of C): (Re b0, Re b1, -Im b0, -Im b1); row qq + 16: (Im b0, Im b1, Re b0, Re b1)
-                        *reinterpret_cast<uint4 *>(hi_img + o_re[h]) = make_uint4(hr0, hr1, hi0 ^ sgn, hi1 ^ sgn);
-                        *reinterpret_cast<uint4 *>(lo_img + o_re[h]) = make_uint4(lr0, lr1, li0 ^ sgn, li1 ^ sgn);
-                        *reinterpret_cast<uint4 *>(hi_img + o_im[h]) = make_uint4(hi0, hi1, hr0, hr1);
-                        *reinterpret_cast<uint4 *>(lo_img + o_im[h]) = make_uint4(li0, li1, lr0, lr1);
-                    }
-                }
-                asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-                mbar_arrive(&sm.r_empty[rs]);
-                mbar_arrive(&sm.b_full[b]);
-            }
-        }
-    }
-    else if (warp == (TC_GEN_THREADS + TC_EXP_THREADS) / 32)
-    {
-        // ------------------------------ bulk-copy producer ------------------------------
-        const int cw = CH * 16;
-        const uint32_t row_bytes = (uint32_t)(cw * sizeof(float2));
-        PieceIter it(plan, k_cta);
-        int cg, blk, tb, te, slot, rot, T = 0;
-        bool ok = true;
-        while (ok && it.next(plan, cg, blk, tb, te, slot, rot))
-        {
-            for (int t = tb; t < te; ++t, ++T)
-            {
-                const int rs = T % TC_RSTAGES;
-                if (!warp_wait(&sm.r_empty[rs], ((uint32_t)(T / TC_RSTAGES) & 1u) ^ 1u, abort_flag, err, 6))
+                if (!warp_wait(&sm.r_empty[rs], ((uint32_t)(T / TC_RSTAGES) & 1u) ^ 1u, abort_flag, err, 6) ||
+                    !warp_wait(&sm.b_empty[b], ((uint32_t)(T / TC_BSTAGES) & 1u) ^ 1u, abort_flag, err, 5))
                 {
                     ok = false;
                     break;
                 }
                 const int ts = t + rot < ntiles ? t + rot : t + rot - ntiles;   // source tile (rot < ntiles)
-                const int j0 = ts * TC_SRC;
-                const int rows = min(TC_SRC, n - j0);
-                if (rows < TC_SRC)
-                {
-                    // the last tile: zero rows past the end, which the expanders read
-                    // (their kernel entries are zero, so the values only need to be finite)
-                    float4 *z = reinterpret_cast<float4 *>(sm.raw[rs].b[rows]);
-                    const int nz = (TC_SRC - rows) * (TC_CHMAX * 16) / 2;
-                    for (int e = lane; e < nz; e += 32) z[e] = make_float4(0.f, 0.f, 0.f, 0.f);
-                    __syncwarp();
-                }
                 if (elect_one())
                 {
-                    mbar_expect_tx(&sm.r_full[rs], (uint32_t)rows * row_bytes + (uint32_t)sizeof(TcTileGeo));
-                    bulk_g2s(&sm.raw[rs].geo, tgeo + ts, (uint32_t)sizeof(TcTileGeo), &sm.r_full[rs]);
-                    // one contiguous block when the tile's rows are whole B_tri rows of
-                    // exactly the raw row width; otherwise one copy per row
-                    if (CH == TC_CHMAX && cw == wc)
-                        bulk_g2s(sm.raw[rs].b, Btri + (int64_t)j0 * wc, (uint32_t)rows * row_bytes, &sm.r_full[rs]);
-                    else
-                        for (int sl = 0; sl < rows; ++sl)
-                            bulk_g2s(sm.raw[rs].b[sl], Btri + (int64_t)(j0 + sl) * wc + cg * cw, row_bytes,
-                                     &sm.r_full[rs]);
+                    mbar_expect_tx(&sm.r_full[rs], (uint32_t)sizeof(TcTileGeo));
+                    bulk_g2s(&sm.geo[rs], V.tgeo + ts, (uint32_t)sizeof(TcTileGeo), &sm.r_full[rs]);
+                    mbar_expect_tx(&sm.b_full[b], img_bytes);
+                    bulk_g2s(sm.img[b], V.img + ((size_t)ts * groups + (size_t)cg * CH) * TC_GROUP_BYTES, img_bytes,
+                             &sm.b_full[b]);
                 }
                 __syncwarp();
             }
@@ -916,9 +933,14 @@ boundary_tc_kernel(const float *__restrict__ mid4, const float *__restrict__ nrm
         // The whole warp runs the loop and waits; one elected lane issues.
         bool ok = true;
         int T = 0, SG = 0;
-        PieceIter it(plan, k_cta);
+        // descriptors and TMEM addresses from bases fixed for the whole kernel: a
+        // (stage, chunk) image is a constant byte offset from img[0][0][0], and
+        // the descriptor's start-address field is that address >> 4
+        const uint64_t desc0 = sw128_desc(&sm.img[0][0][0][0]);
+        Pieces<PACK> it(plan, k_cta, V0);
+        TcView V;
         int cg, blk, tb, te, slot, rot;
-        while (ok && it.next(plan, cg, blk, tb, te, slot, rot))
+        while (ok && it.next(plan, V, cg, blk, tb, te, slot, rot))
         {
             for (int t = tb; t < te; ++t, ++T)
             {
@@ -944,7 +966,7 @@ boundary_tc_kernel(const float *__restrict__ mid4, const float *__restrict__ nrm
                     const uint32_t a_lo = a_hi + 32u;
                     // the hi image's 32 rows are followed by the lo image's 32 rows
                     // (same 1024-byte group stride): one N = 64 operand [Bhi | Blo]
-                    const uint64_t b_hilo = sw128_desc(sm.img[b][c][0]);
+                    const uint64_t b_hilo = desc0 + (uint64_t)(((b * TC_CHMAX + c) * TC_GROUP_BYTES) >> 4);
                     if (elect_one())
                     {
                         #pragma unroll
@@ -988,6 +1010,42 @@ boundary_tc_kernel(const float *__restrict__ mid4, const float *__restrict__ nrm
     }
 }
 
+// The MMA's B operand for every 16-source tile t and 16-column group G, as the
+// bytes a B stage holds (TC_GROUP_BYTES at (t * groups + G) * TC_GROUP_BYTES):
+// the hi image, then the lo image, each 32 K-major SWIZZLE_128B rows of 128
+// bytes.  Row q < 16 (real part of column q's result) holds per source pair
+// sp = (s0, s1) = (2 sp, 2 sp + 1) the 16-byte group (Re b_s0, Re b_s1,
+// -Im b_s0, -Im b_s1); row 16 + q holds (Im b_s0, Im b_s1, Re b_s0, Re b_s1);
+// group sp of row r sits at ((sp ^ (r & 7)) * 16) (img_off16).  hi = tf32(x)
+// rounded to nearest, lo = x - hi (split_tf32).  Sources past n are zero.
+// Thread (t, G, q, sp), sp fastest: 8 threads fill one row's 128 bytes.
+__global__ void tc_expand_kernel(const float2 *__restrict__ Btri, int n, int wc, int64_t total,
+                                 uint8_t *__restrict__ img)
+{
+    const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= total) return;
+    const int groups = wc / 16;
+    const int sp = (int)(e & 7), q = (int)((e >> 3) & 15);
+    const int64_t tg = e >> 7;                       // t * groups + G
+    const int64_t t = tg / groups;
+    const int G = (int)(tg - t * groups);
+    const int64_t j0 = t * TC_SRC + 2 * sp;
+    const int col = G * 16 + q;
+    const float2 v0 = j0 < n ? Btri[j0 * wc + col] : make_float2(0.f, 0.f);
+    const float2 v1 = j0 + 1 < n ? Btri[(j0 + 1) * wc + col] : make_float2(0.f, 0.f);
+    uint32_t hr0, lr0, hi0, li0, hr1, lr1, hi1, li1;
+    split_tf32(v0.x, hr0, lr0);
+    split_tf32(v0.y, hi0, li0);
+    split_tf32(v1.x, hr1, lr1);
+    split_tf32(v1.y, hi1, li1);
+    constexpr uint32_t sgn = 0x80000000u;
+    uint8_t *hi_img = img + tg * TC_GROUP_BYTES, *lo_img = hi_img + TC_IMG;
+    *reinterpret_cast<uint4 *>(hi_img + img_off16(q, sp)) = make_uint4(hr0, hr1, hi0 ^ sgn, hi1 ^ sgn);
+    *reinterpret_cast<uint4 *>(lo_img + img_off16(q, sp)) = make_uint4(lr0, lr1, li0 ^ sgn, li1 ^ sgn);
+    *reinterpret_cast<uint4 *>(hi_img + img_off16(q + 16, sp)) = make_uint4(hi0, hi1, hr0, hr1);
+    *reinterpret_cast<uint4 *>(lo_img + img_off16(q + 16, sp)) = make_uint4(li0, li1, lr0, lr1);
+}
+
 // Midpoints and normals of each 16-source tile as structure of arrays (zeros
 // past the last triangle).
 __global__ void tc_tile_geometry_kernel(const float *__restrict__ mid4, const float *__restrict__ nrm4,
@@ -1007,6 +1065,24 @@ __global__ void tc_tile_geometry_kernel(const float *__restrict__ mid4, const fl
     G.mx[s] = v.x; G.my[s] = v.y; G.mz[s] = v.z;
 }
 
+} // namespace
+
+const uint8_t *launch_tc_expand(const float2 *Btri, int64_t n, int wc, DevBuf<uint8_t> &img, cudaStream_t st)
+{
+    const int64_t ntiles = ceil_div(n, TC_SRC), groups = wc / 16;
+    const size_t bytes = (size_t)(ntiles * groups) * TC_GROUP_BYTES;
+    uint8_t *out = img.reserve(bytes);
+    const int64_t total = ntiles * groups * 128;
+    if (total > 0)
+    {
+        tc_expand_kernel<<<ceil_div(total, 256), 256, 0, st>>>(Btri, (int)n, wc, total, out);
+        BAEMM_LAUNCH_CHECK();
+    }
+    return out;
+}
+
+namespace
+{
 // Adds the workspace slots of every target block that was split between CTAs,
 // in CTA order, and writes the block's rows of C_tri.
 __global__ void tc_fixup_kernel(const float2 *__restrict__ ws, float2 *__restrict__ Ctri, const TcPlan plan, int cw)
@@ -1036,8 +1112,8 @@ __global__ void tc_fixup_kernel(const float2 *__restrict__ ws, float2 *__restric
     }
 }
 
-template <int GW, int CH, bool SL, bool DL, bool ADL, bool RI, bool KI>
-void tc_launch(cudaStream_t st, const float *mid, const float *nrm, const TcTileGeo *tg, const float2 *B, float2 *C,
+template <int GW, int CH, bool SL, bool DL, bool ADL, bool RI, bool KI, bool PACK = false>
+void tc_launch(cudaStream_t st, const float *mid, const float *nrm, const TcTileGeo *tg, const uint8_t *B, float2 *C,
                float2 *ws, const ChunkParamsF *p, const TcPlan &plan, int *err)
 {
     // More than half of the SM's shared memory, so one CTA per SM: the CTA
@@ -1053,17 +1129,17 @@ void tc_launch(cudaStream_t st, const float *mid, const float *nrm, const TcTile
         std::lock_guard<std::mutex> lock(mu);
         if (dev < 0 || dev >= 64 || !done[dev])
         {
-            BAEMM_CUDA(cudaFuncSetAttribute(boundary_tc_kernel<GW, CH, SL, DL, ADL, RI, KI>,
+            BAEMM_CUDA(cudaFuncSetAttribute(boundary_tc_kernel<GW, CH, SL, DL, ADL, RI, KI, PACK>,
                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
             if (dev >= 0 && dev < 64) done[dev] = true;
         }
     }
-    boundary_tc_kernel<GW, CH, SL, DL, ADL, RI, KI><<<plan.ctas, TcShape<GW>::THREADS, bytes, st>>>(
+    boundary_tc_kernel<GW, CH, SL, DL, ADL, RI, KI, PACK><<<plan.ctas, TcShape<GW>::THREADS, bytes, st>>>(
         mid, nrm, tg, B, C, ws, p, plan, err);
 }
 
 template <int GW, int CH, bool RI>
-void tc_flags(int code, cudaStream_t st, const float *mid, const float *nrm, const TcTileGeo *tg, const float2 *B,
+void tc_flags(int code, cudaStream_t st, const float *mid, const float *nrm, const TcTileGeo *tg, const uint8_t *B,
               float2 *C, float2 *ws, const ChunkParamsF *p, const TcPlan &plan, int *err)
 {
     switch (code)
@@ -1082,7 +1158,7 @@ void tc_flags(int code, cudaStream_t st, const float *mid, const float *nrm, con
 // The KI form for the operator combinations of the solves: the mixed BIE
 // (SL + DL), the DtN operator (SL + ADL) and all three layers.
 template <int GW, int CH>
-bool tc_flags_ki(int code, cudaStream_t st, const float *mid, const float *nrm, const TcTileGeo *tg, const float2 *B,
+bool tc_flags_ki(int code, cudaStream_t st, const float *mid, const float *nrm, const TcTileGeo *tg, const uint8_t *B,
                  float2 *C, float2 *ws, const ChunkParamsF *p, const TcPlan &plan, int *err)
 {
     switch (code)
@@ -1159,7 +1235,7 @@ namespace
 {
 template <int GW>
 void tc_dispatch(int CH, bool ri, bool ki, int code, cudaStream_t st, const float *pts4, const float *nrm,
-                 const TcTileGeo *tg, const float2 *Btri, float2 *Ctri, float2 *ws, const ChunkParamsF *p,
+                 const TcTileGeo *tg, const uint8_t *Btri, float2 *Ctri, float2 *ws, const ChunkParamsF *p,
                  const TcPlan &plan, int *err)
 {
     bool done = false;
@@ -1189,7 +1265,8 @@ void tc_dispatch(int CH, bool ri, bool ki, int code, cudaStream_t st, const floa
 // off .. off + m_targets - 1 and the pair i == j is excluded.
 void tc_run(const MeshDev &m, const OpFlags &f, const void *chunk_params, const TcCoeffForm &form, int wc, int wcs,
             const float *tgeo, const float *pts4, int64_t m_targets, int self, int64_t off, const float2 *Btri,
-            float2 *Ctri, float2 *ws, size_t ws_elems, int *err, cudaStream_t st, const TcTuning &tune)
+            float2 *Ctri, float2 *ws, size_t ws_elems, DevBuf<uint8_t> &img, int *err, cudaStream_t st,
+            const TcTuning &tune)
 {
     BAEMM_REQUIRE(tc_supported(wc, wcs), BAEMM_ERR_SIZE,
                   "tensor-core apply needs wave_chunk_size a multiple of 16 and wave_count <= 512");
@@ -1223,8 +1300,9 @@ void tc_run(const MeshDev &m, const OpFlags &f, const void *chunk_params, const 
     BAEMM_REQUIRE(tg, BAEMM_ERR_ARG, "tensor-core tile geometry missing");
     // the real / imaginary coefficient structure of the BIE solves (see boundary_tc_kernel)
     const bool ri = !f.re_sl && !f.im_dl && !f.im_adl && (f.dl() || f.adl());
-    if (tune.gen_warps == 8) tc_dispatch<8>(CH, ri, form.ki, code, st, pts4, nrm, tg, Btri, Ctri, ws, p, plan, err);
-    else tc_dispatch<16>(CH, ri, form.ki, code, st, pts4, nrm, tg, Btri, Ctri, ws, p, plan, err);
+    const uint8_t *im = launch_tc_expand(Btri, m.nt, wc, img, st);
+    if (tune.gen_warps == 8) tc_dispatch<8>(CH, ri, form.ki, code, st, pts4, nrm, tg, im, Ctri, ws, p, plan, err);
+    else tc_dispatch<16>(CH, ri, form.ki, code, st, pts4, nrm, tg, im, Ctri, ws, p, plan, err);
     BAEMM_LAUNCH_CHECK();
     if (plan.tail_blocks > 0)
     {
@@ -1234,22 +1312,194 @@ void tc_run(const MeshDev &m, const OpFlags &f, const void *chunk_params, const 
 }
 } // namespace
 
+namespace
+{
+// After a packed launch: a time-out the launch reported goes to every packed
+// problem's own error word (read by its context like a single launch's), and
+// the packer's word is cleared for the next launch.
+__global__ void tc_pack_err_kernel(int *err, const TcProblem *probs, int count)
+{
+    const int e = *(volatile int *)err;
+    if (e == 0) return;
+    for (int q = threadIdx.x; q < count; q += blockDim.x) atomicExch(probs[q].err, e);
+    __syncthreads();
+    if (threadIdx.x == 0) *err = 0;
+}
+
+// The KI-form operators the packed launch serves (the solves' mixed BIE and
+// DtN operators and all three layers); false for any other structure.
+template <int GW, int CH>
+bool tc_pack_flags(int code, cudaStream_t st, const TcPlan &plan, int *err)
+{
+    switch (code)
+    {
+        case 3: tc_launch<GW, CH, true, true, false, true, true, true>(st, 0, 0, 0, 0, 0, 0, 0, plan, err); return true;
+        case 5: tc_launch<GW, CH, true, false, true, true, true, true>(st, 0, 0, 0, 0, 0, 0, 0, plan, err); return true;
+        case 7: tc_launch<GW, CH, true, true, true, true, true, true>(st, 0, 0, 0, 0, 0, 0, 0, plan, err); return true;
+        default: return false;
+    }
+}
+} // namespace
+
+TcPackScratch::~TcPackScratch()
+{
+    if (uploaded) cudaEventDestroy(uploaded);
+    if (host) cudaFreeHost(host);
+}
+
+void TcPackScratch::reserve(size_t bytes)
+{
+    dev.reserve(bytes);
+    if (bytes > host_cap)
+    {
+        if (uploaded) BAEMM_CUDA(cudaEventSynchronize(uploaded));
+        if (host) cudaFreeHost(host);
+        host = nullptr;
+        host_cap = 0;
+        BAEMM_CUDA(cudaMallocHost(&host, bytes));
+        host_cap = bytes;
+    }
+    if (!uploaded) BAEMM_CUDA(cudaEventCreateWithFlags(&uploaded, cudaEventDisableTiming));
+}
+
+uint8_t *TcPackScratch::stage(const void *src, size_t bytes, cudaStream_t st)
+{
+    BAEMM_CUDA(cudaEventSynchronize(uploaded));   // the previous upload has read the pinned copy
+    std::memcpy(host, src, bytes);
+    BAEMM_CUDA(cudaMemcpyAsync(dev.p, host, bytes, cudaMemcpyHostToDevice, st));
+    BAEMM_CUDA(cudaEventRecord(uploaded, st));
+    return dev.p;
+}
+
+void tc_broadcast_params(const ChunkParamsF *h, int groups, std::vector<float2> &out)
+{
+    out.resize((size_t)groups * 8);
+    for (int g = 0; g < groups; ++g)
+    {
+        const ChunkParamsF &p = h[g];
+        const float v[8] = {p.kappa, -p.kappa, p.c[1].x, p.c[1].y, -p.c[2].x, -p.c[2].y, p.c[3].x, p.c[3].y};
+        for (int k = 0; k < 8; ++k) out[(size_t)g * 8 + k] = make_float2(v[k], v[k]);
+    }
+}
+
+int tc_sm_count() { return device_sm_count(); }
+
+bool tc_packable(const OpFlags &f, const TcCoeffForm &form, int wc, int wcs)
+{
+    const bool ri = !f.re_sl && !f.im_dl && !f.im_adl && (f.dl() || f.adl());
+    const int code = (f.sl() ? 1 : 0) | (f.dl() ? 2 : 0) | (f.adl() ? 4 : 0);
+    return tc_supported(wc, wcs) && ri && form.ki && (code == 3 || code == 5 || code == 7);
+}
+
+int tc_pack_class(const OpFlags &f, int wc, const TcTuning &tune)
+{
+    const int code = (f.sl() ? 1 : 0) | (f.dl() ? 2 : 0) | (f.adl() ? 4 : 0);
+    // operator structure, chunk groups, warps and segment length: a packed launch runs one of each
+    return ((code * 8 + tc_chunks_per_unit(wc, tune.chunks)) * 2 + (tune.gen_warps == 8 ? 1 : 0)) * 4096 +
+           std::min(std::max(tune.seg_tiles, 1), 4095);
+}
+
+void launch_boundary_tc_packed(const TcPackItem *items, int count, const OpFlags &f, const TcTuning &tune,
+                               TcPackScratch &scr, int *err, cudaStream_t st)
+{
+    BAEMM_REQUIRE(count >= 1, BAEMM_ERR_ARG, "packed launch without problems");
+    const int code = (f.sl() ? 1 : 0) | (f.dl() ? 2 : 0) | (f.adl() ? 4 : 0);
+    const int CH = tc_chunks_per_unit(items[0].wc, tune.chunks);
+    // the problem table and the blocks (problem, block), costed by their source tiles
+    std::vector<TcProblem> probs((size_t)count);
+    std::vector<std::pair<int, int2>> blocks;   // (tiles, (problem, block))
+    for (int q = 0; q < count; ++q)
+    {
+        const TcPackItem &it = items[q];
+        BAEMM_REQUIRE(tc_chunks_per_unit(it.wc, tune.chunks) == CH, BAEMM_ERR_ARG,
+                      "packed problems need the same chunk groups per unit");
+        TcProblem &P = probs[(size_t)q];
+        P.mid4 = it.mid4;
+        P.nrm4 = it.nrm4;
+        P.tgeo = reinterpret_cast<const TcTileGeo *>(it.tgeo);
+        P.img = it.img;
+        P.Ctri = it.Ctri;
+        P.prm = it.prm_bcast;
+        P.err = it.err;
+        P.n = (int)it.nt;
+        P.m = (int)it.nt;
+        P.wc = it.wc;
+        P.nblk = ceil_div(it.nt, TC_M);
+        P.ntiles = ceil_div(it.nt, TC_SRC);
+        P.self = 1;
+        P.off = 0;
+        P.ki_s = it.ki_s;
+        const int nb = (it.wc / (16 * CH)) * P.nblk;
+        for (int b = 0; b < nb; ++b) blocks.push_back({P.ntiles, make_int2(q, b)});
+    }
+    // longest first onto the least loaded CTA (deterministic: ties by index)
+    std::stable_sort(blocks.begin(), blocks.end(),
+                     [](const std::pair<int, int2> &a, const std::pair<int, int2> &b) { return a.first > b.first; });
+    const int ctas = (int)std::min<size_t>((size_t)(tune.ctas > 0 ? tune.ctas : device_sm_count()), blocks.size());
+    std::vector<int64_t> load((size_t)ctas, 0);
+    std::vector<std::vector<int2>> per((size_t)ctas);
+    for (const auto &b : blocks)
+    {
+        const size_t k = (size_t)(std::min_element(load.begin(), load.end()) - load.begin());
+        load[k] += b.first;
+        per[k].push_back(b.second);
+    }
+    // one staging block: problems, then cta_begin, then the pieces
+    const size_t nprob_b = sizeof(TcProblem) * (size_t)count;
+    const size_t nbeg_b = sizeof(int) * (size_t)(ctas + 1);
+    const size_t npiece_b = sizeof(int2) * blocks.size();
+    const size_t off_beg = (nprob_b + 15) / 16 * 16, off_piece = (off_beg + nbeg_b + 15) / 16 * 16;
+    const size_t total = off_piece + npiece_b;
+    scr.reserve(total);
+    std::vector<uint8_t> host(total);
+    std::memcpy(host.data(), probs.data(), nprob_b);
+    int *beg = reinterpret_cast<int *>(host.data() + off_beg);
+    int2 *pcs = reinterpret_cast<int2 *>(host.data() + off_piece);
+    int e = 0;
+    for (int k = 0; k < ctas; ++k)
+    {
+        beg[k] = e;
+        for (const int2 &q : per[(size_t)k]) pcs[e++] = q;
+    }
+    beg[ctas] = e;
+    uint8_t *dev = scr.stage(host.data(), total, st);
+    TcPlan plan{};
+    plan.ctas = ctas;
+    plan.seg_tiles = std::max(1, tune.seg_tiles);
+    plan.probs = reinterpret_cast<const TcProblem *>(dev);
+    plan.cta_begin = reinterpret_cast<const int *>(dev + off_beg);
+    plan.pieces = reinterpret_cast<const int2 *>(dev + off_piece);
+    bool ok;
+    if (tune.gen_warps == 8)
+        ok = (CH == 4) ? tc_pack_flags<8, 4>(code, st, plan, err)
+             : (CH == 2) ? tc_pack_flags<8, 2>(code, st, plan, err) : tc_pack_flags<8, 1>(code, st, plan, err);
+    else
+        ok = (CH == 4) ? tc_pack_flags<16, 4>(code, st, plan, err)
+             : (CH == 2) ? tc_pack_flags<16, 2>(code, st, plan, err) : tc_pack_flags<16, 1>(code, st, plan, err);
+    BAEMM_REQUIRE(ok, BAEMM_ERR_ARG, "packed launch: operator structure not packable");
+    BAEMM_LAUNCH_CHECK();
+    tc_pack_err_kernel<<<1, 32, 0, st>>>(err, plan.probs, count);
+    BAEMM_LAUNCH_CHECK();
+}
+
 void launch_boundary_tc(const MeshDev &m, const OpFlags &f, const void *chunk_params, const TcCoeffForm &form, int wc,
                         int wcs, const float *tgeo, const float2 *Btri, float2 *Ctri, float2 *ws, size_t ws_elems,
-                        int *err, cudaStream_t st, const TcTuning &tune, int64_t row_begin, int64_t row_end)
+                        DevBuf<uint8_t> &img, int *err, cudaStream_t st, const TcTuning &tune, int64_t row_begin,
+                        int64_t row_end)
 {
     const int64_t r0 = std::max<int64_t>(0, row_begin), r1 = row_end < 0 ? m.nt : std::min<int64_t>(row_end, m.nt);
     if (r1 <= r0) return;
     tc_run(m, f, chunk_params, form, wc, wcs, tgeo, m.mid_f + 4 * r0, r1 - r0, 1, r0, Btri, Ctri + r0 * wc, ws, ws_elems,
-           err, st, tune);
+           img, err, st, tune);
 }
 
 void launch_nearfield_tc(const MeshDev &m, const OpFlags &f, const void *chunk_params, const TcCoeffForm &form,
                          int wc, int wcs, const float *tgeo, const float *pts4, int64_t npts, const float2 *Btri,
-                         float2 *Cpts, float2 *ws, size_t ws_elems, int *err, cudaStream_t st, const TcTuning &tune)
+                         float2 *Cpts, float2 *ws, size_t ws_elems, DevBuf<uint8_t> &img, int *err, cudaStream_t st,
+                         const TcTuning &tune)
 {
     BAEMM_REQUIRE(!f.adl() && !f.mass(), BAEMM_ERR_ARG, "near field: single and double layer only");
-    tc_run(m, f, chunk_params, form, wc, wcs, tgeo, pts4, npts, 0, 0, Btri, Cpts, ws, ws_elems, err, st, tune);
+    tc_run(m, f, chunk_params, form, wc, wcs, tgeo, pts4, npts, 0, 0, Btri, Cpts, ws, ws_elems, img, err, st, tune);
 }
 
 } // namespace baemm

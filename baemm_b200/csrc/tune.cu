@@ -16,10 +16,14 @@
 // Choices are cached for the process per (device, mesh size, wave shape,
 // arithmetic form, operator structure): a second context with the same key,
 // or the same context after a re-mesh of equal size, takes the cached choice
-// without timing anything.
+// without timing anything.  One context at a time times a key; a concurrent
+// caller with the same key waits and takes that choice, so every context of
+// the process runs a key with the same settings.
 #include <algorithm>
+#include <condition_variable>
 #include <map>
 #include <mutex>
+#include <set>
 #include <tuple>
 #include <vector>
 
@@ -41,7 +45,9 @@ struct TuneChoice
 };
 
 std::mutex g_tune_mutex;
+std::condition_variable g_tune_cv;
 std::map<TuneKey, TuneChoice> g_tune_cache;
+std::set<TuneKey> g_tuning;   // keys being timed now: a second caller waits for the first one's choice
 
 } // namespace
 
@@ -75,7 +81,8 @@ void Ctx::autotune(int mode, int repeats, baemm_tune_result *out)
         out->cached = cached;
     };
     {
-        std::lock_guard<std::mutex> lock(g_tune_mutex);
+        std::unique_lock<std::mutex> lock(g_tune_mutex);
+        g_tune_cv.wait(lock, [&] { return g_tuning.count(key) == 0; });
         auto it = g_tune_cache.find(key);
         if (it != g_tune_cache.end())
         {
@@ -85,7 +92,14 @@ void Ctx::autotune(int mode, int repeats, baemm_tune_result *out)
             report(it->second, -1.0, 1);
             return;
         }
+        g_tuning.insert(key);   // one context times a key; the others take its choice
     }
+    auto release = [&](const TuneChoice *ch) {
+        std::lock_guard<std::mutex> lock(g_tune_mutex);
+        if (ch) g_tune_cache[key] = *ch;
+        g_tuning.erase(key);
+        g_tune_cv.notify_all();
+    };
 
     const size_t elems = (size_t)mesh.nt * (size_t)wave_count;
     float2 *Bt = Btri_f.reserve(elems), *Ct = Ctri_f.reserve(elems);
@@ -172,12 +186,12 @@ void Ctx::autotune(int mode, int repeats, baemm_tune_result *out)
         tc_tune = saved_tc;
         cudaEventDestroy(e0);
         cudaEventDestroy(e1);
+        release(nullptr);
         throw;
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
-    std::lock_guard<std::mutex> lock(g_tune_mutex);
-    g_tune_cache[key] = choice;
+    release(&choice);
 }
 
 void autotune_forget()

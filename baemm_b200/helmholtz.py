@@ -100,6 +100,38 @@ def _check_out(a, dtype, name):
         raise TypeError(f"{name} must be a C-contiguous 2-D numpy array of dtype {np.dtype(dtype).name}")
 
 
+class Packer:
+    """Packing of concurrent solves' tensor-core applies into one launch
+    (baemm_packer_create; no reference counterpart).  Attach the contexts that
+    serve concurrent solves (each driven by its own thread) with
+    Helmholtz_CUDA.SetPacker; detach them before closing the packer."""
+
+    def __init__(self, device: int = 0, max_wait_us: int = 2000):
+        self._lib = _capi.lib()
+        self._h = self._lib.baemm_packer_create(int(device), int(max_wait_us))
+        if not self._h:
+            raise BaemmError(2, self._lib.baemm_last_error(None).decode())
+
+    def stats(self) -> dict:
+        """Packed launches so far and the problems they carried."""
+        a, b = C.c_int64(), C.c_int64()
+        st = self._lib.baemm_packer_stats(self._h, C.byref(a), C.byref(b))
+        if st != 0:
+            raise BaemmError(st, "packer stats")
+        return {"launches": int(a.value), "problems": int(b.value)}
+
+    def close(self):
+        if self._h:
+            self._lib.baemm_packer_destroy(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+
 class Helmholtz_CUDA:
     """Drop-in for Helmholtz_OpenCL(coords, nv, tris, nt, meas, nm, device, threads)
     (Helmholtz_OpenCL.hpp:175-249)."""
@@ -243,6 +275,10 @@ class Helmholtz_CUDA:
     def SetGraphs(self, on: bool = True):
         """Replay the solvers' inner operators as CUDA graphs (baemm_set_graphs)."""
         self._ck(self._lib.baemm_set_graphs(self._h, 1 if on else 0))
+
+    def SetPacker(self, packer):
+        """Submit the solves' dense stages to `packer` (a Packer; None detaches)."""
+        self._ck(self._lib.baemm_set_packer(self._h, packer._h if packer is not None else None))
 
     def GraphStats(self) -> tuple:
         """(captures, replays) since the context was created."""

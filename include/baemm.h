@@ -302,6 +302,32 @@ int baemm_apply_boundary_operators_rows_dev_c(baemm_ctx *ctx, const float alpha[
                                               const float beta[2], float *C_out, int64_t ldC, int64_t row_begin,
                                               int64_t row_end, int with_mass);
 
+/* Packing of concurrent solves' tensor-core applies into one launch (no
+ * reference counterpart; the reference solves one request per GMRES call,
+ * FarField.hpp:706-708).  Contexts attached to one packer (same device, each
+ * driven by its own thread, e.g. the slots of a server) submit the dense
+ * stage of every operator apply inside their solves (BoundaryPotential,
+ * DirichletToNeumann, FarField, the derivatives) to the packer instead of
+ * launching it.  A submission waits until every attached context that is
+ * inside a solve has submitted too, or until max_wait_us has passed, and then
+ * one persistent tensor-core launch covers all pending problems of the same
+ * operator structure, chunk grouping and warp count (whole target blocks per
+ * CTA, longest first), after which each context's stream continues.  Only
+ * problems whose own launch cannot fill the GPU (at most two 128-triangle
+ * target blocks per SM, counting chunk groups) are packed; larger ones launch
+ * alone.  Each
+ * problem's result is the same whatever it is packed with.  Applies outside
+ * the KI coefficient structure of the solve operators (and row shards) are
+ * launched alone as before; with a packer the solve's operator apply is not
+ * captured in a CUDA graph (the mass inverse still is).  Destroy a packer only
+ * after detaching every context from it.
+ * baemm_packer_create returns NULL on failure (message: baemm_last_error(NULL)). */
+typedef struct baemm_packer baemm_packer;
+baemm_packer *baemm_packer_create(int device, int max_wait_us);
+void baemm_packer_destroy(baemm_packer *packer);
+int baemm_set_packer(baemm_ctx *ctx, baemm_packer *packer);   /* NULL detaches */
+int baemm_packer_stats(const baemm_packer *packer, int64_t *launches, int64_t *problems);
+
 /* The dense stage alone, the device counterpart of the reference's private
  * BoundaryOperatorKernel() (BoundaryOperatorKernel.hpp:5-28, kernel
  * BoundaryOperatorKernel.cl:5-239; no public counterpart): on device

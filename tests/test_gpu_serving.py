@@ -95,3 +95,81 @@ def test_served_tensor_core_matches_plain():
         rb = b.run(reqs, realtime=False)
     for r in reqs:
         assert relerr(ra[r.rid].far_field, rb[r.rid].far_field) < 1e-5
+
+
+def test_packed_solves_are_the_same_alone_and_packed():
+    """Two contexts on one packer (two meshes), each solving a BoundaryPotential
+    in its own thread: the GMRES applies of the two solves share launches, and
+    each solution equals the same solve run alone on the packer bit for bit
+    (whole target blocks, the same sums); the packed apply meets the bar of the
+    FP64 oracle."""
+    import threading
+
+    from baemm_b200 import APPLY_TC, Packer
+    from oracle import oracle as O
+
+    meshes_ = [meshes.icosphere(2), meshes.icosphere(3)]
+    kap = np.array([3.0])
+    rng = np.random.default_rng(3)
+    waves = [crandn(rng, c.shape[0], 16) for c, _ in meshes_]
+    with Packer(0, max_wait_us=100000) as P:
+        Hs = [Helmholtz_CUDA(c, t, np.eye(3)) for c, t in meshes_]
+        try:
+            for H in Hs:
+                H.SetApplyMode(APPLY_TC)
+                H.SetPacker(P)
+
+            def solve(q):
+                phi = np.zeros_like(waves[q])
+                Hs[q].BoundaryPotential(kap, np.zeros((1, 4), complex), waves[q], phi, 16, 1e-10, 1e-10)
+                return phi
+
+            alone = [solve(0), solve(1)]        # one at a time: every launch carries one problem
+            before = P.stats()
+            assert before["problems"] == before["launches"]
+            outs = [None, None]
+            barrier = threading.Barrier(2)
+
+            def run(q):
+                barrier.wait()
+                outs[q] = solve(q)
+
+            th = [threading.Thread(target=run, args=(q,)) for q in range(2)]
+            for t in th:
+                t.start()
+            for t in th:
+                t.join()
+            after = P.stats()
+            for q in range(2):
+                assert np.array_equal(outs[q], alone[q])
+            assert after["problems"] - before["problems"] > after["launches"] - before["launches"]
+            # one packed apply against the FP64 oracle
+            coeff = np.array([[0.5, -3j, 1.0, 0.0]])
+            c, t = meshes_[1]
+            B = crandn(rng, c.shape[0], 16)
+            Cg, Co = np.zeros_like(B), np.zeros_like(B)
+            Hs[1].ApplyBoundaryOperators_PL(1.0, B, 0.0, Cg, kap, coeff, 16, 16)
+            O.Oracle(c, t, np.eye(3), precision=64).ApplyBoundaryOperators_PL(1.0, B, 0.0, Co, kap, coeff, 16, 16)
+            assert relerr(Cg, Co) < 1e-5
+        finally:
+            for H in Hs:
+                H.SetPacker(None)
+                H.close()
+
+
+def test_packed_server_same_alone_and_in_the_mix():
+    """The packing server: each request's far field alone equals the same
+    request in a concurrent mix (1e-10), and the mix's applies shared launches."""
+    meas = meshes.fibonacci_sphere(24)
+    reqs = _requests(8, seed=5)
+    with SolveServer(meas, slots=4, graphs=True, pack=True, pack_wait_us=5000) as srv:
+        mix = srv.run(reqs, realtime=False)
+        st = srv.pack_stats()
+        assert srv.scheduler.peak_running > 1
+    assert st["launches"] > 0 and st["problems"] > st["launches"]   # some launches carried several problems
+    for r in reqs[:3]:
+        with SolveServer(meas, slots=1, graphs=True, pack=True) as alone:
+            one = alone.run([SolveRequest(r.rid, r.coords, r.triangles, r.kappa, r.directions,
+                                          gmres_tol=r.gmres_tol)], realtime=False)
+        assert one[r.rid].converged and mix[r.rid].converged
+        assert relerr(mix[r.rid].far_field, one[r.rid].far_field) < 1e-10
