@@ -818,8 +818,10 @@ def serve_runs(n_requests, slots=6, seed=0, seq_sample=0, seq_tc=True, latency=T
                              time (the same arithmetic as the server: the server's own
                              gain over it is the batching);
       capacity               the serving loop (slots of resident contexts, memory-budget
-                             admission, tensor-core apply, CUDA-graph replay) with every
-                             request queued at once: solves/s is its throughput;
+                             admission, tensor-core apply packed across the slots' solves,
+                             CUDA-graph replay) with every request queued at once: solves/s
+                             is its throughput (capacity_without_packing: the same without
+                             the packer);
       latency                the serving loop with Poisson arrivals at 80 % of that
                              capacity: p50 / p99 of finish - arrival.
     The far fields of the served runs are compared with the sequential ones."""
@@ -857,15 +859,26 @@ def serve_runs(n_requests, slots=6, seed=0, seq_sample=0, seq_tc=True, latency=T
     if seq_tc:
         _, t_tc = sequential(APPLY_TC, True)
         res["sequential_tc"] = {"solves_per_s": n_seq / t_tc, "seconds": t_tc, "requests": n_seq}
-    with SolveServer(meas, slots=slots, apply_mode=APPLY_TC, graphs=True) as srv:
+    # the server without packing (each slot launches its own applies), for the packing's own gain
+    with SolveServer(meas, slots=slots, apply_mode=APPLY_TC, graphs=True, pack=False) as srv0:
+        srv0.run(warm, realtime=False)
+        t0 = time.perf_counter()
+        srv0.run(at_once(), realtime=False)
+        res["capacity_without_packing"] = {"solves_per_s": len(reqs) / (time.perf_counter() - t0)}
+    with SolveServer(meas, slots=slots, apply_mode=APPLY_TC, graphs=True, pack=True) as srv:
         srv.run(warm, realtime=False)
+        p0 = srv.pack_stats()
         t0 = time.perf_counter()
         cap = srv.run(at_once(), realtime=False)
         t_cap = time.perf_counter() - t0
+        p1 = srv.pack_stats()
         thr_served = len(reqs) / t_cap
+        launches, probs = p1["launches"] - p0["launches"], p1["problems"] - p0["problems"]
         res["capacity"] = {"solves_per_s": thr_served, "seconds": t_cap,
                            "peak_concurrent": srv.scheduler.peak_running,
-                           "converged": int(sum(r.converged for r in cap.values())), "requests": len(reqs)}
+                           "converged": int(sum(r.converged for r in cap.values())), "requests": len(reqs),
+                           "packed_launches": launches, "packed_problems": probs,
+                           "problems_per_packed_launch": probs / launches if launches else None}
         served = [cap]
         if latency:
             rate = 0.8 * thr_served
@@ -881,6 +894,7 @@ def serve_runs(n_requests, slots=6, seed=0, seq_sample=0, seq_tc=True, latency=T
                                             "solves_per_s": s_lat["solves_per_s"]}
             served.append(lat)
     res["speedup_vs_sequential_plain"] = thr_served / res["sequential_plain_fp32"]["solves_per_s"]
+    res["speedup_of_packing"] = thr_served / res["capacity_without_packing"]["solves_per_s"]
     if seq_tc:
         res["speedup_vs_sequential_tc"] = thr_served / res["sequential_tc"]["solves_per_s"]
     res["max_far_field_rel_diff_served_vs_sequential"] = max(
