@@ -357,6 +357,26 @@ def run_gpu_arm(args, rank, world, local_rank):
     Cd = torch.zeros_like(Bd)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
     H.LoadBoundaryOperators_PL(kap, coeff, WC, WCS)
+    # the library's autotuner picks the kernel shape of the timed form and of the plain FP32 form it is
+    # compared with (both tuned, so the comparison is against the best plain variant)
+    tuned = {}
+    if args.shape:
+        # a fixed tensor-core shape (profiling runs: the tuner's timing would be distorted under a profiler)
+        from baemm_b200 import _capi as _cp
+        gw, ch, seg = (int(x) for x in args.shape.split(","))
+        H.SetTuning(_cp.TUNE_TC_GEN_WARPS, gw)
+        H.SetTuning(_cp.TUNE_TC_CHUNKS, ch)
+        H.SetTuning(_cp.TUNE_TC_SEGMENT, seg)
+        tuned["fixed_shape"] = {"tc_gen_warps": gw, "tc_chunks": ch, "tc_segment": seg}
+    elif not args.no_tune and args.mode in ("tc", "fp32"):
+        from baemm_b200 import APPLY_FP32 as _F32, APPLY_TC as _TC
+        for name, m in (("fp32", _F32), ("tc", _TC)):
+            if name == "tc" and args.mode != "tc":
+                continue
+            r = H.Autotune(m, repeats=2)
+            tuned[name] = {k: r[k] for k in ("dense_variant", "tc_gen_warps", "tc_chunks", "tc_segment", "candidates",
+                                             "best_ms", "cached")}
+        H.SetApplyMode(mode)
     S = None
     if args.shard:
         # one apply split by target rows over the ranks, shards summed by an all-reduce
@@ -486,7 +506,7 @@ def run_gpu_arm(args, rank, world, local_rank):
                    "parallelism": (f"target rows x{world} + all-reduce" if S is not None else
                                    f"replicas x{world}" if world > 1 else "single GPU"),
                    "l2": "flushed (256 MiB write) before every timed step",
-                   "phase_ms_last": list(H.LastApplyTimes()) if False else None},
+                   "autotuned": tuned or None},
         "roofline": {"bound": model["limiter"][:-3], "kernel": kernel_name, "achieved": model["achieved"],
                      "peak": model["peak"], "unit": model["unit"], "frac": model["frac"],
                      "peak_source": ("nominal SM pipe rates at the sampled clock" if model["limiter"] != "tensor_tf32_ms"
@@ -1005,6 +1025,8 @@ def main(argv=None):
                     help="apply: the headline operator-apply line; solve: the scattering-solve configuration; "
                          "serve: the request stream through the serving loop")
     ap.add_argument("--requests", type=int, default=100, help="requests of --workload serve")
+    ap.add_argument("--no-tune", action="store_true", help="time the default kernel shapes (no autotuning)")
+    ap.add_argument("--shape", default="", help="fixed tensor-core shape 'gen_warps,chunks,segment' (no autotuning)")
     ap.add_argument("--no-extras", dest="extras", action="store_false",
                     help="default apply line without the solve and serving keys")
     ap.add_argument("--serve-sample", type=int, default=48, help="requests of the default line's serving sample")
