@@ -25,23 +25,23 @@
 // tail piece of a CTA) writes its partial sums to a workspace slot, and
 // tc_fixup_kernel adds the slots of each split block in CTA order
 // (deterministic).
-// Warp roles (640 threads):
-//   warps 0-15  generators: thread (lane quarter q = warp % 4, group g = warp / 4)
-//               owns target row 32 q + lane and sources 4 g .. 4 g + 3 of each
-//               16-source K tile; it evaluates the kernel entries in registers,
-//               two sources per FP32x2 instruction (geometry shared by all
-//               chunks), splits them into hi / lo and writes them straight into
-//               TMEM (tcgen05.st), so the A operand never touches shared memory;
-//   warps 16-17 expanders: expand the tile's 16 B_tri rows into hi / lo K-major
-//               SWIZZLE_128B images in shared memory;
-//   warp 18     bulk-copy producer: cp.async.bulk of the raw tile (B_tri rows,
-//               midpoints, normals) into shared memory;
-//   warp 19     MMA issuer: 8 tcgen05.mma (kind::tf32, A from TMEM, B from
-//               shared memory, M 128, K 8) per chunk and tile.
-// Pipelines use mbarriers (A stages in TMEM, B stages in shared memory).  All
-// roles wait with mbarrier.try_wait, which suspends the warp in hardware (on
-// the torus this measured 1 % faster than polling the producer's and the
-// expanders' barriers with __nanosleep in between).
+// Warp roles (GW generator warps + 1 + 2 = 19 or 11 warps):
+//   warps 0 .. GW-1  generators: thread (lane quarter q = warp % 4, group
+//               g = warp / 4) owns target row 32 q + lane and 16 / (GW / 4)
+//               sources of each 16-source K tile; it evaluates the kernel
+//               entries in registers, two sources per FP32x2 instruction
+//               (geometry shared by all chunks), splits them into hi / lo and
+//               writes them straight into TMEM (tcgen05.st), so the A operand
+//               never touches shared memory;
+//   warp GW     bulk-copy producer: cp.async.bulk (no multicast) of the tile's
+//               geometry and of its B images, expanded once per apply by
+//               tc_expand_kernel, into shared memory;
+//   warps GW+1, GW+2  MMA issuers, every other chunk each: 8 tcgen05.mma
+//               (kind::tf32, A from TMEM, B from shared memory, M 128, K 8)
+//               per chunk and tile.
+// Pipelines use mbarriers (A stages in TMEM, B and geometry stages in shared
+// memory).  All roles wait with mbarrier.try_wait, which suspends the warp in
+// hardware.
 // Every wait is bounded: on time-out the CTA raises a shared abort flag, writes
 // an error code for the host, waits (bounded) for its issued MMAs and frees
 // its TMEM before returning.
@@ -78,15 +78,30 @@ struct TcShape
     static constexpr int PPT = SPT / 2;          // their pairs
     static constexpr int KPT = 2 * SPT;          // their K columns of an A stage
     static constexpr int CPG = 16 / GROUPS;      // right-hand sides per thread in the drain
-    static constexpr int THREADS = GEN_THREADS + 64;   // + bulk-copy warp + MMA warp
 };
-constexpr int TC_ASTAGES = 4;      // A stages in TMEM (one chunk of one tile each)
+// MMA-issuing warps of a block: two (each takes every other chunk), so that
+// the issue work of a tile is split between two SM sub-partitions.  The
+// register file is split between the sub-partitions, so a block's register
+// cap is set by the sub-partition with the most warps: 16 generator warps +
+// the bulk-copy warp + 2 issuers are 19 warps (5 on a sub-partition, 96
+// registers); one issuer per chunk would make 21 (6, 80 registers: the
+// generators spill).  With 8 generator warps, 4 issuers measured slower than
+// 2 (128 instead of 168 registers for the generators).
+template <int GW, int CH>
+constexpr int tc_mma_warps() { return CH >= 2 ? 2 : 1; }
+// generators + the bulk-copy warp + the MMA issuers
+template <int GW, int CH>
+constexpr int tc_threads() { return 32 * GW + 32 + 32 * tc_mma_warps<GW, CH>(); }
 constexpr int TC_BSTAGES = 4;      // B image stages in shared memory (bulk copies of the expanded images)
 constexpr int TC_RSTAGES = 6;      // tile geometry stages (bulk copies)
 constexpr uint32_t TC_TMEM_COLS = 512;
 constexpr uint32_t TC_DCOLS = 2 * TC_N;             // per chunk: main (Ahi Bhi) | correction (Ahi Blo + Alo Bhi)
-constexpr uint32_t TC_ACC_COLS = TC_CHMAX * TC_DCOLS;   // the TMEM accumulator (256 columns)
-constexpr uint32_t TC_ACOL = TC_ACC_COLS;             // A stages after the accumulator
+// A stages in TMEM (one chunk of one tile each, 64 columns: hi | lo) take
+// the columns after the accumulator of a CH-chunk work unit: 4 stages for 4
+// chunks, 6 for 2, 7 for 1.
+template <int CH>
+constexpr int tc_astages() { return (int)(TC_TMEM_COLS / TC_DCOLS) - CH; }
+constexpr int TC_ASTAGES_MAX = (int)(TC_TMEM_COLS / TC_DCOLS) - 1;
 constexpr int TC_IMG = TC_N * 128;                   // one K-major SW128 image: 32 rows x 128 B
 constexpr uint64_t kWaitNs = 200ull * 1000 * 1000;   // 200 ms per wait (a pipeline stage takes microseconds)
 
@@ -109,10 +124,11 @@ struct __align__(1024) TcSmem
 {
     uint8_t img[TC_BSTAGES][TC_CHMAX][2][TC_IMG];   // [stage][chunk][hi, lo]
     TcTileGeo geo[TC_RSTAGES];
-    uint64_t a_full[TC_ASTAGES], a_empty[TC_ASTAGES];
+    uint64_t a_full[TC_ASTAGES_MAX], a_empty[TC_ASTAGES_MAX];
     uint64_t b_full[TC_BSTAGES], b_empty[TC_BSTAGES];
     uint64_t r_full[TC_RSTAGES], r_empty[TC_RSTAGES];
     uint64_t seg_full, seg_empty;   // TMEM accumulator: segment summed / drained
+    uint64_t mma_done[TC_CHMAX];    // an issuer's MMAs in flight completed (abort path only)
     uint32_t tmem_base;
     int abort_flag;
     // per chunk, broadcast pairs (v, v): kappa, -kappa, c1.x, c1.y, -c2.x, -c2.y, c3.x, c3.y
@@ -616,7 +632,7 @@ __device__ __forceinline__ void tc_entries_ki(const float2 *__restrict__ P, cons
 // RI, KI: see tc_entries and tc_entries_ki.  GW: generator warps (TcShape).
 // PACK: a packed launch over plan.probs (the pointer arguments are unused).
 template <int GW, int CH, bool SL, bool DL, bool ADL, bool RI, bool KI, bool PACK>
-__global__ void __launch_bounds__(TcShape<GW>::THREADS, 1)
+__global__ void __launch_bounds__(tc_threads<GW, CH>(), 1)
 boundary_tc_kernel(const float *__restrict__ mid4, const float *__restrict__ nrm4, const TcTileGeo *__restrict__ tgeo,
                    const uint8_t *__restrict__ img, float2 *__restrict__ Ctri, float2 *__restrict__ ws,
                    const ChunkParamsF *__restrict__ prm, const TcPlan plan, int *err)
@@ -642,15 +658,16 @@ boundary_tc_kernel(const float *__restrict__ mid4, const float *__restrict__ nrm
 
     if (tid == 0)
     {
-        for (int k = 0; k < TC_ASTAGES; ++k) { mbar_init(&sm.a_full[k], TC_GEN_THREADS); mbar_init(&sm.a_empty[k], 1); }
-        for (int k = 0; k < TC_BSTAGES; ++k) { mbar_init(&sm.b_full[k], 1); mbar_init(&sm.b_empty[k], 1); }
+        for (int k = 0; k < tc_astages<CH>(); ++k) { mbar_init(&sm.a_full[k], TC_GEN_THREADS); mbar_init(&sm.a_empty[k], 1); }
+        for (int k = 0; k < TC_BSTAGES; ++k) { mbar_init(&sm.b_full[k], 1); mbar_init(&sm.b_empty[k], tc_mma_warps<GW, CH>()); }
         for (int k = 0; k < TC_RSTAGES; ++k)
         {
             mbar_init(&sm.r_full[k], 1);
             mbar_init(&sm.r_empty[k], TC_GEN_THREADS);
         }
-        mbar_init(&sm.seg_full, 1);
+        mbar_init(&sm.seg_full, tc_mma_warps<GW, CH>());
         mbar_init(&sm.seg_empty, TC_GEN_THREADS);
+        for (int k = 0; k < TC_CHMAX; ++k) mbar_init(&sm.mma_done[k], 1);
         sm.abort_flag = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
@@ -680,14 +697,16 @@ boundary_tc_kernel(const float *__restrict__ mid4, const float *__restrict__ nrm
     {
         // ------------------------------ generators ------------------------------
         // Per tile: the pair geometry (shared by every chunk), then per chunk
-        // (unrolled): its entries, publication of the previous chunk's A stage,
-        // the wait for this chunk's stage, two TMEM stores.  The ring index of
-        // chunk c of tile T is (T CH + c) mod TC_ASTAGES, a compile-time
-        // column offset when CH == TC_ASTAGES.
+        // (unrolled): its entries, the wait for this chunk's A stage, two TMEM
+        // stores and the stage's publication (with 8 warps deferred until the
+        // next chunk's entries are computed, so the stores land meanwhile).
+        // The ring index of chunk c of tile T is (T CH + c) mod AS, a
+        // compile-time column offset when CH == AS (4 chunks).
         const int q = warp & 3, g = warp >> 2;
         const int row = q * 32 + lane;
         const uint32_t lane_addr = tbase + ((uint32_t)(q * 32) << 16);
-        const uint32_t a_addr = lane_addr + (uint32_t)(TC_ACOL + g * TC_KPT);
+        constexpr int AS = tc_astages<CH>();
+        const uint32_t a_addr = lane_addr + (uint32_t)(CH * TC_DCOLS + g * TC_KPT);
         float2 *acc_row = &sm.acc[row][g * TC_CPG];
         bool ok = true;
         bool pend = false;          // an A stage is written and not yet published
@@ -761,6 +780,7 @@ boundary_tc_kernel(const float *__restrict__ mid4, const float *__restrict__ nrm
             // A finished segment is drained right after the next segment's first
             // chunk is stored, so the tensor core has work waiting when it resumes.
             int drain_due = -1;
+            int sp = 0;   // tiles of the current segment done (a counter: S is a runtime value)
             for (int t = tb; t < te; ++t, ++T)
             {
                 const int rs = T % TC_RSTAGES;
@@ -829,11 +849,11 @@ boundary_tc_kernel(const float *__restrict__ mid4, const float *__restrict__ nrm
                     if (KI) tc_entries_ki<TC_PPT>(Pg + 8 * c, r, kux, knux, kv, hi, lo);
                     else tc_entries<TC_PPT, SL, DL, ADL, RI>(Pg + 8 * c, rinv, r, dmu, dnu, hi, lo);
                     const uint32_t u = (uint32_t)T * CH + c;
-                    const uint32_t stage = u % TC_ASTAGES;
-                    // publish the previous chunk's stage now that its stores had this math to land
+                    const uint32_t stage = u % AS;
+                    // (8 warps) publish the previous chunk's stage now that its stores had this math to land
                     publish();
-                    // the stage is free once the MMAs that read it four chunks ago completed
-                    if (!warp_wait(&sm.a_empty[stage], ((u / TC_ASTAGES) & 1u) ^ 1u, abort_flag, err, 3))
+                    // the stage is free once the MMAs that read it AS chunks ago completed
+                    if (!warp_wait(&sm.a_empty[stage], ((u / AS) & 1u) ^ 1u, abort_flag, err, 3))
                     {
                         ok = false;
                         break;
@@ -843,6 +863,9 @@ boundary_tc_kernel(const float *__restrict__ mid4, const float *__restrict__ nrm
                     tmem_st<TC_KPT>(a_addr + stage * 64u + 32u, lo);
                     pend = true;
                     pend_stage = stage;
+                    // 16 warps: publish at once, the issuers wait for it; the other three
+                    // generator warps of the sub-partition cover the wait for the stores
+                    if (GW == 16) publish();
                     if (c == 0 && drain_due >= 0)
                     {
                         publish();
@@ -852,9 +875,9 @@ boundary_tc_kernel(const float *__restrict__ mid4, const float *__restrict__ nrm
                     }
                 }
                 if (!ok) break;
-                const int lt = t - tb;
-                if (lt % S == S - 1 || t == te - 1)
+                if (++sp == S || t == te - 1)
                 {
+                    sp = 0;
                     // segment SG finished generating
                     if (t == te - 1)
                     {
@@ -929,8 +952,16 @@ boundary_tc_kernel(const float *__restrict__ mid4, const float *__restrict__ nrm
     }
     else
     {
-        // ------------------------------ MMA issuer ------------------------------
-        // The whole warp runs the loop and waits; one elected lane issues.
+        // ------------------------------ MMA issuers ------------------------------
+        // MW warps; warp w issues the MMAs of chunks w, w + MW, ... of every
+        // tile (their own accumulator columns and A stages), so the issue work
+        // is spread over SM sub-partitions instead of queueing behind the
+        // generator warps of one.  Each warp runs its loop warp-wide and waits;
+        // one elected lane issues.  B stages and the segment's end are
+        // released by a commit of every issuer (barrier counts MW).
+        constexpr int MW = tc_mma_warps<GW, CH>();
+        constexpr int AS = tc_astages<CH>();
+        const int w = warp - (TC_GEN_THREADS / 32 + 1);
         bool ok = true;
         int T = 0, SG = 0;
         // descriptors and TMEM addresses from bases fixed for the whole kernel: a
@@ -942,11 +973,11 @@ boundary_tc_kernel(const float *__restrict__ mid4, const float *__restrict__ nrm
         int cg, blk, tb, te, slot, rot;
         while (ok && it.next(plan, V, cg, blk, tb, te, slot, rot))
         {
+            int sp = 0;   // tiles of the current segment done (a counter: S is a runtime value)
             for (int t = tb; t < te; ++t, ++T)
             {
                 const int b = T % TC_BSTAGES;
-                const int lt = t - tb;
-                const bool first = (lt % S) == 0;
+                const bool first = sp == 0;
                 {
                     bool got = wait_bar(&sm.b_full[b], (uint32_t)(T / TC_BSTAGES) & 1u, abort_flag, err, 7);
                     // a new segment overwrites the accumulator: the previous one must be drained
@@ -954,15 +985,17 @@ boundary_tc_kernel(const float *__restrict__ mid4, const float *__restrict__ nrm
                         got = wait_bar(&sm.seg_empty, (uint32_t)(SG - 1) & 1u, abort_flag, err, 8);
                     if (!__all_sync(0xffffffffu, got)) { ok = false; break; }
                 }
-                for (int c = 0; c < CH; ++c)
+                #pragma unroll
+                for (int k = 0; k < CH / MW; ++k)
                 {
-                    const int u = T * CH + c;
-                    const int stage = u % TC_ASTAGES;
-                    const bool got = wait_bar(&sm.a_full[stage], (uint32_t)(u / TC_ASTAGES) & 1u, abort_flag, err, 9);
+                    const int c = w + k * MW;
+                    const uint32_t u = (uint32_t)T * CH + c;
+                    const uint32_t stage = u % AS;
+                    const bool got = wait_bar(&sm.a_full[stage], (u / AS) & 1u, abort_flag, err, 9);
                     if (!__all_sync(0xffffffffu, got)) { ok = false; break; }
                     tc_fence_after();
                     const uint32_t d = tbase + (uint32_t)(c * TC_DCOLS);
-                    const uint32_t a_hi = tbase + TC_ACOL + (uint32_t)stage * 64u;
+                    const uint32_t a_hi = tbase + (uint32_t)(CH * TC_DCOLS) + stage * 64u;
                     const uint32_t a_lo = a_hi + 32u;
                     // the hi image's 32 rows are followed by the lo image's 32 rows
                     // (same 1024-byte group stride): one N = 64 operand [Bhi | Blo]
@@ -983,21 +1016,23 @@ boundary_tc_kernel(const float *__restrict__ mid4, const float *__restrict__ nrm
                     __syncwarp();
                 }
                 if (!ok) break;
+                const bool seg_end = sp + 1 == S || t == te - 1;
+                sp = seg_end ? 0 : sp + 1;
                 if (elect_one())
                 {
                     mma_commit(&sm.b_empty[b]);
-                    if (lt % S == S - 1 || t == te - 1) mma_commit(&sm.seg_full);
+                    if (seg_end) mma_commit(&sm.seg_full);
                 }
                 __syncwarp();
-                if (lt % S == S - 1 || t == te - 1) ++SG;
+                if (seg_end) ++SG;
             }
         }
         if (!ok)
         {
-            // wait (bounded) for the MMAs already issued before the TMEM is freed
-            if (elect_one()) mma_commit(&sm.seg_full);
+            // wait (bounded) for this warp's MMAs already issued before the TMEM is freed
+            if (elect_one()) mma_commit(&sm.mma_done[w]);
             __syncwarp();
-            wait_bar(&sm.seg_full, (uint32_t)SG & 1u, abort_flag, err, 10, false);
+            wait_bar(&sm.mma_done[w], 0u, abort_flag, err, 10, false);
         }
     }
 
@@ -1134,7 +1169,7 @@ void tc_launch(cudaStream_t st, const float *mid, const float *nrm, const TcTile
             if (dev >= 0 && dev < 64) done[dev] = true;
         }
     }
-    boundary_tc_kernel<GW, CH, SL, DL, ADL, RI, KI, PACK><<<plan.ctas, TcShape<GW>::THREADS, bytes, st>>>(
+    boundary_tc_kernel<GW, CH, SL, DL, ADL, RI, KI, PACK><<<plan.ctas, tc_threads<GW, CH>(), bytes, st>>>(
         mid, nrm, tg, B, C, ws, p, plan, err);
 }
 
