@@ -96,9 +96,12 @@ constexpr int TC_BSTAGES = 4;      // B image stages in shared memory (bulk copi
 constexpr int TC_RSTAGES = 6;      // tile geometry stages (bulk copies)
 constexpr uint32_t TC_TMEM_COLS = 512;
 constexpr uint32_t TC_DCOLS = 2 * TC_N;             // per chunk: main (Ahi Bhi) | correction (Ahi Blo + Alo Bhi)
-// A stages in TMEM (one chunk of one tile each, 64 columns: hi | lo) take
-// the columns after the accumulator of a CH-chunk work unit: 4 stages for 4
-// chunks, 6 for 2, 7 for 1.
+// A stages in TMEM (one chunk of one tile each, 64 columns) take the columns
+// after the accumulator of a CH-chunk work unit: 4 stages for 4 chunks, 6 for
+// 2, 7 for 1.  Within a stage, K step ks (8 K columns) has its hi part at
+// columns 16 ks .. 16 ks + 7 and its lo part right after, so a generator
+// thread writes the hi and lo parts of its K step with one 16-column store
+// (1.3 % faster than separate hi and lo halves of the stage).
 template <int CH>
 constexpr int tc_astages() { return (int)(TC_TMEM_COLS / TC_DCOLS) - CH; }
 constexpr int TC_ASTAGES_MAX = (int)(TC_TMEM_COLS / TC_DCOLS) - 1;
@@ -260,20 +263,6 @@ __device__ __forceinline__ void tmem_st16(uint32_t taddr, const uint32_t (&v)[16
                  "r"(v[0]), "r"(v[1]), "r"(v[2]), "r"(v[3]), "r"(v[4]), "r"(v[5]), "r"(v[6]), "r"(v[7]), "r"(v[8]),
                  "r"(v[9]), "r"(v[10]), "r"(v[11]), "r"(v[12]), "r"(v[13]), "r"(v[14]), "r"(v[15])
                  : "memory");
-}
-
-__device__ __forceinline__ void tmem_st8(uint32_t taddr, const uint32_t (&v)[8])
-{
-    asm volatile("tcgen05.st.sync.aligned.32x32b.x8.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8};" ::"r"(taddr),
-                 "r"(v[0]), "r"(v[1]), "r"(v[2]), "r"(v[3]), "r"(v[4]), "r"(v[5]), "r"(v[6]), "r"(v[7])
-                 : "memory");
-}
-
-template <int N>
-__device__ __forceinline__ void tmem_st(uint32_t taddr, const uint32_t (&v)[N])
-{
-    if constexpr (N == 16) tmem_st16(taddr, v);
-    else tmem_st8(taddr, v);
 }
 
 __device__ __forceinline__ void tmem_ld4(uint32_t taddr, uint32_t (&v)[4])
@@ -699,8 +688,9 @@ boundary_tc_kernel(const float *__restrict__ mid4, const float *__restrict__ nrm
     {
         // ------------------------------ generators ------------------------------
         // Per tile: the pair geometry (shared by every chunk), then per chunk
-        // (unrolled): its entries, the wait for this chunk's A stage, two TMEM
-        // stores and the stage's publication (with 8 warps deferred until the
+        // (unrolled): its entries, the wait for this chunk's A stage, one
+        // 16-column TMEM store per K step the thread covers (hi | lo) and the
+        // stage's publication (with 8 warps deferred until the
         // next chunk's entries are computed, so the stores land meanwhile).
         // The ring index of chunk c of tile T is (T CH + c) mod AS, a
         // compile-time column offset when CH == AS (4 chunks).
@@ -708,7 +698,7 @@ boundary_tc_kernel(const float *__restrict__ mid4, const float *__restrict__ nrm
         const int row = q * 32 + lane;
         const uint32_t lane_addr = tbase + ((uint32_t)(q * 32) << 16);
         constexpr int AS = tc_astages<CH>();
-        const uint32_t a_addr = lane_addr + (uint32_t)(CH * TC_DCOLS + g * TC_KPT);
+        const uint32_t a_addr = lane_addr + (uint32_t)(CH * TC_DCOLS + g * 2 * TC_KPT);
         float2 *acc_row = &sm.acc[row][g * TC_CPG];
         bool ok = true;
         bool pend = false;          // an A stage is written and not yet published
@@ -861,8 +851,14 @@ boundary_tc_kernel(const float *__restrict__ mid4, const float *__restrict__ nrm
                         break;
                     }
                     tc_fence_after();
-                    tmem_st<TC_KPT>(a_addr + stage * 64u, hi);
-                    tmem_st<TC_KPT>(a_addr + stage * 64u + 32u, lo);
+                    #pragma unroll
+                    for (int h = 0; h < TC_KPT / 8; ++h)
+                    {
+                        uint32_t v[16];
+                        #pragma unroll
+                        for (int k = 0; k < 8; ++k) { v[k] = hi[8 * h + k]; v[8 + k] = lo[8 * h + k]; }
+                        tmem_st16(a_addr + stage * 64u + 16u * h, v);
+                    }
                     pend = true;
                     pend_stage = stage;
                     // 16 warps: publish at once, the issuers wait for it; the other three
@@ -997,7 +993,7 @@ boundary_tc_kernel(const float *__restrict__ mid4, const float *__restrict__ nrm
                     tc_fence_after();
                     const uint32_t d = tbase + (uint32_t)(c * TC_DCOLS);
                     const uint32_t a_hi = tbase + (uint32_t)(CH * TC_DCOLS) + stage * 64u;
-                    const uint32_t a_lo = a_hi + 32u;
+                    const uint32_t a_lo = a_hi + 8u;
                     // the hi image's 32 rows are followed by the lo image's 32 rows
                     // (same 1024-byte group stride): one N = 64 operand [Bhi | Blo]
                     const uint64_t b_hilo = desc0 + (uint64_t)(((b * TC_CHMAX + c) * TC_GROUP_BYTES) >> 4);
@@ -1008,9 +1004,9 @@ boundary_tc_kernel(const float *__restrict__ mid4, const float *__restrict__ nrm
                         {
                             const uint64_t koff = (uint64_t)(ks * 32 >> 4);
                             // [main | corr] (+)= Ahi [Bhi | Blo];  corr += Alo Bhi
-                            mma_tf32(d, a_hi + 8u * ks, b_hilo + koff, (!first || ks > 0) ? 1u : 0u,
+                            mma_tf32(d, a_hi + 16u * ks, b_hilo + koff, (!first || ks > 0) ? 1u : 0u,
                                      idesc_tf32(2 * TC_N));
-                            mma_tf32(d + (uint32_t)TC_N, a_lo + 8u * ks, b_hilo + koff, 1u, idesc_tf32(TC_N));
+                            mma_tf32(d + (uint32_t)TC_N, a_lo + 16u * ks, b_hilo + koff, 1u, idesc_tf32(TC_N));
                         }
                         mma_commit(&sm.a_empty[stage]);
                     }
