@@ -186,6 +186,8 @@ struct TcPackItem
     int64_t nt;
     int wc;
     float ki_s;
+    int ch;                         // chunk groups per work unit under the problem's own tuning
+                                    // (tc_chunks_per_unit; set by Packer::apply)
 };
 // Tables of packed launches: a grow-only device block and a pinned host copy
 // it is uploaded from (on the launch's stream; reused once the last upload

@@ -76,6 +76,7 @@ void Packer::apply(const TcPackItem &item, const OpFlags &f, const TcTuning &tun
 {
     Pending p;
     p.item = item;
+    p.item.ch = tc_chunks_per_unit(item.wc, tune.chunks);
     p.flags = f;
     p.tune = tune;
     p.cls = tc_pack_class(f, item.wc, tune);

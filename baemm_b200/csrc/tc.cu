@@ -1436,14 +1436,16 @@ void launch_boundary_tc_packed(const TcPackItem *items, int count, const OpFlags
 {
     BAEMM_REQUIRE(count >= 1, BAEMM_ERR_ARG, "packed launch without problems");
     const int code = (f.sl() ? 1 : 0) | (f.dl() ? 2 : 0) | (f.adl() ? 4 : 0);
-    const int CH = tc_chunks_per_unit(items[0].wc, tune.chunks);
+    // every problem's chunk groups per unit under its own tuning (the packing
+    // class holds it; tune is the first problem's, so it does not decide this)
+    const int CH = items[0].ch;
     // the problem table and the blocks (problem, block), costed by their source tiles
     std::vector<TcProblem> probs((size_t)count);
     std::vector<std::pair<int, int2>> blocks;   // (tiles, (problem, block))
     for (int q = 0; q < count; ++q)
     {
         const TcPackItem &it = items[q];
-        BAEMM_REQUIRE(tc_chunks_per_unit(it.wc, tune.chunks) == CH, BAEMM_ERR_ARG,
+        BAEMM_REQUIRE(it.ch == CH && (CH == 1 || CH == 2 || CH == 4) && it.wc % (16 * CH) == 0, BAEMM_ERR_ARG,
                       "packed problems need the same chunk groups per unit");
         TcProblem &P = probs[(size_t)q];
         P.mid4 = it.mid4;

@@ -157,6 +157,65 @@ def test_packed_solves_are_the_same_alone_and_packed():
                 H.close()
 
 
+def test_packed_problems_with_different_wave_shapes():
+    """Two solves of one packing class whose chunk groups per unit come from
+    different settings (64 columns tuned to 2 chunks per unit, 32 columns with
+    the automatic choice, also 2) share packed launches in either order, and
+    each solution equals the same solve run alone bit for bit."""
+    import threading
+
+    from baemm_b200 import APPLY_TC, Packer, _capi
+
+    meshes_ = [meshes.icosphere(2), meshes.icosphere(3)]
+    kaps = [np.array([2.0, 3.0, 4.0, 5.0]), np.array([3.0, 6.0])]
+    rng = np.random.default_rng(11)
+    waves = [crandn(rng, c.shape[0], 16 * len(ka)) for (c, _), ka in zip(meshes_, kaps)]
+    with Packer(0, max_wait_us=100000) as P:
+        Hs = [Helmholtz_CUDA(c, t, np.eye(3)) for c, t in meshes_]
+        try:
+            Hs[0].SetTuning(_capi.TUNE_TC_CHUNKS, 2)
+            for H in Hs:
+                H.SetApplyMode(APPLY_TC)
+                H.SetPacker(P)
+
+            def solve(q):
+                phi = np.zeros_like(waves[q])
+                Hs[q].BoundaryPotential(kaps[q], np.zeros((len(kaps[q]), 4), complex), waves[q], phi, 16,
+                                        1e-10, 1e-10)
+                return phi
+
+            alone = [solve(0), solve(1)]
+            before = P.stats()
+            outs = [[], []]
+            barrier = threading.Barrier(2)
+            errors = []
+
+            def run(q):
+                try:
+                    for _ in range(2):
+                        barrier.wait()
+                        outs[q].append(solve(q))
+                except Exception as e:   # surfaced below
+                    errors.append(e)
+                    barrier.abort()
+
+            th = [threading.Thread(target=run, args=(q,)) for q in range(2)]
+            for t in th:
+                t.start()
+            for t in th:
+                t.join()
+            assert not errors, errors
+            after = P.stats()
+            for q in range(2):
+                for phi in outs[q]:
+                    assert np.array_equal(phi, alone[q])
+            assert after["problems"] - before["problems"] > after["launches"] - before["launches"]
+        finally:
+            for H in Hs:
+                H.SetPacker(None)
+                H.close()
+
+
 def test_packed_server_same_alone_and_in_the_mix():
     """The packing server: each request's far field alone equals the same
     request in a concurrent mix (1e-10), and the mix's applies shared launches."""
