@@ -15,7 +15,7 @@ namespace
 {
 
 constexpr int RT = 256;          // threads per reduction block
-constexpr int kTargetBlocks = 296;
+constexpr int kTargetBlocks = 592;   // reduction blocks over the rows (4 per SM: the Gram-Schmidt dots ran 117 -> 72 us at level 6 with twice 296)
 
 struct Layout
 {
@@ -85,68 +85,121 @@ __device__ __forceinline__ void block_reduce_store(double v, double *sm, int tr,
 
 
 // Sum of one column of the per-block partial sums, partial[q * ld + off] over
-// q < nblk, by one warp: lane l takes q = l, l + 32, ..., a shuffle tree adds
-// the lanes in a fixed order and every lane returns lane 0's total (so the
-// result does not depend on timing).  The finalize kernels below give each
-// column its own warp, instead of one thread summing all nblk values in turn.
+// q < nblk, by one warp: lane l takes q = l, l + 32, ... into four running
+// sums (q / 32 mod 4), so four loads per lane are in flight instead of one
+// dependent chain of round trips; the four are added in a fixed order and a
+// shuffle tree adds the lanes in a fixed order, every lane returning lane 0's
+// total (so the result does not depend on timing).  The finalize kernels
+// below give each column its own warp, instead of one thread summing all
+// nblk values in turn.
 __device__ __forceinline__ double warp_sum_partials(const double *__restrict__ partial, int64_t ld, int64_t off,
                                                     int nblk)
 {
     const int lane = threadIdx.x & 31;
-    double s = 0.0;
-    for (int q = lane; q < nblk; q += 32) s += partial[(int64_t)q * ld + off];
+    double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
+    int q = lane;
+    for (; q + 96 < nblk; q += 128)
+    {
+        const double v0 = partial[(int64_t)q * ld + off], v1 = partial[(int64_t)(q + 32) * ld + off];
+        const double v2 = partial[(int64_t)(q + 64) * ld + off], v3 = partial[(int64_t)(q + 96) * ld + off];
+        s0 += v0; s1 += v1; s2 += v2; s3 += v3;
+    }
+    if (q < nblk) s0 += partial[(int64_t)q * ld + off];
+    if (q + 32 < nblk) s1 += partial[(int64_t)(q + 32) * ld + off];
+    if (q + 64 < nblk) s2 += partial[(int64_t)(q + 64) * ld + off];
+    double s = (s0 + s1) + (s2 + s3);
     #pragma unroll
     for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
     return __shfl_sync(0xffffffffu, s, 0);
 }
 
-// The same over partial sums written by other blocks of the running kernel:
-// loads that bypass L1 (the lines may be stale there).
-__device__ __forceinline__ double warp_sum_partials_cg(const double *partial, int64_t ld, int64_t off, int nblk)
+// Two-level column totals of per-block partial sums, run inside the kernel
+// that produced them (the "last block" reduction: no launch of its own).
+constexpr int kSumGroup = 16;   // blocks per first-level group
+__host__ __device__ constexpr int cg_groups(int nblk) { return (nblk + kSumGroup - 1) / kSumGroup; }
+
+// dst[m] = sum of src[q * S + m] over q < nrows, for m < S, by all threads of
+// the block: thread t takes m = t, t + blockDim.x, ...; eight loads in flight
+// into eight running sums (q mod 8), added in a fixed order.  The rows were
+// written by other blocks of the running kernel: loads bypass L1.
+__device__ void block_sum_rows(const double *src, int S, int nrows, double *dst)
 {
-    const int lane = threadIdx.x & 31;
-    double s = 0.0;
-    for (int q = lane; q < nblk; q += 32) s += __ldcg(partial + (int64_t)q * ld + off);
-    #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
-    return __shfl_sync(0xffffffffu, s, 0);
+    for (int m = threadIdx.x; m < S; m += blockDim.x)
+    {
+        double a[8] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+        int q = 0;
+        for (; q + 8 <= nrows; q += 8)
+        {
+            double v[8];
+            #pragma unroll
+            for (int j = 0; j < 8; ++j) v[j] = __ldcg(src + (int64_t)(q + j) * S + m);
+            #pragma unroll
+            for (int j = 0; j < 8; ++j) a[j] += v[j];
+        }
+        #pragma unroll
+        for (int j = 0; j < 7; ++j)
+            if (q + j < nrows) a[j] += __ldcg(src + (int64_t)(q + j) * S + m);
+        dst[m] = ((a[0] + a[1]) + (a[2] + a[3])) + ((a[4] + a[5]) + (a[6] + a[7]));
+    }
 }
 
-// Called by every thread of every block after the block has written its
-// partial sums: true (in all threads) in the one block that finished last,
-// which then sees every block's partials.  The counter is back at zero when
-// the kernel ends.  (The "last block" reduction: the finalize step runs in
-// the producing kernel instead of a launch of its own.)
-__device__ __forceinline__ bool last_block(unsigned int *counter)
+// Called by every thread of every block after the block has written its part
+// of row blockIdx.x of the S partial sums (partial[blockIdx.x * S ...]).  The
+// last block of each group of kSumGroup rows sums the group's rows into its
+// group row, and the last group to finish sums the group rows into the totals;
+// true (in all threads) in that one block, with *tot = the S totals.  Layout
+// of `partial`: gridDim.x rows, then cg_groups(gridDim.x) group rows, then the
+// totals.  counter[0] counts finished groups, counter[1 + g] the blocks of
+// group g; both are back at zero when the kernel ends.  Fixed summation orders
+// throughout, so the totals do not depend on timing.  (One block summing all
+// rows directly took 58 us of an 85 us CG update on 40962 x 64 values.)
+__device__ bool cg_column_totals(double *partial, int S, unsigned int *counter, const double **tot)
 {
     __shared__ bool last;
+    const int nblk = gridDim.x, ng = cg_groups(nblk);
+    const int g = blockIdx.x / kSumGroup, g0 = g * kSumGroup, g1 = min(nblk, g0 + kSumGroup);
+    double *gpart = partial + (int64_t)nblk * S;
+    double *tt = gpart + (int64_t)ng * S;
     __threadfence();
     __syncthreads();
     if (threadIdx.x == 0)
     {
-        const unsigned int nb = gridDim.x * gridDim.y;
-        last = atomicAdd(counter, 1u) == nb - 1;
-        if (last) *counter = 0u;
+        const unsigned int members = (unsigned int)(g1 - g0) * gridDim.y;
+        last = atomicAdd(counter + 1 + g, 1u) == members - 1;
+        if (last) counter[1 + g] = 0u;
     }
     __syncthreads();
-    if (last) __threadfence();
-    return last;
+    if (!last) return false;
+    __threadfence();
+    block_sum_rows(partial + (int64_t)g0 * S, S, g1 - g0, gpart + (int64_t)g * S);
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0)
+    {
+        last = atomicAdd(counter, 1u) == (unsigned int)ng - 1;
+        if (last) counter[0] = 0u;
+    }
+    __syncthreads();
+    if (!last) return false;
+    __threadfence();
+    block_sum_rows(gpart, S, ng, tt);
+    __syncthreads();
+    *tot = tt;
+    return true;
 }
 
-// Column sums of the CG phases, one warp per column (ApplyMassInverse.hpp:67-147):
-//   init:  rz = <r, z>, bn = ||b||, convergence of zero columns
-//   alpha: alpha = rz / <p, q>
-//   beta:  beta = rz_new / rz, rz = rz_new, convergence ||r|| <= tol ||b||
+// Column steps of the CG phases over the column totals tot (one thread per
+// column; ApplyMassInverse.hpp:67-147):
+//   init:  rz = <r, z>, bn = ||b||, convergence of zero columns    tot = [rz | bb]
+//   alpha: alpha = rz / <p, q>                                       tot = [pq]
+//   beta:  beta = rz_new / rz, rz = rz_new, convergence ||r|| <= tol ||b||   tot = [rz_new | rr]
 // col layout: [0,c) rz  [c,2c) bn  [2c,3c) alpha  [3c,4c) beta ; flags: [0] done [1] iters [2..) conv
-__device__ void cg_fin_init(int c, int nblk, const double *partial, double *col, int *flags, double tol)
+__device__ void cg_fin_init(int c, const double *tot, double *col, int *flags, double tol)
 {
     int all = 1;
-    const int warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5, lane = threadIdx.x & 31;
-    for (int k = warp; k < c; k += nwarps)
+    for (int k = threadIdx.x; k < c; k += blockDim.x)
     {
-        const double rz = warp_sum_partials_cg(partial, 2 * c, k, nblk);
-        const double bb = warp_sum_partials_cg(partial, 2 * c, c + k, nblk);
-        if (lane != 0) continue;
+        const double rz = __ldcg(tot + k), bb = __ldcg(tot + c + k);
         const double bn = sqrt(bb);
         col[k] = rz;
         col[c + k] = bn;
@@ -160,25 +213,21 @@ __device__ void cg_fin_init(int c, int nblk, const double *partial, double *col,
     if (threadIdx.x == 0) { flags[0] = all; flags[1] = 0; }
 }
 
-__device__ void cg_fin_alpha(int c, int nblk, const double *partial, double *col, const int *flags)
+__device__ void cg_fin_alpha(int c, const double *tot, double *col, const int *flags)
 {
-    const int warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5, lane = threadIdx.x & 31;
-    for (int k = warp; k < c; k += nwarps)
+    for (int k = threadIdx.x; k < c; k += blockDim.x)
     {
-        const double pq = warp_sum_partials_cg(partial, c, k, nblk);
-        if (lane == 0) col[2 * c + k] = (flags[2 + k] || pq == 0.0) ? 0.0 : col[k] / pq;
+        const double pq = __ldcg(tot + k);
+        col[2 * c + k] = (flags[2 + k] || pq == 0.0) ? 0.0 : col[k] / pq;
     }
 }
 
-__device__ void cg_fin_beta(int c, int nblk, const double *partial, double *col, int *flags, double tol)
+__device__ void cg_fin_beta(int c, const double *tot, double *col, int *flags, double tol)
 {
     int all = 1;
-    const int warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5, lane = threadIdx.x & 31;
-    for (int k = warp; k < c; k += nwarps)
+    for (int k = threadIdx.x; k < c; k += blockDim.x)
     {
-        const double rzn = warp_sum_partials_cg(partial, 2 * c, k, nblk);
-        const double rr = warp_sum_partials_cg(partial, 2 * c, c + k, nblk);
-        if (lane != 0) continue;
+        const double rzn = __ldcg(tot + k), rr = __ldcg(tot + c + k);
         const int was = flags[2 + k];
         col[3 * c + k] = (was || col[k] == 0.0) ? 0.0 : rzn / col[k];
         col[k] = rzn;
@@ -218,7 +267,8 @@ __global__ void cg_init_kernel(int64_t n, int c, int cp, int rp, int64_t rpb, co
     double *out = partial + (int64_t)blockIdx.x * 2 * c;
     block_reduce_store(rz, sm, tr, tc, cp, rp, active, out + k);
     block_reduce_store(bb, sm, tr, tc, cp, rp, active, out + c + k);
-    if (last_block(counter)) cg_fin_init(c, gridDim.x, partial, col, flags, tol);
+    const double *tot;
+    if (cg_column_totals(partial, 2 * c, counter, &tot)) cg_fin_init(c, tot, col, flags, tol);
 }
 
 template <class RV>
@@ -238,14 +288,35 @@ __global__ void cg_matvec_kernel(int64_t n, int c, int cp, int rp, int64_t rpb, 
         const int64_t r0 = blockIdx.x * rpb, r1 = min(n, r0 + rpb);
         for (int64_t row = r0 + tr; row < r1; row += rp)
         {
+            // the row's first kPf entries (a P1 mass row has 1 + the vertex
+            // degree, ~7) are loaded before any gather, so their gathers are in
+            // flight together instead of one dependent chain per entry; the sum
+            // runs in entry order as before
+            constexpr int kPf = 8;
+            const int32_t e0 = mo[row], e1 = mo[row + 1];
+            int32_t ci[kPf];
+            double cv[kPf], pv[kPf];
+            #pragma unroll
+            for (int j = 0; j < kPf; ++j)
+            {
+                const bool in = e0 + j < e1;
+                ci[j] = in ? mi[e0 + j] : 0;
+                cv[j] = in ? (double)mv[e0 + j] : 0.0;
+            }
+            #pragma unroll
+            for (int j = 0; j < kPf; ++j) pv[j] = e0 + j < e1 ? p[(int64_t)ci[j] * c + k] : 0.0;
             double s = 0.0;
-            for (int32_t e = mo[row]; e < mo[row + 1]; ++e) s += (double)mv[e] * p[(int64_t)mi[e] * c + k];
+            #pragma unroll
+            for (int j = 0; j < kPf; ++j)
+                if (e0 + j < e1) s += cv[j] * pv[j];
+            for (int32_t e = e0 + kPf; e < e1; ++e) s += (double)mv[e] * p[(int64_t)mi[e] * c + k];
             q[row * c + k] = s;
             pq += p[row * c + k] * s;
         }
     }
     block_reduce_store(pq, sm, tr, tc, cp, rp, active, partial + (int64_t)blockIdx.x * c + k);
-    if (last_block(counter)) cg_fin_alpha(c, gridDim.x, partial, col, flags);
+    const double *tot;
+    if (cg_column_totals(partial, c, counter, &tot)) cg_fin_alpha(c, tot, col, flags);
 }
 
 
@@ -265,22 +336,50 @@ __global__ void cg_update_kernel(int64_t n, int c, int cp, int rp, int64_t rpb, 
     {
         const double a = col[2 * c + k];
         const int64_t r0 = blockIdx.x * rpb, r1 = min(n, r0 + rpb);
-        for (int64_t row = r0 + tr; row < r1; row += rp)
+        // four rows' operands are loaded before any of them is used (four
+        // times the loads in flight per thread); the dots accumulate in row
+        // order as in the one-row loop below
+        int64_t row = r0 + tr;
+        for (; row + 3 * rp < r1; row += 4 * rp)
+        {
+            double pv[4], xv[4], rv[4], qv[4], lv[4];
+            #pragma unroll
+            for (int u = 0; u < 4; ++u)
+            {
+                const int64_t e = (row + u * rp) * c + k;
+                pv[u] = p[e]; xv[u] = x[e]; rv[u] = r[e]; qv[u] = q[e];
+                lv[u] = (double)L[row + u * rp];
+            }
+            #pragma unroll
+            for (int u = 0; u < 4; ++u)
+            {
+                const int64_t e = (row + u * rp) * c + k;
+                x[e] = xv[u] + a * pv[u];
+                const double rn = rv[u] - a * qv[u];
+                r[e] = rn;
+                const double zv = lv[u] * rn;
+                z[e] = zv;
+                rz += rn * zv;
+                rr += rn * rn;
+            }
+        }
+        for (; row < r1; row += rp)
         {
             const int64_t e = row * c + k;
             x[e] += a * p[e];
-            const double rv = r[e] - a * q[e];
-            r[e] = rv;
-            const double zv = (double)L[row] * rv;
+            const double rn = r[e] - a * q[e];
+            r[e] = rn;
+            const double zv = (double)L[row] * rn;
             z[e] = zv;
-            rz += rv * zv;
-            rr += rv * rv;
+            rz += rn * zv;
+            rr += rn * rn;
         }
     }
     double *out = partial + (int64_t)blockIdx.x * 2 * c;
     block_reduce_store(rz, sm, tr, tc, cp, rp, active, out + k);
     block_reduce_store(rr, sm, tr, tc, cp, rp, active, out + c + k);
-    if (last_block(counter)) cg_fin_beta(c, gridDim.x, partial, col, flags, tol);
+    const double *tot;
+    if (cg_column_totals(partial, 2 * c, counter, &tot)) cg_fin_beta(c, tot, col, flags, tol);
 }
 
 
@@ -583,6 +682,18 @@ bool CgSolver::finish(cudaStream_t st, int *iterations)
     return host_flags_[0] != 0;
 }
 
+void CgSolver::reserve_totals(int nblk, int S, cudaStream_t st)
+{
+    const int ng = cg_groups(nblk);
+    partial_.reserve((size_t)(nblk + ng + 1) * S);
+    const size_t nc = 1 + (size_t)ng;
+    if (counter_.n < nc)
+    {
+        counter_.reserve(nc);
+        BAEMM_CUDA(cudaMemsetAsync(counter_.p, 0, counter_.n * sizeof(unsigned int), st));
+    }
+}
+
 void CgSolver::enqueue_mass(const MeshDev &m, bool fp64_values, const double *b, int64_t ldb, double *y,
                             int64_t ldy, int c, double tol, int max_iter, cudaStream_t st)
 {
@@ -593,12 +704,7 @@ void CgSolver::enqueue_mass(const MeshDev &m, bool fp64_values, const double *b,
     col_.reserve(4 * (size_t)c);
     flags_.reserve(2 + (size_t)c);
     const Layout L = make_layout(n, c);
-    partial_.reserve((size_t)L.nblk * 2 * c);
-    if (!counter_.p)
-    {
-        counter_.reserve(1);
-        BAEMM_CUDA(cudaMemsetAsync(counter_.p, 0, sizeof(unsigned int), st));
-    }
+    reserve_totals(L.nblk, 2 * c, st);
     if (!host_flags_) BAEMM_CUDA(cudaMallocHost(&host_flags_, 2 * sizeof(int)));
     dim3 grid(L.nblk, L.nchunk);
     auto run = [&](auto Lv, auto Mv) {
@@ -637,12 +743,7 @@ void CgSolver::profile(const MeshDev &m, bool fp64_values, int c, int iterations
     col_.reserve(4 * (size_t)c);
     flags_.reserve(2 + (size_t)c);
     const Layout L = make_layout(n, c);
-    partial_.reserve((size_t)L.nblk * 2 * c);
-    if (!counter_.p)
-    {
-        counter_.reserve(1);
-        BAEMM_CUDA(cudaMemsetAsync(counter_.p, 0, sizeof(unsigned int), st));
-    }
+    reserve_totals(L.nblk, 2 * c, st);
     dim3 grid(L.nblk, L.nchunk);
     cudaEvent_t ev[4];
     for (auto &e : ev) BAEMM_CUDA(cudaEventCreate(&e));

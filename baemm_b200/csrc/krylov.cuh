@@ -46,9 +46,13 @@ public:
     void profile(const MeshDev &m, bool fp64_values, int c, int iterations, cudaStream_t st, double ms_out[3]);
 
 private:
+    // partial_: per-block partial sums, group rows and totals of the
+    // two-level column sums; counter_: their group and block counters (zero
+    // between kernels; zeroed whenever the buffer grows)
+    void reserve_totals(int nblk, int S, cudaStream_t st);
     DevBuf<double> x_, r_, z_, p_, q_, col_, partial_;
     DevBuf<int> flags_;
-    DevBuf<unsigned int> counter_;   // last-block detection of the column sums (zero between kernels)
+    DevBuf<unsigned int> counter_;
     int *host_flags_ = nullptr;
 };
 
