@@ -169,17 +169,21 @@ class SolveServer:
     slots: concurrent solves; budget_bytes: device-memory admission budget
     (default: half the free device memory at start-up).
     apply_mode: APPLY_TC (default) or APPLY_FP32; graphs: replay the solver's
-    inner operators as CUDA graphs; pack (default on, tensor-core form): the
+    inner operators as CUDA graphs; pack (default off, tensor-core form): the
     slots' operator applies of small problems share one persistent launch
     (helmholtz.Packer, waiting at most pack_wait_us for the other solves in
-    progress); autotune (default on): tune the dense
+    progress).  Off by default because it measured no faster: the slots' own
+    streams already run small solves' kernels side by side on the GPU, and the
+    packer's rendezvous of the host threads costs about what a shared launch
+    saves (level-4 stream: 0.74-1.02x of the server without it, levels 4-6:
+    0.97x).  autotune (default on): tune the dense
     kernel per problem shape (mesh size, right-hand-side count); the library
     caches the choice per shape for the process, so each shape is timed once.
     """
 
     def __init__(self, meas_directions, slots: int = 6, budget_bytes: Optional[int] = None, apply_mode=None,
                  graphs: bool = True, autotune: bool = True, device: int = 0,
-                 executor: Optional[Callable] = None, pack: bool = True, pack_wait_us: int = 2000):
+                 executor: Optional[Callable] = None, pack: bool = False, pack_wait_us: int = 2000):
         from ._capi import APPLY_TC
         self.meas = np.ascontiguousarray(np.asarray(meas_directions, dtype=np.float64).reshape(-1, 3))
         self.slots = slots

@@ -828,8 +828,9 @@ def run_solve_workload(args):
 # ---------------------------------------------------------------------------
 # the serving workload (--workload serve): not the headline line
 # ---------------------------------------------------------------------------
-def serve_runs(n_requests, slots=6, seed=0, seq_sample=0, seq_tc=True, latency=True):
-    """Stream of scattering-solve requests (icosphere levels 4-6 radially
+def serve_runs(n_requests, slots=6, seed=0, seq_sample=0, seq_tc=True, latency=True, levels=(4, 5, 6),
+               pack_wait_us=None):
+    """Stream of scattering-solve requests (icosphere levels `levels` (4-6) radially
     perturbed by a random degree-8 spherical-harmonic field of amplitude 0.1,
     kappa ~ U[1, 10], 1-64 plane waves, GMRES to 1e-6, far field at 128
     directions).  Runs over the same requests:
@@ -837,11 +838,11 @@ def serve_runs(n_requests, slots=6, seed=0, seq_sample=0, seq_tc=True, latency=T
       sequential_tc          the tensor-core apply with graph replay, one request at a
                              time (the same arithmetic as the server: the server's own
                              gain over it is the batching);
-      capacity               the serving loop (slots of resident contexts, memory-budget
-                             admission, tensor-core apply packed across the slots' solves,
-                             CUDA-graph replay) with every request queued at once: solves/s
-                             is its throughput (capacity_without_packing: the same without
-                             the packer);
+      capacity               the serving loop as configured by default (slots of resident
+                             contexts on their own streams, memory-budget admission,
+                             tensor-core apply, CUDA-graph replay) with every request queued
+                             at once: solves/s is its throughput (capacity_with_packing: the
+                             same with the slots' applies packed into shared launches);
       latency                the serving loop with Poisson arrivals at 80 % of that
                              capacity: p50 / p99 of finish - arrival.
     The far fields of the served runs are compared with the sequential ones."""
@@ -849,11 +850,11 @@ def serve_runs(n_requests, slots=6, seed=0, seq_sample=0, seq_tc=True, latency=T
     from baemm_b200.serving import SolveServer, make_stream, summarize
     from baemm_b200.serving import SolveRequest
     meas = meshes.fibonacci_sphere(128)
-    reqs = make_stream(n_requests, rate=0.0, seed=seed)
+    reqs = make_stream(n_requests, rate=0.0, levels=tuple(levels), seed=seed)
     # warm-up: one request per problem shape (mesh level x padded right-hand sides), so the
     # autotuner's choices and the device buffers exist before any timing
     warm = []
-    for level in (4, 5, 6):
+    for level in levels:
         coords_w, tris_w = meshes.icosphere(level)
         for nrhs in (16, 32, 64):
             d = meshes.fibonacci_sphere(nrhs)
@@ -879,27 +880,31 @@ def serve_runs(n_requests, slots=6, seed=0, seq_sample=0, seq_tc=True, latency=T
     if seq_tc:
         _, t_tc = sequential(APPLY_TC, True)
         res["sequential_tc"] = {"solves_per_s": n_seq / t_tc, "seconds": t_tc, "requests": n_seq}
-    # the server without packing (each slot launches its own applies), for the packing's own gain
-    with SolveServer(meas, slots=slots, apply_mode=APPLY_TC, graphs=True, pack=False) as srv0:
-        srv0.run(warm, realtime=False)
+    # the server with packing (the slots' GMRES applies share launches), for the packing's own effect
+    pkw = {} if pack_wait_us is None else {"pack_wait_us": pack_wait_us}
+    with SolveServer(meas, slots=slots, apply_mode=APPLY_TC, graphs=True, pack=True, **pkw) as srvp:
+        srvp.run(warm, realtime=False)
+        p0 = srvp.pack_stats()
         t0 = time.perf_counter()
-        srv0.run(at_once(), realtime=False)
-        res["capacity_without_packing"] = {"solves_per_s": len(reqs) / (time.perf_counter() - t0)}
-    with SolveServer(meas, slots=slots, apply_mode=APPLY_TC, graphs=True, pack=True) as srv:
+        packed = srvp.run(at_once(), realtime=False)
+        t_p = time.perf_counter() - t0
+        p1 = srvp.pack_stats()
+        launches, probs = p1["launches"] - p0["launches"], p1["problems"] - p0["problems"]
+        res["capacity_with_packing"] = {"solves_per_s": len(reqs) / t_p, "packed_launches": launches,
+                                        "packed_problems": probs,
+                                        "problems_per_packed_launch": probs / launches if launches else None}
+    served = [packed]
+    # the server as configured by default (packing off: each slot launches its own applies on its stream)
+    with SolveServer(meas, slots=slots, apply_mode=APPLY_TC, graphs=True) as srv:
         srv.run(warm, realtime=False)
-        p0 = srv.pack_stats()
         t0 = time.perf_counter()
         cap = srv.run(at_once(), realtime=False)
         t_cap = time.perf_counter() - t0
-        p1 = srv.pack_stats()
         thr_served = len(reqs) / t_cap
-        launches, probs = p1["launches"] - p0["launches"], p1["problems"] - p0["problems"]
         res["capacity"] = {"solves_per_s": thr_served, "seconds": t_cap,
                            "peak_concurrent": srv.scheduler.peak_running,
-                           "converged": int(sum(r.converged for r in cap.values())), "requests": len(reqs),
-                           "packed_launches": launches, "packed_problems": probs,
-                           "problems_per_packed_launch": probs / launches if launches else None}
-        served = [cap]
+                           "converged": int(sum(r.converged for r in cap.values())), "requests": len(reqs)}
+        served.append(cap)
         if latency:
             rate = 0.8 * thr_served
             rng = np.random.default_rng(seed + 1)
@@ -914,7 +919,7 @@ def serve_runs(n_requests, slots=6, seed=0, seq_sample=0, seq_tc=True, latency=T
                                             "solves_per_s": s_lat["solves_per_s"]}
             served.append(lat)
     res["speedup_vs_sequential_plain"] = thr_served / res["sequential_plain_fp32"]["solves_per_s"]
-    res["speedup_of_packing"] = thr_served / res["capacity_without_packing"]["solves_per_s"]
+    res["speedup_of_packing"] = res["capacity_with_packing"]["solves_per_s"] / thr_served
     if seq_tc:
         res["speedup_vs_sequential_tc"] = thr_served / res["sequential_tc"]["solves_per_s"]
     res["max_far_field_rel_diff_served_vs_sequential"] = max(
@@ -924,11 +929,13 @@ def serve_runs(n_requests, slots=6, seed=0, seq_sample=0, seq_tc=True, latency=T
 
 
 def run_serve_workload(args):
-    res = serve_runs(args.requests, args.slots, args.serve_seed, args.seq_sample)
+    levels = tuple(int(v) for v in args.serve_levels.split(","))
+    res = serve_runs(args.requests, args.slots, args.serve_seed, args.seq_sample, levels=levels,
+                     pack_wait_us=args.pack_wait_us)
     line = {"metric": "served solves/s (scattering, FarField)", "value": res["capacity"]["solves_per_s"],
             "unit": "solves/s", "n_gpus": 1, "higher_is_better": True, "data": "synthetic",
-            "config": {"workload": "perturbed-icosphere scattering solves, levels 4-6, kappa U[1,10], 1-64 plane "
-                                   "waves, GMRES 1e-6, far field at 128 directions",
+            "config": {"workload": f"perturbed-icosphere scattering solves, levels {','.join(map(str, levels))}, "
+                                   "kappa U[1,10], 1-64 plane waves, GMRES 1e-6, far field at 128 directions",
                        "requests": args.requests, "slots": args.slots, "seed": args.serve_seed}}
     line.update(res)
     print(json.dumps(line), flush=True)
@@ -1032,6 +1039,9 @@ def main(argv=None):
     ap.add_argument("--serve-sample", type=int, default=48, help="requests of the default line's serving sample")
     ap.add_argument("--slots", type=int, default=6, help="serving slots of --workload serve")
     ap.add_argument("--serve-seed", type=int, default=0)
+    ap.add_argument("--serve-levels", default="4,5,6", help="icosphere levels of --workload serve's stream")
+    ap.add_argument("--pack-wait-us", type=int, default=None,
+                    help="the packer's wait for partners in --workload serve (default: the server's)")
     ap.add_argument("--seq-sample", type=int, default=0,
                     help="--workload serve: run the sequential baseline on the first N requests only (0: all)")
     ap.add_argument("--gn-level", type=int, default=5, help="icosphere level of --workload gauss-newton")
