@@ -679,6 +679,31 @@ int baemm_packer_stats(const baemm_packer *p, int64_t *launches, int64_t *proble
     return BAEMM_OK;
 }
 
+int baemm_selftest_bounded_wait(int device, double *elapsed_ms, int *code)
+{
+    try
+    {
+        BAEMM_REQUIRE(elapsed_ms && code, BAEMM_ERR_ARG, "null output");
+        int n = 0;
+        BAEMM_CUDA(cudaGetDeviceCount(&n));
+        BAEMM_REQUIRE(device >= 0 && device < n, BAEMM_ERR_ARG, "no such device");
+        DeviceScope scope(device);
+        baemm::tc_bounded_wait_probe(99, elapsed_ms, code);
+        g_create_error.clear();
+        return BAEMM_OK;
+    }
+    catch (const Error &e)
+    {
+        g_create_error = e.what();
+        return e.code;
+    }
+    catch (const std::exception &e)
+    {
+        g_create_error = e.what();
+        return BAEMM_ERR_ARG;
+    }
+}
+
 int baemm_profile_krylov(baemm_ctx *ctx, int columns, int iterations, int basis, double out[10])
 {
     return guarded(ctx, [&](Ctx &c) {

@@ -171,6 +171,9 @@ void launch_nearfield_tc(const MeshDev &m, const OpFlags &f, const void *chunk_p
 // The tensor-core form's B operand: every 16-source tile's hi / lo images of
 // B_tri (n x wc) per 16-column group, as the kernel's B stages hold them
 // (8 KB each); returns img's device block (grown as needed).
+// Self-test of the bounded pipeline waits: one warp waits on an mbarrier that
+// nothing arrives on; returns the error code the wait wrote and its duration.
+void tc_bounded_wait_probe(int code, double *elapsed_ms, int *code_out);
 const uint8_t *launch_tc_expand(const float2 *Btri, int64_t n, int wc, DevBuf<uint8_t> &img, cudaStream_t st);
 // ---- packed tensor-core launches (several problems in one persistent launch) ----
 // One problem as the host describes it: the boundary operator of one mesh

@@ -1371,7 +1371,45 @@ bool tc_pack_flags(int code, cudaStream_t st, const TcPlan &plan, int *err)
         default: return false;
     }
 }
+
+// One warp waits, through the kernel's own bounded waits, on an mbarrier that
+// nothing arrives on: the wait gives up after kWaitNs and writes `code` to
+// the error word, as a pipeline wait of the tensor-core kernel does.
+__global__ void bounded_wait_probe_kernel(int *err, unsigned long long *ns, int code)
+{
+    __shared__ uint64_t bar;
+    __shared__ int abort_flag;
+    if (threadIdx.x == 0)
+    {
+        mbar_init(&bar, 1);
+        abort_flag = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    const uint64_t t0 = global_ns();
+    const bool got = warp_wait(&bar, 0u, &abort_flag, err, code);
+    if (threadIdx.x == 0) ns[0] = got ? 0ull : global_ns() - t0;
+}
 } // namespace
+
+void tc_bounded_wait_probe(int code, double *elapsed_ms, int *code_out)
+{
+    DevBuf<int> err;
+    DevBuf<unsigned long long> ns;
+    err.reserve(1);
+    ns.reserve(1);
+    BAEMM_CUDA(cudaMemset(err.p, 0, sizeof(int)));
+    BAEMM_CUDA(cudaMemset(ns.p, 0, sizeof(unsigned long long)));
+    bounded_wait_probe_kernel<<<1, 32>>>(err.p, ns.p, code);
+    BAEMM_LAUNCH_CHECK();
+    BAEMM_CUDA(cudaDeviceSynchronize());
+    int e = 0;
+    unsigned long long t = 0;
+    BAEMM_CUDA(cudaMemcpy(&e, err.p, sizeof(int), cudaMemcpyDeviceToHost));
+    BAEMM_CUDA(cudaMemcpy(&t, ns.p, sizeof(t), cudaMemcpyDeviceToHost));
+    *code_out = e;
+    *elapsed_ms = (double)t * 1e-6;
+}
 
 TcPackScratch::~TcPackScratch()
 {

@@ -328,6 +328,15 @@ void baemm_packer_destroy(baemm_packer *packer);
 int baemm_set_packer(baemm_ctx *ctx, baemm_packer *packer);   /* NULL detaches */
 int baemm_packer_stats(const baemm_packer *packer, int64_t *launches, int64_t *problems);
 
+/* Self-test of the tensor-core kernel's bounded pipeline waits (no reference
+ * counterpart): one warp on `device` waits on an mbarrier that nothing
+ * arrives on, through the same wait code as the kernel's pipeline stages.
+ * The wait gives up after its bound (200 ms of device time); *code receives
+ * the error code it wrote (99) and *elapsed_ms the time until it gave up.
+ * Faults, traps and hangs nothing; the device stays usable.  Errors: message
+ * in baemm_last_error(NULL). */
+int baemm_selftest_bounded_wait(int device, double *elapsed_ms, int *code);
+
 /* The dense stage alone, the device counterpart of the reference's private
  * BoundaryOperatorKernel() (BoundaryOperatorKernel.hpp:5-28, kernel
  * BoundaryOperatorKernel.cl:5-239; no public counterpart): on device
