@@ -953,6 +953,52 @@ def run_serve_workload(args):
 # ---------------------------------------------------------------------------
 # the Gauss-Newton workload (--workload gauss-newton): not the headline line
 # ---------------------------------------------------------------------------
+def run_sizes_workload(args):
+    """The boundary apply's dense stage against mesh size (not the headline
+    line): icosphere levels 3-7 (1280 to 327680 triangles), 64 RHS = kappa
+    {2, 4, 8, 16} x 16, SL + DL of the mixed BIE; the tensor-core and the
+    plain FP32 form, each autotuned for the size first.  Dense-kernel time =
+    median of 5 applies after one (CUDA events of the library's profiling;
+    L2 not flushed: the smaller meshes are L2-resident, as they are inside a
+    solve)."""
+    from baemm_b200 import APPLY_FP32, APPLY_TC, Helmholtz_CUDA, meshes
+    import torch
+    levels = [int(v) for v in args.size_levels.split(",")]
+    rows = []
+    for level in levels:
+        coords, tris = meshes.icosphere(level)
+        nt = int(tris.shape[0])
+        H = Helmholtz_CUDA(coords, tris, np.eye(3))
+        H.SetProfiling(True)
+        H.LoadBoundaryOperators_PL(KAPPA, coefficients(KAPPA), WC, WCS)
+        rng = np.random.default_rng(0)
+        B = (rng.standard_normal((coords.shape[0], WC)) + 1j * rng.standard_normal((coords.shape[0], WC))).astype(
+            np.complex64)
+        Bd = torch.from_numpy(B).cuda()
+        Cd = torch.zeros_like(Bd)
+        row = {"level": level, "triangles": nt, "interactions": nt * nt * WC}
+        for name, mode in (("tc", APPLY_TC), ("fp32", APPLY_FP32)):
+            H.SetApplyMode(mode)
+            tr = H.Autotune(mode, repeats=2)
+            ts = []
+            for _ in range(6):
+                H.ApplyBoundaryOperators_PL(1.0, Bd, 0.0, Cd)
+                ts.append(H.LastApplyTimes()[1])
+            ms = float(np.median(ts[1:]))
+            row[name] = {"dense_ms": ms, "GInteractions_s": nt * nt * WC / (ms * 1e-3) / 1e9,
+                         "tuned": {k: tr[k] for k in ("dense_variant", "tc_gen_warps", "tc_chunks", "tc_segment")}}
+        row["speedup_tc_vs_fp32"] = row["fp32"]["dense_ms"] / row["tc"]["dense_ms"]
+        rows.append(row)
+        H.close()
+    line = {"metric": "dense-stage GInteractions/s vs mesh size", "unit": "GInteractions/s", "n_gpus": 1,
+            "higher_is_better": True, "data": "synthetic",
+            "config": {"workload": "icosphere levels " + ",".join(map(str, levels)) + ", 64 RHS = kappa {2,4,8,16} x "
+                                   "16, SL+DL of the mixed BIE, each form autotuned per size"},
+            "sizes": rows}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def run_gn_workload(args):
     """One Gauss-Newton shape step (GaussNewtonSolve, FarField.hpp:457-604) on
     the configuration: initial shape the icosphere level 5 (10242 V, 20480 T),
@@ -1036,7 +1082,7 @@ def main(argv=None):
                     help="apply arithmetic: plain FP32, compensated tensor-core (default), FP64")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-compare", action="store_true", help="skip the plain-FP32 and FP64 comparison applies")
-    ap.add_argument("--workload", default="apply", choices=["apply", "nearfield", "solve", "serve", "gauss-newton"],
+    ap.add_argument("--workload", default="apply", choices=["apply", "nearfield", "solve", "serve", "gauss-newton", "apply-sizes"],
                     help="apply: the headline operator-apply line; solve: the scattering-solve configuration; "
                          "serve: the request stream through the serving loop")
     ap.add_argument("--requests", type=int, default=100, help="requests of --workload serve")
@@ -1053,6 +1099,7 @@ def main(argv=None):
     ap.add_argument("--seq-sample", type=int, default=0,
                     help="--workload serve: run the sequential baseline on the first N requests only (0: all)")
     ap.add_argument("--gn-level", type=int, default=5, help="icosphere level of --workload gauss-newton")
+    ap.add_argument("--size-levels", default="3,4,5,6,7", help="icosphere levels of --workload apply-sizes")
     ap.add_argument("--solve-level", type=int, default=6, help="icosphere level of --workload solve")
     ap.add_argument("--solve-modes", default="fp64,fp32,tc,tc_ir",
                     help="--workload solve: the runs to make (fp64 is the error reference; without it the errors "
@@ -1074,6 +1121,8 @@ def main(argv=None):
         return run_serve_workload(args) if rank == 0 else 0
     if args.workload == "gauss-newton":
         return run_gn_workload(args) if rank == 0 else 0
+    if args.workload == "apply-sizes":
+        return run_sizes_workload(args) if rank == 0 else 0
     if world > 1:
         import datetime
 
