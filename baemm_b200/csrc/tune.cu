@@ -101,13 +101,24 @@ void Ctx::autotune(int mode, int repeats, baemm_tune_result *out)
         g_tune_cv.notify_all();
     };
 
-    const size_t elems = (size_t)mesh.nt * (size_t)wave_count;
-    float2 *Bt = Btri_f.reserve(elems), *Ct = Ctri_f.reserve(elems);
-    BAEMM_CUDA(cudaMemsetAsync(Bt, 0x3c, elems * sizeof(float2), stream));   // every float 0.0115
-
+    // from here on every exit releases the key (the set-up below can throw too)
+    float2 *Bt = nullptr, *Ct = nullptr;
     cudaEvent_t e0 = nullptr, e1 = nullptr;
-    BAEMM_CUDA(cudaEventCreate(&e0));
-    BAEMM_CUDA(cudaEventCreate(&e1));
+    try
+    {
+        const size_t elems = (size_t)mesh.nt * (size_t)wave_count;
+        Bt = Btri_f.reserve(elems);
+        Ct = Ctri_f.reserve(elems);
+        BAEMM_CUDA(cudaMemsetAsync(Bt, 0x3c, elems * sizeof(float2), stream));   // every float 0.0115
+        BAEMM_CUDA(cudaEventCreate(&e0));
+        BAEMM_CUDA(cudaEventCreate(&e1));
+    }
+    catch (...)
+    {
+        if (e0) cudaEventDestroy(e0);
+        release(nullptr);
+        throw;
+    }
     const int saved_mode = apply_mode, saved_variant = dense_variant;
     const TcTuning saved_tc = tc_tune;
     auto time_current = [&]() {
