@@ -151,6 +151,7 @@ SIGNATURES = {
     "baemm_set_packer": (I, [vp, vp]),
     "baemm_packer_stats": (I, [vp, i64p, i64p]),
     "baemm_selftest_bounded_wait": (I, [I, dp, i32p]),
+    "baemm_profile_cg": (I, [vp, I, I, dp]),
     "baemm_last_apply_times": (I, [vp, fp]),
     "baemm_kernel_launch_count": (I64, []),
     "baemm_free": (None, [vp]),

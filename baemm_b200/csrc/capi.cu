@@ -728,6 +728,36 @@ int baemm_profile_krylov(baemm_ctx *ctx, int columns, int iterations, int basis,
     });
 }
 
+int baemm_profile_cg(baemm_ctx *ctx, int columns, int iterations, double out[3])
+{
+    return guarded(ctx, [&](Ctx &c) {
+        BAEMM_REQUIRE(out, BAEMM_ERR_ARG, "null output");
+        BAEMM_REQUIRE(columns >= 1 && 2 * columns <= baemm::kMaxKrylovColumns && iterations >= 1, BAEMM_ERR_ARG,
+                      "profile_cg: sizes out of range");
+        const bool v64 = c.mass_values_fp64();
+        const int rc = 2 * columns;   // complex columns as interleaved real columns (ApplyMassInverse.hpp:71-98)
+        baemm::CgSolver cg;
+        const double n = (double)c.mesh.nv, nnz = (double)c.mass_inner_h.size(), vs = v64 ? 8.0 : 4.0;
+        const double vec = n * rc * 8.0;
+        // algorithmic bytes of one iteration: the matvec (CSR, p gathered once, q written), the update
+        // (L; x, p, r, q read; x, r, z written) and the p update (z, p read; p written)
+        out[1] = (n + 1) * 4 + nnz * (4 + vs) + 2 * vec + n * vs + 7 * vec + 3 * vec;
+        const double blk = cg.profile_block(c.mesh, v64, rc, iterations, c.stream);
+        if (blk > 0.0)
+        {
+            out[0] = blk;
+            out[2] = 1.0;
+        }
+        else
+        {
+            double ms[3];
+            cg.profile(c.mesh, v64, rc, iterations, c.stream, ms);
+            out[0] = ms[0] + ms[1] + ms[2];
+            out[2] = 0.0;
+        }
+    });
+}
+
 int baemm_boundary_operator_kernel_dev_c(baemm_ctx *ctx, const float *B_tri, float *C_tri, int64_t row_begin,
                                          int64_t row_end)
 {

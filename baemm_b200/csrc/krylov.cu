@@ -393,6 +393,138 @@ __global__ void cg_pupdate_kernel(int64_t total, int c, const double *__restrict
     p[e] = z[e] + col[3 * c + k] * p[e];
 }
 
+// CG mass inverse on meshes of up to kCgBlockMaxRows vertices: one block per
+// column, every iteration in one launch.  The CG's columns are independent
+// (each has its own dot products and step lengths), so a block that owns a
+// column needs no other block: the phases of an iteration are separated by
+// __syncthreads only, and the 3 launches and 3 cross-block column sums of
+// an iteration of the multi-block kernels become block sums.  The block's
+// vectors are column-major in global memory (column k at x + k n),
+// L2-resident at these sizes.  Same steps and stopping rule as the
+// multi-block kernels (ApplyMassInverse.hpp:48-156): x = 0, r = b, z = L r,
+// p = z; per iteration q = M p, alpha = <r,z> / <p,q>, x += alpha p,
+// r -= alpha q, z = L r, beta = <r,z>_new / <r,z>, converged once
+// ||r|| <= tol ||b|| (a column of zeros at once), p = z + beta p.  Block sums
+// add the threads' row-ordered partials by a fixed shuffle and shared-memory
+// tree, so runs are reproducible.  flags: [0] columns not converged, [1] the
+// largest iteration count (both zeroed before the launch), [2 + k] column k
+// converged.
+constexpr int kCgBlockThreads = 1024;
+// Up to this many rows one block per column is faster: on the icosphere of
+// level 5 (10242 vertices, 128 real columns) one iteration takes 29.8 us
+// against 60.3 us for the three multi-block kernels; on level 6 (40962
+// vertices, 64 columns) 130 us against 92 us, too few blocks for the rows.
+constexpr int64_t kCgBlockMaxRows = 16384;
+
+// totals of a and b over the block, in every thread (red: 2 x 33 doubles)
+__device__ __forceinline__ void block_sum2(double &a, double &b, double *red)
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    #pragma unroll
+    for (int o = 16; o > 0; o >>= 1)
+    {
+        a += __shfl_down_sync(0xffffffffu, a, o);
+        b += __shfl_down_sync(0xffffffffu, b, o);
+    }
+    __syncthreads();   // red is free (its previous totals have been read)
+    if (lane == 0) { red[warp] = a; red[33 + warp] = b; }
+    __syncthreads();
+    if (warp == 0)
+    {
+        double ta = lane < nw ? red[lane] : 0.0, tb = lane < nw ? red[33 + lane] : 0.0;
+        #pragma unroll
+        for (int o = 16; o > 0; o >>= 1)
+        {
+            ta += __shfl_down_sync(0xffffffffu, ta, o);
+            tb += __shfl_down_sync(0xffffffffu, tb, o);
+        }
+        if (lane == 0) { red[32] = ta; red[65] = tb; }
+    }
+    __syncthreads();
+    a = red[32];
+    b = red[65];
+}
+
+template <class RV>
+__global__ void __launch_bounds__(kCgBlockThreads)
+cg_block_kernel(int64_t n, int c, const double *__restrict__ b, int64_t ldb, const int32_t *__restrict__ mo,
+                const int32_t *__restrict__ mi, const RV *__restrict__ mv, const RV *__restrict__ L, double *xs,
+                double *rs, double *zs, double *ps, double *qs, double *__restrict__ y, int64_t ldy, int *flags,
+                double tol, int max_iter)
+{
+    __shared__ double red[66];
+    const int k = blockIdx.x;
+    const int64_t off = (int64_t)k * n;
+    double *x = xs + off, *r = rs + off, *z = zs + off, *p = ps + off, *q = qs + off;
+    double rz = 0.0, bb = 0.0;
+    for (int64_t row = threadIdx.x; row < n; row += blockDim.x)
+    {
+        const double bv = b[row * ldb + k];
+        const double zv = (double)L[row] * bv;
+        x[row] = 0.0; r[row] = bv; z[row] = zv; p[row] = zv;
+        rz += bv * zv;
+        bb += bv * bv;
+    }
+    block_sum2(rz, bb, red);   // ends with a barrier: p is complete
+    const double bn = sqrt(bb);
+    bool conv = bn <= tol * bn;
+    int it = 0;
+    for (; it < max_iter && !conv; ++it)   // conv and it are block-uniform
+    {
+        double pq = 0.0, unused = 0.0;
+        for (int64_t row = threadIdx.x; row < n; row += blockDim.x)
+        {
+            // the row's first 8 entries (1 + the vertex degree, ~7) loaded before their gathers
+            constexpr int kPf = 8;
+            const int32_t e0 = mo[row], e1 = mo[row + 1];
+            int32_t ci[kPf];
+            double cv[kPf], pv[kPf];
+            #pragma unroll
+            for (int j = 0; j < kPf; ++j)
+            {
+                const bool in = e0 + j < e1;
+                ci[j] = in ? mi[e0 + j] : 0;
+                cv[j] = in ? (double)mv[e0 + j] : 0.0;
+            }
+            #pragma unroll
+            for (int j = 0; j < kPf; ++j) pv[j] = e0 + j < e1 ? p[ci[j]] : 0.0;
+            double sacc = 0.0;
+            #pragma unroll
+            for (int j = 0; j < kPf; ++j)
+                if (e0 + j < e1) sacc += cv[j] * pv[j];
+            for (int32_t e = e0 + kPf; e < e1; ++e) sacc += (double)mv[e] * p[mi[e]];
+            q[row] = sacc;
+            pq += p[row] * sacc;
+        }
+        block_sum2(pq, unused, red);
+        const double alpha = pq == 0.0 ? 0.0 : rz / pq;
+        double rzn = 0.0, rr = 0.0;
+        for (int64_t row = threadIdx.x; row < n; row += blockDim.x)
+        {
+            x[row] += alpha * p[row];
+            const double rv = r[row] - alpha * q[row];
+            r[row] = rv;
+            const double zv = (double)L[row] * rv;
+            z[row] = zv;
+            rzn += rv * zv;
+            rr += rv * rv;
+        }
+        block_sum2(rzn, rr, red);
+        const double beta = rz == 0.0 ? 0.0 : rzn / rz;
+        rz = rzn;
+        conv = sqrt(rr) <= tol * bn;
+        for (int64_t row = threadIdx.x; row < n; row += blockDim.x) p[row] = z[row] + beta * p[row];
+        __syncthreads();   // p complete before the next iteration's gathers
+    }
+    for (int64_t row = threadIdx.x; row < n; row += blockDim.x) y[row * ldy + k] = x[row];
+    if (threadIdx.x == 0)
+    {
+        flags[2 + k] = conv ? 1 : 0;
+        if (!conv) atomicAdd(&flags[0], 1);
+        atomicMax(&flags[1], it);
+    }
+}
+
 __global__ void cg_output_kernel(int64_t n, int c, const double *__restrict__ x, double *__restrict__ y, int64_t ldy)
 {
     const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -679,7 +811,8 @@ bool CgSolver::finish(cudaStream_t st, int *iterations)
 {
     BAEMM_CUDA(cudaStreamSynchronize(st));
     if (iterations) *iterations = host_flags_[1];
-    return host_flags_[0] != 0;
+    // flags[0]: all converged (multi-block kernels) or columns not converged (cg_block_kernel)
+    return block_path_ ? host_flags_[0] == 0 : host_flags_[0] != 0;
 }
 
 void CgSolver::reserve_totals(int nblk, int S, cudaStream_t st)
@@ -703,9 +836,24 @@ void CgSolver::enqueue_mass(const MeshDev &m, bool fp64_values, const double *b,
     x_.reserve(N); r_.reserve(N); z_.reserve(N); p_.reserve(N); q_.reserve(N);
     col_.reserve(4 * (size_t)c);
     flags_.reserve(2 + (size_t)c);
+    if (!host_flags_) BAEMM_CUDA(cudaMallocHost(&host_flags_, 2 * sizeof(int)));
+    block_path_ = n <= kCgBlockMaxRows;
+    if (block_path_)
+    {
+        // one block per column, all iterations in one launch
+        BAEMM_CUDA(cudaMemsetAsync(flags_.p, 0, 2 * sizeof(int), st));
+        auto runb = [&](auto Lv, auto Mv) {
+            cg_block_kernel<<<c, kCgBlockThreads, 0, st>>>(n, c, b, ldb, m.mass_outer, m.mass_inner, Mv, Lv, x_.p,
+                                                           r_.p, z_.p, p_.p, q_.p, y, ldy, flags_.p, tol, max_iter);
+        };
+        if (fp64_values) runb(m.lumped_d.p, m.mass_d.p);
+        else runb(m.lumped_f.p, m.mass_f.p);
+        BAEMM_LAUNCH_CHECK();
+        BAEMM_CUDA(cudaMemcpyAsync(host_flags_, flags_.p, 2 * sizeof(int), cudaMemcpyDeviceToHost, st));
+        return;
+    }
     const Layout L = make_layout(n, c);
     reserve_totals(L.nblk, 2 * c, st);
-    if (!host_flags_) BAEMM_CUDA(cudaMallocHost(&host_flags_, 2 * sizeof(int)));
     dim3 grid(L.nblk, L.nchunk);
     auto run = [&](auto Lv, auto Mv) {
         // three launches per iteration: each column-sum step runs in the last
@@ -727,6 +875,45 @@ void CgSolver::enqueue_mass(const MeshDev &m, bool fp64_values, const double *b,
     cg_output_kernel<<<eg(N), 256, 0, st>>>(n, c, x_.p, y, ldy);
     BAEMM_LAUNCH_CHECK();
     BAEMM_CUDA(cudaMemcpyAsync(host_flags_, flags_.p, 2 * sizeof(int), cudaMemcpyDeviceToHost, st));
+}
+
+double CgSolver::profile_block(const MeshDev &m, bool fp64_values, int c, int iterations, cudaStream_t st)
+{
+    const int64_t n = m.nv;
+    BAEMM_REQUIRE(c >= 1 && c <= kMaxKrylovColumns, BAEMM_ERR_SIZE, "CG column count out of range");
+    BAEMM_REQUIRE(iterations >= 1, BAEMM_ERR_ARG, "at least one iteration");
+    if (n > kCgBlockMaxRows) return 0.0;
+    const int64_t N = n * c;
+    DevBuf<double> b, y;
+    b.reserve(N);
+    y.reserve(N);
+    std::vector<double> ones((size_t)N, 1.0);
+    BAEMM_CUDA(cudaMemcpyAsync(b.p, ones.data(), N * sizeof(double), cudaMemcpyHostToDevice, st));
+    x_.reserve(N); r_.reserve(N); z_.reserve(N); p_.reserve(N); q_.reserve(N);
+    flags_.reserve(2 + (size_t)c);
+    cudaEvent_t e0, e1;
+    BAEMM_CUDA(cudaEventCreate(&e0));
+    BAEMM_CUDA(cudaEventCreate(&e1));
+    float ms = 0.f;
+    auto runb = [&](auto Lv, auto Mv) {
+        // tol < 0: no column converges, every iteration does its work; a first launch warms up
+        for (int rep = 0; rep < 2; ++rep)
+        {
+            BAEMM_CUDA(cudaMemsetAsync(flags_.p, 0, 2 * sizeof(int), st));
+            BAEMM_CUDA(cudaEventRecord(e0, st));
+            cg_block_kernel<<<c, kCgBlockThreads, 0, st>>>(n, c, b.p, c, m.mass_outer, m.mass_inner, Mv, Lv, x_.p,
+                                                           r_.p, z_.p, p_.p, q_.p, y.p, c, flags_.p, -1.0, iterations);
+            BAEMM_CUDA(cudaEventRecord(e1, st));
+        }
+    };
+    if (fp64_values) runb(m.lumped_d.p, m.mass_d.p);
+    else runb(m.lumped_f.p, m.mass_f.p);
+    BAEMM_LAUNCH_CHECK();
+    BAEMM_CUDA(cudaEventSynchronize(e1));
+    BAEMM_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    return (double)ms / iterations;
 }
 
 void CgSolver::profile(const MeshDev &m, bool fp64_values, int c, int iterations, cudaStream_t st, double ms_out[3])

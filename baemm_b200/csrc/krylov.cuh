@@ -44,6 +44,10 @@ public:
     // no column allowed to converge), each launch bracketed by CUDA events.
     // ms_out: mean ms per launch of {matvec, update, p update}.
     void profile(const MeshDev &m, bool fp64_values, int c, int iterations, cudaStream_t st, double ms_out[3]);
+    // Device time per iteration of cg_block_kernel (the path of meshes of up
+    // to 16384 vertices) on c real columns, `iterations` iterations, no column
+    // allowed to converge; 0 on larger meshes.
+    double profile_block(const MeshDev &m, bool fp64_values, int c, int iterations, cudaStream_t st);
 
 private:
     // partial_: per-block partial sums, group rows and totals of the
@@ -54,6 +58,7 @@ private:
     DevBuf<int> flags_;
     DevBuf<unsigned int> counter_;
     int *host_flags_ = nullptr;
+    bool block_path_ = false;   // the last enqueue_mass ran cg_block_kernel (small meshes)
 };
 
 // Device time of one classical Gram-Schmidt pass of a GMRES iteration on an

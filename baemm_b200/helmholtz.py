@@ -506,13 +506,23 @@ class Helmholtz_CUDA:
         counterpart): the CG mass inverse on 2 * columns real columns and one
         Gram-Schmidt pass of a GMRES iteration on `columns` complex columns
         against `basis` vectors.  Per kernel: ms per launch, algorithmic bytes
-        per launch and the rate (GB/s)."""
+        per launch and the rate (GB/s); `cg_iteration`: one whole CG iteration
+        on the path this mesh's solves take."""
         out = np.zeros(10)
         self._ck(self._lib.baemm_profile_krylov(self._h, int(columns), int(iterations), int(basis), _dp(out)))
         names = ("cg_matvec", "cg_update", "cg_pupdate", "gs_dot", "gs_update")
-        return {n: {"ms": float(out[q]), "algorithmic_bytes": float(out[5 + q]),
-                    "GB_s": float(out[5 + q] / (out[q] * 1e-3) / 1e9) if out[q] > 0 else None}
-                for q, n in enumerate(names)}
+        res = {n: {"ms": float(out[q]), "algorithmic_bytes": float(out[5 + q]),
+                   "GB_s": float(out[5 + q] / (out[q] * 1e-3) / 1e9) if out[q] > 0 else None}
+               for q, n in enumerate(names)}
+        # one CG iteration on the path this mesh's solves take (baemm_profile_cg): on meshes of up to
+        # 16384 vertices one block per column runs every iteration in one launch, so the three kernels
+        # above are not what the solver runs there
+        cg = np.zeros(3)
+        self._ck(self._lib.baemm_profile_cg(self._h, int(columns), int(iterations), _dp(cg)))
+        res["cg_iteration"] = {"ms": float(cg[0]), "algorithmic_bytes": float(cg[1]),
+                               "GB_s": float(cg[1] / (cg[0] * 1e-3) / 1e9) if cg[0] > 0 else None,
+                               "one_launch_path": bool(cg[2])}
+        return res
 
     def BoundaryOperatorKernel(self, B_tri, C_tri, row_begin=0, row_end=None):
         """The dense stage alone on torch CUDA triangle blocks (simplex_count x

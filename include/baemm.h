@@ -337,6 +337,16 @@ int baemm_packer_stats(const baemm_packer *packer, int64_t *launches, int64_t *p
  * in baemm_last_error(NULL). */
 int baemm_selftest_bounded_wait(int device, double *elapsed_ms, int *code);
 
+/* Device time of one CG iteration of the mass inverse on this context's mesh,
+ * on the path its solves take (no reference counterpart): 2 * columns real
+ * columns (columns complex), `iterations` iterations with no column allowed
+ * to converge.  out[0] = ms per iteration, out[1] = algorithmic bytes of one
+ * iteration (matvec, update and p update), out[2] = 1 when the mesh (at most
+ * 16384 vertices) takes the one-launch path (one block per column, every
+ * iteration in one launch), 0 for the three-launches-per-iteration kernels
+ * of larger meshes. */
+int baemm_profile_cg(baemm_ctx *ctx, int columns, int iterations, double out[3]);
+
 /* The dense stage alone, the device counterpart of the reference's private
  * BoundaryOperatorKernel() (BoundaryOperatorKernel.hpp:5-28, kernel
  * BoundaryOperatorKernel.cl:5-239; no public counterpart): on device

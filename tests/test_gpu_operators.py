@@ -502,10 +502,10 @@ def test_mass_inverse_and_lumped(env, mode):
 @pytest.mark.parametrize("ncols,cplx", [(1, False), (31, False), (33, False), (100, False), (1024, False),
                                         (512, True)])
 def test_mass_inverse_column_counts(env, ncols, cplx):
-    """FP64 CG on 1 ... 1024 real columns (512 complex = 1024 real): the
-    finalizers give each column one warp of a block of at most 1024 threads,
-    so above 32 columns each warp takes several.  Column 0 is zero and
-    converges at once while the others iterate."""
+    """FP64 CG on 1 ... 1024 real columns (512 complex = 1024 real) on the
+    642-vertex mesh, which takes the one-launch path (one block per column,
+    every iteration in one launch).  Column 0 is zero and converges at once
+    while the others iterate."""
     coords, tris, meas, H, o32, o64 = env
     rng = np.random.default_rng(40 + ncols)
     nv = coords.shape[0]
@@ -518,6 +518,38 @@ def test_mass_inverse_column_counts(env, ncols, cplx):
     finally:
         H.SetApplyMode(APPLY_FP32)
     o64.ApplyMassInverse(X, Yo, 1e-10)
+    assert np.all(Yg[:, 0] == 0)
+    assert relerr(Yg, Yo) < 1e-11
+
+
+def test_mass_inverse_small_mesh_takes_one_launch_path(env):
+    """The 642-vertex test mesh's CG runs one block per column in one launch
+    (the path the column-count tests above check against the oracle)."""
+    coords, tris, meas, H, o32, o64 = env
+    prof = H.ProfileKrylov(2, 2, 2)
+    assert prof["cg_iteration"]["one_launch_path"]
+    assert prof["cg_iteration"]["ms"] > 0
+
+
+@pytest.mark.parametrize("ncols,cplx", [(3, False), (40, True)])
+def test_mass_inverse_multi_block_path(ncols, cplx):
+    """The CG mass inverse on a mesh above the one-launch path's 16384
+    vertices (icosphere level 6, 40962): the three-launches-per-iteration
+    kernels with two-level column sums, against the FP64 oracle; column 0 is
+    zero and converges at once."""
+    from oracle import oracle as O
+    coords, tris = meshes.icosphere(6)
+    rng = np.random.default_rng(60 + ncols)
+    nv = coords.shape[0]
+    X = crandn(rng, nv, ncols) if cplx else rng.standard_normal((nv, ncols))
+    X[:, 0] = 0
+    Yg, Yo = np.zeros_like(X), np.zeros_like(X)
+    with Helmholtz_CUDA(coords, tris, np.eye(3)) as H:
+        H.SetApplyMode(APPLY_FP64)
+        H.ApplyMassInverse(X, Yg, 1e-10)
+        prof = H.ProfileKrylov(4, 2, 2)
+    O.Oracle(coords, tris, np.eye(3), precision=64).ApplyMassInverse(X, Yo, 1e-10)
+    assert not prof["cg_iteration"]["one_launch_path"]
     assert np.all(Yg[:, 0] == 0)
     assert relerr(Yg, Yo) < 1e-11
 
