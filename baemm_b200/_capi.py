@@ -27,6 +27,7 @@ TUNE_TC_CTAS = 3
 TUNE_TC_STAGGER = 4
 TUNE_TC_GEN_WARPS = 5
 TUNE_TC_CHUNKS = 6
+TUNE_TC_SHARE = 7
 
 dp = C.POINTER(C.c_double)
 fp = C.POINTER(C.c_float)
@@ -96,6 +97,7 @@ SIGNATURES = {
     "baemm_graph_stats": (I, [vp, i64p, i64p]),
     "baemm_autotune": (I, [vp, I, I, C.POINTER(TuneResult)]),
     "baemm_get_tuning": (I, [vp, I]),
+    "baemm_tc_entry_sharing": (I, [vp]),
     "baemm_set_refinement": (I, [vp, I, D]),
     "baemm_get_areas": (I, [vp, fp]),
     "baemm_get_triangle_normals": (I, [vp, fp]),

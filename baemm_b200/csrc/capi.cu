@@ -475,6 +475,11 @@ int baemm_set_tuning(baemm_ctx *ctx, int key, int value)
                               "chunks per unit must be 0, 1, 2 or 4");
                 c.tc_tune.chunks = value;
                 break;
+            case BAEMM_TUNE_TC_SHARE:
+                BAEMM_REQUIRE(value == 1 || value == 2 || value == 4, BAEMM_ERR_ARG,
+                              "groups per shared entry set must be 1, 2 or 4");
+                c.tc_tune.share = value;
+                break;
             default: throw Error(BAEMM_ERR_ARG, "unknown tuning key");
         }
     });
@@ -488,7 +493,15 @@ int baemm_get_tuning(const baemm_ctx *ctx, int key)
     if (key == BAEMM_TUNE_TC_STAGGER) return ctx->impl->tc_tune.stagger;
     if (key == BAEMM_TUNE_TC_GEN_WARPS) return ctx->impl->tc_tune.gen_warps;
     if (key == BAEMM_TUNE_TC_CHUNKS) return ctx->impl->tc_tune.chunks;
+    if (key == BAEMM_TUNE_TC_SHARE) return ctx->impl->tc_tune.share;
     return -1;
+}
+int baemm_tc_entry_sharing(const baemm_ctx *ctx)
+{
+    if (!ctx || !ctx->impl) return BAEMM_ERR_ARG;
+    const baemm::Ctx &c = *ctx->impl;
+    if (!c.operators_loaded) return BAEMM_ERR_NOT_LOADED;
+    return baemm::tc_entry_sharing(c.flags, c.tc_form, c.wave_count, c.tc_tune);
 }
 int baemm_get_apply_mode(const baemm_ctx *ctx) { return (ctx && ctx->impl) ? ctx->impl->apply_mode : -1; }
 int baemm_set_refinement(baemm_ctx *ctx, int max_steps, double inner_tol)

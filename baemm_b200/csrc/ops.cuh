@@ -139,6 +139,7 @@ struct TcCoeffForm
 {
     bool ki = false;
     float s = 0.f;
+    int share = 1;   // KI form: groups per aligned block with one wavenumber (1, 2 or 4)
 };
 TcCoeffForm tc_coeff_form(const ChunkParamsF *host_params, int groups);
 // Settings of the tensor-core form (the autotuner's search space):
@@ -155,9 +156,14 @@ struct TcTuning
     int stagger = 0;
     int gen_warps = 16;
     int chunks = 0;
+    int share = 4;   // most groups of 16 columns sharing one evaluation of the kernel entries (1, 2 or 4)
 };
 // The chunk groups per work unit a launch uses for wave_count wc and the setting `chunks`.
 int tc_chunks_per_unit(int wc, int chunks);
+// The groups per entry set a launch uses: groups with one wavenumber share the
+// kernel entries in the KI form of the mixed BIE / DtN operators, up to the
+// setting `share` and the chunk groups per work unit (packed launches use 1).
+int tc_entry_sharing(const OpFlags &f, const TcCoeffForm &form, int wc, const TcTuning &tune);
 void launch_boundary_tc(const MeshDev &m, const OpFlags &f, const void *chunk_params, const TcCoeffForm &form, int wc,
                         int wcs, const float *tgeo, const float2 *Btri, float2 *Ctri, float2 *ws, size_t ws_elems,
                         DevBuf<uint8_t> &img, int *err, cudaStream_t st, const TcTuning &tune,

@@ -87,11 +87,13 @@ struct TcShape
 // registers); one issuer per chunk would make 21 (6, 80 registers: the
 // generators spill).  With 8 generator warps, 4 issuers measured slower than
 // 2 (128 instead of 168 registers for the generators).
-template <int GW, int CH>
-constexpr int tc_mma_warps() { return CH >= 2 ? 2 : 1; }
+// With R > 1 the R groups of an entry set share one A stage and one issuer,
+// so the issuers split the CH / R entry sets of a tile.
+template <int GW, int CH, int R>
+constexpr int tc_mma_warps() { return CH / R >= 2 ? 2 : 1; }
 // generators + the bulk-copy warp + the MMA issuers
-template <int GW, int CH>
-constexpr int tc_threads() { return 32 * GW + 32 + 32 * tc_mma_warps<GW, CH>(); }
+template <int GW, int CH, int R>
+constexpr int tc_threads() { return 32 * GW + 32 + 32 * tc_mma_warps<GW, CH, R>(); }
 constexpr int TC_BSTAGES = 4;      // B image stages in shared memory (bulk copies of the expanded images)
 constexpr int TC_RSTAGES = 6;      // tile geometry stages (bulk copies)
 constexpr uint32_t TC_TMEM_COLS = 512;
@@ -622,8 +624,16 @@ __device__ __forceinline__ void tc_entries_ki(const float2 *__restrict__ P, cons
 
 // RI, KI: see tc_entries and tc_entries_ki.  GW: generator warps (TcShape).
 // PACK: a packed launch over plan.probs (the pointer arguments are unused).
-template <int GW, int CH, bool SL, bool DL, bool ADL, bool RI, bool KI, bool PACK>
-__global__ void __launch_bounds__(tc_threads<GW, CH>(), 1)
+// R: groups of 16 columns that share one evaluation of the kernel entries (the
+// KI form, whose entries depend on a group only through its wavenumber, with
+// equal wavenumbers in every aligned block of R groups).  The CH groups of a
+// work unit are CH / R entry sets; per tile the generators evaluate each set
+// once into one A stage, and its issuer multiplies it with the R groups' B
+// images in one MMA of N = 64 R ([Bhi | Blo] of each group, which are
+// consecutive in the B stage and whose accumulators are consecutive in TMEM)
+// plus R correction MMAs Alo Bhi of N = 32.
+template <int GW, int CH, int R, bool SL, bool DL, bool ADL, bool RI, bool KI, bool PACK>
+__global__ void __launch_bounds__(tc_threads<GW, CH, R>(), 1)
 boundary_tc_kernel(const float *__restrict__ mid4, const float *__restrict__ nrm4, const TcTileGeo *__restrict__ tgeo,
                    const uint8_t *__restrict__ img, float2 *__restrict__ Ctri, float2 *__restrict__ ws,
                    const ChunkParamsF *__restrict__ prm, const TcPlan plan, int *err)
@@ -631,6 +641,8 @@ boundary_tc_kernel(const float *__restrict__ mid4, const float *__restrict__ nrm
     constexpr int TC_GEN_THREADS = TcShape<GW>::GEN_THREADS;
     constexpr int TC_SPT = TcShape<GW>::SPT, TC_PPT = TcShape<GW>::PPT, TC_KPT = TcShape<GW>::KPT;
     constexpr int TC_CPG = TcShape<GW>::CPG;
+    static_assert(R == 1 || (KI && !PACK && CH % R == 0), "shared entry sets need the KI form and R | CH");
+    constexpr int E = CH / R;   // entry sets per tile
     extern __shared__ __align__(1024) uint8_t smem_raw[];
     // Align inside the shared window by pointer arithmetic on the shared array,
     // so every access below compiles to a shared-memory instruction.
@@ -650,13 +662,13 @@ boundary_tc_kernel(const float *__restrict__ mid4, const float *__restrict__ nrm
     if (tid == 0)
     {
         for (int k = 0; k < tc_astages<CH>(); ++k) { mbar_init(&sm.a_full[k], TC_GEN_THREADS); mbar_init(&sm.a_empty[k], 1); }
-        for (int k = 0; k < TC_BSTAGES; ++k) { mbar_init(&sm.b_full[k], 1); mbar_init(&sm.b_empty[k], tc_mma_warps<GW, CH>()); }
+        for (int k = 0; k < TC_BSTAGES; ++k) { mbar_init(&sm.b_full[k], 1); mbar_init(&sm.b_empty[k], tc_mma_warps<GW, CH, R>()); }
         for (int k = 0; k < TC_RSTAGES; ++k)
         {
             mbar_init(&sm.r_full[k], 1);
             mbar_init(&sm.r_empty[k], TC_GEN_THREADS);
         }
-        mbar_init(&sm.seg_full, tc_mma_warps<GW, CH>());
+        mbar_init(&sm.seg_full, tc_mma_warps<GW, CH, R>());
         mbar_init(&sm.seg_empty, TC_GEN_THREADS);
         for (int k = 0; k < TC_CHMAX; ++k) mbar_init(&sm.mma_done[k], 1);
         sm.abort_flag = 0;
@@ -687,13 +699,12 @@ boundary_tc_kernel(const float *__restrict__ mid4, const float *__restrict__ nrm
     if (tid < TC_GEN_THREADS)
     {
         // ------------------------------ generators ------------------------------
-        // Per tile: the pair geometry (shared by every chunk), then per chunk
-        // (unrolled): its entries, the wait for this chunk's A stage, one
-        // 16-column TMEM store per K step the thread covers (hi | lo) and the
-        // stage's publication (with 8 warps deferred until the
-        // next chunk's entries are computed, so the stores land meanwhile).
-        // The ring index of chunk c of tile T is (T CH + c) mod AS, a
-        // compile-time column offset when CH == AS (4 chunks).
+        // Per tile: the pair geometry (shared by every chunk), then per entry
+        // set (unrolled; a set is R chunks): its entries, the wait for its A
+        // stage, one 16-column TMEM store per K step the thread covers
+        // (hi | lo) and the stage's publication (with 8 warps deferred until
+        // the next set's entries are computed, so the stores land meanwhile).
+        // The ring index of set e of tile T is (T E + e) mod AS.
         const int q = warp & 3, g = warp >> 2;
         const int row = q * 32 + lane;
         const uint32_t lane_addr = tbase + ((uint32_t)(q * 32) << 16);
@@ -835,16 +846,16 @@ boundary_tc_kernel(const float *__restrict__ mid4, const float *__restrict__ nrm
                     }
                 }
                 #pragma unroll
-                for (int c = 0; c < CH; ++c)
+                for (int e = 0; e < E; ++e)
                 {
                     uint32_t hi[TC_KPT], lo[TC_KPT];
-                    if (KI) tc_entries_ki<TC_PPT>(Pg + 8 * c, r, kux, knux, kv, hi, lo);
-                    else tc_entries<TC_PPT, SL, DL, ADL, RI>(Pg + 8 * c, rinv, r, dmu, dnu, hi, lo);
-                    const uint32_t u = (uint32_t)T * CH + c;
+                    if (KI) tc_entries_ki<TC_PPT>(Pg + 8 * (e * R), r, kux, knux, kv, hi, lo);
+                    else tc_entries<TC_PPT, SL, DL, ADL, RI>(Pg + 8 * e, rinv, r, dmu, dnu, hi, lo);
+                    const uint32_t u = (uint32_t)T * E + e;
                     const uint32_t stage = u % AS;
-                    // (8 warps) publish the previous chunk's stage now that its stores had this math to land
+                    // (8 warps) publish the previous set's stage now that its stores had this math to land
                     publish();
-                    // the stage is free once the MMAs that read it AS chunks ago completed
+                    // the stage is free once the MMAs that read it AS sets ago completed
                     if (!warp_wait(&sm.a_empty[stage], ((u / AS) & 1u) ^ 1u, abort_flag, err, 3))
                     {
                         ok = false;
@@ -864,7 +875,7 @@ boundary_tc_kernel(const float *__restrict__ mid4, const float *__restrict__ nrm
                     // 16 warps: publish at once, the issuers wait for it; the other three
                     // generator warps of the sub-partition cover the wait for the stores
                     if (GW == 16) publish();
-                    if (c == 0 && drain_due >= 0)
+                    if (e == 0 && drain_due >= 0)
                     {
                         publish();
                         if (!drain(drain_due, first_drain)) { ok = false; break; }
@@ -951,13 +962,14 @@ boundary_tc_kernel(const float *__restrict__ mid4, const float *__restrict__ nrm
     else
     {
         // ------------------------------ MMA issuers ------------------------------
-        // MW warps; warp w issues the MMAs of chunks w, w + MW, ... of every
-        // tile (their own accumulator columns and A stages), so the issue work
-        // is spread over SM sub-partitions instead of queueing behind the
-        // generator warps of one.  Each warp runs its loop warp-wide and waits;
-        // one elected lane issues.  B stages and the segment's end are
-        // released by a commit of every issuer (barrier counts MW).
-        constexpr int MW = tc_mma_warps<GW, CH>();
+        // MW warps; warp w issues the MMAs of entry sets w, w + MW, ... of
+        // every tile (their own accumulator columns and A stages), so the
+        // issue work is spread over SM sub-partitions instead of queueing
+        // behind the generator warps of one.  Each warp runs its loop
+        // warp-wide and waits; one elected lane issues.  B stages and the
+        // segment's end are released by a commit of every issuer (barrier
+        // counts MW).
+        constexpr int MW = tc_mma_warps<GW, CH, R>();
         constexpr int AS = tc_astages<CH>();
         const int w = warp - (TC_GEN_THREADS / 32 + 1);
         bool ok = true;
@@ -984,29 +996,33 @@ boundary_tc_kernel(const float *__restrict__ mid4, const float *__restrict__ nrm
                     if (!got) { ok = false; break; }
                 }
                 #pragma unroll
-                for (int k = 0; k < CH / MW; ++k)
+                for (int k = 0; k < E / MW; ++k)
                 {
-                    const int c = w + k * MW;
-                    const uint32_t u = (uint32_t)T * CH + c;
+                    const int e = w + k * MW, c0 = e * R;   // entry set e: chunks c0 .. c0 + R - 1
+                    const uint32_t u = (uint32_t)T * E + e;
                     const uint32_t stage = u % AS;
                     if (!warp_wait(&sm.a_full[stage], (u / AS) & 1u, abort_flag, err, 9)) { ok = false; break; }
                     tc_fence_after();
-                    const uint32_t d = tbase + (uint32_t)(c * TC_DCOLS);
+                    const uint32_t d = tbase + (uint32_t)(c0 * TC_DCOLS);
                     const uint32_t a_hi = tbase + (uint32_t)(CH * TC_DCOLS) + stage * 64u;
                     const uint32_t a_lo = a_hi + 8u;
-                    // the hi image's 32 rows are followed by the lo image's 32 rows
-                    // (same 1024-byte group stride): one N = 64 operand [Bhi | Blo]
-                    const uint64_t b_hilo = desc0 + (uint64_t)(((b * TC_CHMAX + c) * TC_GROUP_BYTES) >> 4);
+                    // the hi image's 32 rows are followed by the lo image's 32 rows and
+                    // by the next chunk's images (same 1024-byte group stride): one
+                    // N = 64 R operand [Bhi | Blo] per chunk of the set
+                    const uint64_t b_hilo = desc0 + (uint64_t)(((b * TC_CHMAX + c0) * TC_GROUP_BYTES) >> 4);
                     if (elect_one())
                     {
                         #pragma unroll
                         for (int ks = 0; ks < 4; ++ks)
                         {
                             const uint64_t koff = (uint64_t)(ks * 32 >> 4);
-                            // [main | corr] (+)= Ahi [Bhi | Blo];  corr += Alo Bhi
+                            // per chunk [main | corr] (+)= Ahi [Bhi | Blo];  corr += Alo Bhi
                             mma_tf32(d, a_hi + 16u * ks, b_hilo + koff, (!first || ks > 0) ? 1u : 0u,
-                                     idesc_tf32(2 * TC_N));
-                            mma_tf32(d + (uint32_t)TC_N, a_lo + 16u * ks, b_hilo + koff, 1u, idesc_tf32(TC_N));
+                                     idesc_tf32(2 * TC_N * R));
+                            #pragma unroll
+                            for (int q = 0; q < R; ++q)
+                                mma_tf32(d + (uint32_t)(q * TC_DCOLS + TC_N), a_lo + 16u * ks,
+                                         b_hilo + (uint64_t)((q * TC_GROUP_BYTES) >> 4) + koff, 1u, idesc_tf32(TC_N));
                         }
                         mma_commit(&sm.a_empty[stage]);
                     }
@@ -1144,7 +1160,7 @@ __global__ void tc_fixup_kernel(const float2 *__restrict__ ws, float2 *__restric
     }
 }
 
-template <int GW, int CH, bool SL, bool DL, bool ADL, bool RI, bool KI, bool PACK = false>
+template <int GW, int CH, int R, bool SL, bool DL, bool ADL, bool RI, bool KI, bool PACK = false>
 void tc_launch(cudaStream_t st, const float *mid, const float *nrm, const TcTileGeo *tg, const uint8_t *B, float2 *C,
                float2 *ws, const ChunkParamsF *p, const TcPlan &plan, int *err)
 {
@@ -1161,12 +1177,12 @@ void tc_launch(cudaStream_t st, const float *mid, const float *nrm, const TcTile
         std::lock_guard<std::mutex> lock(mu);
         if (dev < 0 || dev >= 64 || !done[dev])
         {
-            BAEMM_CUDA(cudaFuncSetAttribute(boundary_tc_kernel<GW, CH, SL, DL, ADL, RI, KI, PACK>,
+            BAEMM_CUDA(cudaFuncSetAttribute(boundary_tc_kernel<GW, CH, R, SL, DL, ADL, RI, KI, PACK>,
                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
             if (dev >= 0 && dev < 64) done[dev] = true;
         }
     }
-    boundary_tc_kernel<GW, CH, SL, DL, ADL, RI, KI, PACK><<<plan.ctas, tc_threads<GW, CH>(), bytes, st>>>(
+    boundary_tc_kernel<GW, CH, R, SL, DL, ADL, RI, KI, PACK><<<plan.ctas, tc_threads<GW, CH, R>(), bytes, st>>>(
         mid, nrm, tg, B, C, ws, p, plan, err);
 }
 
@@ -1176,28 +1192,28 @@ void tc_flags(int code, cudaStream_t st, const float *mid, const float *nrm, con
 {
     switch (code)
     {
-        case 1: tc_launch<GW, CH, true, false, false, RI, false>(st, mid, nrm, tg, B, C, ws, p, plan, err); break;
-        case 2: tc_launch<GW, CH, false, true, false, RI, false>(st, mid, nrm, tg, B, C, ws, p, plan, err); break;
-        case 3: tc_launch<GW, CH, true, true, false, RI, false>(st, mid, nrm, tg, B, C, ws, p, plan, err); break;
-        case 4: tc_launch<GW, CH, false, false, true, RI, false>(st, mid, nrm, tg, B, C, ws, p, plan, err); break;
-        case 5: tc_launch<GW, CH, true, false, true, RI, false>(st, mid, nrm, tg, B, C, ws, p, plan, err); break;
-        case 6: tc_launch<GW, CH, false, true, true, RI, false>(st, mid, nrm, tg, B, C, ws, p, plan, err); break;
-        case 7: tc_launch<GW, CH, true, true, true, RI, false>(st, mid, nrm, tg, B, C, ws, p, plan, err); break;
+        case 1: tc_launch<GW, CH, 1, true, false, false, RI, false>(st, mid, nrm, tg, B, C, ws, p, plan, err); break;
+        case 2: tc_launch<GW, CH, 1, false, true, false, RI, false>(st, mid, nrm, tg, B, C, ws, p, plan, err); break;
+        case 3: tc_launch<GW, CH, 1, true, true, false, RI, false>(st, mid, nrm, tg, B, C, ws, p, plan, err); break;
+        case 4: tc_launch<GW, CH, 1, false, false, true, RI, false>(st, mid, nrm, tg, B, C, ws, p, plan, err); break;
+        case 5: tc_launch<GW, CH, 1, true, false, true, RI, false>(st, mid, nrm, tg, B, C, ws, p, plan, err); break;
+        case 6: tc_launch<GW, CH, 1, false, true, true, RI, false>(st, mid, nrm, tg, B, C, ws, p, plan, err); break;
+        case 7: tc_launch<GW, CH, 1, true, true, true, RI, false>(st, mid, nrm, tg, B, C, ws, p, plan, err); break;
         default: break;
     }
 }
 
 // The KI form for the operator combinations of the solves: the mixed BIE
 // (SL + DL), the DtN operator (SL + ADL) and all three layers.
-template <int GW, int CH>
+template <int GW, int CH, int R>
 bool tc_flags_ki(int code, cudaStream_t st, const float *mid, const float *nrm, const TcTileGeo *tg, const uint8_t *B,
                  float2 *C, float2 *ws, const ChunkParamsF *p, const TcPlan &plan, int *err)
 {
     switch (code)
     {
-        case 3: tc_launch<GW, CH, true, true, false, true, true>(st, mid, nrm, tg, B, C, ws, p, plan, err); return true;
-        case 5: tc_launch<GW, CH, true, false, true, true, true>(st, mid, nrm, tg, B, C, ws, p, plan, err); return true;
-        case 7: tc_launch<GW, CH, true, true, true, true, true>(st, mid, nrm, tg, B, C, ws, p, plan, err); return true;
+        case 3: tc_launch<GW, CH, R, true, true, false, true, true>(st, mid, nrm, tg, B, C, ws, p, plan, err); return true;
+        case 5: tc_launch<GW, CH, R, true, false, true, true, true>(st, mid, nrm, tg, B, C, ws, p, plan, err); return true;
+        case 7: tc_launch<GW, CH, R, true, true, true, true, true>(st, mid, nrm, tg, B, C, ws, p, plan, err); return true;
         default: return false;
     }
 }
@@ -1231,7 +1247,23 @@ TcCoeffForm tc_coeff_form(const ChunkParamsF *h, int groups)
     }
     out.ki = true;
     out.s = s;
+    // In this form a group's entries depend on the group only through kappa:
+    // the most groups of an aligned block (4, 2, 1) with one wavenumber.
+    for (out.share = 4; out.share > 1; out.share /= 2)
+    {
+        bool same = true;
+        for (int i = 0; i < groups && same; ++i) same = h[i].kappa == h[i - i % out.share].kappa;
+        if (same) break;
+    }
     return out;
+}
+
+int tc_entry_sharing(const OpFlags &f, const TcCoeffForm &form, int wc, const TcTuning &tune)
+{
+    const bool ri = !f.re_sl && !f.im_dl && !f.im_adl && (f.dl() || f.adl());
+    const int code = (f.sl() ? 1 : 0) | (f.dl() ? 2 : 0) | (f.adl() ? 4 : 0);
+    if (!ri || !form.ki || !(code == 3 || code == 5 || code == 7)) return 1;
+    return std::min({form.share, std::max(1, tune.share), tc_chunks_per_unit(wc, tune.chunks)});
 }
 
 int tc_chunks_per_unit(int wc, int chunks)
@@ -1266,16 +1298,19 @@ void launch_tc_tile_geometry(const MeshDev &m, float *tgeo, cudaStream_t st)
 namespace
 {
 template <int GW>
-void tc_dispatch(int CH, bool ri, bool ki, int code, cudaStream_t st, const float *pts4, const float *nrm,
+void tc_dispatch(int CH, int R, bool ri, bool ki, int code, cudaStream_t st, const float *pts4, const float *nrm,
                  const TcTileGeo *tg, const uint8_t *Btri, float2 *Ctri, float2 *ws, const ChunkParamsF *p,
                  const TcPlan &plan, int *err)
 {
     bool done = false;
     if (ri && ki)
     {
-        if (CH == 4) done = tc_flags_ki<GW, 4>(code, st, pts4, nrm, tg, Btri, Ctri, ws, p, plan, err);
-        else if (CH == 2) done = tc_flags_ki<GW, 2>(code, st, pts4, nrm, tg, Btri, Ctri, ws, p, plan, err);
-        else done = tc_flags_ki<GW, 1>(code, st, pts4, nrm, tg, Btri, Ctri, ws, p, plan, err);
+        if (CH == 4 && R == 4) done = tc_flags_ki<GW, 4, 4>(code, st, pts4, nrm, tg, Btri, Ctri, ws, p, plan, err);
+        else if (CH == 4 && R == 2) done = tc_flags_ki<GW, 4, 2>(code, st, pts4, nrm, tg, Btri, Ctri, ws, p, plan, err);
+        else if (CH == 4) done = tc_flags_ki<GW, 4, 1>(code, st, pts4, nrm, tg, Btri, Ctri, ws, p, plan, err);
+        else if (CH == 2 && R == 2) done = tc_flags_ki<GW, 2, 2>(code, st, pts4, nrm, tg, Btri, Ctri, ws, p, plan, err);
+        else if (CH == 2) done = tc_flags_ki<GW, 2, 1>(code, st, pts4, nrm, tg, Btri, Ctri, ws, p, plan, err);
+        else done = tc_flags_ki<GW, 1, 1>(code, st, pts4, nrm, tg, Btri, Ctri, ws, p, plan, err);
     }
     if (done) return;
     if (ri)
@@ -1333,8 +1368,9 @@ void tc_run(const MeshDev &m, const OpFlags &f, const void *chunk_params, const 
     // the real / imaginary coefficient structure of the BIE solves (see boundary_tc_kernel)
     const bool ri = !f.re_sl && !f.im_dl && !f.im_adl && (f.dl() || f.adl());
     const uint8_t *im = launch_tc_expand(Btri, m.nt, wc, img, st);
-    if (tune.gen_warps == 8) tc_dispatch<8>(CH, ri, form.ki, code, st, pts4, nrm, tg, im, Ctri, ws, p, plan, err);
-    else tc_dispatch<16>(CH, ri, form.ki, code, st, pts4, nrm, tg, im, Ctri, ws, p, plan, err);
+    const int R = tc_entry_sharing(f, form, wc, tune);
+    if (tune.gen_warps == 8) tc_dispatch<8>(CH, R, ri, form.ki, code, st, pts4, nrm, tg, im, Ctri, ws, p, plan, err);
+    else tc_dispatch<16>(CH, R, ri, form.ki, code, st, pts4, nrm, tg, im, Ctri, ws, p, plan, err);
     BAEMM_LAUNCH_CHECK();
     if (plan.tail_blocks > 0)
     {
@@ -1365,9 +1401,9 @@ bool tc_pack_flags(int code, cudaStream_t st, const TcPlan &plan, int *err)
 {
     switch (code)
     {
-        case 3: tc_launch<GW, CH, true, true, false, true, true, true>(st, 0, 0, 0, 0, 0, 0, 0, plan, err); return true;
-        case 5: tc_launch<GW, CH, true, false, true, true, true, true>(st, 0, 0, 0, 0, 0, 0, 0, plan, err); return true;
-        case 7: tc_launch<GW, CH, true, true, true, true, true, true>(st, 0, 0, 0, 0, 0, 0, 0, plan, err); return true;
+        case 3: tc_launch<GW, CH, 1, true, true, false, true, true, true>(st, 0, 0, 0, 0, 0, 0, 0, plan, err); return true;
+        case 5: tc_launch<GW, CH, 1, true, false, true, true, true, true>(st, 0, 0, 0, 0, 0, 0, 0, plan, err); return true;
+        case 7: tc_launch<GW, CH, 1, true, true, true, true, true, true>(st, 0, 0, 0, 0, 0, 0, 0, plan, err); return true;
         default: return false;
     }
 }

@@ -66,7 +66,8 @@ void Ctx::autotune(int mode, int repeats, baemm_tune_result *out)
 
     const int code = (flags.sl() ? 1 : 0) | (flags.dl() ? 2 : 0) | (flags.adl() ? 4 : 0);
     const bool ri = !flags.re_sl && !flags.im_dl && !flags.im_adl && (flags.dl() || flags.adl());
-    const int form = (ri ? 1 : 0) | (tc_form.ki ? 2 : 0);
+    const int form = (ri ? 1 : 0) | (tc_form.ki ? 2 : 0) | (tc_entry_sharing(flags, tc_form, wave_count, TcTuning{}) << 2) |
+                     (tc_tune.share << 5);
     const TuneKey key{device, mesh.nt, mesh.nv, wave_count, wave_chunk_size, mode, code, form};
     auto report = [&](const TuneChoice &ch, double before, int cached) {
         out->dense_variant = dense_variant;
@@ -87,7 +88,7 @@ void Ctx::autotune(int mode, int repeats, baemm_tune_result *out)
         if (it != g_tune_cache.end())
         {
             ++graph_state;
-            if (mode == BAEMM_APPLY_TC) tc_tune = it->second.tc;
+            if (mode == BAEMM_APPLY_TC) tc_tune = it->second.tc;   // the key holds the share setting
             else dense_variant = it->second.dense_variant;
             report(it->second, -1.0, 1);
             return;

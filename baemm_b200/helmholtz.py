@@ -263,6 +263,14 @@ class Helmholtz_CUDA:
     def GetTuning(self, key: int) -> int:
         return int(self._lib.baemm_get_tuning(self._h, int(key)))
 
+    def TcEntrySharing(self) -> int:
+        """Groups of 16 columns per shared kernel-entry evaluation of the
+        tensor-core apply of the loaded operators (1, 2 or 4)."""
+        r = int(self._lib.baemm_tc_entry_sharing(self._h))
+        if r < 0:
+            self._ck(r)
+        return r
+
     def SetKernelVariant(self, variant: int):
         self.SetTuning(_capi.TUNE_DENSE_VARIANT, variant)
 

@@ -149,15 +149,25 @@ int baemm_get_apply_mode(const baemm_ctx *ctx);
  *                             entries, 8 or 16 (default 16)
  *   BAEMM_TUNE_TC_CHUNKS      tensor-core form: 16-column groups per work unit,
  *                             1, 2 or 4 (default 0: the most the wave shape
- *                             allows; fewer give small meshes more work units) */
+ *                             allows; fewer give small meshes more work units)
+ *   BAEMM_TUNE_TC_SHARE       tensor-core form: most 16-column groups with one
+ *                             wavenumber that share one evaluation of the
+ *                             kernel entries, 1, 2 or 4 (default 4; used by the
+ *                             mixed BIE and DtN coefficient forms) */
 #define BAEMM_TUNE_DENSE_VARIANT 1
 #define BAEMM_TUNE_TC_SEGMENT    2
 #define BAEMM_TUNE_TC_CTAS       3
 #define BAEMM_TUNE_TC_STAGGER    4
 #define BAEMM_TUNE_TC_GEN_WARPS  5
 #define BAEMM_TUNE_TC_CHUNKS     6
+#define BAEMM_TUNE_TC_SHARE      7
 int baemm_set_tuning(baemm_ctx *ctx, int key, int value);
 int baemm_get_tuning(const baemm_ctx *ctx, int key);
+/* Groups of 16 columns per shared entry evaluation that the tensor-core apply
+ * of the loaded operators uses (1, 2 or 4; from the wavenumbers, the operator
+ * combination, BAEMM_TUNE_TC_CHUNKS and BAEMM_TUNE_TC_SHARE), or a negative
+ * error code when no operators are loaded. */
+int baemm_tc_entry_sharing(const baemm_ctx *ctx);
 /* CUDA graphs for the solvers' inner operators (no reference counterpart;
  * default off).  When on, the GMRES operator apply and the CG mass inverse of
  * BoundaryPotential / DirichletToNeumann / FarField and the derivative solves

@@ -31,6 +31,7 @@ WAVES = {  # name: (wave_count, wave_chunk_size, kappa list)
     "w8x4": (8, 4, [1.0, 3.0]),
     "w64": (64, 16, [2.0, 4.0, 8.0, 16.0]),
     "w64x32": (64, 32, [3.0, 6.0]),
+    "w64x64": (64, 64, [3.0]),
 }
 
 
@@ -101,9 +102,11 @@ def test_nearfield_fp64(env, cname, wname):
 
 
 @pytest.mark.parametrize("cname", list(COEFFS))
-@pytest.mark.parametrize("wname", ["w16", "w32", "w64", "w64x32"])
+@pytest.mark.parametrize("wname", ["w16", "w32", "w64", "w64x32", "w64x64"])
 def test_nearfield_tensor_core(env, cname, wname):
-    """Compensated tensor-core form at arbitrary targets (no pair excluded)."""
+    """Compensated tensor-core form at arbitrary targets (no pair excluded);
+    with the BIE tuple, w64x32 and w64x64 evaluate each kernel entry once for
+    2 and 4 column groups of one wavenumber."""
     coords, tris, H, o32, o64, pts = env
     wc, wcs, kap = WAVES[wname]
     coeff = _coeff(cname, kap)

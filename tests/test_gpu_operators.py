@@ -277,6 +277,72 @@ def test_tensor_core_shapes_same_results(env, gw, chunks, cname):
     assert relerr(C, C64) < FP32_VS64_TOL
 
 
+# (wave_count, wave_chunk_size, kappas, operator tuple, generator warps,
+#  chunks setting, share setting, CTAs, groups per shared entry set)
+SHARED_CASES = [
+    (64, 64, [3.0], "bie", 16, 0, 4, 0, 4),
+    (64, 16, [3.0] * 4, "bie", 16, 0, 4, 0, 4),     # equal wavenumbers in separate wave chunks
+    (64, 32, [3.0, 5.0], "dtn", 16, 0, 4, 0, 2),
+    (64, 64, [3.0], "bie3", 16, 0, 4, 0, 4),        # all three layers in the KI form
+    (64, 64, [3.0], "bie", 8, 0, 4, 0, 4),
+    (64, 64, [3.0], "bie", 16, 2, 4, 0, 2),
+    (64, 64, [3.0], "bie", 16, 0, 2, 0, 2),
+    (64, 64, [3.0], "bie", 16, 0, 1, 0, 1),
+    (128, 64, [2.0, 5.0], "bie", 16, 0, 4, 3, 4),   # 3 CTAs: whole blocks, several segments each
+    (128, 64, [2.0, 5.0], "dtn", 8, 0, 4, 7, 4),
+    (32, 32, [4.0], "bie", 16, 0, 4, 0, 2),
+    (48, 16, [4.0] * 3, "bie", 16, 0, 4, 0, 1),     # 3 groups of one wavenumber: one group per unit
+    (64, 64, [3.0], "all", 16, 0, 4, 0, 1),         # not the KI form
+]
+
+
+@pytest.mark.parametrize("case", SHARED_CASES)
+def test_tensor_core_shared_entries(env, case):
+    """Groups of 16 columns with one wavenumber share one evaluation of the
+    kernel entries (KI coefficient form): one MMA of N = 64 R per shared set.
+    Within the bar of the FP64 oracle, and within 1e-6 of the same apply with
+    every group evaluated on its own."""
+    wc, wcs, kap, cname, gw, chunks, share, ctas, expect = case
+    coords, tris, meas, H, o32, o64 = env
+    # c1 = -i kappa with real common c2, c3: the KI form (not for "all")
+    layers = {"bie": (1, 0), "dtn": (0, 1), "bie3": (1, 0.5)}
+    if cname in layers:
+        coeff = np.array([[0.5, -1j * k, *layers[cname]] for k in kap], np.complex128)
+    else:
+        coeff = _coeff(cname, kap)
+    rng = np.random.default_rng(71 + wc + gw + share)
+    B = crandn(rng, coords.shape[0], wc)
+    C64 = np.zeros_like(B)
+    o64.ApplyBoundaryOperators_PL(1.0, B, 0.0, C64, kap, coeff, wc, wcs)
+    H.LoadBoundaryOperators_PL(kap, coeff, wc, wcs)
+    H.SetApplyMode(APPLY_TC)
+    try:
+        H.SetTuning(_capi.TUNE_TC_GEN_WARPS, gw)
+        H.SetTuning(_capi.TUNE_TC_CHUNKS, chunks)
+        H.SetTuning(_capi.TUNE_TC_CTAS, ctas)
+        H.SetTuning(_capi.TUNE_TC_SHARE, share)
+        assert H.GetTuning(_capi.TUNE_TC_SHARE) == share
+        assert H.TcEntrySharing() == expect
+        C = np.zeros_like(B)
+        H.ApplyBoundaryOperators_PL(1.0, B, 0.0, C)
+        H.SetTuning(_capi.TUNE_TC_SHARE, 1)
+        assert H.TcEntrySharing() == 1
+        C1 = np.zeros_like(B)
+        H.ApplyBoundaryOperators_PL(1.0, B, 0.0, C1)
+        with pytest.raises(BaemmError):
+            H.SetTuning(_capi.TUNE_TC_SHARE, 3)
+    finally:
+        H.SetTuning(_capi.TUNE_TC_GEN_WARPS, 16)
+        H.SetTuning(_capi.TUNE_TC_CHUNKS, 0)
+        H.SetTuning(_capi.TUNE_TC_CTAS, 0)
+        H.SetTuning(_capi.TUNE_TC_SHARE, 4)
+        H.SetApplyMode(APPLY_FP32)
+        H.UnloadBoundaryOperators_PL()
+    assert relerr(C, C64) < FP32_VS64_TOL
+    assert relerr(C1, C64) < FP32_VS64_TOL
+    assert relerr(C, C1) < 1e-6
+
+
 def test_device_path_follows_torch_stream(env):
     """Without SetStream, torch CUDA tensors are processed on torch's current
     stream, so reading the result back through torch needs no extra sync."""
