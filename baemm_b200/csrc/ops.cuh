@@ -180,7 +180,9 @@ void launch_nearfield_tc(const MeshDev &m, const OpFlags &f, const void *chunk_p
 // Self-test of the bounded pipeline waits: one warp waits on an mbarrier that
 // nothing arrives on; returns the error code the wait wrote and its duration.
 void tc_bounded_wait_probe(int code, double *elapsed_ms, int *code_out);
-const uint8_t *launch_tc_expand(const float2 *Btri, int64_t n, int wc, DevBuf<uint8_t> &img, cudaStream_t st);
+// share: groups per aligned block that share the kernel entries (tc_entry_sharing; 1 for packed launches)
+const uint8_t *launch_tc_expand(const float2 *Btri, int64_t n, int wc, DevBuf<uint8_t> &img, cudaStream_t st,
+                                int share = 1);
 // ---- packed tensor-core launches (several problems in one persistent launch) ----
 // One problem as the host describes it: the boundary operator of one mesh
 // (targets = sources = its nt triangles) on its device blocks.

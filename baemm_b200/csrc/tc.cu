@@ -176,6 +176,20 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity)
     return ok != 0;
 }
 
+// Non-blocking test of a phase: the result is not needed until it is used, so
+// a test issued ahead of other work hides the latency of the barrier access.
+__device__ __forceinline__ bool mbar_test(uint64_t *bar, uint32_t parity)
+{
+    uint32_t ok;
+    asm volatile("{\n\t.reg .pred p;\n\t"
+                 "mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+                 "selp.u32 %0, 1, 0, p;\n\t}"
+                 : "=r"(ok)
+                 : "r"(smem_u32(bar)), "r"(parity)
+                 : "memory");
+    return ok != 0;
+}
+
 __device__ __forceinline__ uint64_t global_ns()
 {
     uint64_t t;
@@ -629,9 +643,10 @@ __device__ __forceinline__ void tc_entries_ki(const float2 *__restrict__ P, cons
 // equal wavenumbers in every aligned block of R groups).  The CH groups of a
 // work unit are CH / R entry sets; per tile the generators evaluate each set
 // once into one A stage, and its issuer multiplies it with the R groups' B
-// images in one MMA of N = 64 R ([Bhi | Blo] of each group, which are
-// consecutive in the B stage and whose accumulators are consecutive in TMEM)
-// plus R correction MMAs Alo Bhi of N = 32.
+// images: per K step one MMA of N = 64 R, Ahi [Bhi | Blo] (the set's R hi
+// images are followed by its R lo images, tc_expand_kernel), into the set's
+// main parts and corrections (consecutive in TMEM), and one of N = 32 R,
+// Alo Bhi, into the corrections.
 template <int GW, int CH, int R, bool SL, bool DL, bool ADL, bool RI, bool KI, bool PACK>
 __global__ void __launch_bounds__(tc_threads<GW, CH, R>(), 1)
 boundary_tc_kernel(const float *__restrict__ mid4, const float *__restrict__ nrm4, const TcTileGeo *__restrict__ tgeo,
@@ -733,11 +748,12 @@ boundary_tc_kernel(const float *__restrict__ mid4, const float *__restrict__ nrm
             for (int c = 0; c < CH; ++c)
             {
                 uint32_t re[TC_CPG], im[TC_CPG], cre[TC_CPG], cim[TC_CPG];
-                const uint32_t col = (uint32_t)(c * TC_DCOLS + g * TC_CPG);
+                // the accumulator of an entry set: the main parts of its R chunks, then their corrections
+                const uint32_t col = (uint32_t)((c - c % R) * TC_DCOLS + (c % R) * TC_N + g * TC_CPG);
                 tmem_ld<TC_CPG>(lane_addr + col, re);
                 tmem_ld<TC_CPG>(lane_addr + col + 16u, im);
-                tmem_ld<TC_CPG>(lane_addr + col + (uint32_t)TC_N, cre);
-                tmem_ld<TC_CPG>(lane_addr + col + (uint32_t)TC_N + 16u, cim);
+                tmem_ld<TC_CPG>(lane_addr + col + (uint32_t)(R * TC_N), cre);
+                tmem_ld<TC_CPG>(lane_addr + col + (uint32_t)(R * TC_N) + 16u, cim);
                 asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
                 float4 *a4 = reinterpret_cast<float4 *>(acc_row + c * 16);
                 #pragma unroll
@@ -974,6 +990,7 @@ boundary_tc_kernel(const float *__restrict__ mid4, const float *__restrict__ nrm
         const int w = warp - (TC_GEN_THREADS / 32 + 1);
         bool ok = true;
         int T = 0, SG = 0;
+        uint32_t pre = 0;   // the next tile's B stage (bit 0) / first A stage (bit 1) found complete by an early test
         // descriptors and TMEM addresses from bases fixed for the whole kernel: a
         // (stage, chunk) image is a constant byte offset from img[0][0][0], and
         // the descriptor's start-address field is that address >> 4
@@ -989,54 +1006,66 @@ boundary_tc_kernel(const float *__restrict__ mid4, const float *__restrict__ nrm
                 const int b = T % TC_BSTAGES;
                 const bool first = sp == 0;
                 {
-                    bool got = warp_wait(&sm.b_full[b], (uint32_t)(T / TC_BSTAGES) & 1u, abort_flag, err, 7);
+                    bool got = (pre & 1u) || warp_wait(&sm.b_full[b], (uint32_t)(T / TC_BSTAGES) & 1u, abort_flag, err, 7);
                     // a new segment overwrites the accumulator: the previous one must be drained
                     if (got && first && SG >= 1)
                         got = warp_wait(&sm.seg_empty, (uint32_t)(SG - 1) & 1u, abort_flag, err, 8);
                     if (!got) { ok = false; break; }
                 }
+                const bool seg_end = sp + 1 == S || t == te - 1;
                 #pragma unroll
                 for (int k = 0; k < E / MW; ++k)
                 {
                     const int e = w + k * MW, c0 = e * R;   // entry set e: chunks c0 .. c0 + R - 1
                     const uint32_t u = (uint32_t)T * E + e;
                     const uint32_t stage = u % AS;
-                    if (!warp_wait(&sm.a_full[stage], (u / AS) & 1u, abort_flag, err, 9)) { ok = false; break; }
+                    if (!(k == 0 && (pre & 2u)) && !warp_wait(&sm.a_full[stage], (u / AS) & 1u, abort_flag, err, 9))
+                    {
+                        ok = false;
+                        break;
+                    }
                     tc_fence_after();
                     const uint32_t d = tbase + (uint32_t)(c0 * TC_DCOLS);
                     const uint32_t a_hi = tbase + (uint32_t)(CH * TC_DCOLS) + stage * 64u;
                     const uint32_t a_lo = a_hi + 8u;
-                    // the hi image's 32 rows are followed by the lo image's 32 rows and
-                    // by the next chunk's images (same 1024-byte group stride): one
-                    // N = 64 R operand [Bhi | Blo] per chunk of the set
+                    // the set's R hi images (32 rows each) are followed by its R lo
+                    // images (same 1024-byte group stride): one N = 64 R operand
+                    // [Bhi | Blo] whose first 32 R rows are the N = 32 R operand Bhi
                     const uint64_t b_hilo = desc0 + (uint64_t)(((b * TC_CHMAX + c0) * TC_GROUP_BYTES) >> 4);
+                    // Before the tile's last MMAs (whose issue waits for the tensor
+                    // core), test the next tile's B stage and this warp's first A
+                    // stage of it; the results are read after the MMAs are issued.
+                    const bool last = k == E / MW - 1;
+                    bool nb = false, na = false;
+                    if (last)
+                    {
+                        const uint32_t un = (uint32_t)(T + 1) * E + w;
+                        nb = mbar_test(&sm.b_full[(T + 1) % TC_BSTAGES], (uint32_t)((T + 1) / TC_BSTAGES) & 1u);
+                        na = mbar_test(&sm.a_full[un % AS], (un / AS) & 1u);
+                    }
                     if (elect_one())
                     {
                         #pragma unroll
                         for (int ks = 0; ks < 4; ++ks)
                         {
                             const uint64_t koff = (uint64_t)(ks * 32 >> 4);
-                            // per chunk [main | corr] (+)= Ahi [Bhi | Blo];  corr += Alo Bhi
+                            // [main | corr] (+)= Ahi [Bhi | Blo];  corr += Alo Bhi (each over the set's chunks)
                             mma_tf32(d, a_hi + 16u * ks, b_hilo + koff, (!first || ks > 0) ? 1u : 0u,
                                      idesc_tf32(2 * TC_N * R));
-                            #pragma unroll
-                            for (int q = 0; q < R; ++q)
-                                mma_tf32(d + (uint32_t)(q * TC_DCOLS + TC_N), a_lo + 16u * ks,
-                                         b_hilo + (uint64_t)((q * TC_GROUP_BYTES) >> 4) + koff, 1u, idesc_tf32(TC_N));
+                            mma_tf32(d + (uint32_t)(TC_N * R), a_lo + 16u * ks, b_hilo + koff, 1u, idesc_tf32(TC_N * R));
                         }
                         mma_commit(&sm.a_empty[stage]);
+                        if (last)
+                        {
+                            mma_commit(&sm.b_empty[b]);
+                            if (seg_end) mma_commit(&sm.seg_full);
+                        }
                     }
                     __syncwarp();
+                    if (last) pre = (__all_sync(0xffffffffu, nb) ? 1u : 0u) | (__all_sync(0xffffffffu, na) ? 2u : 0u);
                 }
                 if (!ok) break;
-                const bool seg_end = sp + 1 == S || t == te - 1;
                 sp = seg_end ? 0 : sp + 1;
-                if (elect_one())
-                {
-                    mma_commit(&sm.b_empty[b]);
-                    if (seg_end) mma_commit(&sm.seg_full);
-                }
-                __syncwarp();
                 if (seg_end) ++SG;
             }
         }
@@ -1059,15 +1088,19 @@ boundary_tc_kernel(const float *__restrict__ mid4, const float *__restrict__ nrm
 }
 
 // The MMA's B operand for every 16-source tile t and 16-column group G, as the
-// bytes a B stage holds (TC_GROUP_BYTES at (t * groups + G) * TC_GROUP_BYTES):
-// the hi image, then the lo image, each 32 K-major SWIZZLE_128B rows of 128
-// bytes.  Row q < 16 (real part of column q's result) holds per source pair
+// bytes a B stage holds: a hi and a lo image, each 32 K-major SWIZZLE_128B
+// rows of 128 bytes.  The groups of tile t take TC_GROUP_BYTES each from
+// t * groups * TC_GROUP_BYTES; within each aligned block of `share` groups
+// (the groups that share one evaluation of the kernel entries) the hi images
+// come first, then the lo images, so that one MMA reads [Bhi | Blo] of the
+// whole block and another its Bhi (share = 1: hi, lo per group).  Row
+// q < 16 (real part of column q's result) holds per source pair
 // sp = (s0, s1) = (2 sp, 2 sp + 1) the 16-byte group (Re b_s0, Re b_s1,
 // -Im b_s0, -Im b_s1); row 16 + q holds (Im b_s0, Im b_s1, Re b_s0, Re b_s1);
 // group sp of row r sits at ((sp ^ (r & 7)) * 16) (img_off16).  hi = tf32(x)
 // rounded to nearest, lo = x - hi (split_tf32).  Sources past n are zero.
 // Thread (t, G, q, sp), sp fastest: 8 threads fill one row's 128 bytes.
-__global__ void tc_expand_kernel(const float2 *__restrict__ Btri, int n, int wc, int64_t total,
+__global__ void tc_expand_kernel(const float2 *__restrict__ Btri, int n, int wc, int64_t total, int share,
                                  uint8_t *__restrict__ img)
 {
     const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -1087,7 +1120,9 @@ __global__ void tc_expand_kernel(const float2 *__restrict__ Btri, int n, int wc,
     split_tf32(v1.x, hr1, lr1);
     split_tf32(v1.y, hi1, li1);
     constexpr uint32_t sgn = 0x80000000u;
-    uint8_t *hi_img = img + tg * TC_GROUP_BYTES, *lo_img = hi_img + TC_IMG;
+    const int r = G % share;   // place in the block of groups sharing the entries
+    uint8_t *blk = img + (tg - r) * TC_GROUP_BYTES;
+    uint8_t *hi_img = blk + r * TC_IMG, *lo_img = blk + (share + r) * TC_IMG;
     *reinterpret_cast<uint4 *>(hi_img + img_off16(q, sp)) = make_uint4(hr0, hr1, hi0 ^ sgn, hi1 ^ sgn);
     *reinterpret_cast<uint4 *>(lo_img + img_off16(q, sp)) = make_uint4(lr0, lr1, li0 ^ sgn, li1 ^ sgn);
     *reinterpret_cast<uint4 *>(hi_img + img_off16(q + 16, sp)) = make_uint4(hi0, hi1, hr0, hr1);
@@ -1115,7 +1150,8 @@ __global__ void tc_tile_geometry_kernel(const float *__restrict__ mid4, const fl
 
 } // namespace
 
-const uint8_t *launch_tc_expand(const float2 *Btri, int64_t n, int wc, DevBuf<uint8_t> &img, cudaStream_t st)
+const uint8_t *launch_tc_expand(const float2 *Btri, int64_t n, int wc, DevBuf<uint8_t> &img, cudaStream_t st,
+                                int share)
 {
     const int64_t ntiles = ceil_div(n, TC_SRC), groups = wc / 16;
     const size_t bytes = (size_t)(ntiles * groups) * TC_GROUP_BYTES;
@@ -1123,7 +1159,7 @@ const uint8_t *launch_tc_expand(const float2 *Btri, int64_t n, int wc, DevBuf<ui
     const int64_t total = ntiles * groups * 128;
     if (total > 0)
     {
-        tc_expand_kernel<<<ceil_div(total, 256), 256, 0, st>>>(Btri, (int)n, wc, total, out);
+        tc_expand_kernel<<<ceil_div(total, 256), 256, 0, st>>>(Btri, (int)n, wc, total, share, out);
         BAEMM_LAUNCH_CHECK();
     }
     return out;
@@ -1367,8 +1403,8 @@ void tc_run(const MeshDev &m, const OpFlags &f, const void *chunk_params, const 
     BAEMM_REQUIRE(tg, BAEMM_ERR_ARG, "tensor-core tile geometry missing");
     // the real / imaginary coefficient structure of the BIE solves (see boundary_tc_kernel)
     const bool ri = !f.re_sl && !f.im_dl && !f.im_adl && (f.dl() || f.adl());
-    const uint8_t *im = launch_tc_expand(Btri, m.nt, wc, img, st);
     const int R = tc_entry_sharing(f, form, wc, tune);
+    const uint8_t *im = launch_tc_expand(Btri, m.nt, wc, img, st, R);
     if (tune.gen_warps == 8) tc_dispatch<8>(CH, R, ri, form.ki, code, st, pts4, nrm, tg, im, Ctri, ws, p, plan, err);
     else tc_dispatch<16>(CH, R, ri, form.ki, code, st, pts4, nrm, tg, im, Ctri, ws, p, plan, err);
     BAEMM_LAUNCH_CHECK();
