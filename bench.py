@@ -486,7 +486,8 @@ def run_gpu_arm(args, rank, world, local_rank):
     dense_avg = float(np.mean(dense_ms))
     flops = 8.0 * inter_kernel
     achieved = flops / (dense_avg * 1e-3) / 1e12
-    traffic, traffic_src = load_traffic(args.mode)
+    traffic, traffic_src = (load_traffic(args.mode) if not args.kappa else
+                            (None, "captured on the default wavenumbers only"))
     kernel_name = {"tc": "boundary_tc_kernel", "fp32": "boundary_dense_kernel", "fp64": "boundary_dense_kernel<double>"}[args.mode]
     cpu = None
     if world == 1 and not args.no_cpu_baseline:
@@ -1105,9 +1106,21 @@ def main(argv=None):
                     help="--workload solve: the runs to make (fp64 is the error reference; without it the errors "
                          "are null)")
     ap.add_argument("--small", action="store_true", help="38400-triangle torus (profiling captures only)")
+    ap.add_argument("--kappa", default="",
+                    help="--workload apply: wavenumbers of the 64 RHS, comma-separated, each over 64 / count columns "
+                         "(default 2,4,8,16 x 16; e.g. 8 = one wavenumber x 64, whose column groups share the "
+                         "tensor-core form's kernel entries)")
     ap.add_argument("--shard", action="store_true",
                     help="split each apply by target rows over the ranks (strong scaling; default: replicas)")
     args = ap.parse_args(argv)
+    if args.kappa:
+        global KAPPA, WCS, WORKLOAD
+        kap = [float(x) for x in args.kappa.split(",")]
+        if WC % len(kap) or (WC // len(kap)) % 16:
+            ap.error("--kappa: 64 / count must be a multiple of 16 (1, 2 or 4 wavenumbers)")
+        KAPPA, WCS = np.array(kap), WC // len(kap)
+        WORKLOAD = WORKLOAD.replace("kappa {2,4,8,16} x 16",
+                                    "kappa {%s} x %d" % (",".join("%g" % k for k in kap), WCS))
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
