@@ -343,6 +343,37 @@ def test_tensor_core_shared_entries(env, case):
     assert relerr(C, C1) < 1e-6
 
 
+@pytest.mark.parametrize("seg", [1, 2, 3, 5, 64])
+@pytest.mark.parametrize("kap,share", [([3.0], 4), ([3.0], 1), ([2.0, 5.0], 4)])
+@pytest.mark.parametrize("ctas", [0, 3])
+def test_tensor_core_segment_lengths(env, seg, kap, share, ctas):
+    """TMEM partial sums drained every `seg` tiles, including segments shorter
+    than the ring of A stages (a segment's drain can then still be pending
+    when the next one ends) and longer than a CTA's piece: same bar against
+    the FP64 oracle."""
+    coords, tris, meas, H, o32, o64 = env
+    wc, wcs = 64, 64 // len(kap)
+    coeff = np.array([[0.5, -1j * k, 1, 0] for k in kap], np.complex128)
+    B = crandn(np.random.default_rng(900 + seg), coords.shape[0], wc)
+    C64 = np.zeros_like(B)
+    o64.ApplyBoundaryOperators_PL(1.0, B, 0.0, C64, kap, coeff, wc, wcs)
+    H.LoadBoundaryOperators_PL(kap, coeff, wc, wcs)
+    H.SetApplyMode(APPLY_TC)
+    try:
+        H.SetTuning(_capi.TUNE_TC_SEGMENT, seg)
+        H.SetTuning(_capi.TUNE_TC_SHARE, share)
+        H.SetTuning(_capi.TUNE_TC_CTAS, ctas)
+        C = np.zeros_like(B)
+        H.ApplyBoundaryOperators_PL(1.0, B, 0.0, C)
+    finally:
+        H.SetTuning(_capi.TUNE_TC_SEGMENT, 16)
+        H.SetTuning(_capi.TUNE_TC_SHARE, 4)
+        H.SetTuning(_capi.TUNE_TC_CTAS, 0)
+        H.SetApplyMode(APPLY_FP32)
+        H.UnloadBoundaryOperators_PL()
+    assert relerr(C, C64) < FP32_VS64_TOL
+
+
 def test_device_path_follows_torch_stream(env):
     """Without SetStream, torch CUDA tensors are processed on torch's current
     stream, so reading the result back through torch needs no extra sync."""
