@@ -119,6 +119,13 @@ public:
     // Additions without reference counterpart (see include/baemm.h).
     void SetTuning(int key, int value) { check(baemm_set_tuning(ctx_, key, value), "SetTuning"); }
     int GetTuning(int key) const { return baemm_get_tuning(ctx_, key); }
+    // 16-column groups per shared kernel-entry evaluation of the tensor-core apply (1, 2 or 4)
+    int TcEntrySharing() const
+    {
+        const int r = baemm_tc_entry_sharing(ctx_);
+        if (r < 0) check(r, "TcEntrySharing");
+        return r;
+    }
     baemm_tune_result Autotune(int mode, int repeats = 2)
     {
         baemm_tune_result r{};

@@ -41,6 +41,7 @@ int main()
     H.SetMesh(coords.data(), Int(6), tris.data(), Int(8));
     H.SetGraphs(true);
     H.SetTuning(BAEMM_TUNE_TC_SEGMENT, 8);
+    H.SetTuning(BAEMM_TUNE_TC_SHARE, 4);
     H.SetApplyMode(BAEMM_APPLY_TC);
     H.FarField<wave_count>(kappa.data(), wave_chunk_count, inc.data(), wave_chunk_size, F.data(), WaveType::Plane,
                            Real(1e-5), Real(1e-4));
