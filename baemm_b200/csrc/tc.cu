@@ -36,9 +36,10 @@
 //   warp GW     bulk-copy producer: cp.async.bulk (no multicast) of the tile's
 //               geometry and of its B images, expanded once per apply by
 //               tc_expand_kernel, into shared memory;
-//   warps GW+1, GW+2  MMA issuers, every other chunk each: 8 tcgen05.mma
-//               (kind::tf32, A from TMEM, B from shared memory, M 128, K 8)
-//               per chunk and tile.
+//   warps GW+1, GW+2  MMA issuers, every other entry set each (a chunk, or
+//               R chunks of one wavenumber sharing their entries; one issuer
+//               when a tile has a single set): 8 tcgen05.mma (kind::tf32, A
+//               from TMEM, B from shared memory, M 128, K 8) per set and tile.
 // Pipelines use mbarriers (A stages in TMEM, B and geometry stages in shared
 // memory).  All roles wait with mbarrier.try_wait, which suspends the warp in
 // hardware.
@@ -97,7 +98,9 @@ constexpr int tc_threads() { return 32 * GW + 32 + 32 * tc_mma_warps<GW, CH, R>(
 constexpr int TC_BSTAGES = 4;      // B image stages in shared memory (bulk copies of the expanded images)
 constexpr int TC_RSTAGES = 6;      // tile geometry stages (bulk copies)
 constexpr uint32_t TC_TMEM_COLS = 512;
-constexpr uint32_t TC_DCOLS = 2 * TC_N;             // per chunk: main (Ahi Bhi) | correction (Ahi Blo + Alo Bhi)
+// per chunk: main (Ahi Bhi) and correction (Ahi Blo + Alo Bhi) accumulators;
+// an entry set of R chunks holds its R main parts, then its R corrections
+constexpr uint32_t TC_DCOLS = 2 * TC_N;
 // A stages in TMEM (one chunk of one tile each, 64 columns) take the columns
 // after the accumulator of a CH-chunk work unit: 4 stages for 4 chunks, 6 for
 // 2, 7 for 1.  Within a stage, K step ks (8 K columns) has its hi part at
@@ -120,14 +123,14 @@ struct TcTileGeo
 static_assert(sizeof(TcTileGeo) % 16 == 0, "bulk copies move multiples of 16 bytes");
 
 // The right-hand sides of one 16-source tile and one 16-column group as the
-// MMA's B operand: the hi and the lo image (32 rows each, see
-// tc_expand_kernel), 8 KB, expanded once per apply into global memory and
-// bulk-copied into a B stage as they are.
+// MMA's B operand: the hi and the lo image (32 rows each, 8 KB; ordered within
+// an entry set as tc_expand_kernel describes), expanded once per apply into
+// global memory and bulk-copied into a B stage as they are.
 constexpr int TC_GROUP_BYTES = 2 * TC_IMG;
 
 struct __align__(1024) TcSmem
 {
-    uint8_t img[TC_BSTAGES][TC_CHMAX][2][TC_IMG];   // [stage][chunk][hi, lo]
+    uint8_t img[TC_BSTAGES][TC_CHMAX][2][TC_IMG];   // per stage the unit's images as tc_expand_kernel lays them out
     TcTileGeo geo[TC_RSTAGES];
     uint64_t a_full[TC_ASTAGES_MAX], a_empty[TC_ASTAGES_MAX];
     uint64_t b_full[TC_BSTAGES], b_empty[TC_BSTAGES];
