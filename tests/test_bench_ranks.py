@@ -57,3 +57,11 @@ def test_reference_arm_runs_on_rank_zero_only(capsys):
     args = bench.main.__globals__["argparse"].Namespace(steps=1, warmup=1, gpus=2, small=False)
     assert bench.run_reference_arm(args, rank=1, world=2) == 0
     assert capsys.readouterr().out == ""
+
+
+def test_kappa_option_rejects_uneven_column_split():
+    """--kappa splits the 64 RHS evenly into wave chunks of a multiple of 16
+    columns (1, 2 or 4 wavenumbers); other counts stop before any work."""
+    with pytest.raises(SystemExit):
+        bench.main(["--kappa", "3,5,7"])
+    assert list(bench.KAPPA) == [2.0, 4.0, 8.0, 16.0] and bench.WCS == 16
