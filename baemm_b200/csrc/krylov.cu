@@ -7,6 +7,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <mutex>
 #include <vector>
 
 namespace baemm
@@ -400,7 +401,9 @@ __global__ void cg_pupdate_kernel(int64_t total, int c, const double *__restrict
 // __syncthreads only, and the 3 launches and 3 cross-block column sums of
 // an iteration of the multi-block kernels become block sums.  The block's
 // vectors are column-major in global memory (column k at x + k n),
-// L2-resident at these sizes.  Same steps and stopping rule as the
+// L2-resident at these sizes, except the search direction p, which lives in
+// the block's shared memory (n doubles, at most 128 KB): the matvec's gathers
+// of p read shared memory instead of L2.  Same steps and stopping rule as the
 // multi-block kernels (ApplyMassInverse.hpp:48-156): x = 0, r = b, z = L r,
 // p = z; per iteration q = M p, alpha = <r,z> / <p,q>, x += alpha p,
 // r -= alpha q, z = L r, beta = <r,z>_new / <r,z>, converged once
@@ -411,9 +414,10 @@ __global__ void cg_pupdate_kernel(int64_t total, int c, const double *__restrict
 // converged.
 constexpr int kCgBlockThreads = 1024;
 // Up to this many rows one block per column is faster: on the icosphere of
-// level 5 (10242 vertices, 128 real columns) one iteration takes 29.8 us
+// level 5 (10242 vertices, 128 real columns) one iteration takes 26.5 us
 // against 60.3 us for the three multi-block kernels; on level 6 (40962
 // vertices, 64 columns) 130 us against 92 us, too few blocks for the rows.
+// The bound also keeps p (n doubles) within a block's shared memory.
 constexpr int64_t kCgBlockMaxRows = 16384;
 
 // totals of a and b over the block, in every thread (red: 2 x 33 doubles)
@@ -446,16 +450,22 @@ __device__ __forceinline__ void block_sum2(double &a, double &b, double *red)
 }
 
 template <class RV>
-__global__ void __launch_bounds__(kCgBlockThreads)
+__global__ void __launch_bounds__(kCgBlockThreads, 1)
 cg_block_kernel(int64_t n, int c, const double *__restrict__ b, int64_t ldb, const int32_t *__restrict__ mo,
                 const int32_t *__restrict__ mi, const RV *__restrict__ mv, const RV *__restrict__ L, double *xs,
-                double *rs, double *zs, double *ps, double *qs, double *__restrict__ y, int64_t ldy, int *flags,
+                double *rs, double *zs, double *qs, double *__restrict__ y, int64_t ldy, int *flags,
                 double tol, int max_iter)
 {
     __shared__ double red[66];
+    extern __shared__ double p[];   // the column's search direction, n doubles
     const int k = blockIdx.x;
     const int64_t off = (int64_t)k * n;
-    double *x = xs + off, *r = rs + off, *z = zs + off, *p = ps + off, *q = qs + off;
+    // the column's vectors are separate buffers: no aliasing, so the loads of a
+    // thread's next row can be issued before the stores of its current one
+    double *__restrict__ x = xs + off;
+    double *__restrict__ r = rs + off;
+    double *__restrict__ z = zs + off;
+    double *__restrict__ q = qs + off;
     double rz = 0.0, bb = 0.0;
     for (int64_t row = threadIdx.x; row < n; row += blockDim.x)
     {
@@ -499,6 +509,7 @@ cg_block_kernel(int64_t n, int c, const double *__restrict__ b, int64_t ldb, con
         block_sum2(pq, unused, red);
         const double alpha = pq == 0.0 ? 0.0 : rz / pq;
         double rzn = 0.0, rr = 0.0;
+        #pragma unroll 2
         for (int64_t row = threadIdx.x; row < n; row += blockDim.x)
         {
             x[row] += alpha * p[row];
@@ -513,6 +524,7 @@ cg_block_kernel(int64_t n, int c, const double *__restrict__ b, int64_t ldb, con
         const double beta = rz == 0.0 ? 0.0 : rzn / rz;
         rz = rzn;
         conv = sqrt(rr) <= tol * bn;
+        #pragma unroll 4
         for (int64_t row = threadIdx.x; row < n; row += blockDim.x) p[row] = z[row] + beta * p[row];
         __syncthreads();   // p complete before the next iteration's gathers
     }
@@ -523,6 +535,30 @@ cg_block_kernel(int64_t n, int c, const double *__restrict__ b, int64_t ldb, con
         if (!conv) atomicAdd(&flags[0], 1);
         atomicMax(&flags[1], it);
     }
+}
+
+// One block per column with p (n doubles) in dynamic shared memory; the limit
+// above 48 KB is a per-device attribute of each instantiation, set once.
+template <class RV>
+void launch_cg_block(cudaStream_t st, int64_t n, int c, const double *b, int64_t ldb, const int32_t *mo,
+                     const int32_t *mi, const RV *mv, const RV *L, double *x, double *r, double *z, double *q,
+                     double *y, int64_t ldy, int *flags, double tol, int max_iter)
+{
+    constexpr int kMaxBytes = (int)(kCgBlockMaxRows * sizeof(double));
+    int dev = 0;
+    BAEMM_CUDA(cudaGetDevice(&dev));
+    static std::mutex mu;
+    static bool done[64] = {};
+    {
+        std::lock_guard<std::mutex> lock(mu);
+        if (dev < 0 || dev >= 64 || !done[dev])
+        {
+            BAEMM_CUDA(cudaFuncSetAttribute(cg_block_kernel<RV>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxBytes));
+            if (dev >= 0 && dev < 64) done[dev] = true;
+        }
+    }
+    cg_block_kernel<<<c, kCgBlockThreads, (size_t)n * sizeof(double), st>>>(n, c, b, ldb, mo, mi, mv, L, x, r, z, q,
+                                                                              y, ldy, flags, tol, max_iter);
 }
 
 __global__ void cg_output_kernel(int64_t n, int c, const double *__restrict__ x, double *__restrict__ y, int64_t ldy)
@@ -843,8 +879,8 @@ void CgSolver::enqueue_mass(const MeshDev &m, bool fp64_values, const double *b,
         // one block per column, all iterations in one launch
         BAEMM_CUDA(cudaMemsetAsync(flags_.p, 0, 2 * sizeof(int), st));
         auto runb = [&](auto Lv, auto Mv) {
-            cg_block_kernel<<<c, kCgBlockThreads, 0, st>>>(n, c, b, ldb, m.mass_outer, m.mass_inner, Mv, Lv, x_.p,
-                                                           r_.p, z_.p, p_.p, q_.p, y, ldy, flags_.p, tol, max_iter);
+            launch_cg_block(st, n, c, b, ldb, m.mass_outer, m.mass_inner, Mv, Lv, x_.p, r_.p, z_.p, q_.p, y, ldy,
+                            flags_.p, tol, max_iter);
         };
         if (fp64_values) runb(m.lumped_d.p, m.mass_d.p);
         else runb(m.lumped_f.p, m.mass_f.p);
@@ -901,8 +937,8 @@ double CgSolver::profile_block(const MeshDev &m, bool fp64_values, int c, int it
         {
             BAEMM_CUDA(cudaMemsetAsync(flags_.p, 0, 2 * sizeof(int), st));
             BAEMM_CUDA(cudaEventRecord(e0, st));
-            cg_block_kernel<<<c, kCgBlockThreads, 0, st>>>(n, c, b.p, c, m.mass_outer, m.mass_inner, Mv, Lv, x_.p,
-                                                           r_.p, z_.p, p_.p, q_.p, y.p, c, flags_.p, -1.0, iterations);
+            launch_cg_block(st, n, c, b.p, c, m.mass_outer, m.mass_inner, Mv, Lv, x_.p, r_.p, z_.p, q_.p, y.p, c,
+                            flags_.p, -1.0, iterations);
             BAEMM_CUDA(cudaEventRecord(e1, st));
         }
     };
